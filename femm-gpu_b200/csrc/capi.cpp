@@ -1,0 +1,276 @@
+// capi.cpp -- the extern "C" boundary (include/femm_gpu.h).
+#include "femm_gpu.h"
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <new>
+#include <vector>
+
+using fg::Status;
+using fg::ToInt;
+
+namespace
+{
+
+Status ToHostModel(const fg_model *m, fg::HostModel *out)
+{
+  if (!m || m->node_count <= 0 || m->triangle_count <= 0 || m->material_count <= 0 || !m->node_xy ||
+      !m->triangle_nodes || !m->triangle_material || !m->materials || m->curve_count < 0 ||
+      (m->curve_count > 0 && !m->curves) || m->dirichlet_count < 0 ||
+      (m->dirichlet_count > 0 && (!m->dirichlet_nodes || !m->dirichlet_values)) ||
+      m->constraint_count < 0 ||
+      (m->constraint_count > 0 && (!m->constraint_nodes || !m->constraint_signs)))
+    return Status::kInvalidArgument;
+  fg::HostModel h;
+  h.problem_type = m->problem_type;
+  if (h.problem_type != FG_PLANAR && h.problem_type != FG_AXISYMMETRIC)
+    return Status::kInvalidArgument;
+  h.xy.assign(m->node_xy, m->node_xy + 2 * static_cast<size_t>(m->node_count));
+  h.tri.assign(m->triangle_nodes, m->triangle_nodes + 3 * static_cast<size_t>(m->triangle_count));
+  h.tri_mat.assign(m->triangle_material, m->triangle_material + m->triangle_count);
+  for (int i = 0; i < m->material_count; ++i) {
+    const fg_material &s = m->materials[i];
+    fg::Material mt;
+    mt.nu0 = s.reluctivity_zero_m_per_h;
+    mt.alpha = s.alpha_per_t2;
+    mt.j_per_a = s.source_j_per_a;
+    mt.hc = s.h_c_a_per_m;
+    mt.deg = s.magnetization_deg;
+    mt.curve = s.bh_curve_index;
+    mt.circuit = s.circuit_index;
+    mt.group = s.group_number;
+    h.materials.push_back(mt);
+  }
+  for (int c = 0; c < m->curve_count; ++c) {
+    const fg_bh_curve &src = m->curves[c];
+    if (src.count < 2 || src.count > 4096 || !src.b_t || !src.h_a_per_m)
+      return Status::kInvalidMaterial;
+    fg::BhCurve curve;
+    curve.b.assign(src.b_t, src.b_t + src.count);
+    curve.h.assign(src.h_a_per_m, src.h_a_per_m + src.count);
+    if (!fg::BuildBhSpline(&curve))
+      return Status::kInvalidMaterial;
+    h.curves.push_back(std::move(curve));
+  }
+  h.dir_nodes.assign(m->dirichlet_nodes, m->dirichlet_nodes + m->dirichlet_count);
+  h.dir_values.assign(m->dirichlet_values, m->dirichlet_values + m->dirichlet_count);
+  for (int i = 0; i < m->constraint_count; ++i) {
+    h.con_a.push_back(m->constraint_nodes[2 * i]);
+    h.con_b.push_back(m->constraint_nodes[2 * i + 1]);
+    h.con_sign.push_back(m->constraint_signs[i]);
+  }
+  h.circuit_count = m->circuit_count;
+  h.depth_m = m->depth_m;
+  *out = std::move(h);
+  return Status::kOk;
+}
+
+} // namespace
+
+extern "C" {
+
+void fg_production_options(fg_solve_options *o)
+{
+  if (!o)
+    return;
+  o->relative_tolerance = 1e-8;
+  o->max_newton_iterations = 128;
+  o->max_linear_iterations = 16384;
+  o->linear_relative_tolerance = 1e-10;
+  o->recover_nonconvergence = 1;
+  o->adaptive_linear_tolerance = 1;
+}
+
+const char *fg_status_name(int status)
+{
+  if (status < 0 || status > 15)
+    return "INTERNAL_ERROR";
+  return fg::StatusName(static_cast<Status>(status));
+}
+
+int fg_abi_version(void) { return FG_ABI_VERSION; }
+
+int fg_plan_create(const fg_model *model, const fg_plan_options *options, fg_plan **plan)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  *plan = nullptr;
+  fg::HostModel h;
+  Status s = ToHostModel(model, &h);
+  if (s != Status::kOk)
+    return ToInt(s);
+  fg_plan_options opts{};
+  if (options)
+    opts = *options;
+  fg_plan *p = new (std::nothrow) fg_plan;
+  if (!p)
+    return ToInt(Status::kInternalError);
+  s = p->plan.Create(std::move(h), opts);
+  if (s != Status::kOk) {
+    delete p;
+    return ToInt(s);
+  }
+  *plan = p;
+  return 0;
+}
+
+void fg_plan_destroy(fg_plan *plan) { delete plan; }
+
+int fg_plan_sizes_get(const fg_plan *plan, fg_plan_sizes *sizes)
+{
+  if (!plan || !sizes)
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostPlan &h = plan->plan.host();
+  sizes->node_count = h.N;
+  sizes->triangle_count = h.E;
+  sizes->rows = h.n;
+  sizes->nnz = h.nnz;
+  sizes->circuit_count = h.C;
+  sizes->problem_type = h.problem_type;
+  sizes->device_bytes = static_cast<int64_t>(plan->plan.DeviceBytes());
+  sizes->matrix_contributors = static_cast<int64_t>(h.contrib.size());
+  sizes->rhs_contributors = static_cast<int64_t>(h.rhs_contrib.size());
+  return 0;
+}
+
+int fg_plan_contributors(const fg_plan *plan, int32_t *slot_offsets, int32_t *slot_entries,
+                         int32_t *row_offsets, int32_t *row_entries, double *pm_rhs,
+                         double *circuit_rhs)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostPlan &h = plan->plan.host();
+  if (slot_offsets)
+    std::copy(h.contrib_off.begin(), h.contrib_off.end(), slot_offsets);
+  if (slot_entries)
+    for (size_t k = 0; k < h.contrib.size(); ++k) {
+      slot_entries[3 * k] = h.contrib[k] >> 4;
+      slot_entries[3 * k + 1] = (h.contrib[k] >> 1) & 7;
+      slot_entries[3 * k + 2] = (h.contrib[k] & 1) ? -1 : 1;
+    }
+  if (row_offsets)
+    std::copy(h.rhs_off.begin(), h.rhs_off.end(), row_offsets);
+  if (row_entries)
+    for (size_t k = 0; k < h.rhs_contrib.size(); ++k) {
+      row_entries[3 * k] = h.rhs_contrib[k] >> 3;
+      row_entries[3 * k + 1] = (h.rhs_contrib[k] >> 1) & 3;
+      row_entries[3 * k + 2] = (h.rhs_contrib[k] & 1) ? -1 : 1;
+    }
+  if (pm_rhs)
+    std::copy(h.pm_rhs.begin(), h.pm_rhs.end(), pm_rhs);
+  if (circuit_rhs)
+    std::copy(h.circuit_rhs.begin(), h.circuit_rhs.end(), circuit_rhs);
+  return 0;
+}
+
+int fg_plan_symbolic(const fg_plan *plan, int32_t *row_offsets, int32_t *columns,
+                     int32_t *node_to_free, int8_t *node_sign, double *boundary_values)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostPlan &h = plan->plan.host();
+  if (row_offsets)
+    std::copy(h.row_offsets.begin(), h.row_offsets.end(), row_offsets);
+  if (columns)
+    std::copy(h.columns.begin(), h.columns.end(), columns);
+  if (node_to_free)
+    std::copy(h.dofs.node_to_free.begin(), h.dofs.node_to_free.end(), node_to_free);
+  if (node_sign)
+    std::copy(h.dofs.node_sign.begin(), h.dofs.node_sign.end(), node_sign);
+  if (boundary_values)
+    std::copy(h.dofs.boundary.begin(), h.dofs.boundary.end(), boundary_values);
+  return 0;
+}
+
+int fg_assemble(fg_plan *plan, int32_t items, const double *states, const double *currents,
+                const int32_t *use_newton, double *values, double *diagonal, double *rhs)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(plan->plan.Assemble(items, states, currents, use_newton, values, diagonal, rhs));
+}
+
+int fg_pcg_solve(fg_plan *plan, int32_t items, const double *values, int32_t values_per_item,
+                 const double *rhs, double relative_tolerance, int32_t max_iterations, double *x,
+                 fg_linear_info *info)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(plan->plan.PcgSolve(items, values, values_per_item, rhs, relative_tolerance,
+                                   max_iterations, x, info));
+}
+
+int fg_solve_batch(fg_plan *plan, int32_t items, const double *currents, const double *hc_scale,
+                   const double *warm_a, const fg_solve_options *options, double *a_out,
+                   double *b1_out, double *b2_out, double *flux_out, fg_item_info *info)
+{
+  if (!plan || !options)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(plan->plan.SolveHost(items, currents, hc_scale, warm_a, *options, a_out, b1_out,
+                                    b2_out, flux_out, info));
+}
+
+int fg_solve_batch_device(fg_plan *plan, int32_t items, const double *currents,
+                          const double *hc_scale, const double *warm_a,
+                          const fg_solve_options *options, double *a_out, double *b1_out,
+                          double *b2_out, double *flux_out, fg_item_info *info, void *stream)
+{
+  if (!plan || !options)
+    return ToInt(Status::kInvalidArgument);
+  fg::SolveRequest r;
+  r.items = items;
+  r.currents = currents;
+  r.hc_scale = hc_scale;
+  r.warm = warm_a;
+  r.options = *options;
+  r.a_out = a_out;
+  r.b1_out = b1_out;
+  r.b2_out = b2_out;
+  r.flux_out = flux_out;
+  r.info = info;
+  r.stream = static_cast<cudaStream_t>(stream);
+  return ToInt(plan->plan.SolveDevice(r));
+}
+
+int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing)
+{
+  if (!plan || !timing)
+    return ToInt(Status::kInvalidArgument);
+  *timing = plan->plan.timing();
+  return 0;
+}
+
+int fg_bh_build(int32_t count, double *b, double *h, double *slope, double *cold_secant,
+                int32_t *smoothing_passes)
+{
+  if (count < 2 || !b || !h || !slope)
+    return 0;
+  fg::BhCurve c;
+  c.b.assign(b, b + count);
+  c.h.assign(h, h + count);
+  if (!fg::BuildBhSpline(&c))
+    return 0;
+  std::copy(c.b.begin(), c.b.end(), b);
+  std::copy(c.h.begin(), c.h.end(), h);
+  std::copy(c.slope.begin(), c.slope.end(), slope);
+  if (cold_secant)
+    *cold_secant = c.cold_secant;
+  if (smoothing_passes)
+    *smoothing_passes = c.smoothing_passes;
+  return 1;
+}
+
+void fg_bh_eval(int32_t count, const double *b, const double *h, const double *slope,
+                double field_b, double *out)
+{
+  fg::BhCurve c;
+  c.b.assign(b, b + count);
+  c.h.assign(h, h + count);
+  c.slope.assign(slope, slope + count);
+  fg::EvaluateBh(c, field_b, out);
+}
+
+} // extern "C"

@@ -1,0 +1,98 @@
+// kernels.cuh -- device views of the plan and batch workspace, and kernel launchers.
+//
+// Batch layout: a batch of k items is padded to KP = next power of two (<= 32) and
+// every per-row / per-node / per-element / per-position array is item-interleaved:
+// element [i][item] lives at i * KP + item.  A warp covers 32 / KP rows x KP items,
+// so every SELL-32 column load of a warp touches 32 consecutive doubles.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace fg
+{
+
+constexpr int kMaxItems = 32;
+
+struct DevicePlan {
+  int32_t N, E, n, n_pad, slices, C, problem_type;
+  int64_t nnz, positions;
+  const int32_t *row_offsets, *columns, *row_len, *slice_off, *sell_col;
+  const int32_t *contrib_off, *contrib, *rhs_off, *rhs_contrib;
+  const double *pm_rhs, *circuit_rhs;
+  const int32_t *elem_nodes, *elem_mat;
+  const double *elem_geo;
+  const double *mat_nu0, *mat_alpha, *mat_cold, *mat_jpa;
+  const int32_t *mat_curve_off, *mat_curve_cnt, *mat_circuit;
+  const double *curve_b, *curve_h, *curve_slope;
+  const int32_t *node_to_free;
+  const int8_t *node_sign;
+  const double *boundary;
+  const int32_t *circuit_elem_off, *circuit_elems;
+  double depth_m;
+};
+
+// Per-item scalar arguments small enough to pass by value.
+struct ItemScalars {
+  double v[kMaxItems];
+};
+
+// One PCG launch over a batch (shared SELL pattern, per-item or shared operator).
+struct PcgArgs {
+  int32_t n, n_pad, slices, kp, items;
+  const int32_t *slice_off, *row_len, *sell_col;
+  const double *values;  // [positions][vs]
+  int32_t value_stride;  // KP (per-item operators) or 1 (one shared operator)
+  int32_t value_item;    // 1 or 0
+  const double *diag, *invd; // [n_pad][ds]
+  int32_t diag_stride, diag_item;
+  int32_t use_inverse;
+  const double *b;
+  double *x, *r, *z, *p0, *p1, *q;
+  double *partials;   // [2][64][grid]
+  unsigned int *barrier;
+  int32_t *error;
+  double *info;       // [items][3]: status, iterations, residual
+  double tolerance;
+  int32_t max_iterations;
+  uint32_t active_mask;
+  long long timeout_ns;
+};
+
+// Launchers (return cudaError_t of the launch).
+cudaError_t LaunchElementKernel(const DevicePlan &p, int kp, const double *state,
+                                uint32_t newton_mask, uint32_t active_mask, double *elem_vals,
+                                double *elem_rhs, int32_t *invalid, cudaStream_t stream);
+cudaError_t LaunchGatherValues(const DevicePlan &p, int kp, const double *elem_vals,
+                               uint32_t active_mask, double *values, double *diag, double *invd,
+                               int32_t *invalid, cudaStream_t stream);
+cudaError_t LaunchGatherRhs(const DevicePlan &p, int kp, const double *elem_rhs,
+                            const double *currents, const double *hc_scale, uint32_t active_mask,
+                            double *rhs, cudaStream_t stream);
+// Cooperative persistent PCG; *grid_out receives the number of CTAs used.
+cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream);
+int PcgMaxGrid(int kp);
+
+cudaError_t LaunchNewtonNorms(const DevicePlan &p, int kp, const double *x, const double *state,
+                              double *partials, double *norms, cudaStream_t stream);
+cudaError_t LaunchNewtonUpdate(const DevicePlan &p, int kp, const double *x, double *state,
+                               ItemScalars relax, uint32_t update_mask, cudaStream_t stream);
+cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm_item_major,
+                            int items, double *state, cudaStream_t stream);
+cudaError_t LaunchFinalize(const DevicePlan &p, int kp, int items, const double *state,
+                           double *a_out, double *b1_out, double *b2_out, double *flux_out,
+                           cudaStream_t stream);
+// CSR-ordered copies of assembled values / diagonal / rhs for item `item`.
+cudaError_t LaunchExtractCsr(const DevicePlan &p, int kp, int item, const double *values,
+                             const double *diag, const double *rhs, double *csr_values,
+                             double *diag_out, double *rhs_out, cudaStream_t stream);
+// Scatter CSR-ordered operator values into the SELL layout (item-major input).
+cudaError_t LaunchScatterCsr(const DevicePlan &p, int kp, int items, const double *csr_values,
+                             int32_t values_per_item, double *values, cudaStream_t stream);
+// Interleave item-major vectors [items][len] into [len_pad][kp] and back.
+cudaError_t LaunchInterleave(int kp, int items, int len, int len_pad, const double *in, double *out,
+                             cudaStream_t stream);
+cudaError_t LaunchDeinterleave(int kp, int items, int len, const double *in, double *out,
+                               cudaStream_t stream);
+
+} // namespace fg

@@ -1,0 +1,280 @@
+// newton.cu -- device side of the Newton update and of B / flux-linkage recovery.
+//
+// Step norm: the reference expands the free solution to nodes and forms
+// ||cand - A|| / ||cand|| on the host (gpu_solver/src/solvers/nonlinear_solver.cu:
+// 326-335); here both sums are a deterministic two-level device reduction and only
+// 2 x items doubles cross to the host.  Relaxation (:344-351) is applied on the
+// device with the per-item factor the host chose.  Recovery (FinalizeResult, :16-83)
+// evaluates element B and the per-circuit flux linkage as fixed-order reductions.
+#include "kernels.cuh"
+
+#include <cmath>
+
+namespace fg
+{
+namespace
+{
+
+constexpr int kThreads = 256;
+constexpr int kNormBlocks = 256;
+
+__device__ __forceinline__ double Candidate(const DevicePlan &p, int kp, const double *x, int node,
+                                            int item)
+{
+  const int row = p.node_to_free[node];
+  return row >= 0 ? static_cast<double>(p.node_sign[node]) * x[static_cast<size_t>(row) * kp + item]
+                  : p.boundary[node];
+}
+
+template <int KP>
+__global__ void __launch_bounds__(kThreads)
+    NormsKernel(DevicePlan p, const double *__restrict__ x, const double *__restrict__ state,
+                double *__restrict__ partials)
+{
+  __shared__ double red[kThreads / 32][2][KP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, item = lane % KP;
+  double dd = 0.0, cc = 0.0;
+  const size_t total = static_cast<size_t>(p.N) * KP;
+  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int node = static_cast<int>(t / KP);
+    const double c = Candidate(p, KP, x, node, item);
+    const double d = c - state[t];
+    dd += d * d;
+    cc += c * c;
+  }
+  for (int off = 16; off >= KP; off >>= 1) {
+    dd += __shfl_xor_sync(0xffffffffu, dd, off);
+    cc += __shfl_xor_sync(0xffffffffu, cc, off);
+  }
+  if (lane < KP) {
+    red[warp][0][lane] = dd;
+    red[warp][1][lane] = cc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * KP) {
+    const int q = threadIdx.x / KP, it = threadIdx.x % KP;
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w)
+      s += red[w][q][it];
+    partials[(static_cast<size_t>(q) * KP + it) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+__global__ void NormsFinalKernel(int kp, int blocks, const double *__restrict__ partials,
+                                 double *__restrict__ norms)
+{
+  // One warp per (quantity, item); lanes stride the block partials in fixed order.
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int qk = 2 * kp;
+  for (int t = warp; t < qk; t += blockDim.x / 32) {
+    double s = 0.0;
+    for (int b = lane; b < blocks; b += 32)
+      s += partials[static_cast<size_t>(t) * blocks + b];
+    for (int off = 16; off > 0; off >>= 1)
+      s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0)
+      norms[t] = s;
+  }
+}
+
+template <int KP>
+__global__ void UpdateKernel(DevicePlan p, const double *__restrict__ x, double *__restrict__ state,
+                             ItemScalars relax, uint32_t mask)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.N) * KP)
+    return;
+  const int node = static_cast<int>(t / KP), item = static_cast<int>(t % KP);
+  if (!((mask >> item) & 1u))
+    return;
+  const double c = Candidate(p, KP, x, node, item);
+  const double s = state[t];
+  state[t] = s + relax.v[item] * (c - s);
+}
+
+__global__ void InitStateKernel(DevicePlan p, int kp, const double *__restrict__ warm, int items,
+                                double *__restrict__ state)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.N) * kp)
+    return;
+  const int node = static_cast<int>(t / kp), item = static_cast<int>(t % kp);
+  // Zero start with the expanded fixed values (nonlinear_solver.cu:193-209, :234-242);
+  // a warm start replaces the free values and keeps the Dirichlet ones (:686-693).
+  double v = p.boundary[node];
+  if (warm && item < items && p.node_to_free[node] >= 0)
+    v = warm[static_cast<size_t>(item) * p.N + node];
+  state[t] = v;
+}
+
+template <bool kAxi>
+__global__ void FieldKernel(DevicePlan p, int kp, int items, const double *__restrict__ state,
+                            double *__restrict__ b1, double *__restrict__ b2)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.E) * items)
+    return;
+  const int item = static_cast<int>(t / p.E), e = static_cast<int>(t % p.E);
+  const size_t E = p.E;
+  double a[3];
+  for (int l = 0; l < 3; ++l)
+    a[l] = state[static_cast<size_t>(p.elem_nodes[3 * e + l]) * kp + item];
+  double f1 = 0.0, f2 = 0.0;
+  if constexpr (!kAxi) {
+    for (int l = 0; l < 3; ++l) {
+      f1 += a[l] * p.elem_geo[(1 + l) * E + e];
+      f2 += a[l] * p.elem_geo[(4 + l) * E + e];
+    }
+  } else {
+    // Centroid of the r-z element (axisymmetric_p1.h:79-94).
+    double r[3], z[3];
+    for (int l = 0; l < 3; ++l) {
+      r[l] = p.elem_geo[l * E + e];
+      z[l] = p.elem_geo[(3 + l) * E + e];
+    }
+    const double det = (r[1] - r[0]) * (z[2] - z[0]) - (r[2] - r[0]) * (z[1] - z[0]);
+    const double dndr[3] = {(z[1] - z[2]) / det, (z[2] - z[0]) / det, (z[0] - z[1]) / det};
+    const double dndz[3] = {(r[2] - r[1]) / det, (r[0] - r[2]) / det, (r[1] - r[0]) / det};
+    double rc = 0.0;
+    for (int l = 0; l < 3; ++l)
+      rc += (1.0 / 3.0) * r[l];
+    for (int l = 0; l < 3; ++l) {
+      f1 += a[l] * (-dndz[l]);
+      f2 += a[l] * (dndr[l] + (1.0 / 3.0) / rc);
+    }
+  }
+  if (b1)
+    b1[t] = f1;
+  if (b2)
+    b2[t] = f2;
+}
+
+// Seven-point rule for the axisymmetric flux integral.
+__constant__ double kBaryF[7][3] = {
+    {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0},
+    {0.059715871789770, 0.470142064105115, 0.470142064105115},
+    {0.470142064105115, 0.059715871789770, 0.470142064105115},
+    {0.470142064105115, 0.470142064105115, 0.059715871789770},
+    {0.797426985353087, 0.101286507323456, 0.101286507323456},
+    {0.101286507323456, 0.797426985353087, 0.101286507323456},
+    {0.101286507323456, 0.101286507323456, 0.797426985353087}};
+__constant__ double kQwF[7] = {0.225, 0.132394152788506, 0.132394152788506, 0.132394152788506,
+                               0.125939180544827, 0.125939180544827, 0.125939180544827};
+
+// One block per (circuit, item): fixed-order block reduction over the circuit's elements.
+template <bool kAxi>
+__global__ void __launch_bounds__(kThreads)
+    FluxKernel(DevicePlan p, int kp, const double *__restrict__ state, double *__restrict__ flux)
+{
+  __shared__ double red[kThreads / 32];
+  const int c = blockIdx.x, item = blockIdx.y;
+  const size_t E = p.E;
+  double sum = 0.0;
+  for (int k = p.circuit_elem_off[c] + threadIdx.x; k < p.circuit_elem_off[c + 1]; k += blockDim.x) {
+    const int e = p.circuit_elems[k];
+    const double jpa = p.mat_jpa[p.elem_mat[e]];
+    double a[3];
+    for (int l = 0; l < 3; ++l)
+      a[l] = state[static_cast<size_t>(p.elem_nodes[3 * e + l]) * kp + item];
+    if constexpr (!kAxi) {
+      sum += p.elem_geo[e] * jpa / 3.0 * (a[0] + a[1] + a[2]);
+    } else {
+      double r[3], z[3];
+      for (int l = 0; l < 3; ++l) {
+        r[l] = p.elem_geo[l * E + e];
+        z[l] = p.elem_geo[(3 + l) * E + e];
+      }
+      const double area = 0.5 * ((r[1] - r[0]) * (z[2] - z[0]) - (r[2] - r[0]) * (z[1] - z[0]));
+      double f = 0.0;
+      for (int q = 0; q < 7; ++q) {
+        double rq = 0.0, av = 0.0;
+        for (int l = 0; l < 3; ++l) {
+          rq += kBaryF[q][l] * r[l];
+          av += kBaryF[q][l] * a[l];
+        }
+        f += 6.283185307179586476925286766559005768 * rq * (area * kQwF[q]) * jpa * av;
+      }
+      sum += f;
+    }
+  }
+  for (int off = 16; off > 0; off >>= 1)
+    sum += __shfl_xor_sync(0xffffffffu, sum, off);
+  if ((threadIdx.x & 31) == 0)
+    red[threadIdx.x >> 5] = sum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w)
+      s += red[w];
+    if (!kAxi)
+      s *= p.depth_m;
+    flux[static_cast<size_t>(item) * p.C + c] = s;
+  }
+}
+
+inline unsigned Blocks(size_t threads) { return static_cast<unsigned>((threads + kThreads - 1) / kThreads); }
+
+} // namespace
+
+#define FG_DISPATCH_KP(kp, CALL)                                                                   \
+  switch (kp) {                                                                                    \
+  case 1: { constexpr int KP = 1; CALL; } break;                                                    \
+  case 2: { constexpr int KP = 2; CALL; } break;                                                    \
+  case 4: { constexpr int KP = 4; CALL; } break;                                                    \
+  case 8: { constexpr int KP = 8; CALL; } break;                                                    \
+  case 16: { constexpr int KP = 16; CALL; } break;                                                  \
+  case 32: { constexpr int KP = 32; CALL; } break;                                                  \
+  default: return cudaErrorInvalidValue;                                                           \
+  }
+
+// partials: [2][kp][kNormBlocks]; norms: [2][kp] (sum of squared step, sum of squared candidate)
+cudaError_t LaunchNewtonNorms(const DevicePlan &p, int kp, const double *x, const double *state,
+                              double *partials, double *norms, cudaStream_t stream)
+{
+  FG_DISPATCH_KP(kp, (NormsKernel<KP><<<kNormBlocks, kThreads, 0, stream>>>(p, x, state, partials)));
+  NormsFinalKernel<<<1, 1024, 0, stream>>>(kp, kNormBlocks, partials, norms);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchNewtonUpdate(const DevicePlan &p, int kp, const double *x, double *state,
+                               ItemScalars relax, uint32_t update_mask, cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.N) * kp);
+  FG_DISPATCH_KP(kp, (UpdateKernel<KP><<<blocks, kThreads, 0, stream>>>(p, x, state, relax, update_mask)));
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm, int items,
+                            double *state, cudaStream_t stream)
+{
+  InitStateKernel<<<Blocks(static_cast<size_t>(p.N) * kp), kThreads, 0, stream>>>(p, kp, warm, items, state);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchFinalize(const DevicePlan &p, int kp, int items, const double *state,
+                           double *a_out, double *b1_out, double *b2_out, double *flux_out,
+                           cudaStream_t stream)
+{
+  if (a_out) {
+    cudaError_t e = LaunchDeinterleave(kp, items, p.N, state, a_out, stream);
+    if (e != cudaSuccess)
+      return e;
+  }
+  if (b1_out || b2_out) {
+    const unsigned blocks = Blocks(static_cast<size_t>(p.E) * items);
+    if (p.problem_type == 0)
+      FieldKernel<false><<<blocks, kThreads, 0, stream>>>(p, kp, items, state, b1_out, b2_out);
+    else
+      FieldKernel<true><<<blocks, kThreads, 0, stream>>>(p, kp, items, state, b1_out, b2_out);
+  }
+  if (flux_out && p.C > 0) {
+    if (p.problem_type == 0)
+      FluxKernel<false><<<dim3(p.C, items), kThreads, 0, stream>>>(p, kp, state, flux_out);
+    else
+      FluxKernel<true><<<dim3(p.C, items), kThreads, 0, stream>>>(p, kp, state, flux_out);
+  }
+  return cudaGetLastError();
+}
+
+} // namespace fg

@@ -1,0 +1,615 @@
+// solver.cpp -- batched Newton driver over the device plan.
+//
+// Newton semantics follow NonlinearP1Solver::SolveBatch (gpu_solver/src/solvers/
+// nonlinear_solver.cu:183-530) with the device-assembly path: zero start with the
+// expanded fixed values, cold-secant operator at iteration zero (Newton from the
+// start for a warm-started item, as Solve() does at :698), one inner tolerance for
+// the batch = the tightest NewtonLinearTolerance of its active items
+// (nonlinear_model.cpp:166-184), relaxation after iteration five, the 1e-6 step gate
+// at the exact inner tolerance (NewtonStepConverged, :186-193), per-item status
+// isolation.  Everything stays on the device except 2 x items step norms and the PCG
+// summaries that cross back once per Newton iteration.
+#include "solver.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+namespace fg
+{
+namespace
+{
+
+int PadItems(int k)
+{
+  int kp = 1;
+  while (kp < k)
+    kp <<= 1;
+  return kp;
+}
+
+double NewtonLinearTolerance(const fg_solve_options &o, bool adaptive, double previous_step)
+{
+  const double exact = o.linear_relative_tolerance;
+  if (!adaptive || !std::isfinite(previous_step) || previous_step <= 100.0 * o.relative_tolerance ||
+      !(exact > 0.0) || !std::isfinite(exact))
+    return exact;
+  return std::max(exact, 1e-8 * std::min(1.0, previous_step));
+}
+
+float Elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+  float ms = 0.0f;
+  if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+    cudaGetLastError();
+    return 0.0f;
+  }
+  return ms;
+}
+
+} // namespace
+
+size_t Plan::DeviceBytes() const
+{
+  size_t b = 0;
+  b += row_offsets_.bytes() + columns_.bytes() + row_len_.bytes() + slice_off_.bytes() +
+       sell_col_.bytes() + contrib_off_.bytes() + contrib_.bytes() + rhs_off_.bytes() +
+       rhs_contrib_.bytes() + elem_nodes_.bytes() + elem_mat_.bytes() + node_to_free_.bytes() +
+       circuit_elem_off_.bytes() + circuit_elems_.bytes() + node_sign_.bytes() + pm_rhs_.bytes() +
+       circuit_rhs_.bytes() + elem_geo_.bytes() + boundary_.bytes();
+  b += state_.bytes() + ev_.bytes() + er_.bytes() + values_.bytes() + diag_.bytes() +
+       invd_.bytes() + rhs_.bytes() + x_.bytes() + r_.bytes() + z_.bytes() + p0_.bytes() +
+       p1_.bytes() + q_.bytes() + pcg_partials_.bytes() + staging_.bytes();
+  b += in_currents_.bytes() + in_hc_.bytes() + in_warm_.bytes() + out_a_.bytes() + out_b1_.bytes() +
+       out_b2_.bytes() + out_flux_.bytes();
+  return b;
+}
+
+Status Plan::Create(HostModel model, const fg_plan_options &options)
+{
+  model_ = std::move(model);
+  options_ = options;
+  if (options_.preconditioner != FG_PRECOND_JACOBI || options_.precision != FG_PRECISION_FP64)
+    return Status::kUnsupportedFeature;
+  Status s = BuildHostPlan(model_, &host_);
+  if (s != Status::kOk)
+    return s;
+  if (host_.E >= (1 << 27) || host_.positions > (int64_t(1) << 31) / kMaxItems)
+    return Status::kUnsupportedFeature;
+  host_only_ = (options_.flags & FG_PLAN_HOST_ONLY) != 0;
+  if (host_only_)
+    return Status::kOk;
+  int devices = 0;
+  if (cudaGetDeviceCount(&devices) != cudaSuccess || devices < 1) {
+    cudaGetLastError();
+    return Status::kGpuUnavailable;
+  }
+  s = Upload();
+  if (s != Status::kOk)
+    return s;
+  if (cudaEventCreate(&ev_start_) != cudaSuccess || cudaEventCreate(&ev_mid_) != cudaSuccess ||
+      cudaEventCreate(&ev_pcg_) != cudaSuccess || cudaEventCreate(&ev_end_) != cudaSuccess)
+    return Status::kInternalError;
+  return Status::kOk;
+}
+
+Status Plan::Upload()
+{
+  const HostPlan &h = host_;
+  Status s = Status::kOk;
+#define FG_UP(dst, vec)                                                                            \
+  if (s == Status::kOk)                                                                            \
+    s = dst.upload(vec.data(), vec.size());
+  FG_UP(row_offsets_, h.row_offsets);
+  FG_UP(columns_, h.columns);
+  FG_UP(row_len_, h.row_len);
+  FG_UP(slice_off_, h.slice_off);
+  FG_UP(sell_col_, h.sell_col);
+  FG_UP(contrib_off_, h.contrib_off);
+  FG_UP(contrib_, h.contrib);
+  FG_UP(rhs_off_, h.rhs_off);
+  FG_UP(rhs_contrib_, h.rhs_contrib);
+  FG_UP(elem_nodes_, h.elem_nodes);
+  FG_UP(elem_mat_, h.elem_mat);
+  FG_UP(mat_curve_off_, h.mat_curve_off);
+  FG_UP(mat_curve_cnt_, h.mat_curve_cnt);
+  FG_UP(mat_circuit_, h.mat_circuit);
+  FG_UP(node_to_free_, h.dofs.node_to_free);
+  FG_UP(circuit_elem_off_, h.circuit_elem_off);
+  FG_UP(circuit_elems_, h.circuit_elems);
+  FG_UP(node_sign_, h.dofs.node_sign);
+  FG_UP(pm_rhs_, h.pm_rhs);
+  FG_UP(circuit_rhs_, h.circuit_rhs);
+  FG_UP(elem_geo_, h.elem_geo);
+  FG_UP(mat_nu0_, h.mat_nu0);
+  FG_UP(mat_alpha_, h.mat_alpha);
+  FG_UP(mat_cold_, h.mat_cold);
+  FG_UP(mat_jpa_, h.mat_jpa);
+  FG_UP(curve_b_, h.curve_b);
+  FG_UP(curve_h_, h.curve_h);
+  FG_UP(curve_slope_, h.curve_slope);
+  FG_UP(boundary_, h.dofs.boundary);
+#undef FG_UP
+  if (s != Status::kOk)
+    return s;
+  if (cudaDeviceSynchronize() != cudaSuccess)
+    return Status::kInternalError;
+  DevicePlan &d = dev_;
+  d.N = h.N;
+  d.E = h.E;
+  d.n = h.n;
+  d.n_pad = h.n_pad;
+  d.slices = h.slices;
+  d.C = h.C;
+  d.problem_type = h.problem_type;
+  d.nnz = h.nnz;
+  d.positions = h.positions;
+  d.row_offsets = row_offsets_.get();
+  d.columns = columns_.get();
+  d.row_len = row_len_.get();
+  d.slice_off = slice_off_.get();
+  d.sell_col = sell_col_.get();
+  d.contrib_off = contrib_off_.get();
+  d.contrib = contrib_.get();
+  d.rhs_off = rhs_off_.get();
+  d.rhs_contrib = rhs_contrib_.get();
+  d.pm_rhs = pm_rhs_.get();
+  d.circuit_rhs = circuit_rhs_.get();
+  d.elem_nodes = elem_nodes_.get();
+  d.elem_mat = elem_mat_.get();
+  d.elem_geo = elem_geo_.get();
+  d.mat_nu0 = mat_nu0_.get();
+  d.mat_alpha = mat_alpha_.get();
+  d.mat_cold = mat_cold_.get();
+  d.mat_jpa = mat_jpa_.get();
+  d.mat_curve_off = mat_curve_off_.get();
+  d.mat_curve_cnt = mat_curve_cnt_.get();
+  d.mat_circuit = mat_circuit_.get();
+  d.curve_b = curve_b_.get();
+  d.curve_h = curve_h_.get();
+  d.curve_slope = curve_slope_.get();
+  d.node_to_free = node_to_free_.get();
+  d.node_sign = node_sign_.get();
+  d.boundary = boundary_.get();
+  d.circuit_elem_off = circuit_elem_off_.get();
+  d.circuit_elems = circuit_elems_.get();
+  d.depth_m = model_.depth_m;
+  return Status::kOk;
+}
+
+Status Plan::EnsureWorkspace(int kp)
+{
+  if (kp <= kp_cap_)
+    return Status::kOk;
+  const HostPlan &h = host_;
+  const size_t vec = static_cast<size_t>(h.n_pad) * kp;
+  Status s = Status::kOk;
+  const int grid = PcgMaxGrid(kp);
+  if (grid <= 0)
+    return Status::kGpuUnavailable;
+  pcg_grid_cap_ = std::max(pcg_grid_cap_, grid);
+#define FG_EN(arr, count)                                                                          \
+  if (s == Status::kOk)                                                                            \
+    s = arr.ensure(count);
+  FG_EN(state_, static_cast<size_t>(h.N) * kp);
+  FG_EN(ev_, static_cast<size_t>(6) * h.E * kp);
+  FG_EN(er_, static_cast<size_t>(3) * h.E * kp);
+  FG_EN(values_, static_cast<size_t>(h.positions) * kp);
+  FG_EN(diag_, vec);
+  FG_EN(invd_, vec);
+  FG_EN(rhs_, vec);
+  FG_EN(x_, vec);
+  FG_EN(r_, vec);
+  FG_EN(z_, vec);
+  FG_EN(p0_, vec);
+  FG_EN(p1_, vec);
+  FG_EN(q_, vec);
+  FG_EN(norm_partials_, static_cast<size_t>(2) * kp * 256);
+  FG_EN(norms_, static_cast<size_t>(2) * kp);
+  FG_EN(pcg_partials_, static_cast<size_t>(2) * 64 * pcg_grid_cap_);
+  FG_EN(pcg_info_, static_cast<size_t>(3) * kp);
+  FG_EN(barrier_, 1);
+  FG_EN(error_, 1);
+  FG_EN(invalid_, static_cast<size_t>(kp));
+  FG_EN(small_, static_cast<size_t>(8) * kp + 8);
+#undef FG_EN
+  if (s != Status::kOk)
+    return s;
+  // Padding rows of the operator must read as an identity with a zero inverse.
+  kp_cap_ = kp;
+  return Status::kOk;
+}
+
+Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
+                    int value_stride, int value_item, int diag_stride, int diag_item,
+                    int use_inverse, cudaStream_t stream)
+{
+  PcgArgs a{};
+  a.n = host_.n;
+  a.n_pad = host_.n_pad;
+  a.slices = host_.slices;
+  a.kp = kp;
+  a.items = items;
+  a.slice_off = slice_off_.get();
+  a.row_len = row_len_.get();
+  a.sell_col = sell_col_.get();
+  a.values = values_.get();
+  a.value_stride = value_stride;
+  a.value_item = value_item;
+  a.diag = diag_.get();
+  a.invd = invd_.get();
+  a.diag_stride = diag_stride;
+  a.diag_item = diag_item;
+  a.use_inverse = use_inverse;
+  a.b = rhs_.get();
+  a.x = x_.get();
+  a.r = r_.get();
+  a.z = z_.get();
+  a.p0 = p0_.get();
+  a.p1 = p1_.get();
+  a.q = q_.get();
+  a.partials = pcg_partials_.get();
+  a.barrier = barrier_.get();
+  a.error = error_.get();
+  a.info = pcg_info_.get();
+  a.tolerance = tolerance;
+  a.max_iterations = max_iterations;
+  a.active_mask = mask;
+  a.timeout_ns = 5000000000LL;
+  int grid = 0, block = 0;
+  const cudaError_t e = LaunchPcg(a, &grid, &block, stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return Status::kInternalError;
+  }
+  timing_.pcg_grid = grid;
+  timing_.pcg_block = block;
+  timing_.pcg_launches += 1;
+  timing_.kernel_launches += 1;
+  return Status::kOk;
+}
+
+Status Plan::SolveDevice(const SolveRequest &req)
+{
+  timing_ = fg_timing{};
+  if (host_only_)
+    return Status::kGpuUnavailable;
+  if (req.items <= 0 || (!req.currents && host_.C > 0) || !req.info)
+    return Status::kInvalidArgument;
+  for (int first = 0; first < req.items; first += kMaxItems) {
+    const Status s = SolveChunk(req, first, std::min(kMaxItems, req.items - first));
+    if (s != Status::kOk)
+      return s;
+  }
+  return Status::kOk;
+}
+
+Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
+{
+  const fg_solve_options &o = req.options;
+  const int N = host_.N, E = host_.E, C = host_.C;
+  cudaStream_t st = req.stream;
+  for (int i = 0; i < k; ++i) {
+    fg_item_info &inf = req.info[first + i];
+    inf = fg_item_info{};
+    inf.status = ToInt(Status::kInvalidArgument);
+    inf.residual_l2 = std::numeric_limits<double>::infinity();
+    inf.last_linear_tolerance = std::numeric_limits<double>::quiet_NaN();
+    inf.verified_equation_residual_relative = std::numeric_limits<double>::infinity();
+  }
+  if (!(o.relative_tolerance > 0.0) || !std::isfinite(o.relative_tolerance) ||
+      o.max_newton_iterations < 0 || o.max_linear_iterations < 0)
+    return Status::kOk; // per-item INVALID_ARGUMENT, as SolveBatch returns
+  const int kp = PadItems(k);
+  Status s = EnsureWorkspace(kp);
+  if (s != Status::kOk)
+    return s;
+  const double *currents = req.currents + static_cast<size_t>(first) * C;
+  const double *hc = req.hc_scale ? req.hc_scale + first : nullptr;
+  const double *warm = req.warm ? req.warm + static_cast<size_t>(first) * N : nullptr;
+
+  // Non-finite currents make an item invalid before any work (nonlinear_solver.cu:198-206).
+  uint32_t active = 0;
+  {
+    std::vector<double> cur(static_cast<size_t>(k) * C);
+    if (C > 0 && cudaMemcpyAsync(cur.data(), currents, cur.size() * sizeof(double),
+                                 cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return Status::kInternalError;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return Status::kInternalError;
+    for (int i = 0; i < k; ++i) {
+      bool finite = true;
+      for (int c = 0; c < C; ++c)
+        finite = finite && std::isfinite(cur[static_cast<size_t>(i) * C + c]);
+      if (finite)
+        active |= 1u << i;
+    }
+  }
+  const bool adaptive = o.adaptive_linear_tolerance != 0 && host_.has_nonlinear;
+  if (LaunchInitState(dev_, kp, warm, k, state_.get(), st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 1;
+  std::vector<double> relax(k, 1.0), prev(k, std::numeric_limits<double>::infinity());
+  double *h = small_.get();
+  for (int iteration = 0; iteration < o.max_newton_iterations && active; ++iteration) {
+    double tol = std::numeric_limits<double>::infinity();
+    for (int i = 0; i < k; ++i)
+      if ((active >> i) & 1u)
+        tol = std::min(tol, NewtonLinearTolerance(o, adaptive, prev[i]));
+    const uint32_t newton_mask = (iteration > 0 || warm) ? active : 0u;
+    cudaEventRecord(ev_start_, st);
+    if (cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) != cudaSuccess ||
+        LaunchElementKernel(dev_, kp, state_.get(), newton_mask, active, ev_.get(), er_.get(),
+                            invalid_.get(), st) != cudaSuccess ||
+        LaunchGatherValues(dev_, kp, ev_.get(), active, values_.get(), diag_.get(), invd_.get(),
+                           invalid_.get(), st) != cudaSuccess ||
+        LaunchGatherRhs(dev_, kp, er_.get(), currents, hc, active, rhs_.get(), st) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 3;
+    cudaEventRecord(ev_mid_, st);
+    s = RunPcg(kp, k, active, tol, o.max_linear_iterations, kp, 1, kp, 1, 1, st);
+    if (s != Status::kOk)
+      return s;
+    cudaEventRecord(ev_pcg_, st);
+    if (LaunchNewtonNorms(dev_, kp, x_.get(), state_.get(), norm_partials_.get(), norms_.get(), st) !=
+        cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 2;
+    // Small summary back to the host: PCG info [3kp], norms [2kp], assembly flags, PCG error.
+    if (cudaMemcpyAsync(h, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(h + 3 * kp, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 5 * kp), invalid_.get(), sizeof(int32_t) * kp,
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 6 * kp), error_.get(), sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, st) != cudaSuccess)
+      return Status::kInternalError;
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.assembly_ms += Elapsed(ev_start_, ev_mid_);
+    timing_.pcg_ms += Elapsed(ev_mid_, ev_pcg_);
+    timing_.newton_iterations += 1;
+    const double *pinfo = h, *norms = h + 3 * kp;
+    const int32_t *invalid = reinterpret_cast<const int32_t *>(h + 5 * kp);
+    const int32_t pcg_error = *reinterpret_cast<const int32_t *>(h + 6 * kp);
+    if (pcg_error != 0)
+      return Status::kInternalError;
+    int max_its = 0;
+    ItemScalars rel{};
+    uint32_t update = 0;
+    const uint32_t was_active = active;
+    for (int i = 0; i < k; ++i) {
+      if (!((was_active >> i) & 1u))
+        continue;
+      fg_item_info &inf = req.info[first + i];
+      if (invalid[i]) {
+        inf.status = ToInt(Status::kAssemblyFailed);
+        active &= ~(1u << i);
+        continue;
+      }
+      const int pstatus = static_cast<int>(pinfo[3 * i]);
+      const int pits = static_cast<int>(pinfo[3 * i + 1]);
+      max_its = std::max(max_its, pits);
+      inf.linear_iterations += pits;
+      inf.last_linear_tolerance = tol;
+      if (pstatus != 0) {
+        inf.status = pstatus;
+        inf.iterations = pits;
+        inf.residual_l2 = pinfo[3 * i + 2];
+        active &= ~(1u << i);
+        continue;
+      }
+      const double dd = norms[i], cc = norms[kp + i];
+      const double residual =
+          std::sqrt(dd) / std::max(std::sqrt(cc), std::numeric_limits<double>::min());
+      inf.iterations = iteration + 1;
+      inf.residual_l2 = residual;
+      if (!std::isfinite(residual)) {
+        inf.status = ToInt(Status::kNumericalNonfinite);
+        active &= ~(1u << i);
+        continue;
+      }
+      if (iteration > 5) {
+        if (residual > prev[i] && relax[i] > 0.125)
+          relax[i] *= 0.5;
+        else
+          relax[i] += 0.1 * (1.0 - relax[i]);
+      }
+      rel.v[i] = relax[i];
+      update |= 1u << i;
+      if (iteration > 0 && residual < 100.0 * o.relative_tolerance &&
+          tol <= o.linear_relative_tolerance) {
+        inf.status = ToInt(Status::kOk);
+        active &= ~(1u << i);
+      } else {
+        prev[i] = residual;
+      }
+    }
+    timing_.pcg_iterations += max_its;
+    cudaEventRecord(ev_start_, st);
+    if (update && LaunchNewtonUpdate(dev_, kp, x_.get(), state_.get(), rel, update, st) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += update ? 1 : 0;
+    cudaEventRecord(ev_end_, st);
+  }
+  for (int i = 0; i < k; ++i)
+    if ((active >> i) & 1u)
+      req.info[first + i].status = ToInt(Status::kNonlinearSolveNotConverged);
+  cudaEventRecord(ev_mid_, st);
+  const cudaError_t fe = LaunchFinalize(
+      dev_, kp, k, state_.get(), req.a_out ? req.a_out + static_cast<size_t>(first) * N : nullptr,
+      req.b1_out ? req.b1_out + static_cast<size_t>(first) * E : nullptr,
+      req.b2_out ? req.b2_out + static_cast<size_t>(first) * E : nullptr,
+      req.flux_out ? req.flux_out + static_cast<size_t>(first) * C : nullptr, st);
+  if (fe != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 3;
+  cudaEventRecord(ev_pcg_, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.finalize_ms += Elapsed(ev_mid_, ev_pcg_);
+  return Status::kOk;
+}
+
+Status Plan::SolveHost(int items, const double *currents, const double *hc_scale,
+                       const double *warm, const fg_solve_options &options, double *a_out,
+                       double *b1_out, double *b2_out, double *flux_out, fg_item_info *info)
+{
+  if (host_only_)
+    return Status::kGpuUnavailable;
+  if (items <= 0 || (!currents && host_.C > 0) || !info)
+    return Status::kInvalidArgument;
+  const size_t N = host_.N, E = host_.E, C = host_.C, k = items;
+  Status s = Status::kOk;
+  if ((s = in_currents_.upload(currents, k * C)) != Status::kOk)
+    return s;
+  if (hc_scale && (s = in_hc_.upload(hc_scale, k)) != Status::kOk)
+    return s;
+  if (warm && (s = in_warm_.upload(warm, k * N)) != Status::kOk)
+    return s;
+  if ((a_out && (s = out_a_.ensure(k * N)) != Status::kOk) ||
+      (b1_out && (s = out_b1_.ensure(k * E)) != Status::kOk) ||
+      (b2_out && (s = out_b2_.ensure(k * E)) != Status::kOk) ||
+      (flux_out && (s = out_flux_.ensure(k * C)) != Status::kOk))
+    return s;
+  SolveRequest req;
+  req.items = items;
+  req.currents = in_currents_.get();
+  req.hc_scale = hc_scale ? in_hc_.get() : nullptr;
+  req.warm = warm ? in_warm_.get() : nullptr;
+  req.options = options;
+  req.a_out = a_out ? out_a_.get() : nullptr;
+  req.b1_out = b1_out ? out_b1_.get() : nullptr;
+  req.b2_out = b2_out ? out_b2_.get() : nullptr;
+  req.flux_out = flux_out ? out_flux_.get() : nullptr;
+  req.info = info;
+  req.stream = nullptr;
+  s = SolveDevice(req);
+  if (s != Status::kOk)
+    return s;
+  if ((a_out && cudaMemcpy(a_out, out_a_.get(), k * N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (b1_out && cudaMemcpy(b1_out, out_b1_.get(), k * E * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (b2_out && cudaMemcpy(b2_out, out_b2_.get(), k * E * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (flux_out && C > 0 && cudaMemcpy(flux_out, out_flux_.get(), k * C * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+    return Status::kInternalError;
+  return Status::kOk;
+}
+
+Status Plan::Assemble(int items, const double *states, const double *currents,
+                      const int32_t *use_newton, double *values, double *diagonal, double *rhs)
+{
+  if (host_only_)
+    return Status::kGpuUnavailable;
+  if (items <= 0 || items > kMaxItems || !states || (!currents && host_.C > 0) || !use_newton)
+    return Status::kInvalidArgument;
+  const int kp = PadItems(items);
+  Status s = EnsureWorkspace(kp);
+  if (s != Status::kOk)
+    return s;
+  const size_t N = host_.N, C = host_.C, n = host_.n, nnz = host_.nnz;
+  if ((s = in_warm_.upload(states, items * N)) != Status::kOk ||
+      (s = in_currents_.upload(currents, items * C)) != Status::kOk ||
+      (s = staging_.ensure(nnz + 2 * n)) != Status::kOk)
+    return s;
+  uint32_t newton = 0, active = 0;
+  for (int i = 0; i < items; ++i) {
+    active |= 1u << i;
+    if (use_newton[i])
+      newton |= 1u << i;
+  }
+  if (LaunchInterleave(kp, items, static_cast<int>(N), static_cast<int>(N), in_warm_.get(), state_.get(), nullptr) != cudaSuccess ||
+      cudaMemset(invalid_.get(), 0, sizeof(int32_t) * kp) != cudaSuccess ||
+      LaunchElementKernel(dev_, kp, state_.get(), newton, active, ev_.get(), er_.get(), invalid_.get(), nullptr) != cudaSuccess ||
+      LaunchGatherValues(dev_, kp, ev_.get(), active, values_.get(), diag_.get(), invd_.get(), invalid_.get(), nullptr) != cudaSuccess ||
+      LaunchGatherRhs(dev_, kp, er_.get(), in_currents_.get(), nullptr, active, rhs_.get(), nullptr) != cudaSuccess)
+    return Status::kInternalError;
+  std::vector<int32_t> invalid(kp);
+  for (int i = 0; i < items; ++i) {
+    double *sv = staging_.get(), *sd = sv + nnz, *sr = sd + n;
+    if (LaunchExtractCsr(dev_, kp, i, values_.get(), diag_.get(), rhs_.get(), sv, sd, sr, nullptr) != cudaSuccess)
+      return Status::kInternalError;
+    if ((values && cudaMemcpy(values + i * nnz, sv, nnz * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (diagonal && cudaMemcpy(diagonal + i * n, sd, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+        (rhs && cudaMemcpy(rhs + i * n, sr, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+      return Status::kInternalError;
+  }
+  if (cudaMemcpy(invalid.data(), invalid_.get(), sizeof(int32_t) * kp, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return Status::kInternalError;
+  for (int i = 0; i < items; ++i)
+    if (invalid[i])
+      return Status::kAssemblyFailed;
+  return Status::kOk;
+}
+
+Status Plan::PcgSolve(int items, const double *values, int values_per_item, const double *rhs,
+                      double tolerance, int max_iterations, double *x, fg_linear_info *info)
+{
+  if (host_only_)
+    return Status::kGpuUnavailable;
+  if (items <= 0 || items > kMaxItems || !values || !rhs || !x || !info)
+    return Status::kInvalidArgument;
+  for (int i = 0; i < items; ++i)
+    info[i] = fg_linear_info{ToInt(Status::kInvalidArgument), 0, std::numeric_limits<double>::infinity()};
+  if (!(tolerance > 0.0) || !(tolerance < 1.0) || !std::isfinite(tolerance) || max_iterations < 0)
+    return Status::kOk;
+  const bool shared = values_per_item == 0;
+  if (!shared && values_per_item != host_.nnz)
+    return Status::kInvalidArgument;
+  const int kp = PadItems(items);
+  Status s = EnsureWorkspace(kp);
+  if (s != Status::kOk)
+    return s;
+  const size_t n = host_.n, n_pad = host_.n_pad, nnz = host_.nnz;
+  const int op_items = shared ? 1 : items;
+  if ((s = staging_.upload(values, op_items * nnz)) != Status::kOk)
+    return s;
+  // Diagonal, inverse (BuildJacobiInverseDiagonal, options.cpp:176-199) and rhs, interleaved.
+  const int dk = shared ? 1 : kp;
+  std::vector<double> d(n_pad * dk, 1.0), inv(n_pad * dk, 0.0), b(n_pad * kp, 0.0);
+  bool usable = true;
+  for (int i = 0; i < op_items; ++i)
+    for (size_t r = 0; r < n; ++r) {
+      const double v = values[i * nnz + host_.diag_slot[r]];
+      d[r * dk + i] = v;
+      const double iv = 1.0 / v;
+      if (!std::isfinite(v) || !(v > 0.0) || !std::isnormal(iv)) {
+        usable = false;
+        inv[r * dk + i] = 0.0;
+      } else {
+        inv[r * dk + i] = iv;
+      }
+    }
+  for (int i = 0; i < items; ++i)
+    for (size_t r = 0; r < n; ++r)
+      b[r * kp + i] = rhs[i * n + r];
+  if ((s = diag_.upload(d.data(), d.size())) != Status::kOk ||
+      (s = invd_.upload(inv.data(), inv.size())) != Status::kOk ||
+      (s = rhs_.upload(b.data(), b.size())) != Status::kOk)
+    return s;
+  const int vk = shared ? 1 : kp;
+  if (LaunchScatterCsr(dev_, vk, op_items, staging_.get(), shared ? 0 : static_cast<int>(nnz), values_.get(), nullptr) != cudaSuccess)
+    return Status::kInternalError;
+  const uint32_t mask = items >= 32 ? 0xffffffffu : ((1u << items) - 1u);
+  s = RunPcg(kp, items, mask, tolerance, max_iterations, vk, shared ? 0 : 1, dk, shared ? 0 : 1,
+             usable ? 1 : 0, nullptr);
+  if (s != Status::kOk)
+    return s;
+  std::vector<double> xi(n_pad * kp), pinfo(3 * kp);
+  int32_t err = 0;
+  if (cudaMemcpy(xi.data(), x_.get(), xi.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(pinfo.data(), pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return Status::kInternalError;
+  if (err)
+    return Status::kInternalError;
+  for (int i = 0; i < items; ++i) {
+    info[i].status = static_cast<int32_t>(pinfo[3 * i]);
+    info[i].iterations = static_cast<int32_t>(pinfo[3 * i + 1]);
+    info[i].residual_l2 = pinfo[3 * i + 2];
+    for (size_t r = 0; r < n; ++r)
+      x[i * n + r] = xi[r * kp + i];
+  }
+  return Status::kOk;
+}
+
+} // namespace fg

@@ -1,0 +1,83 @@
+// solver.h -- the plan object behind the C ABI: device-resident model, workspace and
+// the batched Newton driver (the role of NonlinearP1Solver + DeviceNonlinearAssemblyPlan
+// + GpuCsrSolver in gpu_solver/src/solvers/nonlinear_solver.cuh:32-85).
+#pragma once
+
+#include "femm_gpu.h"
+#include "common.h"
+#include "kernels.cuh"
+#include "model.h"
+
+#include <vector>
+
+namespace fg
+{
+
+struct SolveRequest {
+  int items = 0;
+  const double *currents = nullptr; // device [items * C]
+  const double *hc_scale = nullptr; // device [items] or null
+  const double *warm = nullptr;     // device [items * N] or null
+  fg_solve_options options{};
+  double *a_out = nullptr, *b1_out = nullptr, *b2_out = nullptr, *flux_out = nullptr; // device
+  fg_item_info *info = nullptr;                                                        // host
+  cudaStream_t stream = nullptr;
+};
+
+class Plan
+{
+public:
+  Status Create(HostModel model, const fg_plan_options &options);
+  Status SolveDevice(const SolveRequest &request);
+  Status SolveHost(int items, const double *currents, const double *hc_scale, const double *warm,
+                   const fg_solve_options &options, double *a_out, double *b1_out,
+                   double *b2_out, double *flux_out, fg_item_info *info);
+  Status Assemble(int items, const double *states, const double *currents,
+                  const int32_t *use_newton, double *values, double *diagonal, double *rhs);
+  Status PcgSolve(int items, const double *values, int values_per_item, const double *rhs,
+                  double tolerance, int max_iterations, double *x, fg_linear_info *info);
+
+  const HostPlan &host() const { return host_; }
+  const fg_timing &timing() const { return timing_; }
+  size_t DeviceBytes() const;
+
+private:
+  Status Upload();
+  Status EnsureWorkspace(int kp);
+  Status SolveChunk(const SolveRequest &request, int first, int count);
+  Status RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
+                int value_stride, int value_item, int diag_stride, int diag_item, int use_inverse,
+                cudaStream_t stream);
+
+  HostModel model_;
+  HostPlan host_;
+  fg_plan_options options_{};
+  DevicePlan dev_{};
+  fg_timing timing_{};
+  int kp_cap_ = 0;
+  bool host_only_ = false;
+  int pcg_grid_cap_ = 0;
+
+  // Plan constants on the device.
+  DeviceArray<int32_t> row_offsets_, columns_, row_len_, slice_off_, sell_col_, contrib_off_,
+      contrib_, rhs_off_, rhs_contrib_, elem_nodes_, elem_mat_, mat_curve_off_, mat_curve_cnt_,
+      mat_circuit_, node_to_free_, circuit_elem_off_, circuit_elems_;
+  DeviceArray<int8_t> node_sign_;
+  DeviceArray<double> pm_rhs_, circuit_rhs_, elem_geo_, mat_nu0_, mat_alpha_, mat_cold_, mat_jpa_,
+      curve_b_, curve_h_, curve_slope_, boundary_;
+  // Batch workspace.
+  DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, p1_, q_;
+  DeviceArray<double> norm_partials_, norms_, pcg_partials_, pcg_info_, staging_;
+  DeviceArray<unsigned> barrier_;
+  DeviceArray<int32_t> error_, invalid_;
+  // Host-pointer API staging.
+  DeviceArray<double> in_currents_, in_hc_, in_warm_, out_a_, out_b1_, out_b2_, out_flux_;
+  PinnedArray<double> small_;
+  cudaEvent_t ev_start_ = nullptr, ev_mid_ = nullptr, ev_pcg_ = nullptr, ev_end_ = nullptr;
+};
+
+} // namespace fg
+
+struct fg_plan {
+  fg::Plan plan;
+};

@@ -1,0 +1,332 @@
+"""ctypes binding of libfemmgpu (include/femm_gpu.h).
+
+The library is the product: every call here goes through the C ABI into the sm_100a
+kernels.  There is no CPU fallback -- if the shared library is missing or no GPU is
+visible, the calls fail with an exception or a GPU_UNAVAILABLE status.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+from typing import List, Optional
+
+import numpy as np
+
+from .model import Model
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libfemmgpu.so")
+
+STATUS_NAMES = [
+    "OK", "INPUT_IO", "INVALID_ARGUMENT", "UNSUPPORTED_FEATURE", "MESH_INVALID",
+    "BOUNDARY_INVALID", "GPU_UNAVAILABLE", "GPU_ALLOCATION_FAILED", "ASSEMBLY_FAILED",
+    "LINEAR_SOLVE_NOT_CONVERGED", "LINEAR_SOLVE_BREAKDOWN", "NUMERICAL_NONFINITE", "OUTPUT_IO",
+    "INTERNAL_ERROR", "NONLINEAR_SOLVE_NOT_CONVERGED", "INVALID_MATERIAL",
+]
+(OK, INPUT_IO, INVALID_ARGUMENT, UNSUPPORTED_FEATURE, MESH_INVALID, BOUNDARY_INVALID,
+ GPU_UNAVAILABLE, GPU_ALLOCATION_FAILED, ASSEMBLY_FAILED, LINEAR_SOLVE_NOT_CONVERGED,
+ LINEAR_SOLVE_BREAKDOWN, NUMERICAL_NONFINITE, OUTPUT_IO, INTERNAL_ERROR,
+ NONLINEAR_SOLVE_NOT_CONVERGED, INVALID_MATERIAL) = range(16)
+
+EXPORTED = [
+    "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
+    "fg_plan_destroy", "fg_plan_sizes_get", "fg_plan_symbolic", "fg_assemble", "fg_pcg_solve",
+    "fg_csr_pcg", "fg_solve_batch", "fg_solve_batch_device", "fg_plan_last_timing",
+    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors",
+]
+
+
+class FgMaterial(C.Structure):
+    _fields_ = [("reluctivity_zero_m_per_h", C.c_double), ("alpha_per_t2", C.c_double),
+                ("source_j_per_a", C.c_double), ("h_c_a_per_m", C.c_double),
+                ("magnetization_deg", C.c_double), ("bh_curve_index", C.c_int32),
+                ("circuit_index", C.c_int32), ("group_number", C.c_int32), ("reserved", C.c_int32)]
+
+
+class FgCurve(C.Structure):
+    _fields_ = [("count", C.c_int32), ("b_t", C.c_void_p), ("h_a_per_m", C.c_void_p)]
+
+
+class FgModel(C.Structure):
+    _fields_ = [
+        ("problem_type", C.c_int32), ("node_count", C.c_int32), ("node_xy", C.c_void_p),
+        ("triangle_count", C.c_int32), ("triangle_nodes", C.c_void_p),
+        ("triangle_material", C.c_void_p), ("material_count", C.c_int32),
+        ("materials", C.c_void_p), ("curve_count", C.c_int32), ("curves", C.c_void_p),
+        ("dirichlet_count", C.c_int32), ("dirichlet_nodes", C.c_void_p),
+        ("dirichlet_values", C.c_void_p), ("constraint_count", C.c_int32),
+        ("constraint_nodes", C.c_void_p), ("constraint_signs", C.c_void_p),
+        ("circuit_count", C.c_int32), ("depth_m", C.c_double),
+    ]
+
+
+class FgPlanOptions(C.Structure):
+    _fields_ = [("preconditioner", C.c_int32), ("block_size", C.c_int32),
+                ("precision", C.c_int32), ("reserved", C.c_int32)]
+
+
+class FgSolveOptions(C.Structure):
+    _fields_ = [("relative_tolerance", C.c_double), ("max_newton_iterations", C.c_int32),
+                ("max_linear_iterations", C.c_int32), ("linear_relative_tolerance", C.c_double),
+                ("recover_nonconvergence", C.c_int32), ("adaptive_linear_tolerance", C.c_int32)]
+
+
+class FgItemInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("residual_l2", C.c_double),
+                ("linear_iterations", C.c_int32), ("reserved", C.c_int32),
+                ("last_linear_tolerance", C.c_double),
+                ("verified_equation_residual_relative", C.c_double)]
+
+
+class FgLinearInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("residual_l2", C.c_double)]
+
+
+class FgPlanSizes(C.Structure):
+    _fields_ = [("node_count", C.c_int64), ("triangle_count", C.c_int64), ("rows", C.c_int64),
+                ("nnz", C.c_int64), ("circuit_count", C.c_int32), ("problem_type", C.c_int32),
+                ("device_bytes", C.c_int64), ("matrix_contributors", C.c_int64),
+                ("rhs_contributors", C.c_int64)]
+
+
+class FgTiming(C.Structure):
+    _fields_ = [("assembly_ms", C.c_double), ("pcg_ms", C.c_double), ("update_ms", C.c_double),
+                ("finalize_ms", C.c_double), ("newton_iterations", C.c_int64),
+                ("pcg_iterations", C.c_int64), ("kernel_launches", C.c_int64),
+                ("pcg_launches", C.c_int64), ("pcg_grid", C.c_int32), ("pcg_block", C.c_int32)]
+
+
+_LIB = None
+
+
+def build_library():
+    subprocess.run(["make", "-s", "-C", PKG_DIR], check=True)
+
+
+def lib():
+    """Loads libfemmgpu.so (building it with nvcc first if it is absent)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            build_library()
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"libfemmgpu.so not found at {LIB_PATH}")
+        _LIB = C.CDLL(LIB_PATH)
+        _LIB.fg_status_name.restype = C.c_char_p
+    return _LIB
+
+
+def status_name(status: int) -> str:
+    return lib().fg_status_name(int(status)).decode()
+
+
+def production_options(**overrides) -> FgSolveOptions:
+    o = FgSolveOptions()
+    lib().fg_production_options(C.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class FgError(RuntimeError):
+    def __init__(self, status, what=""):
+        super().__init__(f"{what}: {STATUS_NAMES[status] if 0 <= status < 16 else status}")
+        self.status = status
+
+
+@dataclass
+class SolveResult:
+    a: np.ndarray  # [k, N]
+    b1: np.ndarray  # [k, E]
+    b2: np.ndarray  # [k, E]
+    flux: np.ndarray  # [k, C]
+    info: List[FgItemInfo]
+
+    @property
+    def status(self):
+        return [i.status for i in self.info]
+
+
+class Plan:
+    """A device-resident model: fg_plan_create ... fg_plan_destroy."""
+
+    def __init__(self, model: Model, preconditioner: int = 0, block_size: int = 8,
+                 precision: int = 0, host_only: bool = False):
+        self.model = model
+        L = lib()
+        self._keep = []
+        mats = (FgMaterial * model.mat_count)()
+        for i in range(model.mat_count):
+            mats[i] = FgMaterial(model.nu0[i], model.alpha[i], model.j_per_a[i], model.hc[i],
+                                 model.mag_deg[i], int(model.curve_index[i]),
+                                 int(model.circuit_index[i]), int(model.group[i]), 0)
+        curves = (FgCurve * max(1, len(model.curves)))()
+        for i, (b, h) in enumerate(model.curves):
+            curves[i] = FgCurve(len(b), _p(b), _p(h))
+        con = np.ascontiguousarray(np.stack([model.con_a, model.con_b], axis=1).ravel(), np.int32) \
+            if model.con_a.size else np.zeros(2, np.int32)
+        self._keep += [mats, curves, con]
+        fm = FgModel(
+            problem_type=model.problem_type, node_count=model.node_count, node_xy=_p(model.xy),
+            triangle_count=model.tri_count, triangle_nodes=_p(model.tri),
+            triangle_material=_p(model.tri_mat), material_count=model.mat_count,
+            materials=C.cast(mats, C.c_void_p), curve_count=len(model.curves),
+            curves=C.cast(curves, C.c_void_p), dirichlet_count=int(model.dir_nodes.size),
+            dirichlet_nodes=_p(model.dir_nodes), dirichlet_values=_p(model.dir_values),
+            constraint_count=int(model.con_a.size), constraint_nodes=_p(con),
+            constraint_signs=_p(model.con_sign), circuit_count=model.circuit_count,
+            depth_m=model.depth_m)
+        opts = FgPlanOptions(preconditioner, block_size, precision, 1 if host_only else 0)
+        self._h = C.c_void_p()
+        status = L.fg_plan_create(C.byref(fm), C.byref(opts), C.byref(self._h))
+        if status != 0:
+            self._h = None
+            raise FgError(status, "fg_plan_create")
+        s = FgPlanSizes()
+        L.fg_plan_sizes_get(self._h, C.byref(s))
+        self.N, self.E, self.rows, self.nnz, self.C = (int(s.node_count), int(s.triangle_count),
+                                                       int(s.rows), int(s.nnz), int(s.circuit_count))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sizes(self) -> FgPlanSizes:
+        s = FgPlanSizes()
+        lib().fg_plan_sizes_get(self._h, C.byref(s))
+        return s
+
+    def symbolic(self):
+        ro = np.zeros(self.rows + 1, np.int32)
+        col = np.zeros(self.nnz, np.int32)
+        n2f = np.zeros(self.N, np.int32)
+        sign = np.zeros(self.N, np.int8)
+        bnd = np.zeros(self.N)
+        lib().fg_plan_symbolic(self._h, _p(ro), _p(col), _p(n2f), _p(sign), _p(bnd))
+        return ro, col, n2f, sign, bnd
+
+    def contributors(self):
+        """Per-slot and per-row element contributor lists and the fixed PM / coil loads."""
+        s = self.sizes()
+        so = np.zeros(self.nnz + 1, np.int32)
+        se = np.zeros((int(s.matrix_contributors), 3), np.int32)
+        ro = np.zeros(self.rows + 1, np.int32)
+        re = np.zeros((int(s.rhs_contributors), 3), np.int32)
+        pm = np.zeros(self.rows)
+        cr = np.zeros(max(self.C, 1) * self.rows)
+        lib().fg_plan_contributors(self._h, _p(so), _p(se), _p(ro), _p(re), _p(pm), _p(cr))
+        return so, se, ro, re, pm, cr[: self.C * self.rows].reshape(self.C, self.rows)
+
+    def assemble(self, states, currents, use_newton):
+        states = np.ascontiguousarray(np.atleast_2d(states), np.float64)
+        k = states.shape[0]
+        currents = np.ascontiguousarray(np.atleast_2d(currents), np.float64).reshape(k, -1)
+        un = np.ascontiguousarray(np.broadcast_to(np.asarray(use_newton, np.int32), (k,)))
+        vals = np.zeros((k, self.nnz))
+        diag = np.zeros((k, self.rows))
+        rhs = np.zeros((k, self.rows))
+        status = lib().fg_assemble(self._h, C.c_int32(k), _p(states), _p(currents), _p(un),
+                                   _p(vals), _p(diag), _p(rhs))
+        if status != 0:
+            raise FgError(status, "fg_assemble")
+        return vals, diag, rhs
+
+    def pcg(self, values, rhs, tol=1e-10, maxit=16384, shared=False):
+        rhs = np.ascontiguousarray(np.atleast_2d(rhs), np.float64)
+        k = rhs.shape[0]
+        values = np.ascontiguousarray(values, np.float64)
+        x = np.zeros((k, self.rows))
+        info = (FgLinearInfo * k)()
+        status = lib().fg_pcg_solve(self._h, C.c_int32(k), _p(values),
+                                    C.c_int32(0 if shared else self.nnz), _p(rhs), C.c_double(tol),
+                                    C.c_int32(maxit), _p(x), info)
+        if status != 0:
+            raise FgError(status, "fg_pcg_solve")
+        return x, [info[i] for i in range(k)]
+
+    def solve(self, currents, hc_scale=None, warm=None, options: Optional[FgSolveOptions] = None,
+              outputs=True) -> SolveResult:
+        currents = np.ascontiguousarray(np.atleast_2d(np.asarray(currents, np.float64)))
+        k = currents.shape[0]
+        currents = currents.reshape(k, self.C) if self.C else currents
+        hc = None if hc_scale is None else np.ascontiguousarray(hc_scale, np.float64)
+        wm = None if warm is None else np.ascontiguousarray(warm, np.float64).reshape(k, self.N)
+        opts = options if options is not None else production_options()
+        a = np.zeros((k, self.N)) if outputs else None
+        b1 = np.zeros((k, self.E)) if outputs else None
+        b2 = np.zeros((k, self.E)) if outputs else None
+        flux = np.zeros((k, max(self.C, 1))) if outputs else None
+        info = (FgItemInfo * k)()
+        status = lib().fg_solve_batch(self._h, C.c_int32(k), _p(currents), _p(hc), _p(wm),
+                                      C.byref(opts), _p(a), _p(b1), _p(b2), _p(flux), info)
+        if status != 0:
+            raise FgError(status, "fg_solve_batch")
+        return SolveResult(a, b1, b2, None if flux is None else flux[:, : self.C],
+                           [info[i] for i in range(k)])
+
+    def solve_device(self, items, currents_ptr, options=None, hc_ptr=None, warm_ptr=None,
+                     a_ptr=None, b1_ptr=None, b2_ptr=None, flux_ptr=None, stream=None):
+        """Device-pointer entry (fg_solve_batch_device); pointers are integers (e.g. torch data_ptr())."""
+        opts = options if options is not None else production_options()
+        info = (FgItemInfo * items)()
+        vp = lambda v: C.c_void_p(v) if v else None  # noqa: E731
+        status = lib().fg_solve_batch_device(self._h, C.c_int32(items), vp(currents_ptr), vp(hc_ptr),
+                                             vp(warm_ptr), C.byref(opts), vp(a_ptr), vp(b1_ptr),
+                                             vp(b2_ptr), vp(flux_ptr), info, vp(stream))
+        if status != 0:
+            raise FgError(status, "fg_solve_batch_device")
+        return [info[i] for i in range(items)]
+
+    def last_timing(self) -> FgTiming:
+        t = FgTiming()
+        lib().fg_plan_last_timing(self._h, C.byref(t))
+        return t
+
+
+def csr_pcg(row_offsets, columns, values, diagonal, rhs, tol=1e-13, maxit=64, shared=False):
+    """fg_csr_pcg on an arbitrary CSR operator (values [k, nnz] or shared [nnz])."""
+    ro = np.ascontiguousarray(row_offsets, np.int32)
+    col = np.ascontiguousarray(columns, np.int32)
+    rhs = np.ascontiguousarray(np.atleast_2d(rhs), np.float64)
+    k, n = rhs.shape
+    vals = np.ascontiguousarray(values, np.float64)
+    diag = np.ascontiguousarray(diagonal, np.float64)
+    x = np.zeros((k, n))
+    info = (FgLinearInfo * k)()
+    status = lib().fg_csr_pcg(C.c_int32(n), _p(ro), _p(col), _p(vals),
+                              C.c_int32(0 if shared else int(ro[-1])), _p(diag), C.c_int32(k),
+                              _p(rhs), C.c_double(tol), C.c_int32(maxit), _p(x), info)
+    if status != 0:
+        raise FgError(status, "fg_csr_pcg")
+    return x, [info[i] for i in range(k)]
+
+
+def bh_build(b, h):
+    b = np.array(b, np.float64)
+    h = np.array(h, np.float64)
+    slope = np.zeros_like(b)
+    cold = C.c_double(0.0)
+    passes = C.c_int32(0)
+    if not lib().fg_bh_build(C.c_int32(b.size), _p(b), _p(h), _p(slope), C.byref(cold),
+                             C.byref(passes)):
+        raise ValueError("invalid B-H curve")
+    return b, h, slope, cold.value, passes.value
+
+
+def bh_eval(b, h, slope, field_b):
+    out = np.zeros(4)
+    lib().fg_bh_eval(C.c_int32(b.size), _p(b), _p(h), _p(slope), C.c_double(field_b), _p(out))
+    return out

@@ -1,0 +1,230 @@
+"""Seeded synthetic meshes for the benchmark workloads.
+
+Each generator is deterministic in its arguments.  The workloads are:
+
+* ``square_linear(m)`` -- plain linear planar solve: 0.1 m square, m x m quads split
+  along the lower-left -> upper-right diagonal, a centred 0.04 m iron block with
+  mu_r = 1000, two 0.01 x 0.03 m coil slabs driven at J = +/-1e6 A/m^2 by one
+  series circuit at 10 A, air elsewhere, A = 0 on the outer boundary.  m = 64 gives
+  4,225 nodes / 8,192 triangles.
+* ``square_nonlinear(m, seed)`` -- the same layout with interior nodes jittered by
+  U(+/-0.3 h), the iron on a 24-point B-H table sampled from B = 2 H / (200 + H)
+  (H = 0 and 23 log-spaced points in [10, 2e5] A/m), a 0.005 m NdFe-like magnet
+  strip (mu_r = 1.05, Hc = 9e5 A/m, seeded angle) and three series circuits.
+  m = 500 gives 251,001 nodes / 500,000 triangles; m = 1414 gives 2,002,225 nodes.
+* ``axisymmetric_plunger(mr, mz)`` -- r-z solenoid plunger: r in [0, 0.05],
+  z in [-0.05, 0.05], iron plunger r < 0.01 on the same B-H table, two coils in
+  r in [0.015, 0.025], A = 0 on the axis and outer boundary.
+
+Jittered meshes can invert a few triangles (about 10 in 500,000 at 0.3 h).  The
+generator repairs them deterministically: nodes of any triangle whose area falls
+below 5 % of the undistorted area get their jitter halved, repeatedly, until every
+triangle is well shaped.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .model import AXISYMMETRIC, MU0, PLANAR, Model
+
+SIDE_M = 0.1
+
+
+def bh_table_saturating(points: int = 24):
+    """B = 2 H / (200 + H): H = 0 plus (points - 1) log-spaced values in [10, 2e5] A/m."""
+    h = np.concatenate([[0.0], np.logspace(1.0, np.log10(2.0e5), points - 1)])
+    b = 2.0 * h / (200.0 + h)
+    return b, h
+
+
+def _structured(m: int, width: float, height: float, x0: float = 0.0, y0: float = 0.0):
+    nx, ny = m if isinstance(m, tuple) else (m, m)
+    xs = x0 + np.linspace(0.0, width, nx + 1)
+    ys = y0 + np.linspace(0.0, height, ny + 1)
+    X, Y = np.meshgrid(xs, ys)  # row = y, column = x -> node = j * (nx + 1) + i
+    xy = np.stack([X.ravel(), Y.ravel()], axis=1)
+    j, i = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    ll = (j * (nx + 1) + i).ravel()
+    lr = ll + 1
+    ul = ll + (nx + 1)
+    ur = ul + 1
+    tri = np.empty((2 * ll.size, 3), dtype=np.int64)
+    tri[0::2] = np.stack([ll, lr, ur], axis=1)
+    tri[1::2] = np.stack([ll, ur, ul], axis=1)
+    return xy, tri.astype(np.int32), nx, ny
+
+
+def _signed_area2(xy, tri):
+    p0, p1, p2 = xy[tri[:, 0]], xy[tri[:, 1]], xy[tri[:, 2]]
+    return (p1[:, 0] - p0[:, 0]) * (p2[:, 1] - p0[:, 1]) - (p2[:, 0] - p0[:, 0]) * (p1[:, 1] - p0[:, 1])
+
+
+def _jitter(xy, tri, nx, ny, hx, hy, seed, fraction=0.3):
+    rng = np.random.default_rng(seed)
+    jit = rng.uniform(-fraction, fraction, size=xy.shape) * np.array([hx, hy])
+    idx = np.arange(xy.shape[0])
+    i = idx % (nx + 1)
+    j = idx // (nx + 1)
+    interior = (i > 0) & (i < nx) & (j > 0) & (j < ny)
+    jit[~interior] = 0.0
+    base = _signed_area2(xy, tri)
+    for _ in range(64):
+        moved = xy + jit
+        area = _signed_area2(moved, tri)
+        bad = area < 0.05 * base
+        if not bad.any():
+            return moved
+        nodes = np.unique(tri[bad].ravel())
+        jit[nodes] *= 0.5
+    raise RuntimeError("jitter repair did not converge")
+
+
+def _centroids(xy, tri):
+    return xy[tri].mean(axis=1)
+
+
+def _in_box(c, x0, x1, y0, y1):
+    return (c[:, 0] >= x0) & (c[:, 0] <= x1) & (c[:, 1] >= y0) & (c[:, 1] <= y1)
+
+
+def _boundary_nodes(nx, ny):
+    idx = np.arange((nx + 1) * (ny + 1))
+    i = idx % (nx + 1)
+    j = idx // (nx + 1)
+    return idx[(i == 0) | (i == nx) | (j == 0) | (j == ny)].astype(np.int32)
+
+
+def square_linear(m: int = 64, current_a: float = 10.0) -> Model:
+    """Linear planar workload; the circuit current is ``current_a`` (J = +/-1e6 at 10 A)."""
+    xy, tri, nx, ny = _structured(m, SIDE_M, SIDE_M)
+    c = _centroids(xy, tri)
+    mat = np.zeros(tri.shape[0], np.int32)  # 0 air
+    mat[_in_box(c, 0.03, 0.07, 0.03, 0.07)] = 1  # iron
+    mat[_in_box(c, 0.015, 0.025, 0.035, 0.065)] = 2  # coil +
+    mat[_in_box(c, 0.075, 0.085, 0.035, 0.065)] = 3  # coil -
+    jpa = 1.0e6 / current_a
+    nu_air = 1.0 / MU0
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air / 1000.0, nu_air, nu_air],
+        alpha=[0.0, 0.0, 0.0, 0.0],
+        j_per_a=[0.0, 0.0, jpa, -jpa],
+        hc=[0.0, 0.0, 0.0, 0.0],
+        mag_deg=[0.0, 0.0, 0.0, 0.0],
+        curve_index=[-1, -1, -1, -1],
+        circuit_index=[-1, -1, 0, 0],
+        group=[0, 1, 2, 3],
+        curves=[],
+        dir_nodes=_boundary_nodes(nx, ny),
+        dir_values=np.zeros(_boundary_nodes(nx, ny).size),
+        circuit_count=1,
+        depth_m=1.0,
+        problem_type=PLANAR,
+        name=f"square_linear_m{m}",
+    )
+
+
+def square_nonlinear(m: int = 500, seed: int = 2, magnet_deg: float | None = None,
+                     jitter: float = 0.3) -> Model:
+    """Nonlinear planar workload (iron B-H, PM strip, three series circuits)."""
+    xy, tri, nx, ny = _structured(m, SIDE_M, SIDE_M)
+    h = SIDE_M / m
+    rng = np.random.default_rng(seed)
+    if jitter > 0.0:
+        xy = _jitter(xy, tri, nx, ny, h, h, seed, jitter)
+    if magnet_deg is None:
+        magnet_deg = float(rng.uniform(0.0, 360.0))
+    c = _centroids(xy, tri)
+    mat = np.zeros(tri.shape[0], np.int32)  # 0 air
+    mat[_in_box(c, 0.03, 0.07, 0.03, 0.07)] = 1  # iron (B-H)
+    mat[_in_box(c, 0.03, 0.07, 0.0175, 0.0225)] = 2  # magnet strip, 5 mm
+    mat[_in_box(c, 0.015, 0.025, 0.035, 0.065)] = 3  # circuit 0
+    mat[_in_box(c, 0.075, 0.085, 0.035, 0.065)] = 4  # circuit 1
+    mat[_in_box(c, 0.035, 0.065, 0.075, 0.085)] = 5  # circuit 2
+    nu_air = 1.0 / MU0
+    jpa = 1.0e6 / 20.0  # 1e6 A/m^2 at the 20 A extreme of the current range
+    b, hh = bh_table_saturating(24)
+    bnd = _boundary_nodes(nx, ny)
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air / 1000.0, nu_air / 1.05, nu_air, nu_air, nu_air],
+        alpha=np.zeros(6),
+        j_per_a=[0.0, 0.0, 0.0, jpa, jpa, jpa],
+        hc=[0.0, 0.0, 9.0e5, 0.0, 0.0, 0.0],
+        mag_deg=[0.0, 0.0, magnet_deg, 0.0, 0.0, 0.0],
+        curve_index=[-1, 0, -1, -1, -1, -1],
+        circuit_index=[-1, -1, -1, 0, 1, 2],
+        group=[0, 1, 2, 3, 4, 5],
+        curves=[(b, hh)],
+        dir_nodes=bnd,
+        dir_values=np.zeros(bnd.size),
+        circuit_count=3,
+        depth_m=1.0,
+        problem_type=PLANAR,
+        name=f"square_nonlinear_m{m}_s{seed}",
+    )
+
+
+def seeded_currents(items: int, circuits: int, limit: float, seed: int) -> np.ndarray:
+    """Circuit currents uniform in [-limit, limit] A, shape [items, circuits]."""
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-limit, limit, size=(items, circuits))
+
+
+def axisymmetric_plunger(mr: int = 223, mz: int = 446) -> Model:
+    """Axisymmetric solenoid plunger (r = x, z = y); about 100k nodes at the defaults."""
+    xy, tri, nx, ny = _structured((mr, mz), 0.05, 0.1, 0.0, -0.05)
+    c = _centroids(xy, tri)
+    mat = np.zeros(tri.shape[0], np.int32)
+    mat[c[:, 0] < 0.01] = 1  # plunger
+    mat[_in_box(c, 0.015, 0.025, 0.005, 0.03)] = 2  # coil 0
+    mat[_in_box(c, 0.015, 0.025, -0.03, -0.005)] = 3  # coil 1
+    nu_air = 1.0 / MU0
+    jpa = 1.0e6 / 30.0
+    b, hh = bh_table_saturating(24)
+    bnd = _boundary_nodes(nx, ny)
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air / 1000.0, nu_air, nu_air],
+        alpha=np.zeros(4),
+        j_per_a=[0.0, 0.0, jpa, jpa],
+        hc=np.zeros(4),
+        mag_deg=np.zeros(4),
+        curve_index=[-1, 0, -1, -1],
+        circuit_index=[-1, -1, 0, 1],
+        group=[0, 1, 2, 3],
+        curves=[(b, hh)],
+        dir_nodes=bnd,
+        dir_values=np.zeros(bnd.size),
+        circuit_count=2,
+        depth_m=1.0,
+        problem_type=AXISYMMETRIC,
+        name=f"axisymmetric_plunger_{mr}x{mz}",
+    )
+
+
+def periodic_strip(m: int = 16, antiperiodic: bool = False, current_a: float = 12.0) -> Model:
+    """Square strip with periodic (or anti-periodic) left/right edges and A = 0 top/bottom."""
+    xy, tri, nx, ny = _structured(m, 0.01, 0.01)
+    c = _centroids(xy, tri)
+    mat = np.zeros(tri.shape[0], np.int32)
+    coil = _in_box(c, 0.003, 0.007, 0.003, 0.007)
+    mat[coil] = 1
+    area = 0.5 * _signed_area2(xy, tri)[coil].sum()
+    idx = np.arange(xy.shape[0])
+    i = idx % (nx + 1)
+    j = idx // (nx + 1)
+    bnd = idx[(j == 0) | (j == ny)].astype(np.int32)
+    left = idx[(i == 0) & (j > 0) & (j < ny)]
+    right = idx[(i == nx) & (j > 0) & (j < ny)]
+    nu_air = 1.0 / MU0
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air], alpha=[0.0, 0.0], j_per_a=[0.0, 1.0 / area], hc=[0.0, 0.0],
+        mag_deg=[0.0, 0.0], curve_index=[-1, -1], circuit_index=[-1, 0], group=[0, 1], curves=[],
+        dir_nodes=bnd, dir_values=np.zeros(bnd.size),
+        con_a=left, con_b=right,
+        con_sign=np.full(left.size, -1 if antiperiodic else 1, np.int8),
+        circuit_count=1, depth_m=0.01, problem_type=PLANAR,
+        name=f"{'anti' if antiperiodic else ''}periodic_strip_m{m}",
+    )

@@ -1,0 +1,239 @@
+/*
+ * femm_gpu.h -- C ABI of libfemmgpu, the B200 (sm_100a) nonlinear magnetostatic solver.
+ *
+ * The library replaces FEMM-GPU's in-process solver seam for the nonlinear DC
+ * magnetostatic path: P1 Newton assembly with B-H reluctivity, permanent-magnet
+ * and series-circuit loads, signed periodic/anti-periodic folding, the batched
+ * deterministic PCG, and B / flux-linkage recovery.  Plain pointers and sizes
+ * only; every call returns a status code with the numbering of the reference's
+ * gpu_femm::Status (gpu_solver/src/core/types.h:11-28).  Errors never cross the
+ * boundary as exceptions; a failing batch item never poisons the others.
+ *
+ * Threading: one thread owns a plan; calls are synchronous on return unless the
+ * name ends in _device, in which case work is ordered on the given CUDA stream.
+ */
+#ifndef FEMM_GPU_H
+#define FEMM_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FG_ABI_VERSION 1
+
+/* Status codes (gpu_solver/src/core/types.h:11-28). */
+enum {
+  FG_OK = 0,
+  FG_INPUT_IO = 1,
+  FG_INVALID_ARGUMENT = 2,
+  FG_UNSUPPORTED_FEATURE = 3,
+  FG_MESH_INVALID = 4,
+  FG_BOUNDARY_INVALID = 5,
+  FG_GPU_UNAVAILABLE = 6,
+  FG_GPU_ALLOCATION_FAILED = 7,
+  FG_ASSEMBLY_FAILED = 8,
+  FG_LINEAR_SOLVE_NOT_CONVERGED = 9,
+  FG_LINEAR_SOLVE_BREAKDOWN = 10,
+  FG_NUMERICAL_NONFINITE = 11,
+  FG_OUTPUT_IO = 12,
+  FG_INTERNAL_ERROR = 13,
+  FG_NONLINEAR_SOLVE_NOT_CONVERGED = 14,
+  FG_INVALID_MATERIAL = 15
+};
+
+enum { FG_PLANAR = 0, FG_AXISYMMETRIC = 1 };
+enum { FG_PRECOND_JACOBI = 0, FG_PRECOND_BLOCK_JACOBI = 1 };
+enum { FG_PRECISION_FP64 = 0, FG_PRECISION_MIXED = 1 };
+
+/* One material label (gpu_solver/src/physics/nonlinear_model.h:38-51). */
+typedef struct fg_material {
+  double reluctivity_zero_m_per_h; /* nu0 = 1 / (mu0 mu_r) */
+  double alpha_per_t2;             /* nu = nu0 (1 + alpha |B|^2) when no B-H curve */
+  double source_j_per_a;           /* coil current density per circuit amp, A/m^2 */
+  double h_c_a_per_m;              /* permanent-magnet coercivity */
+  double magnetization_deg;        /* permanent-magnet direction */
+  int32_t bh_curve_index;          /* -1: no B-H curve */
+  int32_t circuit_index;           /* -1: not driven */
+  int32_t group_number;
+  int32_t reserved;
+} fg_material;
+
+/* Raw B-H points, origin first; the library builds FEMM's DC spline from them
+ * (gpu_solver/src/physics/nonlinear_model.cpp:13-113). */
+typedef struct fg_bh_curve {
+  int32_t count;
+  const double *b_t;
+  const double *h_a_per_m;
+} fg_bh_curve;
+
+/* The model (NonlinearModel, gpu_solver/src/physics/nonlinear_model.h:83-100). */
+typedef struct fg_model {
+  int32_t problem_type; /* FG_PLANAR or FG_AXISYMMETRIC (x = r, y = z) */
+  int32_t node_count;
+  const double *node_xy; /* [2 * node_count] metres, interleaved */
+  int32_t triangle_count;
+  const int32_t *triangle_nodes;    /* [3 * triangle_count], counter-clockwise */
+  const int32_t *triangle_material; /* [triangle_count] */
+  int32_t material_count;
+  const fg_material *materials;
+  int32_t curve_count;
+  const fg_bh_curve *curves;
+  int32_t dirichlet_count;
+  const int32_t *dirichlet_nodes;
+  const double *dirichlet_values;
+  int32_t constraint_count;
+  const int32_t *constraint_nodes; /* [2 * constraint_count]: A(b) = sign * A(a) */
+  const int8_t *constraint_signs;  /* [constraint_count], +1 periodic / -1 anti-periodic */
+  int32_t circuit_count;
+  double depth_m;
+} fg_model;
+
+typedef struct fg_plan_options {
+  int32_t preconditioner; /* FG_PRECOND_* */
+  int32_t block_size;     /* block-Jacobi rows per block: 8 or 32 */
+  int32_t precision;      /* FG_PRECISION_*: mixed = FP32 inner PCG in FP64 defect correction */
+  int32_t flags;          /* FG_PLAN_HOST_ONLY: build and validate the host topology only */
+} fg_plan_options;
+
+/* fg_plan_options.flags: a host-only plan needs no GPU; it answers the topology and
+ * introspection calls, and every device call on it returns FG_GPU_UNAVAILABLE. */
+enum { FG_PLAN_HOST_ONLY = 1 };
+
+/* NonlinearOptions (gpu_solver/src/physics/nonlinear_model.h:102-109). */
+typedef struct fg_solve_options {
+  double relative_tolerance;
+  int32_t max_newton_iterations;
+  int32_t max_linear_iterations;
+  double linear_relative_tolerance;
+  int32_t recover_nonconvergence;
+  int32_t adaptive_linear_tolerance;
+} fg_solve_options;
+
+/* Per-item result summary (NonlinearSolveResult fields, nonlinear_model.h:132-145). */
+typedef struct fg_item_info {
+  int32_t status;
+  int32_t iterations;  /* Newton iterations */
+  double residual_l2;  /* last relative Newton step */
+  int32_t linear_iterations;
+  int32_t reserved;
+  double last_linear_tolerance;
+  double verified_equation_residual_relative;
+} fg_item_info;
+
+/* SolveInfo of one linear solve (gpu_solver/src/core/types.h:51-55). */
+typedef struct fg_linear_info {
+  int32_t status;
+  int32_t iterations;
+  double residual_l2;
+} fg_linear_info;
+
+typedef struct fg_plan_sizes {
+  int64_t node_count;
+  int64_t triangle_count;
+  int64_t rows;  /* free rows after signed folding */
+  int64_t nnz;   /* symbolic CSR entries */
+  int32_t circuit_count;
+  int32_t problem_type;
+  int64_t device_bytes; /* device memory currently held by the plan */
+  int64_t matrix_contributors; /* element terms summed into CSR slots */
+  int64_t rhs_contributors;    /* element terms summed into free rows */
+} fg_plan_sizes;
+
+typedef struct fg_timing {
+  double assembly_ms;
+  double pcg_ms;
+  double update_ms;
+  double finalize_ms;
+  int64_t newton_iterations;
+  int64_t pcg_iterations;   /* summed over the PCG launches (max over items per launch) */
+  int64_t kernel_launches;  /* of this library's kernels */
+  int64_t pcg_launches;
+  int32_t pcg_grid;         /* cooperative CTAs of the last PCG launch */
+  int32_t pcg_block;
+} fg_timing;
+
+typedef struct fg_plan fg_plan;
+
+/* Reference production options: ProductionSampleOptions
+ * (gpu_solver/src/physics/nonlinear_model.cpp:195-205). */
+void fg_production_options(fg_solve_options *options);
+
+const char *fg_status_name(int status);
+int fg_abi_version(void);
+
+/* NonlinearP1Solver::Initialize + device plan set-up (nonlinear_solver.cu:784-800,
+ * nonlinear_assembly.cu:362-441, nonlinear_topology.cpp:12-248). */
+int fg_plan_create(const fg_model *model, const fg_plan_options *options, fg_plan **plan);
+void fg_plan_destroy(fg_plan *plan);
+int fg_plan_sizes_get(const fg_plan *plan, fg_plan_sizes *sizes);
+
+/* Symbolic CSR and signed maps (Assembly fields row_offsets, column_indices,
+ * node_to_free, node_sign, boundary_values; linear_model.h:9-23).  Any pointer may be NULL. */
+int fg_plan_symbolic(const fg_plan *plan, int32_t *row_offsets, int32_t *columns,
+                     int32_t *node_to_free, int8_t *node_sign, double *boundary_values);
+
+/* Gather plan of the device assembly (the per-slot / per-row contributor lists of
+ * PreparedNonlinearAssembly, nonlinear_topology.cpp:87-179 and :234-248), in
+ * element order.  slot_offsets [nnz + 1]; slot_entries [3 * matrix_contributors] as
+ * (triangle, symmetric local pair 0..5 = 00,01,02,11,12,22, sign);
+ * row_offsets [rows + 1]; row_entries [3 * rhs_contributors] as (triangle, local row, sign);
+ * pm_rhs [rows]; circuit_rhs [circuits * rows].  Any pointer may be NULL. */
+int fg_plan_contributors(const fg_plan *plan, int32_t *slot_offsets, int32_t *slot_entries,
+                         int32_t *row_offsets, int32_t *row_entries, double *pm_rhs,
+                         double *circuit_rhs);
+
+/* Device Newton assembly at given nodal states (DeviceNonlinearAssemblyPlan::Assemble,
+ * nonlinear_assembly.cu:229-309).  states [items * N]; currents [items * C];
+ * use_newton [items]; outputs in CSR order: values [items * nnz], diagonal and
+ * rhs [items * rows].  Any output may be NULL. */
+int fg_assemble(fg_plan *plan, int32_t items, const double *states, const double *currents,
+                const int32_t *use_newton, double *values, double *diagonal, double *rhs);
+
+/* Deterministic Jacobi PCG on the plan's CSR pattern (GpuCsrSolver batch modes,
+ * csr_solver.cu:204-503).  values [items * nnz] CSR order (values_per_item = 0
+ * shares one operator), rhs [items * rows] -> x [items * rows]. */
+int fg_pcg_solve(fg_plan *plan, int32_t items, const double *values, int32_t values_per_item,
+                 const double *rhs, double relative_tolerance, int32_t max_iterations, double *x,
+                 fg_linear_info *info);
+
+/* Generic CSR PCG on an arbitrary SPD system (GpuCsrSolver::Initialize + Solve /
+ * SolveBatch / SolveCurrentOperatorBatch, csr_solver.cu:25-390). */
+int fg_csr_pcg(int32_t n, const int32_t *row_offsets, const int32_t *columns,
+               const double *values, int32_t values_per_item, const double *diagonal,
+               int32_t items, const double *rhs, double relative_tolerance,
+               int32_t max_iterations, double *x, fg_linear_info *info);
+
+/* Batched nonlinear solve (NonlinearP1Solver::SolveBatch, nonlinear_solver.cu:183-530;
+ * warm starts as in Solve, :686-698).  Host buffers:
+ *   currents [items * C]; hc_scale [items] or NULL (per-item permanent-magnet
+ *   coercivity scale); warm_a [items * N] or NULL;
+ *   a_out [items * N], b1_out / b2_out [items * E] (Bx/By or Br/Bz), flux_out [items * C],
+ *   info [items].  Output pointers may be NULL. */
+int fg_solve_batch(fg_plan *plan, int32_t items, const double *currents, const double *hc_scale,
+                   const double *warm_a, const fg_solve_options *options, double *a_out,
+                   double *b1_out, double *b2_out, double *flux_out, fg_item_info *info);
+
+/* Same, with every array a device pointer and work ordered on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  info stays a host pointer. */
+int fg_solve_batch_device(fg_plan *plan, int32_t items, const double *currents,
+                          const double *hc_scale, const double *warm_a,
+                          const fg_solve_options *options, double *a_out, double *b1_out,
+                          double *b2_out, double *flux_out, fg_item_info *info, void *stream);
+
+/* Timing and launch counters of the last solve on this plan. */
+int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing);
+
+/* FEMM DC B-H spline and evaluation (nonlinear_model.cpp:13-148): host functions
+ * exposed for parity checks.  b/h are smoothed in place; slope [count]. */
+int fg_bh_build(int32_t count, double *b, double *h, double *slope, double *cold_secant,
+                int32_t *smoothing_passes);
+void fg_bh_eval(int32_t count, const double *b, const double *h, const double *slope,
+                double field_b, double *h_dh_nu_dnu);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
