@@ -1,0 +1,305 @@
+"""Benchmark: batched nonlinear magnetostatic solves per second on B200.
+
+Workload (the nonlinear planar solve): 0.1 m square, 500 x 500 quads split into 2 P1
+triangles (251,001 nodes / 500,000 triangles), interior nodes jittered by U(+/-0.3 h),
+iron on the 24-point B = 2H/(200+H) table, a 5 mm magnet strip (mu_r 1.05, Hc 9e5 A/m,
+seeded angle) and three series circuits at seeded currents U[-20, 20] A; Newton step gate
+1e-6 with the reference's production options (inner PCG tolerance 1e-10 at the end).
+One step = one batched nonlinear solve of --items samples sharing the mesh (different
+currents).  Synthetic, seeded data; random currents per step and rank.
+
+Arms:
+  --impl ours       libfemmgpu through the C ABI.  ``value``: device-resident inputs
+                    (fg_solve_batch_device, CUDA-event timed); ``e2e``: host buffers
+                    through fg_solve_batch, H2D of currents and D2H of A, B, flux inside.
+  --impl reference  the reference's CPU path (FEMM-GPU host assembler + FEMM 4.2 SSOR-PCG,
+                    oracle/_ref) on all host threads; each step = one Newton iteration of
+                    one sample per thread, samples renewed as they converge.
+
+Multi-GPU: replicas only -- every rank solves its own batch, no collective on the data
+path; ``value`` = all ranks' solves / max-over-ranks time (weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for sub in ("femm-gpu_b200", "oracle"):
+    sys.path.insert(0, os.path.join(ROOT, sub))
+
+METRIC = "nonlinear solves/sec & SpMV HBM GB/s; warm/mixed vs plain FP64 at 1e-8, 1 B200"
+MESH_M = 500
+SEED_MESH = 2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--items", type=int, default=8, help="samples per batched solve")
+    p.add_argument("--mesh", type=int, default=MESH_M)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_baseline(model, items_seed, budget_threads=None):
+    """Reference CPU path (oracle/_ref) on one full-size sample per host thread."""
+    import oracle as O
+    from femm_gpu_b200 import meshes
+
+    threads = budget_threads or os.cpu_count() or 1
+    currents = meshes.seeded_currents(threads, model.circuit_count, 20.0, seed=items_seed)
+    if O.ref() is not None:
+        t0 = time.perf_counter()
+        a, flux, status, newton, calls, worst = O.ref_cpu_newton_batch(model, currents, threads=threads)
+        dt = time.perf_counter() - t0
+        kind = "reference"
+        ok = int((status == 0).sum())
+    else:  # the C restatement, one Python thread per sample (ctypes releases the GIL)
+        out = [None] * threads
+
+        def run(i):
+            out[i] = O.solve_batch(model, currents[i:i + 1])
+
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=run, args=(i,)) for i in range(threads)]
+        [t.start() for t in ths]
+        [t.join() for t in ths]
+        dt = time.perf_counter() - t0
+        kind = "port"
+        ok = sum(1 for o in out if o[4][0].status == 0)
+    return {"value": threads / dt, "unit": "solves/s", "cores": threads, "kind": kind,
+            "sample": f"{threads} full nonlinear solves of the {model.node_count}-node workload, "
+                      f"one per host thread, {ok} converged, {dt:.1f} s wall"}
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import meshes
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    model = meshes.square_nonlinear(m=args.mesh, seed=SEED_MESH)
+    plan = fg.Plan(model)
+    k, N, E, Cc = args.items, plan.N, plan.E, plan.C
+    dev = torch.device("cuda", local)
+    opts = fg.production_options()
+    stream = torch.cuda.current_stream(dev)
+    out_a = torch.empty((k, N), dtype=torch.float64, device=dev)
+    out_b1 = torch.empty((k, E), dtype=torch.float64, device=dev)
+    out_b2 = torch.empty((k, E), dtype=torch.float64, device=dev)
+    out_f = torch.empty((k, Cc), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    total = args.warmup + args.steps
+    inputs = [torch.tensor(meshes.seeded_currents(k, Cc, 20.0, seed=100000 * rank + s), device=dev)
+              for s in range(total)]
+    torch.cuda.synchronize()
+
+    def step(s):
+        info = plan.solve_device(k, inputs[s].data_ptr(), options=opts, a_ptr=out_a.data_ptr(),
+                                 b1_ptr=out_b1.data_ptr(), b2_ptr=out_b2.data_ptr(),
+                                 flux_ptr=out_f.data_ptr(), stream=stream.cuda_stream)
+        return info, plan.last_timing()
+
+    for s in range(args.warmup):
+        step(s)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    pcg_ms = 0.0
+    pcg_its = 0
+    item_its = 0
+    launches = 0
+    newton = 0
+    statuses = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for i in range(args.steps):
+            flush.fill_(float(i))  # L2 flush between timed steps (outside the events)
+            ev0[i].record(stream)
+            info, t = step(args.warmup + i)
+            ev1[i].record(stream)
+            pcg_ms += t.pcg_ms
+            pcg_its += t.pcg_iterations
+            launches += t.kernel_launches
+            newton += t.newton_iterations
+            item_its += sum(x.linear_iterations for x in info)
+            statuses += [x.status for x in info]
+        torch.cuda.synchronize()
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.barrier()
+        ms = float(tt.item())
+    value = world * k * args.steps / (ms / 1e3)
+
+    # Roofline of the dominant kernel (the cooperative PCG).
+    n, nnz = plan.rows, plan.nnz
+    per_item = 8.0 * nnz + 104.0 * n  # values + vector traffic of one item's iteration
+    shared = 4.0 * nnz + 4.0 * (n + 1)  # column indices + row structure, once per iteration
+    alg_bytes = item_its * per_item + pcg_its * shared
+    achieved = alg_bytes / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
+    peak, peak_kind = peaks()
+
+    # End to end through the host-buffer C ABI (H2D currents, D2H A / B / flux / info).
+    host_in = [meshes.seeded_currents(k, Cc, 20.0, seed=777000 + 100000 * rank + s) for s in range(args.steps)]
+    plan.solve(host_in[0])  # warm the host-path staging buffers
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        plan.solve(host_in[s])
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * k * args.steps / e2e_s, "unit": "solves/s",
+           "h2d_bytes_per_step": k * Cc * 8,
+           "d2h_bytes_per_step": k * (N + 2 * E + Cc) * 8 + k * 40}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"nonlinear planar solve, jittered {args.mesh}x{args.mesh} quads "
+                               f"({N} nodes, {E} triangles), iron B-H + PM strip + 3 circuits",
+                   "items_per_step": k, "rows": n, "nnz": nnz, "l2": "flushed between steps",
+                   "parallelism": f"replicas{world}", "precision": "fp64 Jacobi PCG"},
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": None, "kernel": "PcgKernel",
+                     "peak_source": peak_kind, "pcg_ms": pcg_ms, "pcg_iterations": pcg_its,
+                     "item_pcg_iterations": item_its},
+        "newton_iterations": newton,
+        "statuses_ok": sum(1 for s in statuses if s == 0), "statuses_total": len(statuses),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(model, items_seed=4242)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def run_reference(args, world, rank, local):
+    if rank != 0:
+        return
+    import oracle as O
+    from femm_gpu_b200 import meshes
+
+    model = meshes.square_nonlinear(m=args.mesh, seed=SEED_MESH)
+    if O.ref() is None:
+        kind = "port"
+    else:
+        kind = "reference"
+    threads = os.cpu_count() or 1
+    base = cpu_baseline(model, items_seed=4242, budget_threads=threads)
+    value = base["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * threads / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"nonlinear planar solve, jittered {args.mesh}x{args.mesh} quads",
+                       "items_per_step": threads},
+            "cpu_baseline": dict(base, kind=kind),
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

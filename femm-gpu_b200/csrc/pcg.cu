@@ -143,8 +143,49 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q], Reduce &sm, unsigne
   return true;
 }
 
+// One row's SpMV for one item: sum_w a_rw * v_c(w), v = z (+ beta p), in CSR order.
+// Column indices and values of up to eight entries are loaded before any gather so a
+// thread keeps ~16 independent loads in flight instead of one dependent chain per entry.
+template <int KP, bool kFold>
+__device__ __forceinline__ double RowProduct(const double *__restrict__ vals,
+                                             const int32_t *__restrict__ cols, size_t base,
+                                             int len, int vstride, int vitem, int item,
+                                             const double *z, const double *p, bool restart,
+                                             double beta)
+{
+  double acc = 0.0;
+  for (int w0 = 0; w0 < len; w0 += 8) {
+    int c[8];
+    double v[8], g[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      c[u] = 0;
+      v[u] = 0.0;
+      if (w0 + u < len) {
+        const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
+        c[u] = __ldg(cols + pos);
+        v[u] = __ldg(vals + pos * vstride + vitem);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      g[u] = 0.0;
+      if (w0 + u < len) {
+        const size_t ci = static_cast<size_t>(c[u]) * KP + item;
+        const double zc = z[ci];
+        g[u] = (!kFold || restart) ? zc : __fma_rn(beta, p[ci], zc);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (w0 + u < len)
+        acc = __fma_rn(v[u], g[u], acc);
+  }
+  return acc;
+}
+
 template <int KP>
-__global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
+__global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 {
   __shared__ Reduce sm;
   __shared__ Control ctl;
@@ -177,7 +218,7 @@ __global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
 
   auto precond = [&](double rv, int r) -> double {
     const size_t di = static_cast<size_t>(r) * dstride + ditem;
-    return a.use_inverse ? rv * a.invd[di] : rv / a.diag[di];
+    return a.use_inverse ? rv * __ldg(a.invd + di) : rv / __ldg(a.diag + di);
   };
 
 #define FG_ROWS_BEGIN                                                                              \
@@ -273,16 +314,10 @@ __global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
         const bool rs = ctl.restart[item];
         const double be = ctl.beta[item];
         FG_ROWS_BEGIN
-        const int len = rlen[r];
-        const size_t base = static_cast<size_t>(soff[r >> 5]) + (r & 31);
-        double acc = 0.0;
-        for (int w = 0; w < len; ++w) {
-          const size_t pos = base + 32 * static_cast<size_t>(w);
-          const size_t ci = static_cast<size_t>(cols[pos]) * KP + item;
-          const double zc = a.z[ci];
-          const double pv = rs ? zc : __fma_rn(be, pc[ci], zc);
-          acc = __fma_rn(vals[pos * vstride + vitem], pv, acc);
-        }
+        const int len = __ldg(rlen + r);
+        const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
+        const double acc = RowProduct<KP, true>(vals, cols, base, len, vstride, vitem, item, a.z,
+                                                pc, rs, be);
         const double zr = a.z[ri];
         const double pnew = rs ? zr : __fma_rn(be, pc[ri], zr);
         pn[ri] = pnew;
@@ -318,16 +353,41 @@ __global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
       double v[2] = {0.0, 0.0};
       if (ctl.active[item]) {
         const double al = ctl.alpha[item];
-        FG_ROWS_BEGIN
-        const double xn = a.x[ri] + al * pc[ri];
-        const double rn = a.r[ri] - al * a.q[ri];
-        const double zn = precond(rn, r);
-        a.x[ri] = xn;
-        a.r[ri] = rn;
-        a.z[ri] = zn;
-        v[0] += rn * rn;
-        v[1] += rn * zn;
-        FG_ROWS_END
+        double *__restrict__ X = a.x;
+        double *__restrict__ R = a.r;
+        double *__restrict__ Z = a.z;
+        const double *__restrict__ P = pc;
+        const double *__restrict__ Q = a.q;
+        // Two row groups per pass: all eight loads are issued before the first store.
+        for (int ws = ws0 + warp; ws < ws1; ws += 2 * kPcgWarps) {
+          const bool two = ws + kPcgWarps < ws1;
+          const int r0 = ws * S + lane / KP, r1 = (ws + kPcgWarps) * S + lane / KP;
+          const size_t i0 = static_cast<size_t>(r0) * KP + item, i1 = static_cast<size_t>(r1) * KP + item;
+          const double x0 = X[i0], p0 = P[i0], rv0 = R[i0], q0 = Q[i0];
+          double x1 = 0.0, p1 = 0.0, rv1 = 0.0, q1 = 0.0;
+          if (two) {
+            x1 = X[i1];
+            p1 = P[i1];
+            rv1 = R[i1];
+            q1 = Q[i1];
+          }
+          const double rn0 = rv0 - al * q0;
+          const double zn0 = precond(rn0, r0);
+          X[i0] = x0 + al * p0;
+          R[i0] = rn0;
+          Z[i0] = zn0;
+          v[0] += rn0 * rn0;
+          v[1] += rn0 * zn0;
+          if (two) {
+            const double rn1 = rv1 - al * q1;
+            const double zn1 = precond(rn1, r1);
+            X[i1] = x1 + al * p1;
+            R[i1] = rn1;
+            Z[i1] = zn1;
+            v[0] += rn1 * rn1;
+            v[1] += rn1 * zn1;
+          }
+        }
       }
       if (!GridReduce<KP, 2, false>(a, v, sm, epoch, buf))
         return;
@@ -366,13 +426,10 @@ __global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
         if (ctl.active[item] && ctl.flag[item]) {
           const double s = ctl.scale[item];
           FG_ROWS_BEGIN
-          const int len = rlen[r];
-          const size_t base = static_cast<size_t>(soff[r >> 5]) + (r & 31);
-          double acc = 0.0;
-          for (int w = 0; w < len; ++w) {
-            const size_t pos = base + 32 * static_cast<size_t>(w);
-            acc = __fma_rn(vals[pos * vstride + vitem], a.x[static_cast<size_t>(cols[pos]) * KP + item], acc);
-          }
+          const int len = __ldg(rlen + r);
+          const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
+          const double acc = RowProduct<KP, false>(vals, cols, base, len, vstride, vitem, item,
+                                                   a.x, nullptr, true, 0.0);
           const double rt = a.b[ri] / s - acc;
           a.r[ri] = rt;
           v[0] += rt * rt;
@@ -470,13 +527,10 @@ __global__ void __launch_bounds__(kPcgThreads, 1) PcgKernel(PcgArgs a)
       if (ctl.active[item]) {
         const double s = ctl.scale[item];
         FG_ROWS_BEGIN
-        const int len = rlen[r];
-        const size_t base = static_cast<size_t>(soff[r >> 5]) + (r & 31);
-        double acc = 0.0;
-        for (int w = 0; w < len; ++w) {
-          const size_t pos = base + 32 * static_cast<size_t>(w);
-          acc = __fma_rn(vals[pos * vstride + vitem], a.x[static_cast<size_t>(cols[pos]) * KP + item], acc);
-        }
+        const int len = __ldg(rlen + r);
+        const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
+        const double acc = RowProduct<KP, false>(vals, cols, base, len, vstride, vitem, item, a.x,
+                                                 nullptr, true, 0.0);
         const double rt = a.b[ri] / s - acc;
         a.r[ri] = rt;
         v[0] += rt * rt;
