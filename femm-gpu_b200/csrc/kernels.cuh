@@ -57,7 +57,12 @@ struct PcgArgs {
   int32_t max_iterations;
   uint32_t active_mask;
   long long timeout_ns;
+  // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
+  // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
+  // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.
+  unsigned long long *trace;
 };
+constexpr int kPcgTraceSlots = 10;
 
 // Launchers (return cudaError_t of the launch).
 cudaError_t LaunchElementKernel(const DevicePlan &p, int kp, const double *state,

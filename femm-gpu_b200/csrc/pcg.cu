@@ -7,15 +7,16 @@
 //
 // B200 mapping: one launch runs the whole solve for up to 32 items that share the
 // SELL-32 pattern.  Every CTA owns a contiguous range of rows for all items, so
-// column indices are read once per row for the whole batch.  A CG iteration has
-// exactly two grid-wide synchronisations, each fused with its reduction: every CTA
-// publishes its per-item partial sums, arrives on a release counter, and after the
-// acquire reads all CTAs' partials and sums them in CTA order -- so every CTA holds
-// bitwise-identical scalars and takes identical branches without a broadcast step.
-// The search-direction update p = z + beta p is folded into the next SpMV
-// (A p = sum a_ij (z_j + beta p_j), p double-buffered), which removes the third
-// barrier a textbook CG needs.  Waits are bounded by a %globaltimer budget: on
-// expiry the kernel records an error and every CTA returns.
+// column indices are read once per row for the whole batch; a thread owns one row and
+// IV adjacent items (16-byte loads of values, gathers and vectors when IV = 2).  A CG
+// iteration has exactly two grid-wide synchronisations, each fused with its
+// reduction: every CTA publishes its per-item partial sums, arrives on a release
+// counter, and after the acquire reads all CTAs' partials and sums them in CTA order,
+// so every CTA holds bitwise-identical scalars and takes identical branches without a
+// broadcast step.  The search-direction update p = z + beta p is folded into the next
+// SpMV (A p = sum a_ij (z_j + beta p_j), p double-buffered), which removes the third
+// barrier a textbook CG needs.  Waits are bounded by a %globaltimer budget: on expiry
+// the kernel records an error and every CTA returns.
 #include "kernels.cuh"
 
 #include <cmath>
@@ -63,6 +64,49 @@ __device__ __forceinline__ unsigned long long GlobalTimer()
   return t;
 }
 
+// IV consecutive doubles (16-byte aligned when IV = 2).
+template <int IV> __device__ __forceinline__ void Load(const double *p, double (&o)[IV])
+{
+  if constexpr (IV == 2) {
+    const double2 t = *reinterpret_cast<const double2 *>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    o[0] = *p;
+  }
+}
+template <int IV> __device__ __forceinline__ void LoadRO(const double *p, double (&o)[IV])
+{
+  if constexpr (IV == 2) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    o[0] = __ldg(p);
+  }
+}
+template <int IV> __device__ __forceinline__ void Store(double *p, const double (&v)[IV])
+{
+  if constexpr (IV == 2)
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  else
+    *p = v[0];
+}
+// A per-item (stride KP) or shared (stride 1, same value for every item) operand.
+template <int IV>
+__device__ __forceinline__ void LoadOperand(const double *base, size_t index, int stride, int per_item,
+                                            int item0, double (&o)[IV])
+{
+  if (per_item) {
+    LoadRO<IV>(base + index * stride + item0, o);
+  } else {
+    const double v = __ldg(base + index);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      o[j] = v;
+  }
+}
+
 // Grid-wide barrier over a monotonically increasing arrival counter, bounded in time.
 __device__ bool GridBarrier(const PcgArgs &a, unsigned &epoch, Reduce &sm)
 {
@@ -95,23 +139,42 @@ __device__ bool GridBarrier(const PcgArgs &a, unsigned &epoch, Reduce &sm)
   return sm.err == 0;
 }
 
-// Sum (or max) of Q per-item quantities over the whole grid, deterministic for a
-// fixed launch shape.  v[q] is this thread's partial for its lane's item.
-template <int KP, int Q, bool kMax>
-__device__ bool GridReduce(const PcgArgs &a, double (&v)[Q], Reduce &sm, unsigned &epoch, int &buf)
+// Phase trace of CTA 0 (PcgArgs::trace): thread 0 accumulates wall-clock intervals.
+struct Trace {
+  unsigned long long slot[kPcgTraceSlots];
+  unsigned long long mark;
+};
+
+__device__ __forceinline__ void TraceMark(const PcgArgs &a, Trace &tr, int slot)
 {
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long now = GlobalTimer();
+    tr.slot[slot] += now - tr.mark;
+    tr.mark = now;
+  }
+}
+
+// Sum (or max) of Q per-item quantities over the whole grid, deterministic for a
+// fixed launch shape.  v[q][j] is this thread's partial for its item item0 + j.
+template <int KP, int IV, int Q, bool kMax>
+__device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, unsigned &epoch,
+                           int &buf, Trace &tr, int phase)
+{
+  constexpr int LR = KP / IV; // lanes per row
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < Q; ++q) {
-    double x = v[q];
+  for (int q = 0; q < Q; ++q)
 #pragma unroll
-    for (int off = 16; off >= KP; off >>= 1) {
-      const double y = __shfl_xor_sync(0xffffffffu, x, off);
-      x = kMax ? fmax(x, y) : x + y;
+    for (int j = 0; j < IV; ++j) {
+      double x = v[q][j];
+#pragma unroll
+      for (int off = 16; off >= LR; off >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, x, off);
+        x = kMax ? fmax(x, y) : x + y;
+      }
+      if (lane < LR)
+        sm.warp[warp][q * KP + lane * IV + j] = x;
     }
-    if (lane < KP)
-      sm.warp[warp][q * KP + lane] = x;
-  }
   __syncthreads();
   constexpr int QK = Q * KP;
   const int G = gridDim.x;
@@ -122,8 +185,10 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q], Reduce &sm, unsigne
       s = kMax ? fmax(s, sm.warp[w][threadIdx.x]) : s + sm.warp[w][threadIdx.x];
     part[static_cast<size_t>(threadIdx.x) * G + blockIdx.x] = s;
   }
+  TraceMark(a, tr, 2 * phase);
   if (!GridBarrier(a, epoch, sm))
     return false;
+  TraceMark(a, tr, 2 * phase + 1);
   for (int t = warp; t < QK; t += kPcgWarps) {
     double s = 0.0;
     for (int g = lane; g < G; g += 32) {
@@ -139,70 +204,78 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q], Reduce &sm, unsigne
       sm.result[t] = s;
   }
   __syncthreads();
+  TraceMark(a, tr, 8);
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0)
+    tr.slot[9] += 1;
   buf ^= 1;
   return true;
 }
 
-// One row's SpMV for one item: sum_w a_rw * v_c(w), v = z (+ beta p), in CSR order.
-// Column indices and values of up to eight entries are loaded before any gather so a
-// thread keeps ~16 independent loads in flight instead of one dependent chain per entry.
-template <int KP, bool kFold>
-__device__ __forceinline__ double RowProduct(const double *__restrict__ vals,
-                                             const int32_t *__restrict__ cols, size_t base,
-                                             int len, int vstride, int vitem, int item,
-                                             const double *z, const double *p, bool restart,
-                                             double beta)
+// One row's product for IV items: acc_j = sum_w a_rw,j * v_j(col_w), v = z (+ beta p),
+// in CSR order.  Column indices and values of a chunk of entries (8 scalar or 4 paired)
+// are loaded before any gather so a thread keeps many independent loads in flight.
+template <int KP, int IV, bool kFold>
+__device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int len, int item0,
+                                           const double *z, const double *p,
+                                           const bool (&fold)[IV], const double (&beta)[IV],
+                                           double (&acc)[IV])
 {
-  double acc = 0.0;
-  for (int w0 = 0; w0 < len; w0 += 8) {
-    int c[8];
-    double v[8], g[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+  for (int j = 0; j < IV; ++j)
+    acc[j] = 0.0;
+  constexpr int U = 8 / IV; // entries per chunk: 8 scalar or 4 paired loads
+  for (int w0 = 0; w0 < len; w0 += U) {
+    int c[U];
+    double v[U][IV];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
       c[u] = 0;
-      v[u] = 0.0;
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        v[u][j] = 0.0;
       if (w0 + u < len) {
         const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
-        c[u] = __ldg(cols + pos);
-        v[u] = __ldg(vals + pos * vstride + vitem);
+        c[u] = __ldg(a.sell_col + pos);
+        LoadOperand<IV>(a.values, pos, a.value_stride, a.value_item, item0, v[u]);
       }
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      g[u] = 0.0;
+    for (int u = 0; u < U; ++u) {
       if (w0 + u < len) {
-        const size_t ci = static_cast<size_t>(c[u]) * KP + item;
-        const double zc = z[ci];
-        g[u] = (!kFold || restart) ? zc : __fma_rn(beta, p[ci], zc);
+        const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
+        double g[IV];
+        Load<IV>(z + ci, g);
+        if constexpr (kFold) {
+          double pv[IV];
+          Load<IV>(p + ci, pv);
+#pragma unroll
+          for (int j = 0; j < IV; ++j)
+            if (fold[j])
+              g[j] = __fma_rn(beta[j], pv[j], g[j]);
+        }
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          acc[j] = __fma_rn(v[u][j], g[j], acc[j]);
       }
     }
-#pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (w0 + u < len)
-        acc = __fma_rn(v[u], g[u], acc);
   }
-  return acc;
 }
 
-template <int KP>
+template <int KP, int IV>
 __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 {
   __shared__ Reduce sm;
   __shared__ Control ctl;
-  constexpr int S = 32 / KP; // rows per warp
+  __shared__ Trace tr;
+  constexpr int LR = KP / IV;  // lanes per row
+  constexpr int S = 32 / LR;   // rows per warp
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int item = lane % KP;
+  const int item0 = (lane % LR) * IV;
   const int WS = a.n_pad / S;
   const int ws0 = static_cast<int>(static_cast<long long>(WS) * blockIdx.x / gridDim.x);
   const int ws1 = static_cast<int>(static_cast<long long>(WS) * (blockIdx.x + 1) / gridDim.x);
   unsigned epoch = 0;
   int buf = 0;
-  const int vstride = a.value_stride, vitem = a.value_item * item;
-  const int dstride = a.diag_stride, ditem = a.diag_item * item;
-  const double *__restrict__ vals = a.values;
-  const int32_t *__restrict__ cols = a.sell_col;
-  const int32_t *__restrict__ soff = a.slice_off;
-  const int32_t *__restrict__ rlen = a.row_len;
 
   if (threadIdx.x < KP) {
     const int it = threadIdx.x;
@@ -213,35 +286,63 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     ctl.restart[it] = 1;
     ctl.flag[it] = 0;
     ctl.beta[it] = 0.0;
+    ctl.scale[it] = 1.0;
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kPcgTraceSlots; ++s)
+      tr.slot[s] = 0;
+    tr.mark = GlobalTimer();
   }
   __syncthreads();
 
-  auto precond = [&](double rv, int r) -> double {
-    const size_t di = static_cast<size_t>(r) * dstride + ditem;
-    return a.use_inverse ? rv * __ldg(a.invd + di) : rv / __ldg(a.diag + di);
+  // z = M^-1 r for this thread's items.
+  auto precond = [&](const double (&rv)[IV], int r, double (&zv)[IV]) {
+    double d[IV];
+    if (a.use_inverse) {
+      LoadOperand<IV>(a.invd, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        zv[j] = rv[j] * d[j];
+    } else {
+      LoadOperand<IV>(a.diag, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        zv[j] = rv[j] / d[j];
+    }
   };
+  auto on = [&](int j) { return ctl.active[item0 + j] != 0; };
 
 #define FG_ROWS_BEGIN                                                                              \
   for (int ws = ws0 + warp; ws < ws1; ws += kPcgWarps) {                                           \
-    const int r = ws * S + lane / KP;                                                              \
-    const size_t ri = static_cast<size_t>(r) * KP + item;
+    const int r = ws * S + lane / LR;                                                              \
+    const size_t ri = static_cast<size_t>(r) * KP + item0;
 #define FG_ROWS_END }
 
   // Validity (first invalid row decides the status) and RHS max-scaling.
   {
-    double v[2] = {0.0, 0.0};
-    const bool on = ctl.active[item];
+    double v[2][IV];
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      v[0][j] = v[1][j] = 0.0;
     FG_ROWS_BEGIN
-    if (on && r < a.n) {
-      const double bb = a.b[ri], dd = a.diag[static_cast<size_t>(r) * dstride + ditem];
-      const bool nonfinite = !isfinite(bb) || !isfinite(dd);
-      if (nonfinite || !(dd > 0.0))
-        v[0] = fmax(v[0], 2.0 * static_cast<double>(a.n - r) + (nonfinite ? 1.0 : 0.0));
-      v[1] = fmax(v[1], fabs(bb));
-    }
-    a.x[ri] = 0.0;
+    double bb[IV], dd[IV];
+    Load<IV>(a.b + ri, bb);
+    LoadOperand<IV>(a.diag, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, dd);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      if (on(j) && r < a.n) {
+        const bool nonfinite = !isfinite(bb[j]) || !isfinite(dd[j]);
+        if (nonfinite || !(dd[j] > 0.0))
+          v[0][j] = fmax(v[0][j], 2.0 * static_cast<double>(a.n - r) + (nonfinite ? 1.0 : 0.0));
+        v[1][j] = fmax(v[1][j], fabs(bb[j]));
+      }
+    double zero[IV];
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      zero[j] = 0.0;
+    Store<IV>(a.x + ri, zero);
     FG_ROWS_END
-    if (!GridReduce<KP, 2, true>(a, v, sm, epoch, buf))
+    if (!GridReduce<KP, IV, 2, true>(a, v, sm, epoch, buf, tr, 3))
       return;
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
@@ -266,19 +367,29 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 
   // r = b / s, z = M^-1 r, rho = r.z
   {
-    double v[2] = {0.0, 0.0};
-    if (ctl.active[item]) {
-      const double s = ctl.scale[item];
-      FG_ROWS_BEGIN
-      const double rv = a.b[ri] / s;
-      const double zv = precond(rv, r);
-      a.r[ri] = rv;
-      a.z[ri] = zv;
-      v[0] += rv * rv;
-      v[1] += rv * zv;
-      FG_ROWS_END
+    double v[2][IV], s[IV];
+#pragma unroll
+    for (int j = 0; j < IV; ++j) {
+      v[0][j] = v[1][j] = 0.0;
+      s[j] = ctl.scale[item0 + j] != 0.0 ? ctl.scale[item0 + j] : 1.0;
     }
-    if (!GridReduce<KP, 2, false>(a, v, sm, epoch, buf))
+    FG_ROWS_BEGIN
+    double bb[IV], rv[IV], zv[IV];
+    Load<IV>(a.b + ri, bb);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      rv[j] = bb[j] / s[j];
+    precond(rv, r, zv);
+    Store<IV>(a.r + ri, rv);
+    Store<IV>(a.z + ri, zv);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      if (on(j)) {
+        v[0][j] += rv[j] * rv[j];
+        v[1][j] += rv[j] * zv[j];
+      }
+    FG_ROWS_END
+    if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 3))
       return;
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
@@ -309,23 +420,39 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 
     // Phase A: p_new = z + beta p (folded into the gather), q = A p_new, p_new . q
     {
-      double v[1] = {0.0};
-      if (ctl.active[item]) {
-        const bool rs = ctl.restart[item];
-        const double be = ctl.beta[item];
+      double v[1][IV];
+      bool fold[IV];
+      double be[IV];
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = 0.0;
+        fold[j] = !ctl.restart[item0 + j];
+        be[j] = ctl.beta[item0 + j];
+      }
+      bool any_mine = false;
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        any_mine = any_mine || on(j);
+      if (any_mine) {
         FG_ROWS_BEGIN
-        const int len = __ldg(rlen + r);
-        const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
-        const double acc = RowProduct<KP, true>(vals, cols, base, len, vstride, vitem, item, a.z,
-                                                pc, rs, be);
-        const double zr = a.z[ri];
-        const double pnew = rs ? zr : __fma_rn(be, pc[ri], zr);
-        pn[ri] = pnew;
-        a.q[ri] = acc;
-        v[0] += pnew * acc;
+        const int len = __ldg(a.row_len + r);
+        const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+        double acc[IV], zr[IV], pr[IV], pnew[IV];
+        RowProduct<KP, IV, true>(a, base, len, item0, a.z, pc, fold, be, acc);
+        Load<IV>(a.z + ri, zr);
+        Load<IV>(pc + ri, pr);
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          pnew[j] = fold[j] ? __fma_rn(be[j], pr[j], zr[j]) : zr[j];
+        Store<IV>(pn + ri, pnew);
+        Store<IV>(a.q + ri, acc);
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          if (on(j))
+            v[0][j] += pnew[j] * acc[j];
         FG_ROWS_END
       }
-      if (!GridReduce<KP, 1, false>(a, v, sm, epoch, buf))
+      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 0))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -350,46 +477,68 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 
     // Phase B: x += alpha p, r -= alpha q, z = M^-1 r, r.r and r.z
     {
-      double v[2] = {0.0, 0.0};
-      if (ctl.active[item]) {
-        const double al = ctl.alpha[item];
-        double *__restrict__ X = a.x;
-        double *__restrict__ R = a.r;
-        double *__restrict__ Z = a.z;
-        const double *__restrict__ P = pc;
-        const double *__restrict__ Q = a.q;
-        // Two row groups per pass: all eight loads are issued before the first store.
+      double v[2][IV], al[IV];
+      bool mine = false;
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = v[1][j] = 0.0;
+        al[j] = on(j) ? ctl.alpha[item0 + j] : 0.0;
+        mine = mine || on(j);
+      }
+      if (mine) {
+        // Two row groups per pass: all loads are issued before the first store.
         for (int ws = ws0 + warp; ws < ws1; ws += 2 * kPcgWarps) {
           const bool two = ws + kPcgWarps < ws1;
-          const int r0 = ws * S + lane / KP, r1 = (ws + kPcgWarps) * S + lane / KP;
-          const size_t i0 = static_cast<size_t>(r0) * KP + item, i1 = static_cast<size_t>(r1) * KP + item;
-          const double x0 = X[i0], p0 = P[i0], rv0 = R[i0], q0 = Q[i0];
-          double x1 = 0.0, p1 = 0.0, rv1 = 0.0, q1 = 0.0;
+          const int r0 = ws * S + lane / LR, r1 = (ws + kPcgWarps) * S + lane / LR;
+          const size_t i0 = static_cast<size_t>(r0) * KP + item0;
+          const size_t i1 = static_cast<size_t>(r1) * KP + item0;
+          double x0[IV], p0[IV], rv0[IV], q0[IV], x1[IV], p1[IV], rv1[IV], q1[IV];
+          Load<IV>(a.x + i0, x0);
+          Load<IV>(pc + i0, p0);
+          Load<IV>(a.r + i0, rv0);
+          Load<IV>(a.q + i0, q0);
           if (two) {
-            x1 = X[i1];
-            p1 = P[i1];
-            rv1 = R[i1];
-            q1 = Q[i1];
+            Load<IV>(a.x + i1, x1);
+            Load<IV>(pc + i1, p1);
+            Load<IV>(a.r + i1, rv1);
+            Load<IV>(a.q + i1, q1);
           }
-          const double rn0 = rv0 - al * q0;
-          const double zn0 = precond(rn0, r0);
-          X[i0] = x0 + al * p0;
-          R[i0] = rn0;
-          Z[i0] = zn0;
-          v[0] += rn0 * rn0;
-          v[1] += rn0 * zn0;
+          double rn[IV], zn[IV], xn[IV];
+#pragma unroll
+          for (int j = 0; j < IV; ++j) {
+            rn[j] = on(j) ? rv0[j] - al[j] * q0[j] : rv0[j];
+            xn[j] = on(j) ? x0[j] + al[j] * p0[j] : x0[j];
+          }
+          precond(rn, r0, zn);
+          Store<IV>(a.x + i0, xn);
+          Store<IV>(a.r + i0, rn);
+          Store<IV>(a.z + i0, zn);
+#pragma unroll
+          for (int j = 0; j < IV; ++j)
+            if (on(j)) {
+              v[0][j] += rn[j] * rn[j];
+              v[1][j] += rn[j] * zn[j];
+            }
           if (two) {
-            const double rn1 = rv1 - al * q1;
-            const double zn1 = precond(rn1, r1);
-            X[i1] = x1 + al * p1;
-            R[i1] = rn1;
-            Z[i1] = zn1;
-            v[0] += rn1 * rn1;
-            v[1] += rn1 * zn1;
+#pragma unroll
+            for (int j = 0; j < IV; ++j) {
+              rn[j] = on(j) ? rv1[j] - al[j] * q1[j] : rv1[j];
+              xn[j] = on(j) ? x1[j] + al[j] * p1[j] : x1[j];
+            }
+            precond(rn, r1, zn);
+            Store<IV>(a.x + i1, xn);
+            Store<IV>(a.r + i1, rn);
+            Store<IV>(a.z + i1, zn);
+#pragma unroll
+            for (int j = 0; j < IV; ++j)
+              if (on(j)) {
+                v[0][j] += rn[j] * rn[j];
+                v[1][j] += rn[j] * zn[j];
+              }
           }
         }
       }
-      if (!GridReduce<KP, 2, false>(a, v, sm, epoch, buf))
+      if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 1))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -422,20 +571,36 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     if (verify) {
       // True residual for items at the threshold.
       {
-        double v[1] = {0.0};
-        if (ctl.active[item] && ctl.flag[item]) {
-          const double s = ctl.scale[item];
+        double v[1][IV];
+        bool mine[IV], any_mine = false;
+        double s[IV];
+#pragma unroll
+        for (int j = 0; j < IV; ++j) {
+          v[0][j] = 0.0;
+          mine[j] = on(j) && ctl.flag[item0 + j];
+          any_mine = any_mine || mine[j];
+          s[j] = ctl.scale[item0 + j];
+        }
+        if (any_mine) {
+          const bool nofold[IV] = {};
+          const double nobeta[IV] = {};
           FG_ROWS_BEGIN
-          const int len = __ldg(rlen + r);
-          const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
-          const double acc = RowProduct<KP, false>(vals, cols, base, len, vstride, vitem, item,
-                                                   a.x, nullptr, true, 0.0);
-          const double rt = a.b[ri] / s - acc;
-          a.r[ri] = rt;
-          v[0] += rt * rt;
+          const int len = __ldg(a.row_len + r);
+          const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+          double acc[IV], bb[IV], rv[IV];
+          RowProduct<KP, IV, false>(a, base, len, item0, a.x, nullptr, nofold, nobeta, acc);
+          Load<IV>(a.b + ri, bb);
+          Load<IV>(a.r + ri, rv);
+#pragma unroll
+          for (int j = 0; j < IV; ++j)
+            if (mine[j]) {
+              rv[j] = bb[j] / s[j] - acc[j];
+              v[0][j] += rv[j] * rv[j];
+            }
+          Store<IV>(a.r + ri, rv);
           FG_ROWS_END
         }
-        if (!GridReduce<KP, 1, false>(a, v, sm, epoch, buf))
+        if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 2))
           return;
         if (threadIdx.x < KP) {
           const int it = threadIdx.x;
@@ -454,25 +619,41 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       }
       // Accept (scale x back) or restart from the true residual.
       {
-        double v[2] = {0.0, 0.0};
-        const int f = ctl.active[item] ? ctl.flag[item] : 0;
-        if (f >= 2) {
-          const double s = ctl.scale[item];
+        double v[2][IV];
+        int f[IV];
+        bool any_mine = false;
+        double s[IV];
+#pragma unroll
+        for (int j = 0; j < IV; ++j) {
+          v[0][j] = v[1][j] = 0.0;
+          f[j] = on(j) ? ctl.flag[item0 + j] : 0;
+          any_mine = any_mine || f[j] >= 2;
+          s[j] = ctl.scale[item0 + j];
+        }
+        if (any_mine) {
           FG_ROWS_BEGIN
-          if (f == 2) {
-            const double xs = a.x[ri] * s;
-            a.x[ri] = xs;
-            if (!isfinite(xs))
-              v[1] += 1.0;
-          } else {
-            const double rv = a.r[ri];
-            const double zv = precond(rv, r);
-            a.z[ri] = zv;
-            v[0] += rv * zv;
+          double xv[IV], rv[IV], zv[IV], zo[IV];
+          Load<IV>(a.x + ri, xv);
+          Load<IV>(a.r + ri, rv);
+          Load<IV>(a.z + ri, zo);
+          precond(rv, r, zv);
+#pragma unroll
+          for (int j = 0; j < IV; ++j) {
+            if (f[j] == 2) {
+              xv[j] *= s[j];
+              if (!isfinite(xv[j]))
+                v[1][j] += 1.0;
+            }
+            if (f[j] == 3)
+              v[0][j] += rv[j] * zv[j];
+            else
+              zv[j] = zo[j];
           }
+          Store<IV>(a.x + ri, xv);
+          Store<IV>(a.z + ri, zv);
           FG_ROWS_END
         }
-        if (!GridReduce<KP, 2, false>(a, v, sm, epoch, buf))
+        if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 2))
           return;
         if (threadIdx.x < KP) {
           const int it = threadIdx.x;
@@ -516,27 +697,38 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     __syncthreads();
   }
 
-  // Iteration budget exhausted: report the true residual of the unscaled iterate.
+  // Iteration budget exhausted: report the true residual and scale the iterate back.
   bool any = false;
 #pragma unroll
   for (int it = 0; it < KP; ++it)
     any = any || ctl.active[it];
   if (any) {
     {
-      double v[1] = {0.0};
-      if (ctl.active[item]) {
-        const double s = ctl.scale[item];
-        FG_ROWS_BEGIN
-        const int len = __ldg(rlen + r);
-        const size_t base = static_cast<size_t>(__ldg(soff + (r >> 5))) + (r & 31);
-        const double acc = RowProduct<KP, false>(vals, cols, base, len, vstride, vitem, item, a.x,
-                                                 nullptr, true, 0.0);
-        const double rt = a.b[ri] / s - acc;
-        a.r[ri] = rt;
-        v[0] += rt * rt;
-        FG_ROWS_END
+      double v[1][IV];
+      double s[IV];
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = 0.0;
+        s[j] = ctl.scale[item0 + j];
       }
-      if (!GridReduce<KP, 1, false>(a, v, sm, epoch, buf))
+      const bool nofold[IV] = {};
+      const double nobeta[IV] = {};
+      FG_ROWS_BEGIN
+      const int len = __ldg(a.row_len + r);
+      const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+      double acc[IV], bb[IV], rv[IV];
+      RowProduct<KP, IV, false>(a, base, len, item0, a.x, nullptr, nofold, nobeta, acc);
+      Load<IV>(a.b + ri, bb);
+      Load<IV>(a.r + ri, rv);
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        if (on(j)) {
+          rv[j] = bb[j] / s[j] - acc[j];
+          v[0][j] += rv[j] * rv[j];
+        }
+      Store<IV>(a.r + ri, rv);
+      FG_ROWS_END
+      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -553,17 +745,26 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       __syncthreads();
     }
     {
-      double v[1] = {0.0};
-      if (ctl.active[item]) {
-        const double s = ctl.scale[item];
-        FG_ROWS_BEGIN
-        const double xs = a.x[ri] * s;
-        a.x[ri] = xs;
-        if (!isfinite(xs))
-          v[0] += 1.0;
-        FG_ROWS_END
+      double v[1][IV];
+      double s[IV];
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = 0.0;
+        s[j] = ctl.scale[item0 + j];
       }
-      if (!GridReduce<KP, 1, false>(a, v, sm, epoch, buf))
+      FG_ROWS_BEGIN
+      double xv[IV];
+      Load<IV>(a.x + ri, xv);
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        if (on(j)) {
+          xv[j] *= s[j];
+          if (!isfinite(xv[j]))
+            v[0][j] += 1.0;
+        }
+      Store<IV>(a.x + ri, xv);
+      FG_ROWS_END
+      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -589,19 +790,25 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     a.info[3 * it + 1] = static_cast<double>(ctl.iters[it]);
     a.info[3 * it + 2] = ctl.resid[it];
   }
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0)
+    for (int s = 0; s < kPcgTraceSlots; ++s)
+      a.trace[s] += tr.slot[s];
 }
 
-template <int KP> const void *KernelFor() { return reinterpret_cast<const void *>(&PcgKernel<KP>); }
+template <int KP, int IV> const void *KernelFor()
+{
+  return reinterpret_cast<const void *>(&PcgKernel<KP, IV>);
+}
 
 const void *SelectKernel(int kp)
 {
   switch (kp) {
-  case 1: return KernelFor<1>();
-  case 2: return KernelFor<2>();
-  case 4: return KernelFor<4>();
-  case 8: return KernelFor<8>();
-  case 16: return KernelFor<16>();
-  case 32: return KernelFor<32>();
+  case 1: return KernelFor<1, 1>();
+  case 2: return KernelFor<2, 2>();
+  case 4: return KernelFor<4, 2>();
+  case 8: return KernelFor<8, 2>();
+  case 16: return KernelFor<16, 2>();
+  case 32: return KernelFor<32, 2>();
   default: return nullptr;
   }
 }
@@ -627,7 +834,8 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   const int max_grid = PcgMaxGrid(args.kp);
   if (max_grid <= 0)
     return cudaErrorInvalidConfiguration;
-  const int rows_per_warp = 32 / args.kp;
+  const int iv = args.kp >= 2 ? 2 : 1;
+  const int rows_per_warp = 32 * iv / args.kp;
   const int warp_slices = args.n_pad / rows_per_warp;
   int grid = (warp_slices + kPcgWarps - 1) / kPcgWarps;
   if (grid > max_grid)

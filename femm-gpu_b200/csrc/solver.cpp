@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <limits>
 
 namespace fg
@@ -87,6 +88,10 @@ Status Plan::Create(HostModel model, const fg_plan_options &options)
   }
   s = Upload();
   if (s != Status::kOk)
+    return s;
+  const char *trace = std::getenv("FG_PCG_TRACE");
+  trace_enabled_ = trace && trace[0] == '1';
+  if (trace_enabled_ && (s = trace_.ensure(kPcgTraceSlots)) != Status::kOk)
     return s;
   if (cudaEventCreate(&ev_start_) != cudaSuccess || cudaEventCreate(&ev_mid_) != cudaSuccess ||
       cudaEventCreate(&ev_pcg_) != cudaSuccess || cudaEventCreate(&ev_end_) != cudaSuccess)
@@ -257,6 +262,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.max_iterations = max_iterations;
   a.active_mask = mask;
   a.timeout_ns = 5000000000LL;
+  a.trace = trace_enabled_ ? trace_.get() : nullptr;
   int grid = 0, block = 0;
   const cudaError_t e = LaunchPcg(a, &grid, &block, stream);
   if (e != cudaSuccess) {
@@ -277,10 +283,21 @@ Status Plan::SolveDevice(const SolveRequest &req)
     return Status::kGpuUnavailable;
   if (req.items <= 0 || (!req.currents && host_.C > 0) || !req.info)
     return Status::kInvalidArgument;
+  if (trace_enabled_ &&
+      cudaMemsetAsync(trace_.get(), 0, sizeof(unsigned long long) * kPcgTraceSlots, req.stream) != cudaSuccess)
+    return Status::kInternalError;
   for (int first = 0; first < req.items; first += kMaxItems) {
     const Status s = SolveChunk(req, first, std::min(kMaxItems, req.items - first));
     if (s != Status::kOk)
       return s;
+  }
+  if (trace_enabled_) {
+    unsigned long long t[kPcgTraceSlots];
+    if (cudaMemcpy(t, trace_.get(), sizeof(t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return Status::kInternalError;
+    for (int s = 0; s < 9; ++s)
+      timing_.pcg_phase_ms[s] = static_cast<double>(t[s]) * 1e-6;
+    timing_.pcg_phase_ms[9] = static_cast<double>(t[9]);
   }
   return Status::kOk;
 }

@@ -69,6 +69,8 @@ private:
   DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, p1_, q_;
   DeviceArray<double> norm_partials_, norms_, pcg_partials_, pcg_info_, staging_;
   DeviceArray<unsigned> barrier_;
+  DeviceArray<unsigned long long> trace_;
+  bool trace_enabled_ = false;
   DeviceArray<int32_t> error_, invalid_;
   // Host-pointer API staging.
   DeviceArray<double> in_currents_, in_hc_, in_warm_, out_a_, out_b1_, out_b2_, out_flux_;

@@ -95,7 +95,8 @@ class FgTiming(C.Structure):
     _fields_ = [("assembly_ms", C.c_double), ("pcg_ms", C.c_double), ("update_ms", C.c_double),
                 ("finalize_ms", C.c_double), ("newton_iterations", C.c_int64),
                 ("pcg_iterations", C.c_int64), ("kernel_launches", C.c_int64),
-                ("pcg_launches", C.c_int64), ("pcg_grid", C.c_int32), ("pcg_block", C.c_int32)]
+                ("pcg_launches", C.c_int64), ("pcg_grid", C.c_int32), ("pcg_block", C.c_int32),
+                ("pcg_phase_ms", C.c_double * 10)]
 
 
 _LIB = None

@@ -153,6 +153,11 @@ typedef struct fg_timing {
   int64_t pcg_launches;
   int32_t pcg_grid;         /* cooperative CTAs of the last PCG launch */
   int32_t pcg_block;
+  /* Phase trace of PCG CTA 0, filled only when the environment variable FG_PCG_TRACE=1
+   * is set when the plan is created: milliseconds of [0] SpMV phase work, [1] its grid
+   * wait, [2] update phase work, [3] its wait, [4] true-residual work, [5] its wait,
+   * [6] set-up work, [7] its wait, [8] final partial sums; [9] number of reductions. */
+  double pcg_phase_ms[10];
 } fg_timing;
 
 typedef struct fg_plan fg_plan;
