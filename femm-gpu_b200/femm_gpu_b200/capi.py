@@ -34,7 +34,7 @@ EXPORTED = [
     "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
     "fg_plan_destroy", "fg_plan_sizes_get", "fg_plan_symbolic", "fg_assemble", "fg_pcg_solve",
     "fg_csr_pcg", "fg_solve_batch", "fg_solve_batch_device", "fg_plan_last_timing",
-    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors",
+    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_csr_pcg_noalloc",
 ]
 
 
@@ -313,6 +313,23 @@ def csr_pcg(row_offsets, columns, values, diagonal, rhs, tol=1e-13, maxit=64, sh
     if status != 0:
         raise FgError(status, "fg_csr_pcg")
     return x, [info[i] for i in range(k)]
+
+
+NOALLOC_MAX_ROWS = 16384
+NOALLOC_MAX_POSITIONS = 262144
+
+
+def csr_pcg_noalloc(n, row_offsets_ptr, columns_ptr, values_ptr, diagonal_ptr, rhs_ptr, x_ptr,
+                    tol=1e-10, maxit=16384, stream=None):
+    """fg_csr_pcg_noalloc: every pointer is a device address the caller owns (for example
+    torch's ``data_ptr()``); the call itself allocates no memory.  Returns (status, info)."""
+    info = FgLinearInfo()
+    vp = lambda v: C.c_void_p(v) if v else None  # noqa: E731
+    status = lib().fg_csr_pcg_noalloc(C.c_int32(n), vp(row_offsets_ptr), vp(columns_ptr),
+                                      vp(values_ptr), vp(diagonal_ptr), vp(rhs_ptr),
+                                      C.c_double(tol), C.c_int32(maxit), vp(x_ptr), C.byref(info),
+                                      vp(stream))
+    return status, info
 
 
 def bh_build(b, h):

@@ -211,6 +211,30 @@ int fg_csr_pcg(int32_t n, const int32_t *row_offsets, const int32_t *columns,
                int32_t items, const double *rhs, double relative_tolerance,
                int32_t max_iterations, double *x, fg_linear_info *info);
 
+/* The same deterministic PCG on one CSR system with no memory allocation at all.  This
+ * entry point has no counterpart in the reference.  It is for callers that may not
+ * allocate GPU memory when they solve -- code running inside a memory pool that owns the
+ * device, real-time loops that forbid allocator calls, plug-in hosts that only lend their
+ * own buffers.  Every array argument is DEVICE memory owned by the caller (row_offsets
+ * [n + 1], columns / values [row_offsets[n]], diagonal / rhs / x [n]); info is host
+ * memory; work is ordered on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * the call returns when x and info are final.  All other memory is one fixed file-scope
+ * device array (about 5.5 MB per device that loads the library, held until exit), so no
+ * cudaMalloc, cudaFree or allocating library routine is called.
+ * Limits: n <= FG_NOALLOC_MAX_ROWS and at most FG_NOALLOC_MAX_POSITIONS SELL-32 slots
+ * (entries after padding each 32-row slice to its longest row); larger systems, bad
+ * offsets or columns and non-finite entries return FG_INVALID_ARGUMENT.
+ * Every call on a device shares that array and overwrites it: calls that overlap on the
+ * GPU race and must be serialised by the caller.  The first call on each device, with
+ * that device current, looks up the array's device address; make it before any stream
+ * capture begins. */
+#define FG_NOALLOC_MAX_ROWS 16384
+#define FG_NOALLOC_MAX_POSITIONS 262144
+int fg_csr_pcg_noalloc(int32_t n, const int32_t *row_offsets, const int32_t *columns,
+                       const double *values, const double *diagonal, const double *rhs,
+                       double relative_tolerance, int32_t max_iterations, double *x,
+                       fg_linear_info *info, void *stream);
+
 /* Batched nonlinear solve (NonlinearP1Solver::SolveBatch, nonlinear_solver.cu:183-530;
  * warm starts as in Solve, :686-698).  Host buffers:
  *   currents [items * C]; hc_scale [items] or NULL (per-item permanent-magnet
