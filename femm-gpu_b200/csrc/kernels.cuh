@@ -41,20 +41,26 @@ struct ItemScalars {
 struct PcgArgs {
   int32_t n, n_pad, slices, kp, items;
   const int32_t *slice_off, *row_len, *sell_col;
-  const double *values;  // [positions][vs]
+  // Storage type of values, diagonal, inverse diagonal and every vector: FP64
+  // (precision 0) or FP32 (precision 1: SpMV accumulated in FP32, dot products in FP64).
+  int32_t precision;
+  const void *values;    // [positions][vs]
   int32_t value_stride;  // KP (per-item operators) or 1 (one shared operator)
   int32_t value_item;    // 1 or 0
-  const double *diag, *invd; // [n_pad][ds]
+  const void *diag, *invd; // [n_pad][ds]
   int32_t diag_stride, diag_item;
   int32_t use_inverse;
-  const double *b;
-  double *x, *r, *z, *p0, *p1, *q;
+  const void *b;
+  void *x, *r, *z, *p0, *p1, *q;
   double *partials;   // [2][64][grid]
   unsigned int *barrier;
   int32_t *error;
   double *info;       // [items][3]: status, iterations, residual
   double tolerance;
   int32_t max_iterations;
+  // 0: verify the true residual at the threshold (the reference's rule).  1: accept on
+  // the recursive residual (inner solves whose caller checks the true residual).
+  int32_t skip_verification;
   uint32_t active_mask;
   long long timeout_ns;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
@@ -94,6 +100,16 @@ cudaError_t LaunchExtractCsr(const DevicePlan &p, int kp, int item, const double
 // Scatter CSR-ordered operator values into the SELL layout (item-major input).
 cudaError_t LaunchScatterCsr(const DevicePlan &p, int kp, int items, const double *csr_values,
                              int32_t values_per_item, double *values, cudaStream_t stream);
+// Mixed-precision form: FP32 copies of the assembled operator, the FP64 accumulation of
+// an FP32 correction, and the FP64 defect r = b - K x with its FP32 copy and norms.
+cudaError_t LaunchToSingle(const DevicePlan &p, int kp, uint32_t mask, const double *val64,
+                           const double *diag64, float *val32, float *diag32, float *invd32,
+                           cudaStream_t stream);
+cudaError_t LaunchAccumulate(const DevicePlan &p, int kp, uint32_t mask, int first, const float *d,
+                             double *x, cudaStream_t stream);
+cudaError_t LaunchDefect(const DevicePlan &p, int kp, uint32_t mask, int zero_x, const double *val64,
+                         const double *b, const double *x, double *r, float *r32,
+                         double *partials, double *norms, cudaStream_t stream);
 // Interleave item-major vectors [items][len] into [len_pad][kp] and back.
 cudaError_t LaunchInterleave(int kp, int items, int len, int len_pad, const double *in, double *out,
                              cudaStream_t stream);

@@ -8,18 +8,24 @@
 // B200 mapping: one launch runs the whole solve for up to 32 items that share the
 // SELL-32 pattern.  Every CTA owns a contiguous range of rows for all items, so
 // column indices are read once per row for the whole batch; a thread owns one row and
-// IV adjacent items (16-byte loads of values, gathers and vectors when IV = 2).  A CG
-// iteration has exactly two grid-wide synchronisations, each fused with its
-// reduction: every CTA publishes its per-item partial sums, arrives on a release
-// counter, and after the acquire reads all CTAs' partials and sums them in CTA order,
-// so every CTA holds bitwise-identical scalars and takes identical branches without a
-// broadcast step.  The search-direction update p = z + beta p is folded into the next
-// SpMV (A p = sum a_ij (z_j + beta p_j), p double-buffered), which removes the third
-// barrier a textbook CG needs.  Waits are bounded by a %globaltimer budget: on expiry
-// the kernel records an error and every CTA returns.
+// IV adjacent items (16-byte loads of values, gathers and vectors).  A CG iteration has
+// exactly two grid-wide synchronisations, each fused with its reduction: every CTA
+// publishes its per-item partial sums, arrives on a release counter, and after the
+// acquire reads all CTAs' partials and sums them in CTA order, so every CTA holds
+// bitwise-identical scalars and takes identical branches without a broadcast step.
+// The search-direction update p = z + beta p is folded into the next SpMV
+// (A p = sum a_ij (z_j + beta p_j), p double-buffered), which removes the third barrier
+// a textbook CG needs.  Waits are bounded by a %globaltimer budget: on expiry the kernel
+// records an error and every CTA returns.
+//
+// Storage type T: double (the drop-in FP64 solve) or float (the inner solve of the mixed
+// form: FP32 values and vectors, SpMV accumulated in FP32, every dot product and every
+// scalar in FP64; with verify = 0 the inner solve stops on its recursive residual and
+// the FP64 defect correction around it checks the true residual).
 #include "kernels.cuh"
 
 #include <cmath>
+#include <type_traits>
 
 namespace fg
 {
@@ -45,6 +51,12 @@ struct Reduce {
   int err;
 };
 
+// Phase trace of CTA 0 (PcgArgs::trace): thread 0 accumulates wall-clock intervals.
+struct Trace {
+  unsigned long long slot[kPcgTraceSlots];
+  unsigned long long mark;
+};
+
 __device__ __forceinline__ unsigned LoadAcquire(const unsigned *p)
 {
   unsigned v;
@@ -64,46 +76,86 @@ __device__ __forceinline__ unsigned long long GlobalTimer()
   return t;
 }
 
-// IV consecutive doubles (16-byte aligned when IV = 2).
-template <int IV> __device__ __forceinline__ void Load(const double *p, double (&o)[IV])
+// IV consecutive elements of T (aligned to IV * sizeof(T)), as one vector access.
+template <typename T, int IV> __device__ __forceinline__ void Load(const T *p, T (&o)[IV])
 {
-  if constexpr (IV == 2) {
+  if constexpr (std::is_same_v<T, double> && IV == 2) {
     const double2 t = *reinterpret_cast<const double2 *>(p);
     o[0] = t.x;
     o[1] = t.y;
-  } else {
-    o[0] = *p;
-  }
-}
-template <int IV> __device__ __forceinline__ void LoadRO(const double *p, double (&o)[IV])
-{
-  if constexpr (IV == 2) {
-    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+  } else if constexpr (std::is_same_v<T, float> && IV == 4) {
+    const float4 t = *reinterpret_cast<const float4 *>(p);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+  } else if constexpr (std::is_same_v<T, float> && IV == 2) {
+    const float2 t = *reinterpret_cast<const float2 *>(p);
     o[0] = t.x;
     o[1] = t.y;
   } else {
+    static_assert(IV == 1, "unsupported vector width");
+    o[0] = *p;
+  }
+}
+template <typename T, int IV> __device__ __forceinline__ void LoadRO(const T *p, T (&o)[IV])
+{
+  if constexpr (std::is_same_v<T, double> && IV == 2) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else if constexpr (std::is_same_v<T, float> && IV == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+  } else if constexpr (std::is_same_v<T, float> && IV == 2) {
+    const float2 t = __ldg(reinterpret_cast<const float2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    static_assert(IV == 1, "unsupported vector width");
     o[0] = __ldg(p);
   }
 }
-template <int IV> __device__ __forceinline__ void Store(double *p, const double (&v)[IV])
+template <typename T, int IV> __device__ __forceinline__ void Store(T *p, const T (&v)[IV])
 {
-  if constexpr (IV == 2)
+  if constexpr (std::is_same_v<T, double> && IV == 2) {
     *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
-  else
+  } else if constexpr (std::is_same_v<T, float> && IV == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (std::is_same_v<T, float> && IV == 2) {
+    *reinterpret_cast<float2 *>(p) = make_float2(v[0], v[1]);
+  } else {
+    static_assert(IV == 1, "unsupported vector width");
     *p = v[0];
+  }
 }
 // A per-item (stride KP) or shared (stride 1, same value for every item) operand.
-template <int IV>
-__device__ __forceinline__ void LoadOperand(const double *base, size_t index, int stride, int per_item,
-                                            int item0, double (&o)[IV])
+template <typename T, int IV>
+__device__ __forceinline__ void LoadOperand(const T *base, size_t index, int stride, int per_item,
+                                            int item0, T (&o)[IV])
 {
   if (per_item) {
-    LoadRO<IV>(base + index * stride + item0, o);
+    LoadRO<T, IV>(base + index * stride + item0, o);
   } else {
-    const double v = __ldg(base + index);
+    const T v = __ldg(base + index);
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       o[j] = v;
+  }
+}
+
+__device__ __forceinline__ double Fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float Fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+__device__ __forceinline__ void TraceMark(const PcgArgs &a, Trace &tr, int slot)
+{
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long now = GlobalTimer();
+    tr.slot[slot] += now - tr.mark;
+    tr.mark = now;
   }
 }
 
@@ -137,21 +189,6 @@ __device__ bool GridBarrier(const PcgArgs &a, unsigned &epoch, Reduce &sm)
   }
   __syncthreads();
   return sm.err == 0;
-}
-
-// Phase trace of CTA 0 (PcgArgs::trace): thread 0 accumulates wall-clock intervals.
-struct Trace {
-  unsigned long long slot[kPcgTraceSlots];
-  unsigned long long mark;
-};
-
-__device__ __forceinline__ void TraceMark(const PcgArgs &a, Trace &tr, int slot)
-{
-  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
-    const unsigned long long now = GlobalTimer();
-    tr.slot[slot] += now - tr.mark;
-    tr.mark = now;
-  }
 }
 
 // Sum (or max) of Q per-item quantities over the whole grid, deterministic for a
@@ -212,56 +249,56 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, uns
 }
 
 // One row's product for IV items: acc_j = sum_w a_rw,j * v_j(col_w), v = z (+ beta p),
-// in CSR order.  Column indices and values of a chunk of entries (8 scalar or 4 paired)
-// are loaded before any gather so a thread keeps many independent loads in flight.
-template <int KP, int IV, bool kFold>
+// in CSR order and in T arithmetic.  Column indices and values of a chunk of entries are
+// loaded before any gather so a thread keeps many independent loads in flight.
+template <typename T, int KP, int IV, bool kFold>
 __device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int len, int item0,
-                                           const double *z, const double *p,
-                                           const bool (&fold)[IV], const double (&beta)[IV],
-                                           double (&acc)[IV])
+                                           const T *z, const T *p, const bool (&fold)[IV],
+                                           const T (&beta)[IV], T (&acc)[IV])
 {
+  const T *vals = static_cast<const T *>(a.values);
 #pragma unroll
   for (int j = 0; j < IV; ++j)
-    acc[j] = 0.0;
-  constexpr int U = 8 / IV; // entries per chunk: 8 scalar or 4 paired loads
+    acc[j] = T(0);
+  constexpr int U = IV >= 2 ? 4 : 8; // entries per chunk
   for (int w0 = 0; w0 < len; w0 += U) {
     int c[U];
-    double v[U][IV];
+    T v[U][IV];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       c[u] = 0;
 #pragma unroll
       for (int j = 0; j < IV; ++j)
-        v[u][j] = 0.0;
+        v[u][j] = T(0);
       if (w0 + u < len) {
         const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
         c[u] = __ldg(a.sell_col + pos);
-        LoadOperand<IV>(a.values, pos, a.value_stride, a.value_item, item0, v[u]);
+        LoadOperand<T, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
       }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (w0 + u < len) {
         const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
-        double g[IV];
-        Load<IV>(z + ci, g);
+        T g[IV];
+        Load<T, IV>(z + ci, g);
         if constexpr (kFold) {
-          double pv[IV];
-          Load<IV>(p + ci, pv);
+          T pv[IV];
+          Load<T, IV>(p + ci, pv);
 #pragma unroll
           for (int j = 0; j < IV; ++j)
             if (fold[j])
-              g[j] = __fma_rn(beta[j], pv[j], g[j]);
+              g[j] = Fma(beta[j], pv[j], g[j]);
         }
 #pragma unroll
         for (int j = 0; j < IV; ++j)
-          acc[j] = __fma_rn(v[u][j], g[j], acc[j]);
+          acc[j] = Fma(v[u][j], g[j], acc[j]);
       }
     }
   }
 }
 
-template <int KP, int IV>
+template <typename T, int KP, int IV>
 __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 {
   __shared__ Reduce sm;
@@ -276,6 +313,13 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   const int ws1 = static_cast<int>(static_cast<long long>(WS) * (blockIdx.x + 1) / gridDim.x);
   unsigned epoch = 0;
   int buf = 0;
+  const T *B = static_cast<const T *>(a.b);
+  const T *DG = static_cast<const T *>(a.diag);
+  const T *IDG = static_cast<const T *>(a.invd);
+  T *X = static_cast<T *>(a.x);
+  T *R = static_cast<T *>(a.r);
+  T *Z = static_cast<T *>(a.z);
+  T *Qv = static_cast<T *>(a.q);
 
   if (threadIdx.x < KP) {
     const int it = threadIdx.x;
@@ -295,19 +339,19 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   }
   __syncthreads();
 
-  // z = M^-1 r for this thread's items.
-  auto precond = [&](const double (&rv)[IV], int r, double (&zv)[IV]) {
-    double d[IV];
+  // z = M^-1 r for this thread's items (FP64 arithmetic, stored in T).
+  auto precond = [&](const double (&rv)[IV], int r, T (&zv)[IV]) {
+    T d[IV];
     if (a.use_inverse) {
-      LoadOperand<IV>(a.invd, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
+      LoadOperand<T, IV>(IDG, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
-        zv[j] = rv[j] * d[j];
+        zv[j] = static_cast<T>(rv[j] * static_cast<double>(d[j]));
     } else {
-      LoadOperand<IV>(a.diag, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
+      LoadOperand<T, IV>(DG, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, d);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
-        zv[j] = rv[j] / d[j];
+        zv[j] = static_cast<T>(rv[j] / static_cast<double>(d[j]));
     }
   };
   auto on = [&](int j) { return ctl.active[item0 + j] != 0; };
@@ -325,22 +369,23 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     for (int j = 0; j < IV; ++j)
       v[0][j] = v[1][j] = 0.0;
     FG_ROWS_BEGIN
-    double bb[IV], dd[IV];
-    Load<IV>(a.b + ri, bb);
-    LoadOperand<IV>(a.diag, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, dd);
+    T bb[IV], dd[IV];
+    Load<T, IV>(B + ri, bb);
+    LoadOperand<T, IV>(DG, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, dd);
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       if (on(j) && r < a.n) {
-        const bool nonfinite = !isfinite(bb[j]) || !isfinite(dd[j]);
-        if (nonfinite || !(dd[j] > 0.0))
+        const double bj = bb[j], dj = dd[j];
+        const bool nonfinite = !isfinite(bj) || !isfinite(dj);
+        if (nonfinite || !(dj > 0.0))
           v[0][j] = fmax(v[0][j], 2.0 * static_cast<double>(a.n - r) + (nonfinite ? 1.0 : 0.0));
-        v[1][j] = fmax(v[1][j], fabs(bb[j]));
+        v[1][j] = fmax(v[1][j], fabs(bj));
       }
-    double zero[IV];
+    T zero[IV];
 #pragma unroll
     for (int j = 0; j < IV; ++j)
-      zero[j] = 0.0;
-    Store<IV>(a.x + ri, zero);
+      zero[j] = T(0);
+    Store<T, IV>(X + ri, zero);
     FG_ROWS_END
     if (!GridReduce<KP, IV, 2, true>(a, v, sm, epoch, buf, tr, 3))
       return;
@@ -374,19 +419,22 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       s[j] = ctl.scale[item0 + j] != 0.0 ? ctl.scale[item0 + j] : 1.0;
     }
     FG_ROWS_BEGIN
-    double bb[IV], rv[IV], zv[IV];
-    Load<IV>(a.b + ri, bb);
+    T bb[IV], rt[IV], zv[IV];
+    double rv[IV];
+    Load<T, IV>(B + ri, bb);
 #pragma unroll
-    for (int j = 0; j < IV; ++j)
-      rv[j] = bb[j] / s[j];
+    for (int j = 0; j < IV; ++j) {
+      rt[j] = static_cast<T>(static_cast<double>(bb[j]) / s[j]);
+      rv[j] = rt[j];
+    }
     precond(rv, r, zv);
-    Store<IV>(a.r + ri, rv);
-    Store<IV>(a.z + ri, zv);
+    Store<T, IV>(R + ri, rt);
+    Store<T, IV>(Z + ri, zv);
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       if (on(j)) {
         v[0][j] += rv[j] * rv[j];
-        v[1][j] += rv[j] * zv[j];
+        v[1][j] += rv[j] * static_cast<double>(zv[j]);
       }
     FG_ROWS_END
     if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 3))
@@ -409,7 +457,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     __syncthreads();
   }
 
-  double *pc = a.p0, *pn = a.p1;
+  T *pc = static_cast<T *>(a.p0), *pn = static_cast<T *>(a.p1);
   for (int iteration = 0; iteration < a.max_iterations; ++iteration) {
     bool any = false;
 #pragma unroll
@@ -422,34 +470,32 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     {
       double v[1][IV];
       bool fold[IV];
-      double be[IV];
+      T be[IV];
+      bool any_mine = false;
 #pragma unroll
       for (int j = 0; j < IV; ++j) {
         v[0][j] = 0.0;
         fold[j] = !ctl.restart[item0 + j];
-        be[j] = ctl.beta[item0 + j];
-      }
-      bool any_mine = false;
-#pragma unroll
-      for (int j = 0; j < IV; ++j)
+        be[j] = static_cast<T>(ctl.beta[item0 + j]);
         any_mine = any_mine || on(j);
+      }
       if (any_mine) {
         FG_ROWS_BEGIN
         const int len = __ldg(a.row_len + r);
         const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-        double acc[IV], zr[IV], pr[IV], pnew[IV];
-        RowProduct<KP, IV, true>(a, base, len, item0, a.z, pc, fold, be, acc);
-        Load<IV>(a.z + ri, zr);
-        Load<IV>(pc + ri, pr);
+        T acc[IV], zr[IV], pr[IV], pnew[IV];
+        RowProduct<T, KP, IV, true>(a, base, len, item0, Z, pc, fold, be, acc);
+        Load<T, IV>(Z + ri, zr);
+        Load<T, IV>(pc + ri, pr);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
-          pnew[j] = fold[j] ? __fma_rn(be[j], pr[j], zr[j]) : zr[j];
-        Store<IV>(pn + ri, pnew);
-        Store<IV>(a.q + ri, acc);
+          pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
+        Store<T, IV>(pn + ri, pnew);
+        Store<T, IV>(Qv + ri, acc);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
           if (on(j))
-            v[0][j] += pnew[j] * acc[j];
+            v[0][j] += static_cast<double>(pnew[j]) * static_cast<double>(acc[j]);
         FG_ROWS_END
       }
       if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 0))
@@ -470,7 +516,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         }
       }
       __syncthreads();
-      double *t = pc;
+      T *t = pc;
       pc = pn;
       pn = t;
     }
@@ -492,48 +538,57 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
           const int r0 = ws * S + lane / LR, r1 = (ws + kPcgWarps) * S + lane / LR;
           const size_t i0 = static_cast<size_t>(r0) * KP + item0;
           const size_t i1 = static_cast<size_t>(r1) * KP + item0;
-          double x0[IV], p0[IV], rv0[IV], q0[IV], x1[IV], p1[IV], rv1[IV], q1[IV];
-          Load<IV>(a.x + i0, x0);
-          Load<IV>(pc + i0, p0);
-          Load<IV>(a.r + i0, rv0);
-          Load<IV>(a.q + i0, q0);
+          T x0[IV], p0[IV], rv0[IV], q0[IV], x1[IV], p1[IV], rv1[IV], q1[IV];
+          Load<T, IV>(X + i0, x0);
+          Load<T, IV>(pc + i0, p0);
+          Load<T, IV>(R + i0, rv0);
+          Load<T, IV>(Qv + i0, q0);
           if (two) {
-            Load<IV>(a.x + i1, x1);
-            Load<IV>(pc + i1, p1);
-            Load<IV>(a.r + i1, rv1);
-            Load<IV>(a.q + i1, q1);
+            Load<T, IV>(X + i1, x1);
+            Load<T, IV>(pc + i1, p1);
+            Load<T, IV>(R + i1, rv1);
+            Load<T, IV>(Qv + i1, q1);
           }
-          double rn[IV], zn[IV], xn[IV];
+          double rn[IV];
+          T rt[IV], zn[IV], xn[IV];
 #pragma unroll
           for (int j = 0; j < IV; ++j) {
-            rn[j] = on(j) ? rv0[j] - al[j] * q0[j] : rv0[j];
-            xn[j] = on(j) ? x0[j] + al[j] * p0[j] : x0[j];
+            const double rr = on(j) ? static_cast<double>(rv0[j]) - al[j] * static_cast<double>(q0[j])
+                                    : static_cast<double>(rv0[j]);
+            rt[j] = static_cast<T>(rr);
+            rn[j] = rt[j];
+            xn[j] = on(j) ? static_cast<T>(static_cast<double>(x0[j]) + al[j] * static_cast<double>(p0[j]))
+                          : x0[j];
           }
           precond(rn, r0, zn);
-          Store<IV>(a.x + i0, xn);
-          Store<IV>(a.r + i0, rn);
-          Store<IV>(a.z + i0, zn);
+          Store<T, IV>(X + i0, xn);
+          Store<T, IV>(R + i0, rt);
+          Store<T, IV>(Z + i0, zn);
 #pragma unroll
           for (int j = 0; j < IV; ++j)
             if (on(j)) {
               v[0][j] += rn[j] * rn[j];
-              v[1][j] += rn[j] * zn[j];
+              v[1][j] += rn[j] * static_cast<double>(zn[j]);
             }
           if (two) {
 #pragma unroll
             for (int j = 0; j < IV; ++j) {
-              rn[j] = on(j) ? rv1[j] - al[j] * q1[j] : rv1[j];
-              xn[j] = on(j) ? x1[j] + al[j] * p1[j] : x1[j];
+              const double rr = on(j) ? static_cast<double>(rv1[j]) - al[j] * static_cast<double>(q1[j])
+                                      : static_cast<double>(rv1[j]);
+              rt[j] = static_cast<T>(rr);
+              rn[j] = rt[j];
+              xn[j] = on(j) ? static_cast<T>(static_cast<double>(x1[j]) + al[j] * static_cast<double>(p1[j]))
+                            : x1[j];
             }
             precond(rn, r1, zn);
-            Store<IV>(a.x + i1, xn);
-            Store<IV>(a.r + i1, rn);
-            Store<IV>(a.z + i1, zn);
+            Store<T, IV>(X + i1, xn);
+            Store<T, IV>(R + i1, rt);
+            Store<T, IV>(Z + i1, zn);
 #pragma unroll
             for (int j = 0; j < IV; ++j)
               if (on(j)) {
                 v[0][j] += rn[j] * rn[j];
-                v[1][j] += rn[j] * zn[j];
+                v[1][j] += rn[j] * static_cast<double>(zn[j]);
               }
           }
         }
@@ -555,8 +610,10 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
             if (!isfinite(ctl.resid[it])) {
               ctl.status[it] = kNonfinite;
               ctl.active[it] = 0;
-            } else {
-              ctl.flag[it] = ctl.resid[it] <= ctl.thr[it] ? 1 : 0;
+            } else if (ctl.resid[it] <= ctl.thr[it]) {
+              // The drop-in solve verifies the true residual; an inner solve of the
+              // mixed form accepts here (its FP64 caller checks the true residual).
+              ctl.flag[it] = a.skip_verification ? 2 : 1;
             }
           }
         }
@@ -564,120 +621,125 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       __syncthreads();
     }
 
-    bool verify = false;
+    bool verify = false, accept = false;
 #pragma unroll
-    for (int it = 0; it < KP; ++it)
-      verify = verify || (ctl.active[it] && ctl.flag[it]);
+    for (int it = 0; it < KP; ++it) {
+      verify = verify || (ctl.active[it] && ctl.flag[it] == 1);
+      accept = accept || (ctl.active[it] && ctl.flag[it] == 2);
+    }
     if (verify) {
       // True residual for items at the threshold.
-      {
-        double v[1][IV];
-        bool mine[IV], any_mine = false;
-        double s[IV];
+      double v[1][IV];
+      bool mine[IV], any_mine = false;
+      double s[IV];
 #pragma unroll
-        for (int j = 0; j < IV; ++j) {
-          v[0][j] = 0.0;
-          mine[j] = on(j) && ctl.flag[item0 + j];
-          any_mine = any_mine || mine[j];
-          s[j] = ctl.scale[item0 + j];
-        }
-        if (any_mine) {
-          const bool nofold[IV] = {};
-          const double nobeta[IV] = {};
-          FG_ROWS_BEGIN
-          const int len = __ldg(a.row_len + r);
-          const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-          double acc[IV], bb[IV], rv[IV];
-          RowProduct<KP, IV, false>(a, base, len, item0, a.x, nullptr, nofold, nobeta, acc);
-          Load<IV>(a.b + ri, bb);
-          Load<IV>(a.r + ri, rv);
-#pragma unroll
-          for (int j = 0; j < IV; ++j)
-            if (mine[j]) {
-              rv[j] = bb[j] / s[j] - acc[j];
-              v[0][j] += rv[j] * rv[j];
-            }
-          Store<IV>(a.r + ri, rv);
-          FG_ROWS_END
-        }
-        if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 2))
-          return;
-        if (threadIdx.x < KP) {
-          const int it = threadIdx.x;
-          if (ctl.active[it] && ctl.flag[it]) {
-            const double tr = sm.result[it];
-            if (!isfinite(tr)) {
-              ctl.status[it] = kNonfinite;
-              ctl.active[it] = 0;
-            } else {
-              ctl.resid[it] = sqrt(tr);
-              ctl.flag[it] = ctl.resid[it] <= ctl.thr[it] ? 2 : 3;
-            }
-          }
-        }
-        __syncthreads();
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = 0.0;
+        mine[j] = on(j) && ctl.flag[item0 + j] == 1;
+        any_mine = any_mine || mine[j];
+        s[j] = ctl.scale[item0 + j];
       }
-      // Accept (scale x back) or restart from the true residual.
-      {
-        double v[2][IV];
-        int f[IV];
-        bool any_mine = false;
-        double s[IV];
+      if (any_mine) {
+        const bool nofold[IV] = {};
+        const T nobeta[IV] = {};
+        FG_ROWS_BEGIN
+        const int len = __ldg(a.row_len + r);
+        const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+        T acc[IV], bb[IV], rv[IV];
+        RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
+        Load<T, IV>(B + ri, bb);
+        Load<T, IV>(R + ri, rv);
 #pragma unroll
-        for (int j = 0; j < IV; ++j) {
-          v[0][j] = v[1][j] = 0.0;
-          f[j] = on(j) ? ctl.flag[item0 + j] : 0;
-          any_mine = any_mine || f[j] >= 2;
-          s[j] = ctl.scale[item0 + j];
-        }
-        if (any_mine) {
-          FG_ROWS_BEGIN
-          double xv[IV], rv[IV], zv[IV], zo[IV];
-          Load<IV>(a.x + ri, xv);
-          Load<IV>(a.r + ri, rv);
-          Load<IV>(a.z + ri, zo);
-          precond(rv, r, zv);
-#pragma unroll
-          for (int j = 0; j < IV; ++j) {
-            if (f[j] == 2) {
-              xv[j] *= s[j];
-              if (!isfinite(xv[j]))
-                v[1][j] += 1.0;
-            }
-            if (f[j] == 3)
-              v[0][j] += rv[j] * zv[j];
-            else
-              zv[j] = zo[j];
+        for (int j = 0; j < IV; ++j)
+          if (mine[j]) {
+            const double t = static_cast<double>(bb[j]) / s[j] - static_cast<double>(acc[j]);
+            rv[j] = static_cast<T>(t);
+            v[0][j] += t * t;
           }
-          Store<IV>(a.x + ri, xv);
-          Store<IV>(a.z + ri, zv);
-          FG_ROWS_END
-        }
-        if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 2))
-          return;
-        if (threadIdx.x < KP) {
-          const int it = threadIdx.x;
-          if (ctl.active[it] && ctl.flag[it] == 2) {
-            if (sm.result[KP + it] != 0.0) {
-              ctl.status[it] = kNonfinite;
-            } else {
-              ctl.resid[it] *= ctl.scale[it];
-              ctl.status[it] = isfinite(ctl.resid[it]) ? kOk : kNonfinite;
-            }
+        Store<T, IV>(R + ri, rv);
+        FG_ROWS_END
+      }
+      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 2))
+        return;
+      if (threadIdx.x < KP) {
+        const int it = threadIdx.x;
+        if (ctl.active[it] && ctl.flag[it] == 1) {
+          const double trr = sm.result[it];
+          if (!isfinite(trr)) {
+            ctl.status[it] = kNonfinite;
             ctl.active[it] = 0;
-          } else if (ctl.active[it] && ctl.flag[it] == 3) {
-            const double rho = sm.result[it];
-            if (!isfinite(rho) || !(rho > 0.0)) {
-              ctl.status[it] = kBreakdown;
-              ctl.active[it] = 0;
-            } else {
-              ctl.rho[it] = rho;
-              ctl.restart[it] = 1;
-            }
+          } else {
+            ctl.resid[it] = sqrt(trr);
+            ctl.flag[it] = ctl.resid[it] <= ctl.thr[it] ? 2 : 3;
           }
         }
-        __syncthreads();
       }
+      __syncthreads();
+    }
+    if (verify || accept) {
+      // Accept (scale x back) or restart from the true residual.
+      double v[2][IV];
+      int f[IV];
+      bool any_mine = false;
+      double s[IV];
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        v[0][j] = v[1][j] = 0.0;
+        f[j] = on(j) ? ctl.flag[item0 + j] : 0;
+        any_mine = any_mine || f[j] >= 2;
+        s[j] = ctl.scale[item0 + j];
+      }
+      if (any_mine) {
+        FG_ROWS_BEGIN
+        T xv[IV], rv[IV], zv[IV], zo[IV];
+        double rd[IV];
+        Load<T, IV>(X + ri, xv);
+        Load<T, IV>(R + ri, rv);
+        Load<T, IV>(Z + ri, zo);
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          rd[j] = rv[j];
+        precond(rd, r, zv);
+#pragma unroll
+        for (int j = 0; j < IV; ++j) {
+          if (f[j] == 2) {
+            xv[j] = static_cast<T>(static_cast<double>(xv[j]) * s[j]);
+            if (!isfinite(static_cast<double>(xv[j])))
+              v[1][j] += 1.0;
+          }
+          if (f[j] == 3)
+            v[0][j] += rd[j] * static_cast<double>(zv[j]);
+          else
+            zv[j] = zo[j];
+        }
+        Store<T, IV>(X + ri, xv);
+        Store<T, IV>(Z + ri, zv);
+        FG_ROWS_END
+      }
+      if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 2))
+        return;
+      if (threadIdx.x < KP) {
+        const int it = threadIdx.x;
+        if (ctl.active[it] && ctl.flag[it] == 2) {
+          if (sm.result[KP + it] != 0.0) {
+            ctl.status[it] = kNonfinite;
+          } else {
+            ctl.resid[it] *= ctl.scale[it];
+            ctl.status[it] = isfinite(ctl.resid[it]) ? kOk : kNonfinite;
+          }
+          ctl.active[it] = 0;
+        } else if (ctl.active[it] && ctl.flag[it] == 3) {
+          const double rho = sm.result[it];
+          if (!isfinite(rho) || !(rho > 0.0)) {
+            ctl.status[it] = kBreakdown;
+            ctl.active[it] = 0;
+          } else {
+            ctl.rho[it] = rho;
+            ctl.restart[it] = 1;
+          }
+        }
+      }
+      __syncthreads();
     }
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
@@ -712,33 +774,34 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         s[j] = ctl.scale[item0 + j];
       }
       const bool nofold[IV] = {};
-      const double nobeta[IV] = {};
+      const T nobeta[IV] = {};
       FG_ROWS_BEGIN
       const int len = __ldg(a.row_len + r);
       const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-      double acc[IV], bb[IV], rv[IV];
-      RowProduct<KP, IV, false>(a, base, len, item0, a.x, nullptr, nofold, nobeta, acc);
-      Load<IV>(a.b + ri, bb);
-      Load<IV>(a.r + ri, rv);
+      T acc[IV], bb[IV], rv[IV];
+      RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
+      Load<T, IV>(B + ri, bb);
+      Load<T, IV>(R + ri, rv);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
         if (on(j)) {
-          rv[j] = bb[j] / s[j] - acc[j];
-          v[0][j] += rv[j] * rv[j];
+          const double t = static_cast<double>(bb[j]) / s[j] - static_cast<double>(acc[j]);
+          rv[j] = static_cast<T>(t);
+          v[0][j] += t * t;
         }
-      Store<IV>(a.r + ri, rv);
+      Store<T, IV>(R + ri, rv);
       FG_ROWS_END
       if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
         if (ctl.active[it]) {
-          const double tr = sm.result[it];
-          if (!isfinite(tr)) {
+          const double trr = sm.result[it];
+          if (!isfinite(trr)) {
             ctl.status[it] = kNonfinite;
             ctl.active[it] = 0;
           } else {
-            ctl.rz[it] = tr;
+            ctl.rz[it] = trr;
           }
         }
       }
@@ -753,16 +816,16 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         s[j] = ctl.scale[item0 + j];
       }
       FG_ROWS_BEGIN
-      double xv[IV];
-      Load<IV>(a.x + ri, xv);
+      T xv[IV];
+      Load<T, IV>(X + ri, xv);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
         if (on(j)) {
-          xv[j] *= s[j];
-          if (!isfinite(xv[j]))
+          xv[j] = static_cast<T>(static_cast<double>(xv[j]) * s[j]);
+          if (!isfinite(static_cast<double>(xv[j])))
             v[0][j] += 1.0;
         }
-      Store<IV>(a.x + ri, xv);
+      Store<T, IV>(X + ri, xv);
       FG_ROWS_END
       if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
         return;
@@ -795,46 +858,69 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       a.trace[s] += tr.slot[s];
 }
 
-template <int KP, int IV> const void *KernelFor()
+template <typename T, int KP, int IV> const void *KernelFor()
 {
-  return reinterpret_cast<const void *>(&PcgKernel<KP, IV>);
+  return reinterpret_cast<const void *>(&PcgKernel<T, KP, IV>);
 }
 
-const void *SelectKernel(int kp)
+const void *SelectKernel(int kp, int precision)
 {
+  if (precision == 0) {
+    switch (kp) {
+    case 1: return KernelFor<double, 1, 1>();
+    case 2: return KernelFor<double, 2, 2>();
+    case 4: return KernelFor<double, 4, 2>();
+    case 8: return KernelFor<double, 8, 2>();
+    case 16: return KernelFor<double, 16, 2>();
+    case 32: return KernelFor<double, 32, 2>();
+    default: return nullptr;
+    }
+  }
   switch (kp) {
-  case 1: return KernelFor<1, 1>();
-  case 2: return KernelFor<2, 2>();
-  case 4: return KernelFor<4, 2>();
-  case 8: return KernelFor<8, 2>();
-  case 16: return KernelFor<16, 2>();
-  case 32: return KernelFor<32, 2>();
+  case 1: return KernelFor<float, 1, 1>();
+  case 2: return KernelFor<float, 2, 2>();
+  case 4: return KernelFor<float, 4, 4>();
+  case 8: return KernelFor<float, 8, 4>();
+  case 16: return KernelFor<float, 16, 4>();
+  case 32: return KernelFor<float, 32, 4>();
   default: return nullptr;
   }
+}
+
+int ItemsPerThread(int kp, int precision)
+{
+  if (precision == 0)
+    return kp >= 2 ? 2 : 1;
+  return kp >= 4 ? 4 : (kp >= 2 ? 2 : 1);
 }
 
 } // namespace
 
 int PcgMaxGrid(int kp)
 {
-  const void *kernel = SelectKernel(kp);
-  int device = 0, sms = 0, per_sm = 0;
-  if (!kernel || cudaGetDevice(&device) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPcgThreads, 0) != cudaSuccess)
-    return 0;
-  return sms * (per_sm < 2 ? per_sm : 2);
+  int grid = 0;
+  for (int precision = 0; precision < 2; ++precision) {
+    const void *kernel = SelectKernel(kp, precision);
+    int device = 0, sms = 0, per_sm = 0;
+    if (!kernel || cudaGetDevice(&device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPcgThreads, 0) != cudaSuccess)
+      return 0;
+    const int g = sms * (per_sm < 2 ? per_sm : 2);
+    grid = precision == 0 ? g : (g < grid ? g : grid);
+  }
+  return grid;
 }
 
 cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream)
 {
-  const void *kernel = SelectKernel(args.kp);
+  const void *kernel = SelectKernel(args.kp, args.precision);
   if (!kernel)
     return cudaErrorInvalidValue;
   const int max_grid = PcgMaxGrid(args.kp);
   if (max_grid <= 0)
     return cudaErrorInvalidConfiguration;
-  const int iv = args.kp >= 2 ? 2 : 1;
+  const int iv = ItemsPerThread(args.kp, args.precision);
   const int rows_per_warp = 32 * iv / args.kp;
   const int warp_slices = args.n_pad / rows_per_warp;
   int grid = (warp_slices + kPcgWarps - 1) / kPcgWarps;

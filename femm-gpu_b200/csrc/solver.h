@@ -48,6 +48,12 @@ private:
   Status RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                 int value_stride, int value_item, int diag_stride, int diag_item, int use_inverse,
                 cudaStream_t stream);
+  // The Newton linear solve of the active items: FP64 PCG, or FP32 PCG inside FP64 defect
+  // correction.  linfo[3 * item] = status, iterations, residual; solution in x_.
+  Status LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
+                     cudaStream_t stream, double *linfo);
+  Status MixedSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
+                    cudaStream_t stream, double *linfo);
 
   HostModel model_;
   HostPlan host_;
@@ -68,6 +74,9 @@ private:
   // Batch workspace.
   DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, p1_, q_;
   DeviceArray<double> norm_partials_, norms_, pcg_partials_, pcg_info_, staging_;
+  // Mixed-precision form: FP32 operator and inner-solve vectors, FP64 defect norms.
+  DeviceArray<float> v32_, d32_, i32_, b32_, x32_, r32_, z32_, p032_, p132_, q32_;
+  DeviceArray<double> defect_partials_, defect_norms_;
   DeviceArray<unsigned> barrier_;
   DeviceArray<unsigned long long> trace_;
   bool trace_enabled_ = false;

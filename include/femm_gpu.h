@@ -158,6 +158,7 @@ typedef struct fg_timing {
    * wait, [2] update phase work, [3] its wait, [4] true-residual work, [5] its wait,
    * [6] set-up work, [7] its wait, [8] final partial sums; [9] number of reductions. */
   double pcg_phase_ms[10];
+  int64_t mixed_fallbacks; /* mixed form: item solves redone by the FP64 PCG */
 } fg_timing;
 
 typedef struct fg_plan fg_plan;
