@@ -265,3 +265,49 @@ def ref_cpu_newton_batch(model, currents, options=None, threads=1):
     if rc:
         raise RuntimeError(f"reference CPU baseline status {rc}")
     return a, flux, status, newton, calls, worst
+
+
+class RefSession:
+    """Step-wise reference CPU path: k samples, each step = one Newton iteration of every
+    unfinished sample (host assembly + FEMM PCG), one sample per host thread."""
+
+    def __init__(self, model, currents, options=None):
+        r = ref()
+        if r is None:
+            raise RuntimeError("oracle/_ref/libfemm_ref.so not built")
+        self.r = r
+        r.ref_session_create.restype = C.c_int32
+        r.ref_session_destroy.restype = None
+        self.view = ModelView(model)
+        currents = np.ascontiguousarray(np.atleast_2d(currents), dtype=np.float64)
+        self.k, self.c = currents.shape
+        self.opts = options if options is not None else production_options()
+        self.handle = C.c_void_p()
+        rc = r.ref_session_create(self.view.ref(), C.c_int32(self.k), _p(currents),
+                                  C.byref(self.opts), C.byref(self.handle))
+        if rc:
+            raise RuntimeError(f"reference session status {rc}")
+        self.done = np.zeros(self.k, np.int32)
+
+    def step(self, threads):
+        self.r.ref_session_step(self.handle, C.c_int32(threads), _p(self.done))
+        return self.done.copy()
+
+    def restart(self, i, currents):
+        cur = np.ascontiguousarray(currents, dtype=np.float64)
+        self.r.ref_session_restart(self.handle, C.c_int32(i), _p(cur))
+        self.done[i] = 0
+
+    def info(self):
+        status = np.zeros(self.k, np.int32)
+        newton = np.zeros(self.k, np.int32)
+        self.r.ref_session_info(self.handle, _p(status), _p(newton))
+        return status, newton
+
+    def close(self):
+        if self.handle:
+            self.r.ref_session_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        self.close()

@@ -105,33 +105,58 @@ struct ItemResult {
   double max_true_residual = 0.0;
 };
 
-ItemResult SolveOne(const NonlinearModel &model, const std::vector<double> &currents,
-                    NonlinearOptions options, double *a_out, double *flux_out)
+// One sample's Newton solve as a state machine: Step() is one Newton iteration
+// (host assembly + FEMM PCG to the inner tolerance + relaxation + step gate), so a
+// benchmark can time a bounded number of iterations and resume the sample later.
+class NewtonSample
 {
-  ItemResult out;
-  const bool nonlinear =
-      std::any_of(model.materials.begin(), model.materials.end(), [](const NonlinearMaterial &m) {
-        return m.bh_curve_index >= 0 || m.alpha_per_t2 != 0.0;
-      });
-  options.adaptive_linear_tolerance &= nonlinear;
-  std::vector<double> a(model.nodes.size(), 0.0);
-  for (size_t i = 0; i < model.dirichlet_nodes.size(); ++i)
-    a[model.dirichlet_nodes[i]] = model.dirichlet_a_wb_per_m[i];
-  double relaxation = 1.0, previous = std::numeric_limits<double>::infinity();
-  CFknDlg dialog;
-  out.status = static_cast<int>(Status::kNonlinearSolveNotConverged);
-  for (int iteration = 0; iteration < options.max_newton_iterations; ++iteration) {
+public:
+  NewtonSample(const NonlinearModel *model, NonlinearOptions options)
+      : model_(model), options_(options)
+  {
+    const bool nonlinear = std::any_of(
+        model->materials.begin(), model->materials.end(), [](const NonlinearMaterial &m) {
+          return m.bh_curve_index >= 0 || m.alpha_per_t2 != 0.0;
+        });
+    options_.adaptive_linear_tolerance &= nonlinear;
+  }
+
+  void Start(const double *currents)
+  {
+    currents_.assign(currents, currents + model_->circuit_count);
+    a_.assign(model_->nodes.size(), 0.0);
+    for (size_t i = 0; i < model_->dirichlet_nodes.size(); ++i)
+      a_[model_->dirichlet_nodes[i]] = model_->dirichlet_a_wb_per_m[i];
+    relaxation_ = 1.0;
+    previous_ = std::numeric_limits<double>::infinity();
+    iteration_ = 0;
+    done_ = false;
+    result_ = ItemResult{};
+    result_.status = static_cast<int>(Status::kNonlinearSolveNotConverged);
+  }
+
+  bool done() const { return done_; }
+  const ItemResult &result() const { return result_; }
+  const std::vector<double> &a() const { return a_; }
+
+  // One Newton iteration; returns done().
+  bool Step()
+  {
+    if (done_)
+      return true;
+    if (iteration_ >= options_.max_newton_iterations)
+      return Finish(static_cast<int>(Status::kNonlinearSolveNotConverged));
     Assembly assembly;
-    const Status status = AssembleNonlinearNewton(model, a, currents, iteration > 0, &assembly);
-    if (status != Status::kOk) {
-      out.status = static_cast<int>(status);
-      return out;
-    }
+    const Status status =
+        AssembleNonlinearNewton(*model_, a_, currents_, iteration_ > 0, &assembly);
+    if (status != Status::kOk)
+      return Finish(static_cast<int>(status));
     const int n = static_cast<int>(assembly.free_nodes.size());
     std::vector<double> rhs(n);
     for (int r = 0; r < n; ++r)
       rhs[r] = assembly.rhs_per_amp[r] + assembly.rhs_offset[r];
-    const double tolerance = NewtonLinearTolerance(options, previous);
+    const double tolerance = NewtonLinearTolerance(options_, previous_);
+    CFknDlg dialog;
     CBigLinProb linear;
     linear.Create(n, 0);
     linear.TheView = &dialog;
@@ -142,66 +167,119 @@ ItemResult SolveOne(const NonlinearModel &model, const std::vector<double> &curr
       linear.b[r] = rhs[r];
     }
     linear.Precision = tolerance;
-    if (!linear.PCGSolve(0)) {
-      out.status = static_cast<int>(Status::kLinearSolveBreakdown);
-      return out;
-    }
-    ++out.femm_pcg_calls;
+    if (!linear.PCGSolve(0))
+      return Finish(static_cast<int>(Status::kLinearSolveBreakdown));
+    ++result_.femm_pcg_calls;
     double true_residual = TrueResidual(assembly, rhs, linear.V);
     while (true_residual > tolerance && linear.Precision > 1e-13) {
       linear.Precision *= 0.1;
       linear.PCGSolve(1);
-      ++out.femm_pcg_calls;
+      ++result_.femm_pcg_calls;
       true_residual = TrueResidual(assembly, rhs, linear.V);
     }
-    out.max_true_residual = std::max(out.max_true_residual, true_residual);
+    result_.max_true_residual = std::max(result_.max_true_residual, true_residual);
     const std::vector<double> candidate =
         ExpandAssemblySolution(assembly, std::vector<double>(linear.V, linear.V + n));
     double difference_sq = 0.0, candidate_sq = 0.0;
     for (size_t i = 0; i < candidate.size(); ++i) {
-      const double d = candidate[i] - a[i];
+      const double d = candidate[i] - a_[i];
       difference_sq += d * d;
       candidate_sq += candidate[i] * candidate[i];
     }
     const double residual = std::sqrt(difference_sq) /
                             std::max(std::sqrt(candidate_sq), std::numeric_limits<double>::min());
-    if (!std::isfinite(residual)) {
-      out.status = static_cast<int>(Status::kNumericalNonfinite);
-      return out;
-    }
-    if (iteration > 5) {
-      if (residual > previous && relaxation > 0.125)
-        relaxation *= 0.5;
+    if (!std::isfinite(residual))
+      return Finish(static_cast<int>(Status::kNumericalNonfinite));
+    if (iteration_ > 5) {
+      if (residual > previous_ && relaxation_ > 0.125)
+        relaxation_ *= 0.5;
       else
-        relaxation += 0.1 * (1.0 - relaxation);
+        relaxation_ += 0.1 * (1.0 - relaxation_);
     }
-    for (size_t i = 0; i < a.size(); ++i)
-      a[i] += relaxation * (candidate[i] - a[i]);
-    out.newton_iterations = iteration + 1;
-    if (NewtonStepConverged(options, iteration, residual, tolerance)) {
-      out.status = 0;
-      break;
-    }
-    previous = residual;
+    for (size_t i = 0; i < a_.size(); ++i)
+      a_[i] += relaxation_ * (candidate[i] - a_[i]);
+    result_.newton_iterations = iteration_ + 1;
+    if (NewtonStepConverged(options_, iteration_, residual, tolerance))
+      return Finish(0);
+    previous_ = residual;
+    ++iteration_;
+    return false;
   }
-  std::copy(a.begin(), a.end(), a_out);
+
   // Flux linkage per circuit (nonlinear_solver.cu:36-42, :74-79, planar form).
-  for (int c = 0; c < model.circuit_count; ++c)
-    flux_out[c] = 0.0;
-  for (const NonlinearTriangle &t : model.triangles) {
-    const NonlinearMaterial &mt = model.materials[t.material];
-    if (mt.circuit_index < 0)
-      continue;
-    Node p[3] = {model.nodes[t.node[0]], model.nodes[t.node[1]], model.nodes[t.node[2]]};
-    NonlinearElementTerms terms;
-    BuildElementTerms(p, &terms);
-    flux_out[mt.circuit_index] += terms.area_m2 * mt.source_j_per_a / 3.0 *
-                                  (a[t.node[0]] + a[t.node[1]] + a[t.node[2]]);
+  void Flux(double *flux_out) const
+  {
+    const NonlinearModel &model = *model_;
+    for (int c = 0; c < model.circuit_count; ++c)
+      flux_out[c] = 0.0;
+    for (const NonlinearTriangle &t : model.triangles) {
+      const NonlinearMaterial &mt = model.materials[t.material];
+      if (mt.circuit_index < 0)
+        continue;
+      Node p[3] = {model.nodes[t.node[0]], model.nodes[t.node[1]], model.nodes[t.node[2]]};
+      NonlinearElementTerms terms;
+      BuildElementTerms(p, &terms);
+      flux_out[mt.circuit_index] += terms.area_m2 * mt.source_j_per_a / 3.0 *
+                                    (a_[t.node[0]] + a_[t.node[1]] + a_[t.node[2]]);
+    }
+    for (int c = 0; c < model.circuit_count; ++c)
+      flux_out[c] *= model.depth_m;
   }
-  for (int c = 0; c < model.circuit_count; ++c)
-    flux_out[c] *= model.depth_m;
-  return out;
+
+private:
+  bool Finish(int status)
+  {
+    result_.status = status;
+    done_ = true;
+    return true;
+  }
+
+  const NonlinearModel *model_;
+  NonlinearOptions options_;
+  std::vector<double> currents_, a_;
+  double relaxation_ = 1.0, previous_ = 0.0;
+  int iteration_ = 0;
+  bool done_ = false;
+  ItemResult result_;
+};
+
+NonlinearOptions ToOptions(const or_options *o)
+{
+  NonlinearOptions options;
+  options.relative_tolerance = o->relative_tolerance;
+  options.max_newton_iterations = o->max_newton_iterations;
+  options.max_linear_iterations = o->max_linear_iterations;
+  options.linear_relative_tolerance = o->linear_relative_tolerance;
+  options.recover_nonconvergence = o->recover_nonconvergence != 0;
+  options.adaptive_linear_tolerance = o->adaptive_linear_tolerance != 0;
+  return options;
 }
+
+// Runs fn(i) for i in [0, count) on `threads` host threads.
+template <class F> void ParallelFor(int count, int threads, F fn)
+{
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const int i = next.fetch_add(1);
+      if (i >= count)
+        return;
+      fn(i);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < std::max(1, std::min(threads, count)); ++t)
+    pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool)
+    t.join();
+}
+
+// A set of samples advanced one Newton iteration at a time (the bounded benchmark step).
+struct Session {
+  NonlinearModel model;
+  std::vector<NewtonSample> samples;
+};
 
 } // namespace
 
@@ -218,37 +296,78 @@ int ref_cpu_newton_batch(const or_model *m, int32_t k, const double *currents,
   NonlinearModel model;
   if (m->problem_type != 0 || !BuildModel(m, &model))
     return static_cast<int>(Status::kInvalidArgument);
-  NonlinearOptions options;
-  options.relative_tolerance = o->relative_tolerance;
-  options.max_newton_iterations = o->max_newton_iterations;
-  options.max_linear_iterations = o->max_linear_iterations;
-  options.linear_relative_tolerance = o->linear_relative_tolerance;
-  options.recover_nonconvergence = o->recover_nonconvergence != 0;
-  options.adaptive_linear_tolerance = o->adaptive_linear_tolerance != 0;
+  const NonlinearOptions options = ToOptions(o);
   const size_t N = model.nodes.size();
   const int C = model.circuit_count;
-  std::atomic<int> next{0};
-  auto worker = [&]() {
-    for (;;) {
-      const int item = next.fetch_add(1);
-      if (item >= k)
-        return;
-      const std::vector<double> cur(currents + (size_t)item * C, currents + (size_t)(item + 1) * C);
-      const ItemResult r = SolveOne(model, cur, options, a_out + (size_t)item * N,
-                                    flux_out + (size_t)item * C);
-      status[item] = r.status;
-      newton_iterations[item] = r.newton_iterations;
-      pcg_calls[item] = r.femm_pcg_calls;
-      max_true_residual[item] = r.max_true_residual;
+  ParallelFor(k, threads, [&](int item) {
+    NewtonSample sample(&model, options);
+    sample.Start(currents + (size_t)item * C);
+    while (!sample.Step()) {
     }
-  };
-  std::vector<std::thread> pool;
-  for (int t = 1; t < std::max(1, threads); ++t)
-    pool.emplace_back(worker);
-  worker();
-  for (auto &t : pool)
-    t.join();
+    std::copy(sample.a().begin(), sample.a().end(), a_out + (size_t)item * N);
+    sample.Flux(flux_out + (size_t)item * C);
+    const ItemResult &r = sample.result();
+    status[item] = r.status;
+    newton_iterations[item] = r.newton_iterations;
+    pcg_calls[item] = r.femm_pcg_calls;
+    max_true_residual[item] = r.max_true_residual;
+  });
   return 0;
 }
+
+// Session of k samples (currents [k*c]) for step-wise timing; *out receives the handle.
+int ref_session_create(const or_model *m, int32_t k, const double *currents,
+                       const or_options *o, void **out)
+{
+  *out = nullptr;
+  auto *session = new Session;
+  if (m->problem_type != 0 || !BuildModel(m, &session->model)) {
+    delete session;
+    return static_cast<int>(Status::kInvalidArgument);
+  }
+  const NonlinearOptions options = ToOptions(o);
+  session->samples.reserve(k);
+  for (int i = 0; i < k; ++i) {
+    session->samples.emplace_back(&session->model, options);
+    session->samples.back().Start(currents + (size_t)i * session->model.circuit_count);
+  }
+  *out = session;
+  return 0;
+}
+
+// One Newton iteration of every unfinished sample, one sample per host thread.
+// done [k] = 1 for samples that have finished (converged or failed).
+int ref_session_step(void *handle, int32_t threads, int32_t *done)
+{
+  auto *session = static_cast<Session *>(handle);
+  const int k = static_cast<int>(session->samples.size());
+  ParallelFor(k, threads, [&](int i) { session->samples[i].Step(); });
+  for (int i = 0; i < k; ++i)
+    done[i] = session->samples[i].done() ? 1 : 0;
+  return 0;
+}
+
+// Restarts sample i from the zero state with new currents [c].
+int ref_session_restart(void *handle, int32_t i, const double *currents)
+{
+  auto *session = static_cast<Session *>(handle);
+  if (i < 0 || i >= static_cast<int>(session->samples.size()))
+    return static_cast<int>(Status::kInvalidArgument);
+  session->samples[i].Start(currents);
+  return 0;
+}
+
+// Per-sample status and Newton iterations so far.
+int ref_session_info(void *handle, int32_t *status, int32_t *newton_iterations)
+{
+  auto *session = static_cast<Session *>(handle);
+  for (size_t i = 0; i < session->samples.size(); ++i) {
+    status[i] = session->samples[i].result().status;
+    newton_iterations[i] = session->samples[i].result().newton_iterations;
+  }
+  return 0;
+}
+
+void ref_session_destroy(void *handle) { delete static_cast<Session *>(handle); }
 
 } // extern "C"
