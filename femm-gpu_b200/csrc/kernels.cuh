@@ -50,6 +50,11 @@ struct PcgArgs {
   const void *diag, *invd; // [n_pad][ds]
   int32_t diag_stride, diag_item;
   int32_t use_inverse;
+  // Block-Jacobi (block_size 8 or 32; 0 = Jacobi): inverses in T, entry (i, j) of block
+  // b at [(b * bs + j) * bs + i] * block_stride (+ item when block_item), NaN first entry
+  // = unusable block.
+  const void *blocks;
+  int32_t block_size, block_stride, block_item;
   const void *b;
   void *x, *r, *z, *p0, *p1, *q;
   double *partials;   // [2][64][grid]
@@ -80,9 +85,17 @@ cudaError_t LaunchGatherValues(const DevicePlan &p, int kp, const double *elem_v
 cudaError_t LaunchGatherRhs(const DevicePlan &p, int kp, const double *elem_rhs,
                             const double *currents, const double *hc_scale, uint32_t active_mask,
                             double *rhs, cudaStream_t stream);
+// Block-Jacobi inverses of the assembled operators (blocks of bs rows, bs = 8 or 32),
+// written in FP64 (out64) or FP32 (out32); per item when value_item, else one shared set.
+// *fallbacks counts the blocks marked unusable.
+cudaError_t LaunchBlockInverse(const DevicePlan &p, int kp, int items, int bs, const double *values,
+                               int value_item, const double *diag, int diag_item, double *out64,
+                               float *out32, int32_t *fallbacks, cudaStream_t stream);
 // Cooperative persistent PCG; *grid_out receives the number of CTAs used.
 cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream);
 int PcgMaxGrid(int kp);
+// Whether a PCG kernel exists for this shape (block size 32 in FP64 stops at 16 items).
+bool PcgSupported(int kp, int precision, int block_size);
 
 cudaError_t LaunchNewtonNorms(const DevicePlan &p, int kp, const double *x, const double *state,
                               double *partials, double *norms, cudaStream_t stream);

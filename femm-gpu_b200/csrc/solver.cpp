@@ -71,9 +71,14 @@ Status Plan::Create(HostModel model, const fg_plan_options &options)
 {
   model_ = std::move(model);
   options_ = options;
-  if (options_.preconditioner != FG_PRECOND_JACOBI ||
+  if ((options_.preconditioner != FG_PRECOND_JACOBI &&
+       options_.preconditioner != FG_PRECOND_BLOCK_JACOBI) ||
+      (options_.preconditioner == FG_PRECOND_BLOCK_JACOBI && options_.block_size != 8 &&
+       options_.block_size != 32) ||
       (options_.precision != FG_PRECISION_FP64 && options_.precision != FG_PRECISION_MIXED))
     return Status::kUnsupportedFeature;
+  // 32-row blocks in FP64 (the mixed form's fallback included) stop at 16 items per launch.
+  chunk_cap_ = block_size() == 32 ? 16 : kMaxItems;
   Status s = BuildHostPlan(model_, &host_);
   if (s != Status::kOk)
     return s;
@@ -219,6 +224,12 @@ Status Plan::EnsureWorkspace(int kp)
   FG_EN(error_, 1);
   FG_EN(invalid_, static_cast<size_t>(kp));
   FG_EN(small_, static_cast<size_t>(10) * kp + 8);
+  if (block_size() > 0) {
+    FG_EN(blocks64_, vec * block_size());
+    FG_EN(block_fallbacks_, 1);
+    if (options_.precision == FG_PRECISION_MIXED)
+      FG_EN(blocks32_, vec * block_size());
+  }
   if (options_.precision == FG_PRECISION_MIXED) {
     FG_EN(v32_, static_cast<size_t>(h.positions) * kp);
     FG_EN(d32_, vec);
@@ -236,16 +247,23 @@ Status Plan::EnsureWorkspace(int kp)
 #undef FG_EN
   if (s != Status::kOk)
     return s;
-  // Padding rows of the operator must read as an identity with a zero inverse.
+  if (block_fallbacks_.get() && cudaMemset(block_fallbacks_.get(), 0, sizeof(int32_t)) != cudaSuccess)
+    return Status::kInternalError;
   kp_cap_ = kp;
   return Status::kOk;
 }
 
 Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                     int value_stride, int value_item, int diag_stride, int diag_item,
-                    int use_inverse, cudaStream_t stream)
+                    int use_inverse, cudaStream_t stream, const double *blocks)
 {
   PcgArgs a{};
+  if (blocks) {
+    a.blocks = blocks;
+    a.block_size = block_size();
+    a.block_stride = value_stride;
+    a.block_item = value_item;
+  }
   a.n = host_.n;
   a.n_pad = host_.n_pad;
   a.slices = host_.slices;
@@ -291,12 +309,33 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   return Status::kOk;
 }
 
+Status Plan::BuildBlocks(int kp, int items, bool per_item, bool single, cudaStream_t stream)
+{
+  const int bs = block_size();
+  if (!bs)
+    return Status::kOk;
+  if (LaunchBlockInverse(dev_, kp, items, bs, values_.get(), per_item ? 1 : 0, diag_.get(),
+                         per_item ? 1 : 0, single ? nullptr : blocks64_.get(),
+                         single ? blocks32_.get() : nullptr, block_fallbacks_.get(),
+                         stream) != cudaSuccess) {
+    cudaGetLastError();
+    return Status::kInternalError;
+  }
+  timing_.kernel_launches += 1;
+  timing_.block_inverses += static_cast<int64_t>(host_.n_pad / bs) * (per_item ? items : 1);
+  return Status::kOk;
+}
+
 Status Plan::LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                          cudaStream_t stream, double *linfo)
 {
   if (options_.precision == FG_PRECISION_MIXED)
     return MixedSolve(kp, items, mask, tolerance, max_iterations, stream, linfo);
-  Status s = RunPcg(kp, items, mask, tolerance, max_iterations, kp, 1, kp, 1, 1, stream);
+  Status s = BuildBlocks(kp, items, true, false, stream);
+  if (s != Status::kOk)
+    return s;
+  s = RunPcg(kp, items, mask, tolerance, max_iterations, kp, 1, kp, 1, 1, stream,
+             block_size() ? blocks64_.get() : nullptr);
   if (s != Status::kOk)
     return s;
   int32_t err = 0;
@@ -338,6 +377,9 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
       cudaStreamSynchronize(st) != cudaSuccess)
     return Status::kInternalError;
   timing_.kernel_launches += 3;
+  Status bs = BuildBlocks(kp, items, true, true, st);
+  if (bs != Status::kOk)
+    return bs;
   std::vector<double> bnorm(kp, 0.0);
   std::vector<int> its(kp, 0);
   uint32_t pending = mask, fallback = 0;
@@ -373,6 +415,12 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
     a.diag_stride = kp;
     a.diag_item = 1;
     a.use_inverse = 1;
+    if (block_size()) {
+      a.blocks = blocks32_.get();
+      a.block_size = block_size();
+      a.block_stride = kp;
+      a.block_item = 1;
+    }
     a.b = b32_.get();
     a.x = x32_.get();
     a.r = r32_.get();
@@ -444,7 +492,10 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   for (int i = 0; i < items; ++i)
     linfo[3 * i + 1] = its[i];
   if (fallback) {
-    Status s = RunPcg(kp, items, fallback, tolerance, max_iterations, kp, 1, kp, 1, 1, st);
+    Status s = BuildBlocks(kp, items, true, false, st);
+    if (s == Status::kOk)
+      s = RunPcg(kp, items, fallback, tolerance, max_iterations, kp, 1, kp, 1, 1, st,
+                 block_size() ? blocks64_.get() : nullptr);
     if (s != Status::kOk)
       return s;
     double f[3 * kMaxItems];
@@ -476,10 +527,21 @@ Status Plan::SolveDevice(const SolveRequest &req)
   if (trace_enabled_ &&
       cudaMemsetAsync(trace_.get(), 0, sizeof(unsigned long long) * kPcgTraceSlots, req.stream) != cudaSuccess)
     return Status::kInternalError;
-  for (int first = 0; first < req.items; first += kMaxItems) {
-    const Status s = SolveChunk(req, first, std::min(kMaxItems, req.items - first));
+  if (block_fallbacks_.get() &&
+      cudaMemsetAsync(block_fallbacks_.get(), 0, sizeof(int32_t), req.stream) != cudaSuccess)
+    return Status::kInternalError;
+  for (int first = 0; first < req.items; first += chunk_cap_) {
+    const Status s = SolveChunk(req, first, std::min(chunk_cap_, req.items - first));
     if (s != Status::kOk)
       return s;
+  }
+  if (block_size()) {
+    int32_t fallbacks = 0;
+    if (cudaMemcpyAsync(&fallbacks, block_fallbacks_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost,
+                        req.stream) != cudaSuccess ||
+        cudaStreamSynchronize(req.stream) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.block_fallbacks = fallbacks;
   }
   if (trace_enabled_) {
     unsigned long long t[kPcgTraceSlots];
@@ -756,6 +818,9 @@ Status Plan::PcgSolve(int items, const double *values, int values_per_item, cons
     return Status::kGpuUnavailable;
   if (items <= 0 || items > kMaxItems || !values || !rhs || !x || !info)
     return Status::kInvalidArgument;
+  if (items > chunk_cap_)
+    return Status::kUnsupportedFeature;
+  timing_ = fg_timing{};
   for (int i = 0; i < items; ++i)
     info[i] = fg_linear_info{ToInt(Status::kInvalidArgument), 0, std::numeric_limits<double>::infinity()};
   if (!(tolerance > 0.0) || !(tolerance < 1.0) || !std::isfinite(tolerance) || max_iterations < 0)
@@ -798,10 +863,20 @@ Status Plan::PcgSolve(int items, const double *values, int values_per_item, cons
   if (LaunchScatterCsr(dev_, vk, op_items, staging_.get(), shared ? 0 : static_cast<int>(nnz), values_.get(), nullptr) != cudaSuccess)
     return Status::kInternalError;
   const uint32_t mask = items >= 32 ? 0xffffffffu : ((1u << items) - 1u);
+  if (block_size() && cudaMemset(block_fallbacks_.get(), 0, sizeof(int32_t)) != cudaSuccess)
+    return Status::kInternalError;
+  if ((s = BuildBlocks(kp, items, !shared, false, nullptr)) != Status::kOk)
+    return s;
   s = RunPcg(kp, items, mask, tolerance, max_iterations, vk, shared ? 0 : 1, dk, shared ? 0 : 1,
-             usable ? 1 : 0, nullptr);
+             usable ? 1 : 0, nullptr, block_size() ? blocks64_.get() : nullptr);
   if (s != Status::kOk)
     return s;
+  if (block_size()) {
+    int32_t fallbacks = 0;
+    if (cudaMemcpy(&fallbacks, block_fallbacks_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.block_fallbacks = fallbacks;
+  }
   std::vector<double> xi(n_pad * kp), pinfo(3 * kp);
   int32_t err = 0;
   if (cudaMemcpy(xi.data(), x_.get(), xi.size() * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess ||

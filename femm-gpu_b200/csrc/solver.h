@@ -47,7 +47,14 @@ private:
   Status SolveChunk(const SolveRequest &request, int first, int count);
   Status RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                 int value_stride, int value_item, int diag_stride, int diag_item, int use_inverse,
-                cudaStream_t stream);
+                cudaStream_t stream, const double *blocks = nullptr);
+  // Block-Jacobi inverses of the current operators (values_, diag_) into blocks64_ or
+  // blocks32_; no-op for the Jacobi preconditioner.
+  Status BuildBlocks(int kp, int items, bool per_item, bool single, cudaStream_t stream);
+  int block_size() const
+  {
+    return options_.preconditioner == FG_PRECOND_BLOCK_JACOBI ? options_.block_size : 0;
+  }
   // The Newton linear solve of the active items: FP64 PCG, or FP32 PCG inside FP64 defect
   // correction.  linfo[3 * item] = status, iterations, residual; solution in x_.
   Status LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
@@ -63,6 +70,7 @@ private:
   int kp_cap_ = 0;
   bool host_only_ = false;
   int pcg_grid_cap_ = 0;
+  int chunk_cap_ = kMaxItems; // items per batched launch
 
   // Plan constants on the device.
   DeviceArray<int32_t> row_offsets_, columns_, row_len_, slice_off_, sell_col_, contrib_off_,
@@ -77,6 +85,10 @@ private:
   // Mixed-precision form: FP32 operator and inner-solve vectors, FP64 defect norms.
   DeviceArray<float> v32_, d32_, i32_, b32_, x32_, r32_, z32_, p032_, p132_, q32_;
   DeviceArray<double> defect_partials_, defect_norms_;
+  // Block-Jacobi inverses [n_pad * bs][KP] (FP64; FP32 for the mixed form's inner solve).
+  DeviceArray<double> blocks64_;
+  DeviceArray<float> blocks32_;
+  DeviceArray<int32_t> block_fallbacks_;
   DeviceArray<unsigned> barrier_;
   DeviceArray<unsigned long long> trace_;
   bool trace_enabled_ = false;

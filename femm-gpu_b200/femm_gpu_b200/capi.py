@@ -96,7 +96,8 @@ class FgTiming(C.Structure):
                 ("finalize_ms", C.c_double), ("newton_iterations", C.c_int64),
                 ("pcg_iterations", C.c_int64), ("kernel_launches", C.c_int64),
                 ("pcg_launches", C.c_int64), ("pcg_grid", C.c_int32), ("pcg_block", C.c_int32),
-                ("pcg_phase_ms", C.c_double * 10), ("mixed_fallbacks", C.c_int64)]
+                ("pcg_phase_ms", C.c_double * 10), ("mixed_fallbacks", C.c_int64),
+                ("block_inverses", C.c_int64), ("block_fallbacks", C.c_int64)]
 
 
 _LIB = None

@@ -92,7 +92,11 @@ typedef struct fg_model {
 } fg_model;
 
 typedef struct fg_plan_options {
-  int32_t preconditioner; /* FG_PRECOND_* */
+  /* FG_PRECOND_JACOBI (the reference default) or FG_PRECOND_BLOCK_JACOBI: dense inverses
+   * of contiguous block_size-row principal blocks (the reference's opt-in
+   * `--preconditioner block-jacobi`, gpu_solver/src/app/cli.cpp:39-46, block_size 8).
+   * block_size 32 runs at most 16 items per launch (fg_pcg_solve: items <= 16). */
+  int32_t preconditioner;
   int32_t block_size;     /* block-Jacobi rows per block: 8 or 32 */
   int32_t precision;      /* FG_PRECISION_*: mixed = FP32 inner PCG in FP64 defect correction */
   int32_t flags;          /* FG_PLAN_HOST_ONLY: build and validate the host topology only */
@@ -159,6 +163,8 @@ typedef struct fg_timing {
    * [6] set-up work, [7] its wait, [8] final partial sums; [9] number of reductions. */
   double pcg_phase_ms[10];
   int64_t mixed_fallbacks; /* mixed form: item solves redone by the FP64 PCG */
+  int64_t block_inverses;  /* block-Jacobi: blocks factored (summed over builds) */
+  int64_t block_fallbacks; /* block-Jacobi: blocks found unusable (diagonal used instead) */
 } fg_timing;
 
 typedef struct fg_plan fg_plan;

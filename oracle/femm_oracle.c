@@ -918,9 +918,152 @@ static double row_dot(int r, const int32_t *off, const int32_t *col, const doubl
   return s;
 }
 
+/* Block-Jacobi preconditioner (block_jacobi_preconditioner.cu:72-167, BuildBlockInverse):
+ * per contiguous block of bs rows, the principal block scaled by D^-1/2 is factored by
+ * Cholesky and inverted column by column; an unusable block (non-positive or subnormal
+ * reciprocal diagonal, asymmetric or non-finite entries, failed pivot, non-finite
+ * inverse) is stored as NaN at its first entry and the PCG falls back to the diagonal
+ * for its rows.  Storage per block: inv[j * bs + i] = (A_block^-1)(i, j). */
+static int g_precond_kind = 0, g_block_size = 8;
+
+void or_set_preconditioner(int32_t kind, int32_t block_size)
+{
+  g_precond_kind = kind;
+  g_block_size = block_size;
+}
+
+int or_block_jacobi(int32_t n, const int32_t *off, const int32_t *col, const double *val,
+                    const double *diag, int32_t bs, double *inv, int32_t *fallback_blocks)
+{
+  if (n <= 0 || bs <= 0 || bs > 64)
+    return OR_INVALID_ARGUMENT;
+  const int blocks = (n + bs - 1) / bs;
+  double *f = malloc(sizeof(double) * (size_t)bs * (size_t)bs);
+  double *xs = malloc(sizeof(double) * (size_t)bs * (size_t)bs);
+  double *sc = malloc(sizeof(double) * (size_t)bs);
+  int fallbacks = 0;
+  for (int b = 0; b < blocks; ++b) {
+    const int first = b * bs, width = n - first < bs ? n - first : bs;
+    double *out = inv + (size_t)b * (size_t)bs * (size_t)bs;
+    int bad = 0;
+    for (int l = 0; l < bs; ++l)
+      sc[l] = l < width ? sqrt(diag[first + l]) : 1.0;
+    for (int k = 0; k < bs * bs; ++k)
+      f[k] = 0.0;
+    for (int l = 0; l < width; ++l)
+      for (int k = off[first + l]; k < off[first + l + 1]; ++k) {
+        const int c = col[k] - first;
+        if (c >= 0 && c < width)
+          f[l * bs + c] += val[k] / sc[l] / sc[c];
+      }
+    for (int row = 0; row < width; ++row) {
+      const double reciprocal = 1.0 / diag[first + row];
+      if (!isfinite(reciprocal) || reciprocal < 2.2250738585072014e-308)
+        bad = 1;
+      for (int c = 0; c <= row; ++c) {
+        const double x = f[row * bs + c], y = f[c * bs + row];
+        if (!isfinite(x) || !isfinite(y) ||
+            fabs(x - y) > 1e-12 * fmax(1.0, fmax(fabs(x), fabs(y))))
+          bad = 1;
+      }
+    }
+    for (int c = 0; c < width && !bad; ++c) {
+      double pivot = f[c * bs + c];
+      for (int k = 0; k < c; ++k)
+        pivot -= f[c * bs + k] * f[c * bs + k];
+      if (!(pivot > 0.0) || !isfinite(pivot)) {
+        bad = 1;
+        break;
+      }
+      f[c * bs + c] = sqrt(pivot);
+      for (int row = c + 1; row < width; ++row) {
+        double v = f[row * bs + c];
+        for (int k = 0; k < c; ++k)
+          v -= f[row * bs + k] * f[c * bs + k];
+        f[row * bs + c] = v / f[c * bs + c];
+      }
+    }
+    for (int l = 0; l < width && !bad; ++l) { /* column l of the inverse */
+      double *x = xs + (size_t)l * bs;
+      for (int row = 0; row < width; ++row) {
+        double v = row == l ? 1.0 : 0.0;
+        for (int k = 0; k < row; ++k)
+          v -= f[row * bs + k] * x[k];
+        x[row] = v / f[row * bs + row];
+      }
+      for (int row = width - 1; row >= 0; --row) {
+        double v = x[row];
+        for (int k = row + 1; k < width; ++k)
+          v -= f[k * bs + row] * x[k];
+        x[row] = v / f[row * bs + row];
+      }
+      for (int row = 0; row < width; ++row) {
+        x[row] = x[row] / sc[row] / sc[l];
+        if (!isfinite(x[row]))
+          bad = 1;
+      }
+    }
+    fallbacks += bad;
+    for (int l = 0; l < bs; ++l)
+      for (int row = 0; row < bs; ++row)
+        out[l * bs + row] = bad ? (row == 0 && l == 0 ? NAN : 0.0)
+                                : (row < width && l < width ? xs[(size_t)l * bs + row] : 0.0);
+  }
+  free(f);
+  free(xs);
+  free(sc);
+  if (fallback_blocks)
+    *fallback_blocks = fallbacks;
+  return OR_OK;
+}
+
+/* z_i = (M^-1 r)_i: the block inverse row (pcg_device.cuh:62-79) or the diagonal. */
+static double precond_row(int i, int n, const double *r, const double *diag, const double *inv,
+                          int use_inv, const double *blocks, int bs)
+{
+  if (blocks) {
+    const int first = i / bs * bs, width = n - first < bs ? n - first : bs;
+    const double *blk = blocks + (size_t)(i / bs) * (size_t)bs * (size_t)bs;
+    if (!isnan(blk[0])) {
+      double v = 0.0;
+      for (int j = 0; j < width; ++j)
+        v += blk[j * bs + i % bs] * r[first + j];
+      return v;
+    }
+  }
+  return use_inv ? r[i] * inv[i] : r[i] / diag[i];
+}
+
+int or_pcg_block(int32_t n, const int32_t *off, const int32_t *col, const double *val,
+                 const double *diag, const double *rhs, double tol, int32_t maxit,
+                 const double *blocks, int32_t bs, double *x, int32_t *iterations,
+                 double *residual_l2);
+
 int or_pcg(int32_t n, const int32_t *off, const int32_t *col, const double *val,
            const double *diag, const double *rhs, double tol, int32_t maxit, double *x,
            int32_t *iterations, double *residual_l2)
+{
+  if (g_precond_kind == 1 && n > 0) {
+    const int bs = g_block_size;
+    double *blocks = malloc(sizeof(double) * (size_t)((n + bs - 1) / bs) * bs * bs);
+    int fb = 0;
+    int st = or_block_jacobi(n, off, col, val, diag, bs, blocks, &fb);
+    if (st == OR_OK)
+      st = or_pcg_block(n, off, col, val, diag, rhs, tol, maxit, blocks, bs, x, iterations,
+                        residual_l2);
+    free(blocks);
+    return st;
+  }
+  return or_pcg_block(n, off, col, val, diag, rhs, tol, maxit, NULL, 0, x, iterations,
+                      residual_l2);
+}
+
+/* Deterministic PCG (pcg_kernels.cu:10-344) with the diagonal or a block-Jacobi
+ * preconditioner (blocks = or_block_jacobi output, or NULL). */
+int or_pcg_block(int32_t n, const int32_t *off, const int32_t *col, const double *val,
+                 const double *diag, const double *rhs, double tol, int32_t maxit,
+                 const double *blocks, int32_t bs, double *x, int32_t *iterations,
+                 double *residual_l2)
 {
   *iterations = 0;
   *residual_l2 = INFINITY;
@@ -940,7 +1083,7 @@ int or_pcg(int32_t n, const int32_t *off, const int32_t *col, const double *val,
   double *r = malloc(sizeof(double) * (size_t)n), *z = malloc(sizeof(double) * (size_t)n);
   double *p = malloc(sizeof(double) * (size_t)n), *q = malloc(sizeof(double) * (size_t)n);
   int status = OR_INTERNAL;
-#define PREC(i) (use_inv ? r[i] * inv[i] : r[i] / diag[i])
+#define PREC(i) precond_row(i, n, r, diag, inv, use_inv, blocks, bs)
   for (int i = 0; i < n; ++i)
     x[i] = 0.0;
   double scale = 0.0;
@@ -952,8 +1095,9 @@ int or_pcg(int32_t n, const int32_t *off, const int32_t *col, const double *val,
     goto done;
   }
   double rr0 = 0.0, rho = 0.0;
-  for (int i = 0; i < n; ++i) {
+  for (int i = 0; i < n; ++i)
     r[i] = rhs[i] / scale;
+  for (int i = 0; i < n; ++i) {
     z[i] = PREC(i);
     p[i] = z[i];
   }
@@ -987,6 +1131,8 @@ int or_pcg(int32_t n, const int32_t *off, const int32_t *col, const double *val,
       x[i] += alpha * p[i];
       r[i] -= alpha * q[i];
       rr += r[i] * r[i];
+    }
+    for (int i = 0; i < n; ++i) {
       z[i] = PREC(i);
       rz += r[i] * z[i];
     }

@@ -111,7 +111,25 @@ void or_system_copy(const or_system *s, int32_t *row_offsets, int32_t *columns, 
                     double *diagonal, double *rhs, int32_t *node_to_free, int8_t *node_sign,
                     double *boundary_values, double *circuit_sources /* [c * rows] signed */);
 
-/* Deterministic Jacobi PCG as run by DeterministicPcgKernel (pcg_kernels.cu:10-344). */
+/* Preconditioner used by or_pcg and the Newton drivers, like the reference's global
+ * selected_preconditioner (solvers/options.cpp:8): kind 0 Jacobi, 1 block-Jacobi with
+ * block_size rows per block (the reference's kJacobiBlockSize is 8). */
+void or_set_preconditioner(int32_t kind, int32_t block_size);
+
+/* Block-Jacobi inverses (block_jacobi_preconditioner.cu:72-167), blocks of bs rows:
+ * inv[(b * bs + j) * bs + i] = (block b)^-1 (i, j); unusable block: inv[b*bs*bs] = NaN. */
+int or_block_jacobi(int32_t n, const int32_t *row_offsets, const int32_t *columns,
+                    const double *values, const double *diagonal, int32_t bs, double *inv,
+                    int32_t *fallback_blocks);
+
+/* PCG with the diagonal (blocks == NULL) or block-Jacobi preconditioner. */
+int or_pcg_block(int32_t n, const int32_t *row_offsets, const int32_t *columns,
+                 const double *values, const double *diagonal, const double *rhs,
+                 double tolerance, int32_t max_iterations, const double *blocks, int32_t bs,
+                 double *x, int32_t *iterations, double *residual_l2);
+
+/* Deterministic PCG as run by DeterministicPcgKernel (pcg_kernels.cu:10-344) with the
+ * preconditioner chosen by or_set_preconditioner. */
 int or_pcg(int32_t n, const int32_t *row_offsets, const int32_t *columns, const double *values,
            const double *diagonal, const double *rhs, double tolerance, int32_t max_iterations,
            double *x, int32_t *iterations, double *residual_l2);

@@ -203,6 +203,54 @@ def pcg(system: System, rhs=None, tol=1e-10, maxit=16384):
     return status, x, its.value, res.value
 
 
+def set_preconditioner(kind=0, block_size=8):
+    """Preconditioner of pcg() and solve_batch(): 0 Jacobi, 1 block-Jacobi (block_size rows)."""
+    lib().or_set_preconditioner(C.c_int32(kind), C.c_int32(block_size))
+
+
+class preconditioner:
+    """with preconditioner(1, 8): ... -- block-Jacobi for the oracle calls inside."""
+
+    def __init__(self, kind, block_size=8):
+        self.kind, self.block_size = kind, block_size
+
+    def __enter__(self):
+        set_preconditioner(self.kind, self.block_size)
+
+    def __exit__(self, *exc):
+        set_preconditioner(0, 8)
+
+
+def block_jacobi(system: System, bs=8):
+    """Block inverses [blocks][bs*bs] (entry (i, j) at j*bs+i; NaN first entry = unusable)
+    and the count of unusable blocks."""
+    blocks = (system.rows + bs - 1) // bs
+    inv = np.zeros(blocks * bs * bs)
+    fb = C.c_int32(0)
+    st = lib().or_block_jacobi(C.c_int32(system.rows), _p(system.off), _p(system.col),
+                               _p(system.val), _p(system.diag), C.c_int32(bs), _p(inv), C.byref(fb))
+    if st:
+        raise RuntimeError(f"or_block_jacobi status {st}")
+    return inv.reshape(blocks, bs * bs), fb.value
+
+
+def csr_system(off, col, val, rhs=None):
+    """A System view of caller CSR arrays (diagonal taken from the entries)."""
+    sysm = System.__new__(System)
+    sysm.off = np.ascontiguousarray(off, dtype=np.int32)
+    sysm.col = np.ascontiguousarray(col, dtype=np.int32)
+    sysm.val = np.ascontiguousarray(val, dtype=np.float64)
+    sysm.rows = sysm.off.size - 1
+    diag = np.zeros(sysm.rows)
+    for r in range(sysm.rows):
+        for k in range(sysm.off[r], sysm.off[r + 1]):
+            if sysm.col[k] == r:
+                diag[r] = sysm.val[k]
+    sysm.diag = diag
+    sysm.rhs = None if rhs is None else np.ascontiguousarray(rhs, dtype=np.float64)
+    return sysm
+
+
 def solve_batch(model, currents, options=None, warm=None):
     """Reference Newton semantics for a batch of circuit-current vectors."""
     currents = np.ascontiguousarray(np.atleast_2d(currents), dtype=np.float64)

@@ -171,3 +171,14 @@ def test_device_calls_refuse_without_gpu_on_host_only_plan():
     with pytest.raises(fg.FgError) as err:
         plan.solve([[10.0]])
     assert err.value.status == fg.capi.GPU_UNAVAILABLE
+
+
+def test_preconditioner_options_are_validated():
+    model = meshes.square_linear(m=6)
+    for bs in (8, 32):
+        fg.Plan(model, preconditioner=1, block_size=bs, host_only=True)
+        fg.Plan(model, preconditioner=1, block_size=bs, precision=1, host_only=True)
+    for pre, bs in ((1, 16), (1, 0), (2, 8)):
+        with pytest.raises(fg.FgError) as e:
+            fg.Plan(model, preconditioner=pre, block_size=bs, host_only=True)
+        assert e.value.status == fg.capi.UNSUPPORTED_FEATURE
