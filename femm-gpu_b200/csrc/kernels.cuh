@@ -68,6 +68,15 @@ struct PcgArgs {
   int32_t skip_verification;
   uint32_t active_mask;
   long long timeout_ns;
+  // Reliable updates (FP32 storage only): values64 / b64 are the FP64 operator (same
+  // layout and strides as values) and right-hand side; the solution accumulates in x64 and
+  // is returned there (scaled back); the residual is replaced by the FP64 true residual
+  // whenever the recursive residual falls below reliable_delta times its largest value
+  // since the previous replacement, and acceptance is the FP64 true-residual rule.
+  int32_t reliable;
+  double reliable_delta;
+  const double *values64, *b64;
+  double *x64;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
   // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
   // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.
@@ -113,16 +122,11 @@ cudaError_t LaunchExtractCsr(const DevicePlan &p, int kp, int item, const double
 // Scatter CSR-ordered operator values into the SELL layout (item-major input).
 cudaError_t LaunchScatterCsr(const DevicePlan &p, int kp, int items, const double *csr_values,
                              int32_t values_per_item, double *values, cudaStream_t stream);
-// Mixed-precision form: FP32 copies of the assembled operator, the FP64 accumulation of
-// an FP32 correction, and the FP64 defect r = b - K x with its FP32 copy and norms.
+// Mixed-precision form: FP32 copies of the assembled operator values, diagonal and
+// inverse diagonal.
 cudaError_t LaunchToSingle(const DevicePlan &p, int kp, uint32_t mask, const double *val64,
                            const double *diag64, float *val32, float *diag32, float *invd32,
                            cudaStream_t stream);
-cudaError_t LaunchAccumulate(const DevicePlan &p, int kp, uint32_t mask, int first, const float *d,
-                             double *x, cudaStream_t stream);
-cudaError_t LaunchDefect(const DevicePlan &p, int kp, uint32_t mask, int zero_x, const double *val64,
-                         const double *b, const double *x, double *r, float *r32,
-                         double *partials, double *norms, cudaStream_t stream);
 // Interleave item-major vectors [items][len] into [len_pad][kp] and back.
 cudaError_t LaunchInterleave(int kp, int items, int len, int len_pad, const double *in, double *out,
                              cudaStream_t stream);

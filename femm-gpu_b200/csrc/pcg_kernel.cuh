@@ -53,7 +53,8 @@ struct Control {
   double rho[kMaxItems], alpha[kMaxItems], beta[kMaxItems], thr[kMaxItems], scale[kMaxItems];
   double resid[kMaxItems], rz[kMaxItems];
   int active[kMaxItems], restart[kMaxItems], status[kMaxItems], iters[kMaxItems];
-  int flag[kMaxItems]; // 1 threshold reached, 2 verified, 3 restart
+  int flag[kMaxItems]; // 1 threshold reached, 2 verified, 3 restart, 4 residual replaced
+  double rmax[kMaxItems]; // reliable updates: largest residual since the last replacement
 };
 
 struct Reduce {
@@ -94,6 +95,13 @@ template <typename T, int IV> __device__ __forceinline__ void Load(const T *p, T
     const double2 t = *reinterpret_cast<const double2 *>(p);
     o[0] = t.x;
     o[1] = t.y;
+  } else if constexpr (std::is_same_v<T, double> && IV == 4) {
+    const double2 t = *reinterpret_cast<const double2 *>(p);
+    const double2 u = *reinterpret_cast<const double2 *>(p + 2);
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = u.x;
+    o[3] = u.y;
   } else if constexpr (std::is_same_v<T, float> && IV == 4) {
     const float4 t = *reinterpret_cast<const float4 *>(p);
     o[0] = t.x;
@@ -115,6 +123,13 @@ template <typename T, int IV> __device__ __forceinline__ void LoadRO(const T *p,
     const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
     o[0] = t.x;
     o[1] = t.y;
+  } else if constexpr (std::is_same_v<T, double> && IV == 4) {
+    const double2 t = __ldg(reinterpret_cast<const double2 *>(p));
+    const double2 u = __ldg(reinterpret_cast<const double2 *>(p + 2));
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = u.x;
+    o[3] = u.y;
   } else if constexpr (std::is_same_v<T, float> && IV == 4) {
     const float4 t = __ldg(reinterpret_cast<const float4 *>(p));
     o[0] = t.x;
@@ -134,6 +149,9 @@ template <typename T, int IV> __device__ __forceinline__ void Store(T *p, const 
 {
   if constexpr (std::is_same_v<T, double> && IV == 2) {
     *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+  } else if constexpr (std::is_same_v<T, double> && IV == 4) {
+    *reinterpret_cast<double2 *>(p) = make_double2(v[0], v[1]);
+    *reinterpret_cast<double2 *>(p + 2) = make_double2(v[2], v[3]);
   } else if constexpr (std::is_same_v<T, float> && IV == 4) {
     *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
   } else if constexpr (std::is_same_v<T, float> && IV == 2) {
@@ -309,6 +327,49 @@ __device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int le
   }
 }
 
+// Reliable updates: one row of the FP64 product A64 (x64 + x32) for IV items, in CSR
+// order and FP64 arithmetic (the FP32 iterate is widened before it is added).
+template <int KP, int IV>
+__device__ __forceinline__ void RowProductReliable(const PcgArgs &a, size_t base, int len, int item0,
+                                                   const double *x64, const float *x32,
+                                                   double (&acc)[IV])
+{
+  const double *vals = a.values64;
+#pragma unroll
+  for (int j = 0; j < IV; ++j)
+    acc[j] = 0.0;
+  constexpr int U = 4;
+  for (int w0 = 0; w0 < len; w0 += U) {
+    int c[U];
+    double v[U][IV];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      c[u] = 0;
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        v[u][j] = 0.0;
+      if (w0 + u < len) {
+        const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
+        c[u] = __ldg(a.sell_col + pos);
+        LoadOperand<double, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (w0 + u < len) {
+        const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
+        double g[IV];
+        float h[IV];
+        Load<double, IV>(x64 + ci, g);
+        Load<float, IV>(x32 + ci, h);
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          acc[j] = __fma_rn(v[u][j], g[j] + static_cast<double>(h[j]), acc[j]);
+      }
+    }
+  }
+}
+
 template <typename T, int KP, int IV, int BS>
 __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 {
@@ -422,6 +483,83 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   };
   auto stage = [&](int s, const T (&v)[IV]) { Store<T, IV>(xb + (s * S + lane / LR) * KP + item0, v); };
 
+  // Reliable updates (FP32 storage only): the solution accumulates in FP64 (x64) and the
+  // residual is replaced by the FP64 true residual b/s - A64 (x64 + x) whenever the
+  // recursive residual has dropped by reliable_delta since the last replacement.
+  constexpr bool kFloat = std::is_same_v<T, float>;
+  const bool rel = kFloat && a.reliable != 0;
+  // The right-hand side in FP64: b64 when reliable, else the stored T values widened.
+  auto load_b = [&](size_t ri, double (&bd)[IV]) {
+    if (rel) {
+      Load<double, IV>(a.b64 + ri, bd);
+    } else {
+      T bb[IV];
+      Load<T, IV>(B + ri, bb);
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        bd[j] = static_cast<double>(bb[j]);
+    }
+  };
+  // Accept-phase update of this lane's iterate for flags f: with reliable updates x is
+  // folded into x64 (flags 2 and 4) and accepted items are scaled back in FP64; otherwise
+  // accepted items are scaled back in place.  bad[j] counts non-finite results.
+  auto settle_x = [&](size_t ri, const int (&f)[IV], const double (&sc)[IV], double (&bad)[IV]) {
+    T xv[IV];
+    Load<T, IV>(X + ri, xv);
+    if (rel) {
+      double xd[IV];
+      Load<double, IV>(a.x64 + ri, xd);
+#pragma unroll
+      for (int j = 0; j < IV; ++j) {
+        if (f[j] == 2 || f[j] == 4) {
+          xd[j] += static_cast<double>(xv[j]);
+          xv[j] = T(0);
+        }
+        if (f[j] == 2) {
+          xd[j] *= sc[j];
+          if (!isfinite(xd[j]))
+            bad[j] += 1.0;
+        }
+      }
+      Store<double, IV>(a.x64 + ri, xd);
+    } else {
+#pragma unroll
+      for (int j = 0; j < IV; ++j)
+        if (f[j] == 2) {
+          xv[j] = static_cast<T>(static_cast<double>(xv[j]) * sc[j]);
+          if (!isfinite(static_cast<double>(xv[j])))
+            bad[j] += 1.0;
+        }
+    }
+    Store<T, IV>(X + ri, xv);
+  };
+  // True residual of one row for IV items: b/s - A x in T arithmetic, or with reliable
+  // updates b64/s - A64 (x64 + x) in FP64.
+  auto true_residual = [&](int r, size_t ri, const double (&sc)[IV], double (&t)[IV]) {
+    const int len = __ldg(a.row_len + r);
+    const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+    double bd[IV];
+    load_b(ri, bd);
+    if constexpr (kFloat) {
+      if (rel) {
+        double acc[IV];
+        RowProductReliable<KP, IV>(a, base, len, item0, a.x64, X, acc);
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          t[j] = bd[j] / sc[j] - acc[j];
+        return;
+      }
+    }
+    const bool nofold[IV] = {};
+    const T nobeta[IV] = {};
+    T acc[IV];
+    RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      t[j] = bd[j] / sc[j] - static_cast<double>(acc[j]);
+  };
+
+
 #define FG_ROWS_BEGIN                                                                              \
   for (int ws = ws0 + warp; ws < ws1; ws += kPcgWarps) {                                           \
     const int r = ws * S + lane / LR;                                                              \
@@ -435,9 +573,14 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     for (int j = 0; j < IV; ++j)
       v[0][j] = v[1][j] = 0.0;
     FG_ROWS_BEGIN
-    T bb[IV], dd[IV];
-    Load<T, IV>(B + ri, bb);
+    T dd[IV];
+    double bb[IV];
+    load_b(ri, bb);
     LoadOperand<T, IV>(DG, static_cast<size_t>(r), a.diag_stride, a.diag_item, item0, dd);
+    if (rel) {
+      const double zd[IV] = {};
+      Store<double, IV>(a.x64 + ri, zd);
+    }
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       if (on(j) && r < a.n) {
@@ -486,13 +629,16 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     }
     if constexpr (BS == 0) {
       FG_ROWS_BEGIN
-      T bb[IV], rt[IV], zv[IV];
-      double rv[IV];
-      Load<T, IV>(B + ri, bb);
+      T rt[IV], zv[IV];
+      double bb[IV], rv[IV], re[IV];
+      load_b(ri, bb);
 #pragma unroll
       for (int j = 0; j < IV; ++j) {
-        rt[j] = static_cast<T>(static_cast<double>(bb[j]) / s[j]);
+        re[j] = bb[j] / s[j];
+        rt[j] = static_cast<T>(re[j]);
         rv[j] = rt[j];
+        if (!rel)
+          re[j] = rv[j];
       }
       precond(rv, r, zv);
       Store<T, IV>(R + ri, rt);
@@ -500,7 +646,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 #pragma unroll
       for (int j = 0; j < IV; ++j)
         if (on(j)) {
-          v[0][j] += rv[j] * rv[j];
+          v[0][j] += re[j] * re[j];
           v[1][j] += rv[j] * static_cast<double>(zv[j]);
         }
       FG_ROWS_END
@@ -509,11 +655,17 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 #pragma unroll
         for (int u = 0; u < SUB; ++u) {
           const size_t ri = static_cast<size_t>(sub_row(wu, u)) * KP + item0;
-          T bb[IV], rt[IV];
-          Load<T, IV>(B + ri, bb);
+          T rt[IV];
+          double bb[IV];
+          load_b(ri, bb);
 #pragma unroll
-          for (int j = 0; j < IV; ++j)
-            rt[j] = static_cast<T>(static_cast<double>(bb[j]) / s[j]);
+          for (int j = 0; j < IV; ++j) {
+            const double re = bb[j] / s[j];
+            rt[j] = static_cast<T>(re);
+            const double rr = rel ? re : static_cast<double>(rt[j]);
+            if (on(j))
+              v[0][j] += rr * rr;
+          }
           Store<T, IV>(R + ri, rt);
           stage(u, rt);
         }
@@ -526,10 +678,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
           Store<T, IV>(Z + static_cast<size_t>(sub_row(wu, u)) * KP + item0, zv);
 #pragma unroll
           for (int j = 0; j < IV; ++j)
-            if (on(j)) {
-              v[0][j] += rv[j] * rv[j];
+            if (on(j))
               v[1][j] += rv[j] * static_cast<double>(zv[j]);
-            }
         }
         __syncwarp();
       }
@@ -548,6 +698,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
           ctl.thr[it] = a.tolerance * sqrt(rr);
           ctl.rho[it] = rho;
           ctl.restart[it] = 1;
+          ctl.rmax[it] = sqrt(rr);
         }
       }
     }
@@ -752,10 +903,14 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
               ctl.status[it] = kNonfinite;
               ctl.active[it] = 0;
             } else if (ctl.resid[it] <= ctl.thr[it]) {
-              // The drop-in solve verifies the true residual; an inner solve of the
-              // mixed form accepts here (its FP64 caller checks the true residual).
-              ctl.flag[it] = a.skip_verification ? 2 : 1;
+              // The drop-in solve verifies the true residual; an inner solve whose caller
+              // checks the true residual may accept here.
+              ctl.flag[it] = a.skip_verification && !rel ? 2 : 1;
+            } else if (rel && ctl.resid[it] < a.reliable_delta * ctl.rmax[it]) {
+              ctl.flag[it] = 4;
             }
+            if (rel)
+              ctl.rmax[it] = fmax(ctl.rmax[it], ctl.resid[it]);
           }
         }
       }
@@ -765,7 +920,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     bool verify = false, accept = false;
 #pragma unroll
     for (int it = 0; it < KP; ++it) {
-      verify = verify || (ctl.active[it] && ctl.flag[it] == 1);
+      verify = verify || (ctl.active[it] && (ctl.flag[it] == 1 || (rel && ctl.flag[it] == 4)));
       accept = accept || (ctl.active[it] && ctl.flag[it] == 2);
     }
     if (verify) {
@@ -776,26 +931,22 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 #pragma unroll
       for (int j = 0; j < IV; ++j) {
         v[0][j] = 0.0;
-        mine[j] = on(j) && ctl.flag[item0 + j] == 1;
+        const int fl = ctl.flag[item0 + j];
+        mine[j] = on(j) && (fl == 1 || (rel && fl == 4));
         any_mine = any_mine || mine[j];
         s[j] = ctl.scale[item0 + j];
       }
       if (any_mine) {
-        const bool nofold[IV] = {};
-        const T nobeta[IV] = {};
         FG_ROWS_BEGIN
-        const int len = __ldg(a.row_len + r);
-        const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-        T acc[IV], bb[IV], rv[IV];
-        RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
-        Load<T, IV>(B + ri, bb);
+        T rv[IV];
+        double t[IV];
+        true_residual(r, ri, s, t);
         Load<T, IV>(R + ri, rv);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
           if (mine[j]) {
-            const double t = static_cast<double>(bb[j]) / s[j] - static_cast<double>(acc[j]);
-            rv[j] = static_cast<T>(t);
-            v[0][j] += t * t;
+            rv[j] = static_cast<T>(t[j]);
+            v[0][j] += t[j] * t[j];
           }
         Store<T, IV>(R + ri, rv);
         FG_ROWS_END
@@ -804,14 +955,18 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
-        if (ctl.active[it] && ctl.flag[it] == 1) {
+        if (ctl.active[it] && (ctl.flag[it] == 1 || (rel && ctl.flag[it] == 4))) {
           const double trr = sm.result[it];
           if (!isfinite(trr)) {
             ctl.status[it] = kNonfinite;
             ctl.active[it] = 0;
           } else {
+            // Reliable updates keep the search direction after a replacement; the
+            // drop-in solve restarts from the true residual as the reference does.
             ctl.resid[it] = sqrt(trr);
-            ctl.flag[it] = ctl.resid[it] <= ctl.thr[it] ? 2 : 3;
+            ctl.flag[it] = ctl.resid[it] <= ctl.thr[it] ? 2 : (rel ? 4 : 3);
+            if (rel)
+              ctl.rmax[it] = ctl.resid[it];
           }
         }
       }
@@ -843,33 +998,27 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 #pragma unroll
             for (int u = 0; u < SUB; ++u) {
               const size_t ri = static_cast<size_t>(sub_row(wu, u)) * KP + item0;
-              T xv[IV], zv[IV], zo[IV];
+              T zv[IV], zo[IV];
               double rd[IV];
-              Load<T, IV>(X + ri, xv);
+              settle_x(ri, f, s, v[1]);
               Load<T, IV>(Z + ri, zo);
               block_row(wu, u, rd, zv);
 #pragma unroll
               for (int j = 0; j < IV; ++j) {
-                if (f[j] == 2) {
-                  xv[j] = static_cast<T>(static_cast<double>(xv[j]) * s[j]);
-                  if (!isfinite(static_cast<double>(xv[j])))
-                    v[1][j] += 1.0;
-                }
-                if (f[j] == 3)
+                if (f[j] == 3 || f[j] == 4)
                   v[0][j] += rd[j] * static_cast<double>(zv[j]);
                 else
                   zv[j] = zo[j];
               }
-              Store<T, IV>(X + ri, xv);
               Store<T, IV>(Z + ri, zv);
             }
             __syncwarp();
           }
       } else if (any_mine) {
         FG_ROWS_BEGIN
-        T xv[IV], rv[IV], zv[IV], zo[IV];
+        T rv[IV], zv[IV], zo[IV];
         double rd[IV];
-        Load<T, IV>(X + ri, xv);
+        settle_x(ri, f, s, v[1]);
         Load<T, IV>(R + ri, rv);
         Load<T, IV>(Z + ri, zo);
 #pragma unroll
@@ -878,17 +1027,11 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         precond(rd, r, zv);
 #pragma unroll
         for (int j = 0; j < IV; ++j) {
-          if (f[j] == 2) {
-            xv[j] = static_cast<T>(static_cast<double>(xv[j]) * s[j]);
-            if (!isfinite(static_cast<double>(xv[j])))
-              v[1][j] += 1.0;
-          }
-          if (f[j] == 3)
+          if (f[j] == 3 || f[j] == 4)
             v[0][j] += rd[j] * static_cast<double>(zv[j]);
           else
             zv[j] = zo[j];
         }
-        Store<T, IV>(X + ri, xv);
         Store<T, IV>(Z + ri, zv);
         FG_ROWS_END
       }
@@ -913,13 +1056,15 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
             ctl.rho[it] = rho;
             ctl.restart[it] = 1;
           }
+        } else if (ctl.active[it] && ctl.flag[it] == 4) {
+          ctl.rz[it] = sm.result[it]; // r.z of the replaced residual; beta follows below
         }
       }
       __syncthreads();
     }
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
-      if (ctl.active[it] && ctl.flag[it] == 0) {
+      if (ctl.active[it] && (ctl.flag[it] == 0 || ctl.flag[it] == 4)) {
         const double rz = ctl.rz[it];
         if (!isfinite(rz) || !(rz > 0.0)) {
           ctl.status[it] = kBreakdown;
@@ -949,21 +1094,16 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         v[0][j] = 0.0;
         s[j] = ctl.scale[item0 + j];
       }
-      const bool nofold[IV] = {};
-      const T nobeta[IV] = {};
       FG_ROWS_BEGIN
-      const int len = __ldg(a.row_len + r);
-      const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-      T acc[IV], bb[IV], rv[IV];
-      RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
-      Load<T, IV>(B + ri, bb);
+      T rv[IV];
+      double t[IV];
+      true_residual(r, ri, s, t);
       Load<T, IV>(R + ri, rv);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
         if (on(j)) {
-          const double t = static_cast<double>(bb[j]) / s[j] - static_cast<double>(acc[j]);
-          rv[j] = static_cast<T>(t);
-          v[0][j] += t * t;
+          rv[j] = static_cast<T>(t[j]);
+          v[0][j] += t[j] * t[j];
         }
       Store<T, IV>(R + ri, rv);
       FG_ROWS_END
@@ -991,17 +1131,12 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         v[0][j] = 0.0;
         s[j] = ctl.scale[item0 + j];
       }
-      FG_ROWS_BEGIN
-      T xv[IV];
-      Load<T, IV>(X + ri, xv);
+      int f[IV];
 #pragma unroll
       for (int j = 0; j < IV; ++j)
-        if (on(j)) {
-          xv[j] = static_cast<T>(static_cast<double>(xv[j]) * s[j]);
-          if (!isfinite(static_cast<double>(xv[j])))
-            v[0][j] += 1.0;
-        }
-      Store<T, IV>(X + ri, xv);
+        f[j] = on(j) ? 2 : 0;
+      FG_ROWS_BEGIN
+      settle_x(ri, f, s, v[0]);
       FG_ROWS_END
       if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
         return;

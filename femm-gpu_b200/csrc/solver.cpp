@@ -234,15 +234,12 @@ Status Plan::EnsureWorkspace(int kp)
     FG_EN(v32_, static_cast<size_t>(h.positions) * kp);
     FG_EN(d32_, vec);
     FG_EN(i32_, vec);
-    FG_EN(b32_, vec);
     FG_EN(x32_, vec);
     FG_EN(r32_, vec);
     FG_EN(z32_, vec);
     FG_EN(p032_, vec);
     FG_EN(p132_, vec);
     FG_EN(q32_, vec);
-    FG_EN(defect_partials_, static_cast<size_t>(2) * kp * 256);
-    FG_EN(defect_norms_, static_cast<size_t>(2) * kp);
   }
 #undef FG_EN
   if (s != Status::kOk)
@@ -346,172 +343,115 @@ Status Plan::LinearSolve(int kp, int items, uint32_t mask, double tolerance, int
   return err ? Status::kInternalError : Status::kOk;
 }
 
-// FP32 PCG inside FP64 defect correction.  Each outer step solves K32 d = r32 to a
-// relative 1e-5 on the recursive residual, accumulates x += d in FP64 and recomputes the
-// FP64 defect; an item is done when ||b - K x|| <= tolerance ||b|| (the reference's
-// acceptance rule).  Items whose inner solve fails or that have not converged after
-// kMaxOuter steps are solved again by the FP64 PCG from x = 0.
+// FP32 PCG inside FP64 defect correction, as one launch with reliable updates: SpMV,
+// preconditioner and vectors in FP32 (dot products and scalars in FP64); the solution
+// accumulates in FP64 and the residual is replaced by the FP64 true residual
+// b - K x (FP64 operator) each time the recursive residual has fallen tenfold, keeping the
+// search direction, so the Krylov space is not rebuilt as it is by restarted refinement.
+// Acceptance is the reference's rule on the FP64 true residual.  Items the FP32 solve
+// cannot finish (breakdown, non-finite, iteration budget) are solved again by the FP64
+// PCG from x = 0.
 Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                         cudaStream_t st, double *linfo)
 {
-  constexpr int kMaxOuter = 8;
-  constexpr double kInnerTolerance = 1e-5;
-  for (int i = 0; i < items; ++i) {
-    linfo[3 * i] = ToInt(Status::kInternalError);
-    linfo[3 * i + 1] = 0;
-    linfo[3 * i + 2] = std::numeric_limits<double>::infinity();
-  }
-  if (!(tolerance > 0.0) || !(tolerance < 1.0) || !std::isfinite(tolerance) || max_iterations < 0) {
-    for (int i = 0; i < items; ++i)
-      linfo[3 * i] = ToInt(Status::kInvalidArgument);
-    return Status::kOk;
-  }
-  const size_t vec = static_cast<size_t>(host_.n_pad) * kp;
-  double *norms_h = small_.get() + 7 * kp; // spare room after the Newton summary
+  constexpr double kReliableDelta = 0.1;
   if (LaunchToSingle(dev_, kp, mask, values_.get(), diag_.get(), v32_.get(), d32_.get(), i32_.get(),
-                     st) != cudaSuccess ||
-      cudaMemsetAsync(x_.get(), 0, sizeof(double) * vec, st) != cudaSuccess ||
-      LaunchDefect(dev_, kp, mask, 1, values_.get(), rhs_.get(), x_.get(), r_.get(), b32_.get(),
-                   defect_partials_.get(), defect_norms_.get(), st) != cudaSuccess ||
-      cudaMemcpyAsync(norms_h, defect_norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                     st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 1;
+  Status s = BuildBlocks(kp, items, true, true, st);
+  if (s != Status::kOk)
+    return s;
+  PcgArgs a{};
+  a.precision = 1;
+  a.n = host_.n;
+  a.n_pad = host_.n_pad;
+  a.slices = host_.slices;
+  a.kp = kp;
+  a.items = items;
+  a.slice_off = slice_off_.get();
+  a.row_len = row_len_.get();
+  a.sell_col = sell_col_.get();
+  a.values = v32_.get();
+  a.value_stride = kp;
+  a.value_item = 1;
+  a.diag = d32_.get();
+  a.invd = i32_.get();
+  a.diag_stride = kp;
+  a.diag_item = 1;
+  a.use_inverse = 1;
+  if (block_size()) {
+    a.blocks = blocks32_.get();
+    a.block_size = block_size();
+    a.block_stride = kp;
+    a.block_item = 1;
+  }
+  a.b = nullptr;
+  a.x = x32_.get();
+  a.r = r32_.get();
+  a.z = z32_.get();
+  a.p0 = p032_.get();
+  a.p1 = p132_.get();
+  a.q = q32_.get();
+  a.reliable = 1;
+  a.reliable_delta = kReliableDelta;
+  a.values64 = values_.get();
+  a.b64 = rhs_.get();
+  a.x64 = x_.get();
+  a.partials = pcg_partials_.get();
+  a.barrier = barrier_.get();
+  a.error = error_.get();
+  a.info = pcg_info_.get();
+  a.tolerance = tolerance;
+  a.max_iterations = max_iterations;
+  a.active_mask = mask;
+  a.timeout_ns = 5000000000LL;
+  a.trace = trace_enabled_ ? trace_.get() : nullptr;
+  int grid = 0, block = 0;
+  if (LaunchPcg(a, &grid, &block, st) != cudaSuccess) {
+    cudaGetLastError();
+    return Status::kInternalError;
+  }
+  timing_.pcg_grid = grid;
+  timing_.pcg_block = block;
+  timing_.pcg_launches += 1;
+  timing_.kernel_launches += 1;
+  int32_t err = 0;
+  if (cudaMemcpyAsync(linfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
       cudaStreamSynchronize(st) != cudaSuccess)
     return Status::kInternalError;
-  timing_.kernel_launches += 3;
-  Status bs = BuildBlocks(kp, items, true, true, st);
-  if (bs != Status::kOk)
-    return bs;
-  std::vector<double> bnorm(kp, 0.0);
-  std::vector<int> its(kp, 0);
-  uint32_t pending = mask, fallback = 0;
+  if (err)
+    return Status::kInternalError;
+  uint32_t fallback = 0;
   for (int i = 0; i < items; ++i) {
     if (!((mask >> i) & 1u))
       continue;
-    bnorm[i] = std::sqrt(norms_h[kp + i]);
-    if (!std::isfinite(bnorm[i])) {
-      linfo[3 * i] = ToInt(Status::kNumericalNonfinite);
-      pending &= ~(1u << i);
-    } else if (bnorm[i] == 0.0) { // x = 0 is exact
-      linfo[3 * i] = ToInt(Status::kOk);
-      linfo[3 * i + 2] = 0.0;
-      pending &= ~(1u << i);
-    }
+    const int status = static_cast<int>(linfo[3 * i]);
+    if (status == ToInt(Status::kInvalidArgument))
+      continue;
+    if (status != ToInt(Status::kOk))
+      fallback |= 1u << i;
   }
-  for (int outer = 0; outer < kMaxOuter && pending; ++outer) {
-    PcgArgs a{};
-    a.precision = 1;
-    a.n = host_.n;
-    a.n_pad = host_.n_pad;
-    a.slices = host_.slices;
-    a.kp = kp;
-    a.items = items;
-    a.slice_off = slice_off_.get();
-    a.row_len = row_len_.get();
-    a.sell_col = sell_col_.get();
-    a.values = v32_.get();
-    a.value_stride = kp;
-    a.value_item = 1;
-    a.diag = d32_.get();
-    a.invd = i32_.get();
-    a.diag_stride = kp;
-    a.diag_item = 1;
-    a.use_inverse = 1;
-    if (block_size()) {
-      a.blocks = blocks32_.get();
-      a.block_size = block_size();
-      a.block_stride = kp;
-      a.block_item = 1;
-    }
-    a.b = b32_.get();
-    a.x = x32_.get();
-    a.r = r32_.get();
-    a.z = z32_.get();
-    a.p0 = p032_.get();
-    a.p1 = p132_.get();
-    a.q = q32_.get();
-    a.partials = pcg_partials_.get();
-    a.barrier = barrier_.get();
-    a.error = error_.get();
-    a.info = pcg_info_.get();
-    a.tolerance = kInnerTolerance;
-    a.max_iterations = max_iterations;
-    a.skip_verification = 1;
-    a.active_mask = pending;
-    a.timeout_ns = 5000000000LL;
-    a.trace = trace_enabled_ ? trace_.get() : nullptr;
-    int grid = 0, block = 0;
-    if (LaunchPcg(a, &grid, &block, st) != cudaSuccess) {
-      cudaGetLastError();
-      return Status::kInternalError;
-    }
-    timing_.pcg_grid = grid;
-    timing_.pcg_block = block;
-    timing_.pcg_launches += 1;
-    double inner[3 * kMaxItems];
-    int32_t err = 0;
-    if (cudaMemcpyAsync(inner, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return Status::kInternalError;
-    if (err)
-      return Status::kInternalError;
-    uint32_t good = 0;
-    for (int i = 0; i < items; ++i) {
-      if (!((pending >> i) & 1u))
-        continue;
-      its[i] += static_cast<int>(inner[3 * i + 1]);
-      if (static_cast<int>(inner[3 * i]) == ToInt(Status::kOk))
-        good |= 1u << i;
-      else
-        fallback |= 1u << i;
-    }
-    pending = good;
-    if (!pending)
-      break;
-    if (LaunchAccumulate(dev_, kp, pending, 0, x32_.get(), x_.get(), st) != cudaSuccess ||
-        LaunchDefect(dev_, kp, pending, 0, values_.get(), rhs_.get(), x_.get(), r_.get(), b32_.get(),
-                     defect_partials_.get(), defect_norms_.get(), st) != cudaSuccess ||
-        cudaMemcpyAsync(norms_h, defect_norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return Status::kInternalError;
-    timing_.kernel_launches += 3;
-    for (int i = 0; i < items; ++i) {
-      if (!((pending >> i) & 1u))
-        continue;
-      const double rn = std::sqrt(norms_h[i]);
-      linfo[3 * i + 2] = rn;
-      if (!std::isfinite(rn)) {
-        fallback |= 1u << i;
-        pending &= ~(1u << i);
-      } else if (rn <= tolerance * bnorm[i]) {
-        linfo[3 * i] = ToInt(Status::kOk);
-        pending &= ~(1u << i);
-      }
-    }
-  }
-  fallback |= pending;
-  for (int i = 0; i < items; ++i)
-    linfo[3 * i + 1] = its[i];
   if (fallback) {
-    Status s = BuildBlocks(kp, items, true, false, st);
-    if (s == Status::kOk)
-      s = RunPcg(kp, items, fallback, tolerance, max_iterations, kp, 1, kp, 1, 1, st,
-                 block_size() ? blocks64_.get() : nullptr);
-    if (s != Status::kOk)
+    double first[3 * kMaxItems];
+    std::copy(linfo, linfo + 3 * kp, first);
+    if ((s = BuildBlocks(kp, items, true, false, st)) != Status::kOk ||
+        (s = RunPcg(kp, items, fallback, tolerance, max_iterations, kp, 1, kp, 1, 1, st,
+                    block_size() ? blocks64_.get() : nullptr)) != Status::kOk)
       return s;
-    double f[3 * kMaxItems];
-    int32_t err = 0;
-    if (cudaMemcpyAsync(f, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(linfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
       return Status::kInternalError;
     if (err)
       return Status::kInternalError;
-    for (int i = 0; i < items; ++i)
-      if ((fallback >> i) & 1u) {
-        linfo[3 * i] = f[3 * i];
-        linfo[3 * i + 1] = its[i] + f[3 * i + 1];
-        linfo[3 * i + 2] = f[3 * i + 2];
-      }
+    for (int i = 0; i < items; ++i) {
+      if ((fallback >> i) & 1u)
+        linfo[3 * i + 1] += first[3 * i + 1];
+      else
+        std::copy(first + 3 * i, first + 3 * i + 3, linfo + 3 * i);
+    }
     timing_.mixed_fallbacks += __builtin_popcount(fallback);
   }
   return Status::kOk;
