@@ -1,6 +1,7 @@
 // capi.cpp -- the extern "C" boundary (include/femm_gpu.h).
 #include "femm_gpu.h"
 #include "solver.h"
+#include "warm.h"
 
 #include <algorithm>
 #include <cmath>
@@ -211,6 +212,140 @@ int fg_solve_batch(fg_plan *plan, int32_t items, const double *currents, const d
     return ToInt(Status::kInvalidArgument);
   return ToInt(plan->plan.SolveHost(items, currents, hc_scale, warm_a, *options, a_out, b1_out,
                                     b2_out, flux_out, info));
+}
+
+int fg_mlp_create(int32_t inputs, int32_t hidden, int32_t outputs, uint64_t seed, fg_mlp **mlp)
+{
+  if (!mlp)
+    return ToInt(Status::kInvalidArgument);
+  *mlp = nullptr;
+  auto *m = new (std::nothrow) fg_mlp;
+  if (!m)
+    return ToInt(Status::kInternalError);
+  const Status s = m->mlp.Create(inputs, hidden, outputs, seed);
+  if (s != Status::kOk) {
+    delete m;
+    return ToInt(s);
+  }
+  *mlp = m;
+  return 0;
+}
+
+void fg_mlp_destroy(fg_mlp *mlp) { delete mlp; }
+
+int64_t fg_mlp_parameter_count(const fg_mlp *mlp) { return mlp ? mlp->mlp.ParameterCount() : 0; }
+
+int fg_mlp_get_parameters(const fg_mlp *mlp, float *parameters)
+{
+  if (!mlp || !parameters)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(mlp->mlp.GetParameters(parameters));
+}
+
+int fg_mlp_set_parameters(fg_mlp *mlp, const float *parameters)
+{
+  if (!mlp || !parameters)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(mlp->mlp.SetParameters(parameters));
+}
+
+int fg_mlp_forward(fg_mlp *mlp, int32_t batch, const float *x, float *y)
+{
+  if (!mlp)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(mlp->mlp.Predict(batch, x, y));
+}
+
+int fg_mlp_loss_gradient(fg_mlp *mlp, int32_t batch, const float *x, const float *t, float *loss,
+                         float *gradient)
+{
+  if (!mlp)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(mlp->mlp.LossGradient(batch, x, t, loss, gradient));
+}
+
+int fg_mlp_train(fg_mlp *mlp, int32_t samples, const float *x, const float *t, int32_t epochs,
+                 int32_t batch, float learning_rate, uint64_t seed, float *final_loss)
+{
+  if (!mlp)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(mlp->mlp.Train(samples, x, t, epochs, batch, learning_rate, seed, final_loss));
+}
+
+int fg_warm_create(const fg_plan *plan, int32_t rank, const double *mean, const double *basis,
+                   fg_mlp *mlp, const float *feature_shift, const float *feature_scale,
+                   const double *coeff_shift, const double *coeff_scale, fg_warm **warm)
+{
+  if (!plan || !warm)
+    return ToInt(Status::kInvalidArgument);
+  *warm = nullptr;
+  auto *w = new (std::nothrow) fg_warm;
+  if (!w)
+    return ToInt(Status::kInternalError);
+  const Status s = w->warm.Create(plan->plan.host().N, rank, mean, basis, mlp ? &mlp->mlp : nullptr,
+                                  feature_shift, feature_scale, coeff_shift, coeff_scale);
+  if (s != Status::kOk) {
+    delete w;
+    return ToInt(s);
+  }
+  *warm = w;
+  return 0;
+}
+
+void fg_warm_destroy(fg_warm *warm) { delete warm; }
+
+int fg_warm_project(fg_warm *warm, int32_t k, const double *a, double *coeffs)
+{
+  if (!warm)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(warm->warm.Project(k, a, coeffs));
+}
+
+int fg_warm_project_device(fg_warm *warm, int32_t k, const double *a, double *coeffs, void *stream)
+{
+  if (!warm || !a || !coeffs)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(warm->warm.ProjectDevice(k, a, coeffs, static_cast<cudaStream_t>(stream)));
+}
+
+int fg_warm_predict(fg_warm *warm, int32_t k, const float *features, double *a)
+{
+  if (!warm)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(warm->warm.Predict(k, features, a));
+}
+
+int fg_solve_batch_learned(fg_plan *plan, fg_warm *warm, int32_t items, const double *currents,
+                           const double *hc_scale, const float *features,
+                           const fg_solve_options *options, double *a_out, double *b1_out,
+                           double *b2_out, double *flux_out, fg_item_info *info)
+{
+  if (!plan || !warm || !options || !features || !info || items <= 0 || warm->warm.inputs() == 0 ||
+      warm->warm.N() != plan->plan.host().N)
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostPlan &h = plan->plan.host();
+  const size_t N = h.N, E = h.E, C = h.C;
+  const int I = warm->warm.inputs();
+  Status s;
+  if ((s = warm->features.upload(features, static_cast<size_t>(items) * I)) != Status::kOk)
+    return ToInt(s);
+  // Warm starts are predicted chunk by chunk (kMaxItems items) into one reused buffer.
+  for (int first = 0; first < items; first += fg::kMaxItems) {
+    const int k = std::min(fg::kMaxItems, items - first);
+    if ((s = warm->starts.ensure(static_cast<size_t>(k) * N)) != Status::kOk ||
+        (s = warm->warm.PredictDevice(k, warm->features.get() + static_cast<size_t>(first) * I,
+                                      warm->starts.get(), nullptr)) != Status::kOk)
+      return ToInt(s);
+    s = plan->plan.SolveHost(k, currents ? currents + first * C : nullptr,
+                             hc_scale ? hc_scale + first : nullptr, nullptr, *options,
+                             a_out ? a_out + first * N : nullptr, b1_out ? b1_out + first * E : nullptr,
+                             b2_out ? b2_out + first * E : nullptr,
+                             flux_out ? flux_out + first * C : nullptr, info + first,
+                             warm->starts.get(), true);
+    if (s != Status::kOk)
+      return ToInt(s);
+  }
+  return 0;
 }
 
 int fg_solve_batch_device(fg_plan *plan, int32_t items, const double *currents,

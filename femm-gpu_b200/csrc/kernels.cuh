@@ -26,6 +26,7 @@ struct DevicePlan {
   const int32_t *mat_curve_off, *mat_curve_cnt, *mat_circuit;
   const double *curve_b, *curve_h, *curve_slope;
   const int32_t *node_to_free;
+  const int32_t *free_roots; // [n] root node of each free row
   const int8_t *node_sign;
   const double *boundary;
   const int32_t *circuit_elem_off, *circuit_elems;
@@ -62,6 +63,7 @@ struct PcgArgs {
   int32_t *error;
   double *info;       // [items][3]: status, iterations, residual
   double tolerance;
+  const double *item_tolerance; // optional per-item tolerance [items], overrides tolerance
   int32_t max_iterations;
   // 0: verify the true residual at the threshold (the reference's rule).  1: accept on
   // the recursive residual (inner solves whose caller checks the true residual).
@@ -110,8 +112,20 @@ cudaError_t LaunchNewtonNorms(const DevicePlan &p, int kp, const double *x, cons
                               double *partials, double *norms, cudaStream_t stream);
 cudaError_t LaunchNewtonUpdate(const DevicePlan &p, int kp, const double *x, double *state,
                                ItemScalars relax, uint32_t update_mask, cudaStream_t stream);
+// State = zero start (fixed values), or warm_item_major for items in warm_mask.
 cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm_item_major,
-                            int items, double *state, cudaStream_t stream);
+                            int items, uint32_t warm_mask, double *state, cudaStream_t stream);
+// x[row][kp] = state[root node of row][kp] (free-row form of a nodal state; padding 0).
+cudaError_t LaunchStateToFree(const DevicePlan &p, int kp, const double *state, double *x,
+                              cudaStream_t stream);
+// d = rhs - J x (d may be null) and norms[2][kp] = ||rhs - J x||^2, ||rhs||^2, for the
+// system J (values), rhs assembled at a state whose free-row form is x.
+cudaError_t LaunchEquationResidual(const DevicePlan &p, int kp, const double *values,
+                                   const double *rhs, const double *x, double *d,
+                                   double *partials, double *norms, cudaStream_t stream);
+// x = x0 + (item in mask ? delta : 0) over [n_pad][kp].
+cudaError_t LaunchAddCorrection(const DevicePlan &p, int kp, uint32_t mask, const double *x0,
+                                const double *delta, double *x, cudaStream_t stream);
 cudaError_t LaunchFinalize(const DevicePlan &p, int kp, int items, const double *state,
                            double *a_out, double *b1_out, double *b2_out, double *flux_out,
                            cudaStream_t stream);

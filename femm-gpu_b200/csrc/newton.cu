@@ -94,7 +94,7 @@ __global__ void UpdateKernel(DevicePlan p, const double *__restrict__ x, double 
 }
 
 __global__ void InitStateKernel(DevicePlan p, int kp, const double *__restrict__ warm, int items,
-                                double *__restrict__ state)
+                                uint32_t warm_mask, double *__restrict__ state)
 {
   const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= static_cast<size_t>(p.N) * kp)
@@ -103,9 +103,84 @@ __global__ void InitStateKernel(DevicePlan p, int kp, const double *__restrict__
   // Zero start with the expanded fixed values (nonlinear_solver.cu:193-209, :234-242);
   // a warm start replaces the free values and keeps the Dirichlet ones (:686-693).
   double v = p.boundary[node];
-  if (warm && item < items && p.node_to_free[node] >= 0)
+  if (warm && item < items && ((warm_mask >> item) & 1u) && p.node_to_free[node] >= 0)
     v = warm[static_cast<size_t>(item) * p.N + node];
   state[t] = v;
+}
+
+// Free-row form of a nodal state: the value of each row's root node (sign +1).
+template <int KP>
+__global__ void StateToFreeKernel(DevicePlan p, const double *__restrict__ state,
+                                  double *__restrict__ x)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.n_pad) * KP)
+    return;
+  const int r = static_cast<int>(t / KP), item = static_cast<int>(t % KP);
+  x[t] = r < p.n ? state[static_cast<size_t>(p.free_roots[r]) * KP + item] : 0.0;
+}
+
+// Defect of the Newton system assembled at a state with free-row form x: with the
+// Jacobian J = K + C and rhs = b + C A (the assembly's own right-hand side),
+// rhs - J x = b - K(A) A, the nonlinear residual at A.  Partials [2][KP][blocks]:
+// ||rhs - J x||^2, ||rhs||^2; d (optional) receives rhs - J x.
+template <int KP>
+__global__ void __launch_bounds__(kThreads)
+    EquationResidualKernel(DevicePlan p, const double *__restrict__ values,
+                           const double *__restrict__ rhs, const double *__restrict__ x,
+                           double *__restrict__ d, double *__restrict__ partials)
+{
+  __shared__ double red[kThreads / 32][2][KP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, item = lane % KP;
+  double rr = 0.0, bb = 0.0;
+  const size_t total = static_cast<size_t>(p.n_pad) * KP;
+  for (size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; t < total;
+       t += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int r = static_cast<int>(t / KP);
+    double e = 0.0, b = 0.0;
+    if (r < p.n) {
+      const size_t base = static_cast<size_t>(p.slice_off[r >> 5]) + (r & 31);
+      const int len = p.row_len[r];
+      double acc = 0.0;
+      for (int w = 0; w < len; ++w) {
+        const size_t pos = base + 32 * static_cast<size_t>(w);
+        acc = fma(values[pos * KP + item], x[static_cast<size_t>(p.sell_col[pos]) * KP + item], acc);
+      }
+      b = rhs[t];
+      e = b - acc;
+    }
+    if (d)
+      d[t] = e;
+    rr += e * e;
+    bb += b * b;
+  }
+  for (int off = 16; off >= KP; off >>= 1) {
+    rr += __shfl_xor_sync(0xffffffffu, rr, off);
+    bb += __shfl_xor_sync(0xffffffffu, bb, off);
+  }
+  if (lane < KP) {
+    red[warp][0][lane] = rr;
+    red[warp][1][lane] = bb;
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * KP) {
+    const int q = threadIdx.x / KP, it = threadIdx.x % KP;
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w)
+      s += red[w][q][it];
+    partials[(static_cast<size_t>(q) * KP + it) * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+template <int KP>
+__global__ void AddCorrectionKernel(int n_pad, uint32_t mask, const double *__restrict__ x0,
+                                    const double *__restrict__ delta, double *__restrict__ x)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(n_pad) * KP)
+    return;
+  const int item = static_cast<int>(t % KP);
+  x[t] = ((mask >> item) & 1u) ? x0[t] + delta[t] : x0[t];
 }
 
 template <bool kAxi>
@@ -246,9 +321,35 @@ cudaError_t LaunchNewtonUpdate(const DevicePlan &p, int kp, const double *x, dou
 }
 
 cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm, int items,
-                            double *state, cudaStream_t stream)
+                            uint32_t warm_mask, double *state, cudaStream_t stream)
 {
-  InitStateKernel<<<Blocks(static_cast<size_t>(p.N) * kp), kThreads, 0, stream>>>(p, kp, warm, items, state);
+  InitStateKernel<<<Blocks(static_cast<size_t>(p.N) * kp), kThreads, 0, stream>>>(p, kp, warm, items,
+                                                                                 warm_mask, state);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchStateToFree(const DevicePlan &p, int kp, const double *state, double *x,
+                              cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.n_pad) * kp);
+  FG_DISPATCH_KP(kp, (StateToFreeKernel<KP><<<blocks, kThreads, 0, stream>>>(p, state, x)));
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchEquationResidual(const DevicePlan &p, int kp, const double *values,
+                                   const double *rhs, const double *x, double *d,
+                                   double *partials, double *norms, cudaStream_t stream)
+{
+  FG_DISPATCH_KP(kp, (EquationResidualKernel<KP><<<kNormBlocks, kThreads, 0, stream>>>(p, values, rhs, x, d, partials)));
+  NormsFinalKernel<<<1, 1024, 0, stream>>>(kp, kNormBlocks, partials, norms);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchAddCorrection(const DevicePlan &p, int kp, uint32_t mask, const double *x0,
+                                const double *delta, double *x, cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.n_pad) * kp);
+  FG_DISPATCH_KP(kp, (AddCorrectionKernel<KP><<<blocks, kThreads, 0, stream>>>(p.n_pad, mask, x0, delta, x)));
   return cudaGetLastError();
 }
 

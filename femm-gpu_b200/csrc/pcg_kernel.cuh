@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
           ctl.active[it] = 0;
         } else {
           ctl.resid[it] = sqrt(rr);
-          ctl.thr[it] = a.tolerance * sqrt(rr);
+          ctl.thr[it] = (a.item_tolerance ? a.item_tolerance[it] : a.tolerance) * sqrt(rr);
           ctl.rho[it] = rho;
           ctl.restart[it] = 1;
           ctl.rmax[it] = sqrt(rr);

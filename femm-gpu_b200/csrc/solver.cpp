@@ -57,6 +57,7 @@ size_t Plan::DeviceBytes() const
   b += row_offsets_.bytes() + columns_.bytes() + row_len_.bytes() + slice_off_.bytes() +
        sell_col_.bytes() + contrib_off_.bytes() + contrib_.bytes() + rhs_off_.bytes() +
        rhs_contrib_.bytes() + elem_nodes_.bytes() + elem_mat_.bytes() + node_to_free_.bytes() +
+       free_roots_.bytes() +
        circuit_elem_off_.bytes() + circuit_elems_.bytes() + node_sign_.bytes() + pm_rhs_.bytes() +
        circuit_rhs_.bytes() + elem_geo_.bytes() + boundary_.bytes();
   b += state_.bytes() + ev_.bytes() + er_.bytes() + values_.bytes() + diag_.bytes() +
@@ -85,6 +86,7 @@ Status Plan::Create(HostModel model, const fg_plan_options &options)
   if (host_.E >= (1 << 27) || host_.positions > (int64_t(1) << 31) / kMaxItems)
     return Status::kUnsupportedFeature;
   host_only_ = (options_.flags & FG_PLAN_HOST_ONLY) != 0;
+  from_iterate_ = (options_.flags & FG_PLAN_PCG_FROM_ITERATE) != 0;
   if (host_only_)
     return Status::kOk;
   int devices = 0;
@@ -127,6 +129,7 @@ Status Plan::Upload()
   FG_UP(mat_curve_cnt_, h.mat_curve_cnt);
   FG_UP(mat_circuit_, h.mat_circuit);
   FG_UP(node_to_free_, h.dofs.node_to_free);
+  FG_UP(free_roots_, h.dofs.free_roots);
   FG_UP(circuit_elem_off_, h.circuit_elem_off);
   FG_UP(circuit_elems_, h.circuit_elems);
   FG_UP(node_sign_, h.dofs.node_sign);
@@ -181,6 +184,7 @@ Status Plan::Upload()
   d.curve_h = curve_h_.get();
   d.curve_slope = curve_slope_.get();
   d.node_to_free = node_to_free_.get();
+  d.free_roots = free_roots_.get();
   d.node_sign = node_sign_.get();
   d.boundary = boundary_.get();
   d.circuit_elem_off = circuit_elem_off_.get();
@@ -224,6 +228,9 @@ Status Plan::EnsureWorkspace(int kp)
   FG_EN(error_, 1);
   FG_EN(invalid_, static_cast<size_t>(kp));
   FG_EN(small_, static_cast<size_t>(10) * kp + 8);
+  FG_EN(x0_, vec);
+  FG_EN(d_, vec);
+  FG_EN(item_tol_, static_cast<size_t>(kp));
   if (block_size() > 0) {
     FG_EN(blocks64_, vec * block_size());
     FG_EN(block_fallbacks_, 1);
@@ -252,9 +259,11 @@ Status Plan::EnsureWorkspace(int kp)
 
 Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                     int value_stride, int value_item, int diag_stride, int diag_item,
-                    int use_inverse, cudaStream_t stream, const double *blocks)
+                    int use_inverse, cudaStream_t stream, const double *blocks, const double *b,
+                    const double *item_tol)
 {
   PcgArgs a{};
+  a.item_tolerance = item_tol;
   if (blocks) {
     a.blocks = blocks;
     a.block_size = block_size();
@@ -277,7 +286,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.diag_stride = diag_stride;
   a.diag_item = diag_item;
   a.use_inverse = use_inverse;
-  a.b = rhs_.get();
+  a.b = b ? b : rhs_.get();
   a.x = x_.get();
   a.r = r_.get();
   a.z = z_.get();
@@ -326,21 +335,72 @@ Status Plan::BuildBlocks(int kp, int items, bool per_item, bool single, cudaStre
 Status Plan::LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                          cudaStream_t stream, double *linfo)
 {
-  if (options_.precision == FG_PRECISION_MIXED)
-    return MixedSolve(kp, items, mask, tolerance, max_iterations, stream, linfo);
-  Status s = BuildBlocks(kp, items, true, false, stream);
-  if (s != Status::kOk)
-    return s;
-  s = RunPcg(kp, items, mask, tolerance, max_iterations, kp, 1, kp, 1, 1, stream,
-             block_size() ? blocks64_.get() : nullptr);
-  if (s != Status::kOk)
-    return s;
-  int32_t err = 0;
-  if (cudaMemcpyAsync(linfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-      cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess)
-    return Status::kInternalError;
-  return err ? Status::kInternalError : Status::kOk;
+  // From the iterate: solve J delta = d, d = rhs - J x0 (x0 = the current state's free
+  // values), to ||d - J delta|| <= tol ||rhs|| (per-item tolerance tol ||rhs|| / ||d||),
+  // then x = x0 + delta -- the reference's acceptance rule, a different starting point.
+  const double *b = rhs_.get();
+  const double *item_tol = nullptr;
+  uint32_t solve = mask;
+  double done[3 * kMaxItems];
+  if (from_iterate_) {
+    double *h = small_.get();
+    if (LaunchStateToFree(dev_, kp, state_.get(), x0_.get(), stream) != cudaSuccess ||
+        LaunchEquationResidual(dev_, kp, values_.get(), rhs_.get(), x0_.get(), d_.get(),
+                               norm_partials_.get(), norms_.get(), stream) != cudaSuccess ||
+        cudaMemcpyAsync(h, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+        cudaStreamSynchronize(stream) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 3;
+    std::vector<double> tol_i(kp, tolerance);
+    for (int i = 0; i < items; ++i) {
+      if (!((mask >> i) & 1u))
+        continue;
+      const double dn = std::sqrt(h[i]), bn = std::sqrt(h[kp + i]);
+      if (std::isfinite(dn) && std::isfinite(bn) && dn <= tolerance * bn) {
+        solve &= ~(1u << i); // the iterate already meets the linear tolerance
+        done[3 * i] = ToInt(Status::kOk);
+        done[3 * i + 1] = 0;
+        done[3 * i + 2] = dn;
+      } else if (std::isfinite(dn) && std::isfinite(bn) && dn > 0.0) {
+        tol_i[i] = tolerance * bn / dn;
+      }
+    }
+    Status s = item_tol_.upload(tol_i.data(), kp, stream);
+    if (s != Status::kOk)
+      return s;
+    b = d_.get();
+    item_tol = item_tol_.get();
+  }
+  if (solve) {
+    if (options_.precision == FG_PRECISION_MIXED) {
+      Status s = MixedSolve(kp, items, solve, tolerance, max_iterations, stream, linfo, b, item_tol);
+      if (s != Status::kOk)
+        return s;
+    } else {
+      Status s = BuildBlocks(kp, items, true, false, stream);
+      if (s == Status::kOk)
+        s = RunPcg(kp, items, solve, tolerance, max_iterations, kp, 1, kp, 1, 1, stream,
+                   block_size() ? blocks64_.get() : nullptr, b, item_tol);
+      if (s != Status::kOk)
+        return s;
+      int32_t err = 0;
+      if (cudaMemcpyAsync(linfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+          cudaStreamSynchronize(stream) != cudaSuccess)
+        return Status::kInternalError;
+      if (err)
+        return Status::kInternalError;
+    }
+  }
+  if (from_iterate_) {
+    if (LaunchAddCorrection(dev_, kp, solve, x0_.get(), x_.get(), x_.get(), stream) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 1;
+    for (int i = 0; i < items; ++i)
+      if (((mask >> i) & 1u) && !((solve >> i) & 1u))
+        std::copy(done + 3 * i, done + 3 * i + 3, linfo + 3 * i);
+  }
+  return Status::kOk;
 }
 
 // FP32 PCG inside FP64 defect correction, as one launch with reliable updates: SpMV,
@@ -352,7 +412,7 @@ Status Plan::LinearSolve(int kp, int items, uint32_t mask, double tolerance, int
 // cannot finish (breakdown, non-finite, iteration budget) are solved again by the FP64
 // PCG from x = 0.
 Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
-                        cudaStream_t st, double *linfo)
+                        cudaStream_t st, double *linfo, const double *b, const double *item_tol)
 {
   constexpr double kReliableDelta = 0.1;
   if (LaunchToSingle(dev_, kp, mask, values_.get(), diag_.get(), v32_.get(), d32_.get(), i32_.get(),
@@ -396,13 +456,14 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   a.reliable = 1;
   a.reliable_delta = kReliableDelta;
   a.values64 = values_.get();
-  a.b64 = rhs_.get();
+  a.b64 = b;
   a.x64 = x_.get();
   a.partials = pcg_partials_.get();
   a.barrier = barrier_.get();
   a.error = error_.get();
   a.info = pcg_info_.get();
   a.tolerance = tolerance;
+  a.item_tolerance = item_tol;
   a.max_iterations = max_iterations;
   a.active_mask = mask;
   a.timeout_ns = 5000000000LL;
@@ -438,7 +499,7 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
     std::copy(linfo, linfo + 3 * kp, first);
     if ((s = BuildBlocks(kp, items, true, false, st)) != Status::kOk ||
         (s = RunPcg(kp, items, fallback, tolerance, max_iterations, kp, 1, kp, 1, 1, st,
-                    block_size() ? blocks64_.get() : nullptr)) != Status::kOk)
+                    block_size() ? blocks64_.get() : nullptr, b, item_tol)) != Status::kOk)
       return s;
     if (cudaMemcpyAsync(linfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
@@ -536,7 +597,37 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
     }
   }
   const bool adaptive = o.adaptive_linear_tolerance != 0 && host_.has_nonlinear;
-  if (LaunchInitState(dev_, kp, warm, k, state_.get(), st) != cudaSuccess)
+  uint32_t warm_mask = warm ? active : 0u;
+  if (warm && req.guard_warm && active) {
+    // Equation residual ||K(A) A - b|| at the zero start and at the warm start; an item
+    // keeps its warm start only if the residual there is smaller.
+    double res[2][kMaxItems];
+    for (int pass = 0; pass < 2; ++pass) {
+      if (LaunchInitState(dev_, kp, warm, k, pass ? active : 0u, state_.get(), st) != cudaSuccess ||
+          cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) != cudaSuccess ||
+          LaunchElementKernel(dev_, kp, state_.get(), active, active, ev_.get(), er_.get(),
+                              invalid_.get(), st) != cudaSuccess ||
+          LaunchGatherValues(dev_, kp, ev_.get(), active, values_.get(), diag_.get(), invd_.get(),
+                             invalid_.get(), st) != cudaSuccess ||
+          LaunchGatherRhs(dev_, kp, er_.get(), currents, hc, active, rhs_.get(), st) != cudaSuccess ||
+          LaunchStateToFree(dev_, kp, state_.get(), x0_.get(), st) != cudaSuccess ||
+          LaunchEquationResidual(dev_, kp, values_.get(), rhs_.get(), x0_.get(), nullptr,
+                                 norm_partials_.get(), norms_.get(), st) != cudaSuccess ||
+          cudaMemcpyAsync(small_.get(), norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+          cudaStreamSynchronize(st) != cudaSuccess)
+        return Status::kInternalError;
+      timing_.kernel_launches += 8;
+      for (int i = 0; i < k; ++i)
+        res[pass][i] = std::sqrt(small_.get()[i]);
+    }
+    for (int i = 0; i < k; ++i)
+      if (((active >> i) & 1u) && !(res[1][i] < res[0][i]))
+        warm_mask &= ~(1u << i);
+  }
+  for (int i = 0; i < k; ++i)
+    if (warm)
+      req.info[first + i].warm_start = ((warm_mask >> i) & 1u) ? 1 : 2;
+  if (LaunchInitState(dev_, kp, warm, k, warm_mask, state_.get(), st) != cudaSuccess)
     return Status::kInternalError;
   timing_.kernel_launches += 1;
   std::vector<double> relax(k, 1.0), prev(k, std::numeric_limits<double>::infinity());
@@ -546,7 +637,9 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
     for (int i = 0; i < k; ++i)
       if ((active >> i) & 1u)
         tol = std::min(tol, NewtonLinearTolerance(o, adaptive, prev[i]));
-    const uint32_t newton_mask = (iteration > 0 || warm) ? active : 0u;
+    // Iteration 0 of a cold start uses the cold secant; a warm start is Newton from the
+    // first iteration (nonlinear_solver.cu:698).
+    const uint32_t newton_mask = iteration > 0 ? active : (active & warm_mask);
     cudaEventRecord(ev_start_, st);
     if (cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) != cudaSuccess ||
         LaunchElementKernel(dev_, kp, state_.get(), newton_mask, active, ev_.get(), er_.get(),
@@ -663,7 +756,8 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
 
 Status Plan::SolveHost(int items, const double *currents, const double *hc_scale,
                        const double *warm, const fg_solve_options &options, double *a_out,
-                       double *b1_out, double *b2_out, double *flux_out, fg_item_info *info)
+                       double *b1_out, double *b2_out, double *flux_out, fg_item_info *info,
+                       const double *warm_device, bool guard_warm)
 {
   if (host_only_)
     return Status::kGpuUnavailable;
@@ -686,7 +780,8 @@ Status Plan::SolveHost(int items, const double *currents, const double *hc_scale
   req.items = items;
   req.currents = in_currents_.get();
   req.hc_scale = hc_scale ? in_hc_.get() : nullptr;
-  req.warm = warm ? in_warm_.get() : nullptr;
+  req.warm = warm_device ? warm_device : (warm ? in_warm_.get() : nullptr);
+  req.guard_warm = guard_warm;
   req.options = options;
   req.a_out = a_out ? out_a_.get() : nullptr;
   req.b1_out = b1_out ? out_b1_.get() : nullptr;

@@ -22,6 +22,9 @@ struct SolveRequest {
   double *a_out = nullptr, *b1_out = nullptr, *b2_out = nullptr, *flux_out = nullptr; // device
   fg_item_info *info = nullptr;                                                        // host
   cudaStream_t stream = nullptr;
+  // Guarded warm start: an item starts from `warm` only if its equation residual there is
+  // below the zero start's, otherwise from the zero start (fg_item_info.warm_start = 2).
+  bool guard_warm = false;
 };
 
 class Plan
@@ -29,9 +32,12 @@ class Plan
 public:
   Status Create(HostModel model, const fg_plan_options &options);
   Status SolveDevice(const SolveRequest &request);
+  // Host buffers in and out.  warm_device (device [items * N], used instead of the host
+  // `warm`) and guard_warm serve the learned warm start.
   Status SolveHost(int items, const double *currents, const double *hc_scale, const double *warm,
                    const fg_solve_options &options, double *a_out, double *b1_out,
-                   double *b2_out, double *flux_out, fg_item_info *info);
+                   double *b2_out, double *flux_out, fg_item_info *info,
+                   const double *warm_device = nullptr, bool guard_warm = false);
   Status Assemble(int items, const double *states, const double *currents,
                   const int32_t *use_newton, double *values, double *diagonal, double *rhs);
   Status PcgSolve(int items, const double *values, int values_per_item, const double *rhs,
@@ -47,7 +53,8 @@ private:
   Status SolveChunk(const SolveRequest &request, int first, int count);
   Status RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                 int value_stride, int value_item, int diag_stride, int diag_item, int use_inverse,
-                cudaStream_t stream, const double *blocks = nullptr);
+                cudaStream_t stream, const double *blocks = nullptr, const double *b = nullptr,
+                const double *item_tol = nullptr);
   // Block-Jacobi inverses of the current operators (values_, diag_) into blocks64_ or
   // blocks32_; no-op for the Jacobi preconditioner.
   Status BuildBlocks(int kp, int items, bool per_item, bool single, cudaStream_t stream);
@@ -60,7 +67,7 @@ private:
   Status LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                      cudaStream_t stream, double *linfo);
   Status MixedSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
-                    cudaStream_t stream, double *linfo);
+                    cudaStream_t stream, double *linfo, const double *b, const double *item_tol);
 
   HostModel model_;
   HostPlan host_;
@@ -69,13 +76,14 @@ private:
   fg_timing timing_{};
   int kp_cap_ = 0;
   bool host_only_ = false;
+  bool from_iterate_ = false; // FG_PLAN_PCG_FROM_ITERATE
   int pcg_grid_cap_ = 0;
   int chunk_cap_ = kMaxItems; // items per batched launch
 
   // Plan constants on the device.
   DeviceArray<int32_t> row_offsets_, columns_, row_len_, slice_off_, sell_col_, contrib_off_,
       contrib_, rhs_off_, rhs_contrib_, elem_nodes_, elem_mat_, mat_curve_off_, mat_curve_cnt_,
-      mat_circuit_, node_to_free_, circuit_elem_off_, circuit_elems_;
+      mat_circuit_, node_to_free_, free_roots_, circuit_elem_off_, circuit_elems_;
   DeviceArray<int8_t> node_sign_;
   DeviceArray<double> pm_rhs_, circuit_rhs_, elem_geo_, mat_nu0_, mat_alpha_, mat_cold_, mat_jpa_,
       curve_b_, curve_h_, curve_slope_, boundary_;
@@ -88,6 +96,8 @@ private:
   DeviceArray<double> blocks64_;
   DeviceArray<float> blocks32_;
   DeviceArray<int32_t> block_fallbacks_;
+  // PCG from the iterate: free-row state x0, defect d, per-item tolerances.
+  DeviceArray<double> x0_, d_, item_tol_;
   DeviceArray<unsigned> barrier_;
   DeviceArray<unsigned long long> trace_;
   bool trace_enabled_ = false;

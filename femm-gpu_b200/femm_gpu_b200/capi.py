@@ -30,11 +30,18 @@ STATUS_NAMES = [
  LINEAR_SOLVE_BREAKDOWN, NUMERICAL_NONFINITE, OUTPUT_IO, INTERNAL_ERROR,
  NONLINEAR_SOLVE_NOT_CONVERGED, INVALID_MATERIAL) = range(16)
 
+PLAN_HOST_ONLY = 1
+PLAN_PCG_FROM_ITERATE = 2
+
 EXPORTED = [
     "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
     "fg_plan_destroy", "fg_plan_sizes_get", "fg_plan_symbolic", "fg_assemble", "fg_pcg_solve",
     "fg_csr_pcg", "fg_solve_batch", "fg_solve_batch_device", "fg_plan_last_timing",
     "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_csr_pcg_noalloc",
+    "fg_mlp_create", "fg_mlp_destroy", "fg_mlp_parameter_count", "fg_mlp_get_parameters",
+    "fg_mlp_set_parameters", "fg_mlp_forward", "fg_mlp_loss_gradient", "fg_mlp_train",
+    "fg_warm_create", "fg_warm_destroy", "fg_warm_project", "fg_warm_project_device",
+    "fg_warm_predict", "fg_solve_batch_learned",
 ]
 
 
@@ -64,7 +71,7 @@ class FgModel(C.Structure):
 
 class FgPlanOptions(C.Structure):
     _fields_ = [("preconditioner", C.c_int32), ("block_size", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32)]
+                ("precision", C.c_int32), ("flags", C.c_int32)]
 
 
 class FgSolveOptions(C.Structure):
@@ -75,7 +82,7 @@ class FgSolveOptions(C.Structure):
 
 class FgItemInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_int32), ("residual_l2", C.c_double),
-                ("linear_iterations", C.c_int32), ("reserved", C.c_int32),
+                ("linear_iterations", C.c_int32), ("warm_start", C.c_int32),
                 ("last_linear_tolerance", C.c_double),
                 ("verified_equation_residual_relative", C.c_double)]
 
@@ -117,6 +124,9 @@ def lib():
             raise RuntimeError(f"libfemmgpu.so not found at {LIB_PATH}")
         _LIB = C.CDLL(LIB_PATH)
         _LIB.fg_status_name.restype = C.c_char_p
+        _LIB.fg_mlp_parameter_count.restype = C.c_int64
+        _LIB.fg_mlp_destroy.restype = None
+        _LIB.fg_warm_destroy.restype = None
     return _LIB
 
 
@@ -159,7 +169,7 @@ class Plan:
     """A device-resident model: fg_plan_create ... fg_plan_destroy."""
 
     def __init__(self, model: Model, preconditioner: int = 0, block_size: int = 8,
-                 precision: int = 0, host_only: bool = False):
+                 precision: int = 0, host_only: bool = False, from_iterate: bool = False):
         self.model = model
         L = lib()
         self._keep = []
@@ -184,7 +194,8 @@ class Plan:
             constraint_count=int(model.con_a.size), constraint_nodes=_p(con),
             constraint_signs=_p(model.con_sign), circuit_count=model.circuit_count,
             depth_m=model.depth_m)
-        opts = FgPlanOptions(preconditioner, block_size, precision, 1 if host_only else 0)
+        flags = (PLAN_HOST_ONLY if host_only else 0) | (PLAN_PCG_FROM_ITERATE if from_iterate else 0)
+        opts = FgPlanOptions(preconditioner, block_size, precision, flags)
         self._h = C.c_void_p()
         status = L.fg_plan_create(C.byref(fm), C.byref(opts), C.byref(self._h))
         if status != 0:
@@ -267,9 +278,10 @@ class Plan:
         hc = None if hc_scale is None else np.ascontiguousarray(hc_scale, np.float64)
         wm = None if warm is None else np.ascontiguousarray(warm, np.float64).reshape(k, self.N)
         opts = options if options is not None else production_options()
+        # outputs: True (A, B, flux), "a" (A and flux only) or False (item info only)
         a = np.zeros((k, self.N)) if outputs else None
-        b1 = np.zeros((k, self.E)) if outputs else None
-        b2 = np.zeros((k, self.E)) if outputs else None
+        b1 = np.zeros((k, self.E)) if outputs is True else None
+        b2 = np.zeros((k, self.E)) if outputs is True else None
         flux = np.zeros((k, max(self.C, 1))) if outputs else None
         info = (FgItemInfo * k)()
         status = lib().fg_solve_batch(self._h, C.c_int32(k), _p(currents), _p(hc), _p(wm),

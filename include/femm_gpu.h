@@ -104,7 +104,12 @@ typedef struct fg_plan_options {
 
 /* fg_plan_options.flags: a host-only plan needs no GPU; it answers the topology and
  * introspection calls, and every device call on it returns FG_GPU_UNAVAILABLE. */
-enum { FG_PLAN_HOST_ONLY = 1 };
+/* FG_PLAN_PCG_FROM_ITERATE (no counterpart in the reference, whose inner PCG starts every
+ * Newton solve from x = 0): the inner PCG solves for the correction from the current
+ * Newton iterate, J delta = rhs - J x0, to ||rhs - J (x0 + delta)|| <= tol ||rhs|| -- the
+ * same acceptance rule from a better starting point, so a good iterate or warm start
+ * costs fewer PCG iterations. */
+enum { FG_PLAN_HOST_ONLY = 1, FG_PLAN_PCG_FROM_ITERATE = 2 };
 
 /* NonlinearOptions (gpu_solver/src/physics/nonlinear_model.h:102-109). */
 typedef struct fg_solve_options {
@@ -122,7 +127,10 @@ typedef struct fg_item_info {
   int32_t iterations;  /* Newton iterations */
   double residual_l2;  /* last relative Newton step */
   int32_t linear_iterations;
-  int32_t reserved;
+  /* 0 zero start; 1 started from the supplied warm start; 2 warm start supplied but
+   * rejected by the learned-warm-start guard (its equation residual was not below the
+   * zero start's), zero start used. */
+  int32_t warm_start;
   double last_linear_tolerance;
   double verified_equation_residual_relative;
 } fg_item_info;
@@ -268,6 +276,57 @@ int fg_bh_build(int32_t count, double *b, double *h, double *slope, double *cold
                 int32_t *smoothing_passes);
 void fg_bh_eval(int32_t count, const double *b, const double *h, const double *slope,
                 double field_b, double *h_dh_nu_dnu);
+
+/* ------------------------------------------------------------------------------------
+ * Learned warm start (no counterpart in the reference).  A reduced basis of A (mean +
+ * rank orthonormal modes) whose coefficients a small MLP predicts from per-sample
+ * features (circuit currents and magnet-angle terms, normalised by the caller's shift and
+ * scale).  The network is trained and evaluated by this library's own kernels in FP32;
+ * the basis and the warm start are FP64.  The Newton solve starts from the prediction only
+ * where its equation residual ||K(A) A - b|| is below the zero start's, and always finishes
+ * at the unchanged tolerances.
+ * ------------------------------------------------------------------------------------ */
+typedef struct fg_mlp fg_mlp;
+typedef struct fg_warm fg_warm;
+
+/* MLP inputs -> hidden -> hidden -> outputs, exact-erf GELU after each hidden layer,
+ * seeded uniform(+-1/sqrt(fan_in)) initialisation.  Parameter vector layout (FP32):
+ * W1[hidden][inputs], b1[hidden], W2[hidden][hidden], b2[hidden], W3[outputs][hidden],
+ * b3[outputs]. */
+int fg_mlp_create(int32_t inputs, int32_t hidden, int32_t outputs, uint64_t seed, fg_mlp **mlp);
+void fg_mlp_destroy(fg_mlp *mlp);
+int64_t fg_mlp_parameter_count(const fg_mlp *mlp);
+int fg_mlp_get_parameters(const fg_mlp *mlp, float *parameters);
+int fg_mlp_set_parameters(fg_mlp *mlp, const float *parameters);
+/* y [batch][outputs] = f(x [batch][inputs]); host arrays. */
+int fg_mlp_forward(fg_mlp *mlp, int32_t batch, const float *x, float *y);
+/* loss = 0.5 / batch * sum (f(x) - t)^2 and d loss / d parameters (parameter layout). */
+int fg_mlp_loss_gradient(fg_mlp *mlp, int32_t batch, const float *x, const float *t, float *loss,
+                         float *gradient);
+/* Adam (beta 0.9 / 0.999, eps 1e-8) over `epochs` seeded shuffles of (x, t) in minibatches
+ * of `batch` rows; *final_loss = the loss over all samples afterwards. */
+int fg_mlp_train(fg_mlp *mlp, int32_t samples, const float *x, const float *t, int32_t epochs,
+                 int32_t batch, float learning_rate, uint64_t seed, float *final_loss);
+
+/* mean [N] and basis [rank][N] of the plan's nodal A; mlp (borrowed, outputs == rank) may
+ * be NULL for a projection-only model.  feature_shift / feature_scale [mlp inputs],
+ * coeff_shift / coeff_scale [rank]: coefficients = coeff_shift + coeff_scale * f(x),
+ * x = (features - feature_shift) / feature_scale. */
+int fg_warm_create(const fg_plan *plan, int32_t rank, const double *mean, const double *basis,
+                   fg_mlp *mlp, const float *feature_shift, const float *feature_scale,
+                   const double *coeff_shift, const double *coeff_scale, fg_warm **warm);
+void fg_warm_destroy(fg_warm *warm);
+/* coeffs [k][rank] = basis (a [k][N] - mean); host arrays, or device arrays on `stream`. */
+int fg_warm_project(fg_warm *warm, int32_t k, const double *a, double *coeffs);
+int fg_warm_project_device(fg_warm *warm, int32_t k, const double *a, double *coeffs, void *stream);
+/* Predicted warm starts a [k][N] from features [k][inputs]; host arrays. */
+int fg_warm_predict(fg_warm *warm, int32_t k, const float *features, double *a);
+/* fg_solve_batch from the learned warm start of each item (features [items][inputs]),
+ * guarded as described above; info[i].warm_start tells which start each item used. */
+int fg_solve_batch_learned(fg_plan *plan, fg_warm *warm, int32_t items, const double *currents,
+                           const double *hc_scale, const float *features,
+                           const fg_solve_options *options, double *a_out, double *b1_out,
+                           double *b2_out, double *flux_out, fg_item_info *info);
 
 #ifdef __cplusplus
 }
