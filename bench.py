@@ -16,6 +16,12 @@ Arms:
                     oracle/_ref) on all host threads; each step = one Newton iteration of
                     one sample per thread, samples restarted as they converge.
 
+Forms (N = 1, rank 0; skipped with --no-forms): the same samples through block-Jacobi,
+the FP32-inner mixed PCG (reliable updates) and the PCG started from the Newton iterate,
+each with solves/s, iterations and its error against the plain FP64 solutions; and the
+learned warm start on the axisymmetric plunger (about 100k nodes; --learned-train training
+solves, 256 held-out samples) against the plain zero start.
+
 Multi-GPU: replicas only -- every rank solves its own batch, no collective on the data
 path; ``value`` = all ranks' solves / max-over-ranks time (weak scaling).
 """
@@ -47,6 +53,9 @@ def parse():
     p.add_argument("--items", type=int, default=8, help="samples per batched solve")
     p.add_argument("--mesh", type=int, default=MESH_M)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-forms", action="store_true", help="skip the mixed / block / learned forms")
+    p.add_argument("--no-learned", action="store_true", help="skip the learned warm start form")
+    p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
     return p.parse_args()
 
 
@@ -258,6 +267,8 @@ def run_ours(args, world, rank, local):
         "statuses_ok": sum(1 for s in statuses if s == 0), "statuses_total": len(statuses),
         "clocks": clocks.summary(),
     }
+    if rank == 0 and world == 1 and not args.no_forms:
+        line["forms"] = run_forms(args, model, plan, dev, stream, flush, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(model, items_seed=4242)
     if world > 1:
@@ -265,6 +276,117 @@ def run_ours(args, world, rank, local):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def time_device(plan, k, inputs, steps, warmup, dev, stream, flush):
+    """Device-timed batched solves (CUDA events on the launching stream, L2 flushed
+    between steps); returns solves/s, per-item info of the timed steps and their A."""
+    import torch
+
+    N, E, Cc = plan.N, plan.E, plan.C
+    out_a = torch.empty((k, N), dtype=torch.float64, device=dev)
+    out_f = torch.empty((k, Cc), dtype=torch.float64, device=dev)
+    opts = None
+    infos, a_all, f_all = [], [], []
+    ms = 0.0
+    for s in range(warmup + steps):
+        if s >= warmup:
+            flush.fill_(float(s))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        info = plan.solve_device(k, inputs[s].data_ptr(), options=opts, a_ptr=out_a.data_ptr(),
+                                 flux_ptr=out_f.data_ptr(), stream=stream.cuda_stream)
+        if s >= warmup:
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            infos += info
+            a_all.append(out_a.cpu().numpy())
+            f_all.append(out_f.cpu().numpy())
+    return k * steps / (ms / 1e3), infos, np.concatenate(a_all), np.concatenate(f_all)
+
+
+def run_forms(args, model, plan, dev, stream, flush, plain_value):
+    """The three forms beside the plain FP64 method, at the same Newton and PCG gates:
+    block-Jacobi, FP32-inner mixed precision (reliable updates) and the PCG started from the
+    Newton iterate on the nonlinear planar workload; the learned warm start on the
+    axisymmetric plunger (about 100k nodes), trained on FP64 solves of the plain method.
+    Errors are relative 2-norms against the plain FP64 solutions of the same samples."""
+    import torch
+
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import learned, meshes
+
+    k, Cc = args.items, plan.C
+    steps, warmup = 3, 1
+    inputs = [torch.tensor(meshes.seeded_currents(k, Cc, 20.0, seed=555000 + s), device=dev)
+              for s in range(warmup + steps)]
+    ref_v, ref_info, ref_a, ref_f = time_device(plan, k, inputs, steps, warmup, dev, stream, flush)
+
+    def err(a, b):
+        return float(max(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i]) for i in range(len(b))))
+
+    out = {"workload": "nonlinear planar solve (as value), same samples",
+           "fp64_jacobi": {"solves_per_s": ref_v,
+                           "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in ref_info]))}}
+    for name, kw in (("fp64_block8", dict(preconditioner=1, block_size=8)),
+                     ("mixed_jacobi", dict(precision=1)),
+                     ("mixed_block8", dict(precision=1, preconditioner=1, block_size=8)),
+                     ("mixed_block8_from_iterate", dict(precision=1, preconditioner=1, block_size=8,
+                                                        from_iterate=True))):
+        p = fg.Plan(model, **kw)
+        v, info, a, f = time_device(p, k, inputs, steps, warmup, dev, stream, flush)
+        out[name] = {"solves_per_s": v, "vs_fp64_jacobi": v / ref_v,
+                     "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in info])),
+                     "newton_iterations_per_item": float(np.mean([i.iterations for i in info])),
+                     "a_rel_err": err(a, ref_a), "flux_rel_err": err(f, ref_f),
+                     "all_converged": all(i.status == 0 for i in info)}
+        p.close()
+    if not args.no_learned:
+        ax = meshes.axisymmetric_plunger()
+        base = fg.Plan(ax)
+        ntrain, nheld = args.learned_train, 256
+        train = np.random.default_rng(2024).uniform(-30, 30, size=(ntrain, 2))
+        held = np.random.default_rng(2025).uniform(-30, 30, size=(nheld, 2))
+        t0 = time.perf_counter()
+        ws = learned.LearnedWarmStart(base, current_scale=30.0, rank=64, hidden=256, seed=1)
+        ws.fit(train, pod_samples=min(512, ntrain), epochs=200, batch=256, lr=2e-3)
+        fit_s = time.perf_counter() - t0
+        fast = fg.Plan(ax, precision=1, preconditioner=1, block_size=8, from_iterate=True)
+        w = ws.warm
+        lw = learned.LearnedWarmStart(fast, 30.0)
+        lw.warm = learned.WarmModel(fast, w.mean, w.basis, ws.mlp, *w._keep)
+        res = {}
+        for name, fn in (("fp64_jacobi_zero_start", lambda c: base.solve(c, outputs="a")),
+                         ("learned_mixed_block8_from_iterate", lambda c: lw.solve(c, outputs="a"))):
+            fn(held[:32])
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rs = [fn(held[i:i + 32]) for i in range(0, nheld, 32)]
+            dt = time.perf_counter() - t0
+            info = [i for r in rs for i in r.info]
+            res[name] = {"solves_per_s_e2e": nheld / dt,
+                         "newton_iterations_per_item": float(np.mean([i.iterations for i in info])),
+                         "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in info])),
+                         "warm_starts_used": int(sum(i.warm_start == 1 for i in info)),
+                         "all_converged": all(i.status == 0 for i in info),
+                         "a": np.concatenate([r.a for r in rs]), "flux": np.concatenate([r.flux for r in rs])}
+        z, l = res["fp64_jacobi_zero_start"], res["learned_mixed_block8_from_iterate"]
+        l["a_rel_err"] = err(l["a"], z["a"])
+        l["flux_rel_err"] = err(l["flux"], z["flux"])
+        l["vs_fp64_zero_start"] = l["solves_per_s_e2e"] / z["solves_per_s_e2e"]
+        for r in res.values():
+            r.pop("a")
+            r.pop("flux")
+        out["learned_warm_start"] = dict(
+            workload=f"axisymmetric plunger r-z, {ax.node_count} nodes, 2 coils U[-30,30] A; "
+                     f"{ntrain} training solves, {nheld} held-out samples; host-buffer API timing",
+            fit_seconds=fit_s, pod_energy=float(ws.stats["pod_energy"]),
+            final_loss=float(ws.stats["final_loss"]), **res)
+        fast.close()
+        base.close()
+    return out
 
 
 def run_reference(args, world, rank, local):
