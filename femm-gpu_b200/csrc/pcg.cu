@@ -2,6 +2,8 @@
 // (kernel template in pcg_kernel.cuh; instantiations in pcg_f64*.cu / pcg_f32*.cu).
 #include "kernels.cuh"
 
+#include <cstdlib>
+
 namespace fg
 {
 
@@ -56,6 +58,20 @@ int KernelGrid(const void *kernel, size_t smem)
   return sms * (per_sm < 2 ? per_sm : 2);
 }
 
+// Dynamic shared memory a launch may use for staging plus the column cache: two CTAs of
+// 512 threads per SM must stay resident (228 KB per SM, about 12 KB static per CTA).
+constexpr size_t kColumnCacheBudget = 100 * 1024;
+
+// FG_PCG_COL_CACHE=0 in the environment turns the column cache off (for A/B timing).
+bool ColumnCacheEnabled()
+{
+  static const bool enabled = [] {
+    const char *v = std::getenv("FG_PCG_COL_CACHE");
+    return !(v && v[0] == '0');
+  }();
+  return enabled;
+}
+
 } // namespace
 
 bool PcgSupported(int kp, int precision, int block_size)
@@ -85,7 +101,7 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   const void *kernel = SelectKernel(args.kp, args.precision, bs);
   if (!kernel)
     return cudaErrorInvalidValue;
-  const size_t smem = StagingBytes(args.kp, args.precision, bs);
+  size_t smem = StagingBytes(args.kp, args.precision, bs);
   int max_grid = PcgMaxGrid(args.kp);
   const int own = KernelGrid(kernel, smem);
   if (own < max_grid)
@@ -100,6 +116,29 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
     grid = max_grid;
   if (grid < 1)
     grid = 1;
+  // Column-index cache: the largest slice range any CTA's rows touch, if it fits in the
+  // shared memory that still leaves the grid co-resident.
+  args.col_cache = 0;
+  args.col_cache_offset = 0;
+  if (args.host_slice_off && ColumnCacheEnabled()) {
+    size_t most = 0;
+    for (int g = 0; g < grid; ++g) {
+      const long long w0 = static_cast<long long>(warp_slices) * g / grid;
+      const long long w1 = static_cast<long long>(warp_slices) * (g + 1) / grid;
+      if (w1 <= w0)
+        continue;
+      const long long s0 = (w0 * rows_per_warp) >> 5, s1 = (w1 * rows_per_warp - 1) >> 5;
+      const size_t p = static_cast<size_t>(args.host_slice_off[s1 + 1] - args.host_slice_off[s0]);
+      most = p > most ? p : most;
+    }
+    const size_t offset = (smem + 15) / 16 * 16;
+    const size_t total = offset + most * sizeof(int32_t);
+    if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
+      args.col_cache = 1;
+      args.col_cache_offset = static_cast<int32_t>(offset);
+      smem = total;
+    }
+  }
   cudaError_t e = cudaMemsetAsync(args.barrier, 0, sizeof(unsigned), stream);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(args.error, 0, sizeof(int32_t), stream);

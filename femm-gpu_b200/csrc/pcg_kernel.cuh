@@ -161,6 +161,52 @@ template <typename T, int IV> __device__ __forceinline__ void Store(T *p, const 
     *p = v[0];
   }
 }
+// Streaming loads (ld.global.cs: evict-first in L1 and L2) for the operator values, which
+// every iteration reads exactly once and which are larger than L2: they should not evict
+// the vectors and column indices that the next iteration reads again.
+template <typename T, int IV> __device__ __forceinline__ void LoadStream(const T *p, T (&o)[IV])
+{
+  if constexpr (std::is_same_v<T, double> && IV == 2) {
+    const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else if constexpr (std::is_same_v<T, double> && IV == 4) {
+    const double2 t = __ldcs(reinterpret_cast<const double2 *>(p));
+    const double2 u = __ldcs(reinterpret_cast<const double2 *>(p + 2));
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = u.x;
+    o[3] = u.y;
+  } else if constexpr (std::is_same_v<T, float> && IV == 4) {
+    const float4 t = __ldcs(reinterpret_cast<const float4 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+    o[2] = t.z;
+    o[3] = t.w;
+  } else if constexpr (std::is_same_v<T, float> && IV == 2) {
+    const float2 t = __ldcs(reinterpret_cast<const float2 *>(p));
+    o[0] = t.x;
+    o[1] = t.y;
+  } else {
+    static_assert(IV == 1, "unsupported vector width");
+    o[0] = __ldcs(p);
+  }
+}
+// Operator values of one position: per item (stride KP, streamed) or one shared operator
+// (stride 1, the same value for every item, cached: a shared operator is small).
+template <typename T, int IV>
+__device__ __forceinline__ void LoadValues(const T *base, size_t index, int stride, int per_item,
+                                           int item0, T (&o)[IV])
+{
+  if (per_item) {
+    LoadStream<T, IV>(base + index * stride + item0, o);
+  } else {
+    const T v = __ldg(base + index);
+#pragma unroll
+    for (int j = 0; j < IV; ++j)
+      o[j] = v;
+  }
+}
 // A per-item (stride KP) or shared (stride 1, same value for every item) operand.
 template <typename T, int IV>
 __device__ __forceinline__ void LoadOperand(const T *base, size_t index, int stride, int per_item,
@@ -280,10 +326,16 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, uns
 // One row's product for IV items: acc_j = sum_w a_rw,j * v_j(col_w), v = z (+ beta p),
 // in CSR order and in T arithmetic.  Column indices and values of a chunk of entries are
 // loaded before any gather so a thread keeps many independent loads in flight.
+// Column index of SELL position pos: from the CTA's shared-memory copy when cached.
+__device__ __forceinline__ int Column(const PcgArgs &a, const int32_t *colc, size_t cbase, size_t pos)
+{
+  return colc ? colc[pos - cbase] : __ldg(a.sell_col + pos);
+}
+
 template <typename T, int KP, int IV, bool kFold>
-__device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int len, int item0,
-                                           const T *z, const T *p, const bool (&fold)[IV],
-                                           const T (&beta)[IV], T (&acc)[IV])
+__device__ __forceinline__ void RowProduct(const PcgArgs &a, const int32_t *colc, size_t cbase,
+                                           size_t base, int len, int item0, const T *z, const T *p,
+                                           const bool (&fold)[IV], const T (&beta)[IV], T (&acc)[IV])
 {
   const T *vals = static_cast<const T *>(a.values);
 #pragma unroll
@@ -301,8 +353,8 @@ __device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int le
         v[u][j] = T(0);
       if (w0 + u < len) {
         const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
-        c[u] = __ldg(a.sell_col + pos);
-        LoadOperand<T, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
+        c[u] = Column(a, colc, cbase, pos);
+        LoadValues<T, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
       }
     }
 #pragma unroll
@@ -330,7 +382,8 @@ __device__ __forceinline__ void RowProduct(const PcgArgs &a, size_t base, int le
 // Reliable updates: one row of the FP64 product A64 (x64 + x32) for IV items, in CSR
 // order and FP64 arithmetic (the FP32 iterate is widened before it is added).
 template <int KP, int IV>
-__device__ __forceinline__ void RowProductReliable(const PcgArgs &a, size_t base, int len, int item0,
+__device__ __forceinline__ void RowProductReliable(const PcgArgs &a, const int32_t *colc, size_t cbase,
+                                                   size_t base, int len, int item0,
                                                    const double *x64, const float *x32,
                                                    double (&acc)[IV])
 {
@@ -350,8 +403,8 @@ __device__ __forceinline__ void RowProductReliable(const PcgArgs &a, size_t base
         v[u][j] = 0.0;
       if (w0 + u < len) {
         const size_t pos = base + 32 * static_cast<size_t>(w0 + u);
-        c[u] = __ldg(a.sell_col + pos);
-        LoadOperand<double, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
+        c[u] = Column(a, colc, cbase, pos);
+        LoadValues<double, IV>(vals, pos, a.value_stride, a.value_item, item0, v[u]);
       }
     }
 #pragma unroll
@@ -438,6 +491,27 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   const int wu0 = static_cast<int>(static_cast<long long>(WU) * blockIdx.x / gridDim.x);
   const int wu1 = static_cast<int>(static_cast<long long>(WU) * (blockIdx.x + 1) / gridDim.x);
   const T *BLK = static_cast<const T *>(a.blocks);
+
+  // Column indices of this CTA's rows (the Phase A partition, fixed for the launch) copied
+  // once into shared memory: the SpMV then gathers without a dependent global load.
+  const int32_t *colc = nullptr;
+  size_t cbase = 0;
+  if (a.col_cache) {
+    int32_t *cs = reinterpret_cast<int32_t *>(fg_dynamic_smem + a.col_cache_offset);
+    if (ws1 > ws0) {
+      const int s0 = (ws0 * S) >> 5, s1 = (ws1 * S - 1) >> 5;
+      const size_t p0 = static_cast<size_t>(__ldg(a.slice_off + s0));
+      const size_t p1 = static_cast<size_t>(__ldg(a.slice_off + s1 + 1));
+      // Positions are multiples of 32 ints (whole slice columns): copy as int4.
+      const int4 *src = reinterpret_cast<const int4 *>(a.sell_col + p0);
+      int4 *dst = reinterpret_cast<int4 *>(cs);
+      for (size_t i = threadIdx.x; i < (p1 - p0) / 4; i += kPcgThreads)
+        dst[i] = __ldg(src + i);
+      cbase = p0;
+    }
+    colc = cs;
+    __syncthreads();
+  }
   // Row of sub-row s of this lane in warp-step wu, and its offset in xb.
   auto sub_row = [&](int wu, int s) { return wu * U + s * S + lane / LR; };
   // z for sub-row s from the staged residuals (after __syncwarp): B^-1 r over the block,
@@ -543,7 +617,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     if constexpr (kFloat) {
       if (rel) {
         double acc[IV];
-        RowProductReliable<KP, IV>(a, base, len, item0, a.x64, X, acc);
+        RowProductReliable<KP, IV>(a, colc, cbase, base, len, item0, a.x64, X, acc);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
           t[j] = bd[j] / sc[j] - acc[j];
@@ -553,7 +627,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
     const bool nofold[IV] = {};
     const T nobeta[IV] = {};
     T acc[IV];
-    RowProduct<T, KP, IV, false>(a, base, len, item0, X, nullptr, nofold, nobeta, acc);
+    RowProduct<T, KP, IV, false>(a, colc, cbase, base, len, item0, X, nullptr, nofold, nobeta, acc);
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       t[j] = bd[j] / sc[j] - static_cast<double>(acc[j]);
@@ -732,7 +806,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         const int len = __ldg(a.row_len + r);
         const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
         T acc[IV], zr[IV], pr[IV], pnew[IV];
-        RowProduct<T, KP, IV, true>(a, base, len, item0, Z, pc, fold, be, acc);
+        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
         Load<T, IV>(Z + ri, zr);
         Load<T, IV>(pc + ri, pr);
 #pragma unroll

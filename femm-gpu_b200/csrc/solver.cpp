@@ -276,6 +276,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.kp = kp;
   a.items = items;
   a.slice_off = slice_off_.get();
+  a.host_slice_off = host_.slice_off.data();
   a.row_len = row_len_.get();
   a.sell_col = sell_col_.get();
   a.values = values_.get();
@@ -430,6 +431,7 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   a.kp = kp;
   a.items = items;
   a.slice_off = slice_off_.get();
+  a.host_slice_off = host_.slice_off.data();
   a.row_len = row_len_.get();
   a.sell_col = sell_col_.get();
   a.values = v32_.get();
