@@ -1,0 +1,41 @@
+// artifact.h -- gpu_femm_magnetostatic_mesh_v1 / gpu_femm_planar_dc_mesh_v1 mesh artifacts.
+#pragma once
+
+#include "femm_gpu.h"
+#include "json.h"
+
+#include <string>
+#include <vector>
+
+namespace fgio
+{
+
+// A parsed artifact owning every array an fg_model points at.
+struct Artifact {
+  std::string schema_version, source_fem_sha256, canonical_identity_sha256;
+  int32_t problem_type = FG_PLANAR;
+  double depth_m = 0.0;
+  std::vector<double> xy;
+  std::vector<int32_t> tri, tri_mat;
+  std::vector<fg_material> materials;
+  std::vector<std::vector<double>> curve_b, curve_h;
+  std::vector<fg_bh_curve> curves;
+  std::vector<int32_t> dir_nodes;
+  std::vector<double> dir_values;
+  std::vector<int32_t> con_nodes;
+  std::vector<int8_t> con_signs;
+  std::vector<double> circuit_currents;
+  std::vector<int32_t> group_numbers; // per expanded label material
+
+  // The fg_model view (valid while this object lives and is not modified).
+  fg_model Model();
+};
+
+// ParseGpuFemmMeshArtifactJson (gpu_solver/src/io/mesh_artifact.cpp:14-715) for the two
+// neutral schemas: the same acceptance rules and the same mapping -- millimetres to metres,
+// nu0 = 1 / (mu0 mu_x), one label material per region appended after the base materials
+// (group, circuit, magnet angle, J = turns / region area), zero outer Dirichlet values,
+// signed node constraints.  Motor schemas (gpu_femm_mesh_v1..v4) are refused.
+bool ParseArtifact(const std::string &text, Artifact *out, std::string *error);
+
+} // namespace fgio

@@ -1,0 +1,595 @@
+// cli.cpp -- femm_gpu: the JSON request / response boundary of libfemmgpu.
+//
+//   femm_gpu [options] --solve REQUEST.json RESPONSE.json
+//   femm_gpu [options] --batch BATCH.json RESPONSE.json
+//   femm_gpu --capabilities
+//   femm_gpu --describe-artifact ARTIFACT.json   (parsed model and plan sizes, as JSON)
+//   femm_gpu --sha256 FILE                        (the file-bytes SHA-256 a request names)
+//   options: --preconditioner jacobi|block-jacobi  --block-size 8|32  --precision fp64|mixed
+//
+// --solve is the reference's `--solve` (PlanarDcSingleSampleAdapter, gpu_solver/src/app/
+// sample_adapter.cpp:407-489): a gpu_femm_planar_dc_sample_v1 or
+// gpu_femm_magnetostatic_sample_v1 request naming a mesh artifact bound by the SHA-256 of
+// its bytes; the response carries PASS / FAIL, the solve status name, flux linkage and,
+// on request, the field solution; it is written to a temporary file and published by an
+// atomic rename.  --batch solves a shared-geometry batch (gpu_femm_magnetostatic_batch_v1,
+// the envelope of the reference's motor batch): items naming the same artifact are read
+// and validated once and solved together in fg_solve_batch launches of up to
+// max_items_per_chunk items; responses keep the input order.
+//
+// Force / torque and air-gap postprocessing (the reference's weighted-stress path) is not
+// served: a request that asks for it gets solve_status from the solve and
+// postprocess_status UNSUPPORTED_FEATURE, status FAIL.
+//
+// Exit codes: 0 every response PASS, 1 a FAIL response or an I/O failure, 2 usage error.
+#include "artifact.h"
+#include "femm_gpu.h"
+#include "json.h"
+#include "request.h"
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+namespace
+{
+
+using fgio::Artifact;
+using fgio::SampleRequest;
+
+constexpr double kTwoPi = 6.283185307179586476925286766559005768;
+
+struct Options {
+  fg_plan_options plan{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, 0};
+};
+
+std::string StatusName(int s) { return fg_status_name(s); }
+
+bool ReadFile(const std::string &path, std::string *out)
+{
+  std::ifstream f(path, std::ios::binary);
+  if (!f)
+    return false;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  *out = ss.str();
+  return static_cast<bool>(f) || f.eof();
+}
+
+// Same file (by device and inode when both exist, else by resolved path).
+bool SameFile(const std::string &a, const std::string &b)
+{
+  struct stat sa {}, sb {};
+  if (stat(a.c_str(), &sa) == 0 && stat(b.c_str(), &sb) == 0)
+    return sa.st_dev == sb.st_dev && sa.st_ino == sb.st_ino;
+  char ra[4096], rb[4096];
+  const char *pa = realpath(a.c_str(), ra), *pb = realpath(b.c_str(), rb);
+  return std::string(pa ? pa : a.c_str()) == std::string(pb ? pb : b.c_str());
+}
+
+// Writes `text` to path.tmp.<clock>.<n> and renames it over `path`.
+bool PublishAtomically(const std::string &path, const std::string &text)
+{
+  static std::atomic<uint64_t> sequence{0};
+  const std::string tmp = path + ".tmp." +
+                          std::to_string(std::chrono::steady_clock::now().time_since_epoch().count()) +
+                          "." + std::to_string(sequence.fetch_add(1));
+  {
+    std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+    if (!f)
+      return false;
+    f << text;
+    f.flush();
+    if (!f) {
+      std::remove(tmp.c_str());
+      return false;
+    }
+  }
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+    std::remove(tmp.c_str());
+    return false;
+  }
+  return true;
+}
+
+// What one solved sample returns.
+struct Solved {
+  std::vector<double> currents, flux, a, b1, b2;
+  int32_t iterations = 0;
+  double residual = 0.0;
+};
+
+template <class V> void List(std::ostream &o, const V &v)
+{
+  for (size_t i = 0; i < v.size(); ++i)
+    o << (i ? ", " : "") << v[i];
+}
+
+// WritePlanarDcSampleResponse's layout (gpu_solver/src/app/sample_adapter.cpp:236-355).
+std::string SampleResponse(int status, int solve_status, bool post_requested, int post_status,
+                           const SampleRequest *req, const Solved *sol, const std::string &diagnostic,
+                           const Artifact *art, const std::string &indent = "")
+{
+  std::ostringstream o;
+  o << std::setprecision(17);
+  const bool solved = solve_status == 0 && req && sol;
+  const std::string protocol = req ? req->protocol : "gpu_femm_planar_dc_sample_v1";
+  const bool generic = protocol == "gpu_femm_magnetostatic_sample_v1";
+  const bool axi = art && art->problem_type == FG_AXISYMMETRIC;
+  const std::string message = status == 0 ? "" : (diagnostic.empty() ? StatusName(status) : diagnostic);
+  const std::string in = indent + "  ";
+  o << "{\n" << in << "\"protocol\": \"" << protocol << "\",\n"
+    << in << "\"mesh_artifact_sha256\": \"" << (req ? req->mesh_artifact_sha256 : "") << "\",\n";
+  if (generic)
+    o << in << "\"problem_type\": \"" << (axi ? "axisymmetric" : "planar") << "\",\n"
+      << in << "\"field_components\": [\"" << (axi ? "Br" : "Bx") << "\", \"" << (axi ? "Bz" : "By") << "\"],\n"
+      << in << "\"node_potential_quantity\": \"" << (axi ? "poloidal_flux_function" : "magnetic_vector_potential") << "\",\n"
+      << in << "\"node_potential_unit\": \"" << (axi ? "Wb" : "Wb/m") << "\",\n";
+  o << in << "\"status\": \"" << (status == 0 ? "PASS" : "FAIL") << "\",\n"
+    << in << "\"solve_status\": \"" << StatusName(solve_status) << "\",\n"
+    << in << "\"postprocess_status\": \""
+    << (!post_requested ? "NOT_REQUESTED" : (solve_status == 0 ? StatusName(post_status) : "NOT_RUN")) << "\",\n"
+    << in << "\"error_identifier\": \"" << (status == 0 ? "" : "GPU_FEMM_" + StatusName(status)) << "\",\n"
+    << in << "\"error_message\": \"" << fgio::Escape(message) << "\",\n"
+    << in << "\"Fx_N\": null,\n" << in << "\"Fy_N\": null,\n" << in << "\"torque_Nm\": null,\n"
+    << in << "\"actual_circuit_currents_A\": [";
+  if (solved)
+    List(o, sol->currents);
+  o << "],\n" << in << "\"circuit_flux_linkage_Wb\": [";
+  if (solved)
+    List(o, sol->flux);
+  o << "],\n" << in << "\"airgap_sample_angles_deg\": [],\n" << in << "\"airgap_radial_flux_density_T\": [],\n"
+    << in << "\"mesh_node_count\": " << (solved ? sol->a.size() : 0) << ",\n"
+    << in << "\"mesh_element_count\": " << (solved ? sol->b1.size() : 0) << ",\n";
+  const bool field = solved && req->include_field_solution;
+  o << in << "\"field_solution_included\": " << (field ? "true" : "false") << ",\n"
+    << in << "\"" << (generic ? "node_potential" : "node_A_Wb_per_m") << "\": [";
+  if (field)
+    for (size_t i = 0; i < sol->a.size(); ++i) {
+      double v = sol->a[i];
+      if (generic && axi && art && 2 * i < art->xy.size())
+        v *= kTwoPi * art->xy[2 * i];
+      o << (i ? ", " : "") << v;
+    }
+  o << "],\n" << in << "\"" << (generic ? "element_B_component_1_T" : "element_Bx_T") << "\": [";
+  if (field)
+    List(o, sol->b1);
+  o << "],\n" << in << "\"" << (generic ? "element_B_component_2_T" : "element_By_T") << "\": [";
+  if (field)
+    List(o, sol->b2);
+  o << "],\n" << in << "\"convergence\": {\"iterations\": " << (sol ? sol->iterations : 0) << ", \"residual_l2\": ";
+  if (sol && std::isfinite(sol->residual))
+    o << sol->residual;
+  else
+    o << "null";
+  o << "}\n" << indent << "}";
+  return o.str();
+}
+
+// PlanarDcRequestMatchesArtifact (sample_adapter.cpp:181-234) for neutral artifacts.
+bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
+{
+  const bool generic_artifact = a.schema_version == "gpu_femm_magnetostatic_mesh_v1";
+  if (r.generic() != generic_artifact || r.circuit_currents_a.size() != a.circuit_currents.size())
+    return false;
+  auto has_group = [&](int32_t g) {
+    for (int32_t x : a.group_numbers)
+      if (x == g)
+        return true;
+    return false;
+  };
+  const bool groups = r.force_group_number >= 0;
+  if (groups && (!has_group(r.force_group_number) || !has_group(r.stress_air_group_number)))
+    return false;
+  const bool post = r.postprocess_requested();
+  if (r.generic())
+    return !post && r.force_group_number == -1 && r.stress_air_group_number == -1 &&
+           r.airgap_radius_mm == 0.0 && r.airgap_angles_deg.empty() && r.sliding_band_angle_deg == 0.0;
+  return r.sliding_band_angle_deg == 0.0 && (!post || groups);
+}
+
+// A verified, parsed artifact and its plan.
+struct Prepared {
+  int status = 0;
+  std::string error;
+  Artifact artifact;
+  fg_plan *plan = nullptr;
+  ~Prepared()
+  {
+    if (plan)
+      fg_plan_destroy(plan);
+  }
+};
+
+void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
+{
+  std::string bytes;
+  if (!ReadFile(path, &bytes)) {
+    p->status = FG_INPUT_IO;
+    p->error = "cannot open mesh artifact";
+  } else if (fgio::Sha256Hex(bytes) != sha) {
+    p->status = FG_INVALID_ARGUMENT;
+    p->error = "mesh artifact SHA mismatch";
+  } else if (!fgio::ParseArtifact(bytes, &p->artifact, &p->error)) {
+    p->status = FG_INVALID_ARGUMENT;
+  }
+}
+
+// The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
+int EnsurePlan(Prepared *p, const Options &opt)
+{
+  if (p->plan)
+    return 0;
+  fg_model m = p->artifact.Model();
+  const int rc = fg_plan_create(&m, &opt.plan, &p->plan);
+  if (rc != 0)
+    p->plan = nullptr;
+  return rc;
+}
+
+// Solves k samples on a prepared plan; statuses[i] = per-item status.
+int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std::vector<Solved> *out,
+               std::vector<int> *statuses, int *launches)
+{
+  const fg_model m = p.artifact.Model();
+  const size_t k = reqs.size(), N = m.node_count, E = m.triangle_count, C = m.circuit_count;
+  std::vector<double> cur(k * C), a(k * N), b1(k * E), b2(k * E), flux(k * (C ? C : 1));
+  for (size_t i = 0; i < k; ++i)
+    for (size_t c = 0; c < C; ++c)
+      cur[i * C + c] = reqs[i]->circuit_currents_a[c];
+  std::vector<fg_item_info> info(k);
+  fg_solve_options o;
+  fg_production_options(&o);
+  const int rc = fg_solve_batch(p.plan, static_cast<int32_t>(k), cur.data(), nullptr, nullptr, &o, a.data(),
+                                b1.data(), b2.data(), flux.data(), info.data());
+  fg_timing t{};
+  fg_plan_last_timing(p.plan, &t);
+  *launches += static_cast<int>(t.pcg_launches);
+  out->assign(k, Solved{});
+  statuses->assign(k, rc);
+  if (rc != 0)
+    return rc;
+  for (size_t i = 0; i < k; ++i) {
+    Solved &s = (*out)[i];
+    s.currents.assign(cur.begin() + i * C, cur.begin() + (i + 1) * C);
+    s.flux.assign(flux.begin() + i * C, flux.begin() + i * C + C);
+    s.a.assign(a.begin() + i * N, a.begin() + (i + 1) * N);
+    s.b1.assign(b1.begin() + i * E, b1.begin() + (i + 1) * E);
+    s.b2.assign(b2.begin() + i * E, b2.begin() + (i + 1) * E);
+    s.iterations = info[i].iterations;
+    s.residual = info[i].residual_l2;
+    (*statuses)[i] = info[i].status;
+  }
+  return 0;
+}
+
+int Solve(const std::string &request_path, const std::string &response_path, const Options &opt)
+{
+  if (SameFile(request_path, response_path)) {
+    std::cerr << "FAIL magnetostatic solve: response must not overwrite request\n";
+    return 1;
+  }
+  std::string text, error;
+  SampleRequest req;
+  const bool read = ReadFile(request_path, &text);
+  const bool parsed = read && fgio::ParseSampleRequestText(text, &req, &error);
+  if (parsed && SameFile(req.mesh_artifact_path, response_path)) {
+    std::cerr << "FAIL magnetostatic solve: response must not overwrite mesh artifact\n";
+    return 1;
+  }
+  if (!parsed) {
+    if (!read)
+      error = "cannot read request";
+    const std::string body =
+        SampleResponse(FG_INVALID_ARGUMENT, FG_INVALID_ARGUMENT, false, 0, nullptr, nullptr, error, nullptr);
+    if (!PublishAtomically(response_path, body + "\n")) {
+      std::cerr << "FAIL magnetostatic solve: could not atomically publish response\n";
+      return 1;
+    }
+    std::cerr << "FAIL planar-DC request: " << error << '\n';
+    return 1;
+  }
+  Prepared p;
+  Prepare(req.mesh_artifact_path, req.mesh_artifact_sha256, opt, &p);
+  int status = p.status;
+  std::string diagnostic = p.error;
+  if (status == 0 && !RequestMatchesArtifact(req, p.artifact)) {
+    status = FG_INVALID_ARGUMENT;
+    diagnostic = "artifact physics, circuit count, group, or sliding-band request mismatch";
+  }
+  std::vector<Solved> sols;
+  std::vector<int> st;
+  int launches = 0;
+  bool attempted = false;
+  if (status == 0)
+    status = EnsurePlan(&p, opt);
+  if (status == 0) {
+    attempted = true;
+    const int rc = SolveItems(p, {&req}, &sols, &st, &launches);
+    status = rc != 0 ? rc : st[0];
+  }
+  const int solve_status = status;
+  const bool post = req.postprocess_requested();
+  int post_status = 0;
+  if (solve_status == 0 && post) {
+    post_status = FG_UNSUPPORTED_FEATURE;
+    status = post_status;
+    diagnostic = "force/torque and air-gap postprocessing are not served by this solver";
+  }
+  const std::string body = SampleResponse(status, solve_status, post, post_status, &req,
+                                          attempted ? &sols[0] : nullptr, diagnostic, &p.artifact);
+  if (!PublishAtomically(response_path, body + "\n")) {
+    std::cerr << "FAIL magnetostatic solve: could not atomically publish response\n";
+    return 1;
+  }
+  if (status != 0) {
+    std::cerr << "FAIL magnetostatic solve: " << (diagnostic.empty() ? StatusName(status) : diagnostic) << '\n';
+    return 1;
+  }
+  return 0;
+}
+
+int Batch(const std::string &request_path, const std::string &response_path, const Options &opt)
+{
+  if (SameFile(request_path, response_path)) {
+    std::cerr << "FAIL magnetostatic batch: response must not overwrite request\n";
+    return 1;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  std::string text, error;
+  fgio::BatchRequest batch;
+  if (!ReadFile(request_path, &text) || !fgio::ParseBatchRequestText(text, &batch, &error)) {
+    std::ostringstream o;
+    o << "{\n  \"protocol\": \"gpu_femm_magnetostatic_batch_v1\",\n  \"status\": \"FAIL\",\n"
+      << "  \"solve_status\": \"" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
+      << "  \"error_identifier\": \"GPU_FEMM_" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
+      << "  \"error_message\": \"" << fgio::Escape(error.empty() ? "cannot read request" : error)
+      << "\",\n  \"items\": []\n}\n";
+    PublishAtomically(response_path, o.str());
+    std::cerr << "FAIL magnetostatic batch request: " << error << '\n';
+    return 1;
+  }
+  const size_t k = batch.items.size();
+  std::vector<std::string> bodies(k);
+  std::vector<int> final_status(k, FG_INTERNAL_ERROR);
+  // Items grouped by artifact (path + SHA): each artifact read, verified and planned once.
+  std::map<std::pair<std::string, std::string>, std::vector<size_t>> groups;
+  for (size_t i = 0; i < k; ++i)
+    groups[{batch.items[i].request.mesh_artifact_path, batch.items[i].request.mesh_artifact_sha256}].push_back(i);
+  int chunks = 0, launches = 0, cache_hits = 0;
+  double artifact_s = 0.0, solve_s = 0.0;
+  for (auto &g : groups) {
+    cache_hits += static_cast<int>(g.second.size()) - 1;
+    const auto a0 = std::chrono::steady_clock::now();
+    Prepared p;
+    Prepare(g.first.first, g.first.second, opt, &p);
+    artifact_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - a0).count();
+    std::vector<size_t> ready;
+    for (size_t i : g.second) {
+      const SampleRequest &r = batch.items[i].request;
+      int status = p.status;
+      std::string diag = p.error;
+      if (status == 0 && !RequestMatchesArtifact(r, p.artifact)) {
+        status = FG_INVALID_ARGUMENT;
+        diag = "artifact physics, circuit count, group, or sliding-band request mismatch";
+      }
+      if (status == 0) {
+        ready.push_back(i);
+        continue;
+      }
+      bodies[i] = SampleResponse(status, status, r.postprocess_requested(), 0, &r, nullptr, diag, nullptr, "    ");
+      final_status[i] = status;
+    }
+    const int plan_status = ready.empty() ? 0 : EnsurePlan(&p, opt);
+    if (plan_status != 0) {
+      for (size_t i : ready) {
+        const SampleRequest &r = batch.items[i].request;
+        bodies[i] = SampleResponse(plan_status, plan_status, r.postprocess_requested(), 0, &r, nullptr, "",
+                                   nullptr, "    ");
+        final_status[i] = plan_status;
+      }
+      ready.clear();
+    }
+    const auto s0 = std::chrono::steady_clock::now();
+    for (size_t first = 0; first < ready.size(); first += batch.max_items_per_chunk) {
+      const size_t n = std::min<size_t>(batch.max_items_per_chunk, ready.size() - first);
+      std::vector<const SampleRequest *> reqs;
+      for (size_t j = 0; j < n; ++j)
+        reqs.push_back(&batch.items[ready[first + j]].request);
+      std::vector<Solved> sols;
+      std::vector<int> st;
+      SolveItems(p, reqs, &sols, &st, &launches);
+      ++chunks;
+      for (size_t j = 0; j < n; ++j) {
+        const size_t i = ready[first + j];
+        const SampleRequest &r = *reqs[j];
+        int status = st[j];
+        const int solve_status = status;
+        int post_status = 0;
+        std::string diag;
+        if (solve_status == 0 && r.postprocess_requested()) {
+          post_status = FG_UNSUPPORTED_FEATURE;
+          status = post_status;
+          diag = "force/torque and air-gap postprocessing are not served by this solver";
+        }
+        bodies[i] = SampleResponse(status, solve_status, r.postprocess_requested(), post_status, &r,
+                                   sols.empty() ? nullptr : &sols[j], diag, &p.artifact, "    ");
+        final_status[i] = status;
+      }
+    }
+    solve_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+  }
+  bool pass = true;
+  for (int s : final_status)
+    pass = pass && s == 0;
+  std::ostringstream o;
+  o << std::setprecision(17) << "{\n  \"protocol\": \"" << batch.protocol << "\",\n"
+    << "  \"status\": \"" << (pass ? "PASS" : "FAIL") << "\",\n"
+    << "  \"solve_status\": \"" << (pass ? "PASS" : "PARTIAL_FAILURE") << "\",\n"
+    << "  \"error_identifier\": \"" << (pass ? "" : "GPU_FEMM_BATCH_PARTIAL_FAILURE") << "\",\n"
+    << "  \"error_message\": \"" << (pass ? "" : "one or more batch items failed") << "\",\n"
+    << "  \"cache\": {\"mesh_cache_hits\": " << cache_hits << ", \"chunk_count\": " << chunks
+    << ", \"requested_chunk_size\": " << batch.max_items_per_chunk
+    << ", \"effective_chunk_size\": " << batch.max_items_per_chunk
+    << ", \"batched_pcg_launches\": " << launches << "},\n"
+    << "  \"timing\": {\"schema_version\": \"gpu_femm_magnetostatic_batch_timing_v1\""
+    << ", \"artifact_read_validate_plan_seconds\": " << artifact_s << ", \"solve_seconds\": " << solve_s
+    << ", \"total_seconds\": " << std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count()
+    << "},\n  \"items\": [\n";
+  for (size_t i = 0; i < k; ++i)
+    o << "    {\"task_id\": \"" << batch.items[i].task_id << "\", \"response\": " << bodies[i]
+      << (i + 1 < k ? "},\n" : "}\n");
+  o << "  ]\n}\n";
+  if (!PublishAtomically(response_path, o.str())) {
+    std::cerr << "FAIL magnetostatic batch: could not atomically publish response\n";
+    return 1;
+  }
+  if (!pass)
+    std::cerr << "FAIL magnetostatic batch: one or more batch items failed\n";
+  return pass ? 0 : 1;
+}
+
+// --describe-artifact: the parsed model as JSON (17 significant digits, exact round trip),
+// and its host-only plan's sizes -- for checking the parser against other readers.
+int DescribeArtifact(const std::string &path)
+{
+  std::string bytes, error;
+  Artifact a;
+  if (!ReadFile(path, &bytes)) {
+    std::cerr << "FAIL describe: cannot open mesh artifact\n";
+    return 1;
+  }
+  if (!fgio::ParseArtifact(bytes, &a, &error)) {
+    std::cout << "{\"status\": \"FAIL\", \"error\": \"" << fgio::Escape(error) << "\"}\n";
+    return 1;
+  }
+  fg_model m = a.Model();
+  fg_plan_options po{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, FG_PLAN_HOST_ONLY};
+  fg_plan *plan = nullptr;
+  const int rc = fg_plan_create(&m, &po, &plan);
+  fg_plan_sizes sz{};
+  if (rc == 0)
+    fg_plan_sizes_get(plan, &sz);
+  std::ostringstream o;
+  o << std::setprecision(17) << "{\"status\": \"PASS\", \"plan_status\": \"" << StatusName(rc)
+    << "\", \"schema_version\": \"" << a.schema_version << "\", \"sha256\": \"" << fgio::Sha256Hex(bytes)
+    << "\", \"canonical_identity_sha256\": \"" << a.canonical_identity_sha256
+    << "\", \"problem_type\": " << a.problem_type << ", \"depth_m\": " << a.depth_m << ", \"xy\": [";
+  List(o, a.xy);
+  o << "], \"tri\": [";
+  List(o, a.tri);
+  o << "], \"tri_mat\": [";
+  List(o, a.tri_mat);
+  o << "], \"materials\": [";
+  for (size_t i = 0; i < a.materials.size(); ++i) {
+    const fg_material &t = a.materials[i];
+    o << (i ? ", " : "") << "[" << t.reluctivity_zero_m_per_h << ", " << t.alpha_per_t2 << ", "
+      << t.source_j_per_a << ", " << t.h_c_a_per_m << ", " << t.magnetization_deg << ", "
+      << t.bh_curve_index << ", " << t.circuit_index << ", " << t.group_number << "]";
+  }
+  o << "], \"curves\": [";
+  for (size_t c = 0; c < a.curve_b.size(); ++c) {
+    o << (c ? ", " : "") << "[[";
+    List(o, a.curve_b[c]);
+    o << "], [";
+    List(o, a.curve_h[c]);
+    o << "]]";
+  }
+  o << "], \"dirichlet_nodes\": [";
+  List(o, a.dir_nodes);
+  o << "], \"constraint_nodes\": [";
+  List(o, a.con_nodes);
+  o << "], \"constraint_signs\": [";
+  for (size_t i = 0; i < a.con_signs.size(); ++i)
+    o << (i ? ", " : "") << static_cast<int>(a.con_signs[i]);
+  o << "], \"circuit_currents_A\": [";
+  List(o, a.circuit_currents);
+  o << "], \"rows\": " << sz.rows << ", \"nnz\": " << sz.nnz << "}\n";
+  if (plan)
+    fg_plan_destroy(plan);
+  std::cout << o.str();
+  return rc == 0 ? 0 : 1;
+}
+
+int Usage()
+{
+  std::cerr << "usage: femm_gpu [--preconditioner jacobi|block-jacobi] [--block-size 8|32] "
+               "[--precision fp64|mixed] (--solve request.json response.json | "
+               "--batch batch.json response.json | --capabilities | --describe-artifact artifact.json)\n";
+  return 2;
+}
+
+} // namespace
+
+int main(int argc, char **argv)
+{
+  Options opt;
+  int next = 1;
+  bool have_pre = false, have_prec = false, have_bs = false;
+  while (next + 1 < argc && (std::strcmp(argv[next], "--preconditioner") == 0 ||
+                             std::strcmp(argv[next], "--block-size") == 0 ||
+                             std::strcmp(argv[next], "--precision") == 0)) {
+    const std::string flag = argv[next], value = argv[next + 1];
+    if (flag == "--preconditioner") {
+      if (have_pre || (value != "jacobi" && value != "block-jacobi")) {
+        std::cerr << "--preconditioner requires jacobi or block-jacobi\n";
+        return 2;
+      }
+      opt.plan.preconditioner = value == "block-jacobi" ? FG_PRECOND_BLOCK_JACOBI : FG_PRECOND_JACOBI;
+      have_pre = true;
+    } else if (flag == "--block-size") {
+      if (have_bs || (value != "8" && value != "32")) {
+        std::cerr << "--block-size requires 8 or 32\n";
+        return 2;
+      }
+      opt.plan.block_size = value == "32" ? 32 : 8;
+      have_bs = true;
+    } else {
+      if (have_prec || (value != "fp64" && value != "mixed")) {
+        std::cerr << "--precision requires fp64 or mixed\n";
+        return 2;
+      }
+      opt.plan.precision = value == "mixed" ? FG_PRECISION_MIXED : FG_PRECISION_FP64;
+      have_prec = true;
+    }
+    next += 2;
+  }
+  const int rest = argc - next;
+  if (rest == 1 && std::strcmp(argv[next], "--capabilities") == 0) {
+    std::cout << "{\n  \"protocols\": [\"gpu_femm_planar_dc_sample_v1\", \"gpu_femm_magnetostatic_sample_v1\", "
+                 "\"gpu_femm_magnetostatic_batch_v1\"],\n"
+              << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\"],\n"
+              << "  \"preconditioners\": [\"jacobi\", \"block-jacobi\"],\n"
+              << "  \"precisions\": [\"fp64\", \"mixed\"],\n"
+              << "  \"abi_version\": " << fg_abi_version() << "\n}\n";
+    return 0;
+  }
+  if (rest == 2 && std::strcmp(argv[next], "--sha256") == 0) {
+    std::string bytes;
+    if (!ReadFile(argv[next + 1], &bytes)) {
+      std::cerr << "FAIL sha256: cannot read " << argv[next + 1] << '\n';
+      return 1;
+    }
+    std::cout << fgio::Sha256Hex(bytes) << '\n';
+    return 0;
+  }
+  if (rest == 2 && std::strcmp(argv[next], "--describe-artifact") == 0)
+    return DescribeArtifact(argv[next + 1]);
+  if (rest == 3 && std::strcmp(argv[next], "--solve") == 0)
+    return Solve(argv[next + 1], argv[next + 2], opt);
+  if (rest == 3 && std::strcmp(argv[next], "--batch") == 0)
+    return Batch(argv[next + 1], argv[next + 2], opt);
+  return Usage();
+}
