@@ -2,6 +2,7 @@
 #include "femm_gpu.h"
 #include "solver.h"
 #include "warm.h"
+#include "multi.h"
 
 #include <algorithm>
 #include <cmath>
@@ -212,6 +213,48 @@ int fg_solve_batch(fg_plan *plan, int32_t items, const double *currents, const d
     return ToInt(Status::kInvalidArgument);
   return ToInt(plan->plan.SolveHost(items, currents, hc_scale, warm_a, *options, a_out, b1_out,
                                     b2_out, flux_out, info));
+}
+
+int fg_multi_create(fg_plan *const *plans, int32_t count, fg_multi **multi)
+{
+  if (!plans || count <= 0 || !multi)
+    return ToInt(Status::kInvalidArgument);
+  *multi = nullptr;
+  std::vector<fg::Plan *> list;
+  for (int32_t i = 0; i < count; ++i) {
+    if (!plans[i])
+      return ToInt(Status::kInvalidArgument);
+    list.push_back(&plans[i]->plan);
+  }
+  auto *m = new (std::nothrow) fg_multi;
+  if (!m)
+    return ToInt(Status::kInternalError);
+  const Status s = m->solver.Create(std::move(list));
+  if (s != Status::kOk) {
+    delete m;
+    return ToInt(s);
+  }
+  *multi = m;
+  return 0;
+}
+
+void fg_multi_destroy(fg_multi *multi) { delete multi; }
+
+int fg_multi_solve(fg_multi *multi, const double *const *currents, const fg_solve_options *options,
+                   double *const *a_out, double *const *b1_out, double *const *b2_out,
+                   double *const *flux_out, fg_item_info *info)
+{
+  if (!multi || !options || !info)
+    return ToInt(Status::kInvalidArgument);
+  return ToInt(multi->solver.Solve(currents, *options, a_out, b1_out, b2_out, flux_out, info));
+}
+
+int fg_multi_last_timing(const fg_multi *multi, fg_multi_timing *timing)
+{
+  if (!multi || !timing)
+    return ToInt(Status::kInvalidArgument);
+  *timing = multi->solver.timing();
+  return 0;
 }
 
 int fg_mlp_create(int32_t inputs, int32_t hidden, int32_t outputs, uint64_t seed, fg_mlp **mlp)

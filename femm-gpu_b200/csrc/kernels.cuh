@@ -91,6 +91,13 @@ struct PcgArgs {
 };
 constexpr int kPcgTraceSlots = 10;
 
+// Groups of a multi-plan PCG launch (device arrays): args [groups]; per CTA its group;
+// per group its first CTA and CTA count.
+struct PcgGroups {
+  const PcgArgs *args;
+  const int32_t *cta_group, *group_first, *group_size;
+};
+
 // Launchers (return cudaError_t of the launch).
 cudaError_t LaunchElementKernel(const DevicePlan &p, int kp, const double *state,
                                 uint32_t newton_mask, uint32_t active_mask, double *elem_vals,
@@ -110,6 +117,11 @@ cudaError_t LaunchBlockInverse(const DevicePlan &p, int kp, int items, int bs, c
 // Cooperative persistent PCG; *grid_out receives the number of CTAs used.
 cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream);
 int PcgMaxGrid(int kp);
+// One cooperative launch of `ctas` CTAs solving every group of t (FP64 Jacobi, one item per
+// group).  The caller zeroes the groups' barrier counters and error flags.
+cudaError_t LaunchMultiPcg(PcgGroups t, int ctas, cudaStream_t stream);
+// Co-resident CTAs of the multi-plan kernel (its grid limit), 0 without a device.
+int MultiPcgMaxGrid();
 // Whether a PCG kernel exists for this shape (block size 32 in FP64 stops at 16 items).
 bool PcgSupported(int kp, int precision, int block_size);
 

@@ -11,6 +11,7 @@ const void *PcgKernelF64(int kp);
 const void *PcgKernelF32(int kp);
 const void *PcgKernelF64Block(int kp, int bs);
 const void *PcgKernelF32Block(int kp, int bs);
+const void *MultiPcgKernelF64();
 
 namespace
 {
@@ -151,6 +152,17 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   if (block_out)
     *block_out = kPcgThreads;
   return e;
+}
+
+int MultiPcgMaxGrid() { return KernelGrid(MultiPcgKernelF64(), 0); }
+
+cudaError_t LaunchMultiPcg(PcgGroups t, int ctas, cudaStream_t stream)
+{
+  const int max_grid = MultiPcgMaxGrid();
+  if (ctas < 1 || ctas > max_grid)
+    return cudaErrorInvalidConfiguration;
+  void *params[] = {&t};
+  return cudaLaunchCooperativeKernel(MultiPcgKernelF64(), dim3(ctas), dim3(kPcgThreads), params, 0, stream);
 }
 
 } // namespace fg

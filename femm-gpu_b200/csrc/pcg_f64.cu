@@ -17,4 +17,10 @@ const void *PcgKernelF64(int kp)
   }
 }
 
+// The multi-plan kernel: one FP64 Jacobi solve of one item per group.
+const void *MultiPcgKernelF64()
+{
+  return reinterpret_cast<const void *>(&MultiPcgKernel<double, 1, 1, 0>);
+}
+
 } // namespace fg

@@ -225,9 +225,15 @@ __device__ __forceinline__ void LoadOperand(const T *base, size_t index, int str
 __device__ __forceinline__ double Fma(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float Fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
-__device__ __forceinline__ void TraceMark(const PcgArgs &a, Trace &tr, int slot)
+// The CTAs that solve one batch together: all of a plain launch, or one group of a
+// multi-plan launch (rank = this CTA's index within its group).
+struct GridShape {
+  int size, rank;
+};
+
+__device__ __forceinline__ void TraceMark(const PcgArgs &a, const GridShape &gs, Trace &tr, int slot)
 {
-  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (a.trace && gs.rank == 0 && threadIdx.x == 0) {
     const unsigned long long now = GlobalTimer();
     tr.slot[slot] += now - tr.mark;
     tr.mark = now;
@@ -235,12 +241,12 @@ __device__ __forceinline__ void TraceMark(const PcgArgs &a, Trace &tr, int slot)
 }
 
 // Grid-wide barrier over a monotonically increasing arrival counter, bounded in time.
-__device__ bool GridBarrier(const PcgArgs &a, unsigned &epoch, Reduce &sm)
+__device__ bool GridBarrier(const PcgArgs &a, const GridShape &gs, unsigned &epoch, Reduce &sm)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
     epoch += 1;
-    const unsigned target = epoch * gridDim.x;
+    const unsigned target = epoch * static_cast<unsigned>(gs.size);
     __threadfence();
     AddRelease(a.barrier, 1u);
     const unsigned long long t0 = GlobalTimer();
@@ -269,7 +275,7 @@ __device__ bool GridBarrier(const PcgArgs &a, unsigned &epoch, Reduce &sm)
 // Sum (or max) of Q per-item quantities over the whole grid, deterministic for a
 // fixed launch shape.  v[q][j] is this thread's partial for its item item0 + j.
 template <int KP, int IV, int Q, bool kMax>
-__device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, unsigned &epoch,
+__device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q][IV], Reduce &sm, unsigned &epoch,
                            int &buf, Trace &tr, int phase)
 {
   constexpr int LR = KP / IV; // lanes per row
@@ -289,18 +295,18 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, uns
     }
   __syncthreads();
   constexpr int QK = Q * KP;
-  const int G = gridDim.x;
+  const int G = gs.size;
   double *part = a.partials + static_cast<size_t>(buf) * kMaxQ * G;
   if (threadIdx.x < QK) {
     double s = sm.warp[0][threadIdx.x];
     for (int w = 1; w < kPcgWarps; ++w)
       s = kMax ? fmax(s, sm.warp[w][threadIdx.x]) : s + sm.warp[w][threadIdx.x];
-    part[static_cast<size_t>(threadIdx.x) * G + blockIdx.x] = s;
+    part[static_cast<size_t>(threadIdx.x) * G + gs.rank] = s;
   }
-  TraceMark(a, tr, 2 * phase);
-  if (!GridBarrier(a, epoch, sm))
+  TraceMark(a, gs, tr, 2 * phase);
+  if (!GridBarrier(a, gs, epoch, sm))
     return false;
-  TraceMark(a, tr, 2 * phase + 1);
+  TraceMark(a, gs, tr, 2 * phase + 1);
   for (int t = warp; t < QK; t += kPcgWarps) {
     double s = 0.0;
     for (int g = lane; g < G; g += 32) {
@@ -316,8 +322,8 @@ __device__ bool GridReduce(const PcgArgs &a, double (&v)[Q][IV], Reduce &sm, uns
       sm.result[t] = s;
   }
   __syncthreads();
-  TraceMark(a, tr, 8);
-  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0)
+  TraceMark(a, gs, tr, 8);
+  if (a.trace && gs.rank == 0 && threadIdx.x == 0)
     tr.slot[9] += 1;
   buf ^= 1;
   return true;
@@ -424,7 +430,7 @@ __device__ __forceinline__ void RowProductReliable(const PcgArgs &a, const int32
 }
 
 template <typename T, int KP, int IV, int BS>
-__global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
+__device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
 {
   __shared__ Reduce sm;
   __shared__ Control ctl;
@@ -434,8 +440,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int item0 = (lane % LR) * IV;
   const int WS = a.n_pad / S;
-  const int ws0 = static_cast<int>(static_cast<long long>(WS) * blockIdx.x / gridDim.x);
-  const int ws1 = static_cast<int>(static_cast<long long>(WS) * (blockIdx.x + 1) / gridDim.x);
+  const int ws0 = static_cast<int>(static_cast<long long>(WS) * gs.rank / gs.size);
+  const int ws1 = static_cast<int>(static_cast<long long>(WS) * (gs.rank + 1) / gs.size);
   unsigned epoch = 0;
   int buf = 0;
   const T *B = static_cast<const T *>(a.b);
@@ -488,8 +494,8 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
   extern __shared__ __align__(16) unsigned char fg_dynamic_smem[];
   T *xb = reinterpret_cast<T *>(fg_dynamic_smem) + static_cast<size_t>(warp) * U * KP;
   const int WU = a.n_pad / U;
-  const int wu0 = static_cast<int>(static_cast<long long>(WU) * blockIdx.x / gridDim.x);
-  const int wu1 = static_cast<int>(static_cast<long long>(WU) * (blockIdx.x + 1) / gridDim.x);
+  const int wu0 = static_cast<int>(static_cast<long long>(WU) * gs.rank / gs.size);
+  const int wu1 = static_cast<int>(static_cast<long long>(WU) * (gs.rank + 1) / gs.size);
   const T *BLK = static_cast<const T *>(a.blocks);
 
   // Column indices of this CTA's rows (the Phase A partition, fixed for the launch) copied
@@ -670,7 +676,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       zero[j] = T(0);
     Store<T, IV>(X + ri, zero);
     FG_ROWS_END
-    if (!GridReduce<KP, IV, 2, true>(a, v, sm, epoch, buf, tr, 3))
+    if (!GridReduce<KP, IV, 2, true>(a, gs, v, sm, epoch, buf, tr, 3))
       return;
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
@@ -758,7 +764,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         __syncwarp();
       }
     }
-    if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 3))
+    if (!GridReduce<KP, IV, 2, false>(a, gs, v, sm, epoch, buf, tr, 3))
       return;
     if (threadIdx.x < KP) {
       const int it = threadIdx.x;
@@ -820,7 +826,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
             v[0][j] += static_cast<double>(pnew[j]) * static_cast<double>(acc[j]);
         FG_ROWS_END
       }
-      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 0))
+      if (!GridReduce<KP, IV, 1, false>(a, gs, v, sm, epoch, buf, tr, 0))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -959,7 +965,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
           }
         }
       }
-      if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 1))
+      if (!GridReduce<KP, IV, 2, false>(a, gs, v, sm, epoch, buf, tr, 1))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -1025,7 +1031,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         Store<T, IV>(R + ri, rv);
         FG_ROWS_END
       }
-      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 2))
+      if (!GridReduce<KP, IV, 1, false>(a, gs, v, sm, epoch, buf, tr, 2))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -1109,7 +1115,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         Store<T, IV>(Z + ri, zv);
         FG_ROWS_END
       }
-      if (!GridReduce<KP, IV, 2, false>(a, v, sm, epoch, buf, tr, 2))
+      if (!GridReduce<KP, IV, 2, false>(a, gs, v, sm, epoch, buf, tr, 2))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -1181,7 +1187,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
         }
       Store<T, IV>(R + ri, rv);
       FG_ROWS_END
-      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
+      if (!GridReduce<KP, IV, 1, false>(a, gs, v, sm, epoch, buf, tr, 3))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -1212,7 +1218,7 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
       FG_ROWS_BEGIN
       settle_x(ri, f, s, v[0]);
       FG_ROWS_END
-      if (!GridReduce<KP, IV, 1, false>(a, v, sm, epoch, buf, tr, 3))
+      if (!GridReduce<KP, IV, 1, false>(a, gs, v, sm, epoch, buf, tr, 3))
         return;
       if (threadIdx.x < KP) {
         const int it = threadIdx.x;
@@ -1232,15 +1238,36 @@ __global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
 #undef FG_ROWS_BEGIN
 #undef FG_ROWS_END
 
-  if (blockIdx.x == 0 && threadIdx.x < a.items) {
+  if (gs.rank == 0 && threadIdx.x < a.items) {
     const int it = threadIdx.x;
     a.info[3 * it] = static_cast<double>(ctl.status[it]);
     a.info[3 * it + 1] = static_cast<double>(ctl.iters[it]);
     a.info[3 * it + 2] = ctl.resid[it];
   }
-  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0)
+  if (a.trace && gs.rank == 0 && threadIdx.x == 0)
     for (int s = 0; s < kPcgTraceSlots; ++s)
       a.trace[s] += tr.slot[s];
+}
+
+template <typename T, int KP, int IV, int BS>
+__global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
+{
+  PcgBody<T, KP, IV, BS>(a, GridShape{static_cast<int>(gridDim.x), static_cast<int>(blockIdx.x)});
+}
+
+// Several independent PCG solves (one per plan: its own operator, vectors, barrier and
+// partials) in one cooperative launch: CTA b belongs to group cta_group[b] and is rank
+// b - group_first of its group's group_size CTAs.
+template <typename T, int KP, int IV, int BS>
+__global__ void __launch_bounds__(kPcgThreads, 2) MultiPcgKernel(PcgGroups t)
+{
+  __shared__ PcgArgs group_args;
+  const int g = t.cta_group[blockIdx.x];
+  if (threadIdx.x == 0)
+    group_args = t.args[g];
+  __syncthreads();
+  PcgBody<T, KP, IV, BS>(group_args,
+                         GridShape{t.group_size[g], static_cast<int>(blockIdx.x) - t.group_first[g]});
 }
 
 } // namespace

@@ -559,9 +559,31 @@ Status Plan::SolveDevice(const SolveRequest &req)
 
 Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
 {
+  Chunk c;
+  Status s = ChunkBegin(req, first, k, &c);
+  if (s != Status::kOk || !c.valid)
+    return s;
+  while (c.iteration < req.options.max_newton_iterations && c.active) {
+    if ((s = ChunkAssemble(&c)) != Status::kOk || (s = ChunkLinear(&c)) != Status::kOk ||
+        (s = ChunkNorms(&c, false)) != Status::kOk)
+      return s;
+    if (cudaStreamSynchronize(req.stream) != cudaSuccess)
+      return Status::kInternalError;
+    if ((s = ChunkDecide(&c)) != Status::kOk || (s = ChunkUpdate(&c)) != Status::kOk)
+      return s;
+  }
+  return ChunkFinish(&c);
+}
+
+Status Plan::ChunkBegin(const SolveRequest &req, int first, int k, Chunk *c)
+{
   const fg_solve_options &o = req.options;
-  const int N = host_.N, E = host_.E, C = host_.C;
+  const int N = host_.N, C = host_.C;
   cudaStream_t st = req.stream;
+  c->req = &req;
+  c->first = first;
+  c->k = k;
+  c->valid = false;
   for (int i = 0; i < k; ++i) {
     fg_item_info &inf = req.info[first + i];
     inf = fg_item_info{};
@@ -574,31 +596,32 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
       o.max_newton_iterations < 0 || o.max_linear_iterations < 0)
     return Status::kOk; // per-item INVALID_ARGUMENT, as SolveBatch returns
   const int kp = PadItems(k);
+  c->kp = kp;
   Status s = EnsureWorkspace(kp);
   if (s != Status::kOk)
     return s;
-  const double *currents = req.currents + static_cast<size_t>(first) * C;
-  const double *hc = req.hc_scale ? req.hc_scale + first : nullptr;
+  c->currents = req.currents + static_cast<size_t>(first) * C;
+  c->hc = req.hc_scale ? req.hc_scale + first : nullptr;
   const double *warm = req.warm ? req.warm + static_cast<size_t>(first) * N : nullptr;
 
   // Non-finite currents make an item invalid before any work (nonlinear_solver.cu:198-206).
   uint32_t active = 0;
   {
     std::vector<double> cur(static_cast<size_t>(k) * C);
-    if (C > 0 && cudaMemcpyAsync(cur.data(), currents, cur.size() * sizeof(double),
+    if (C > 0 && cudaMemcpyAsync(cur.data(), c->currents, cur.size() * sizeof(double),
                                  cudaMemcpyDeviceToHost, st) != cudaSuccess)
       return Status::kInternalError;
     if (cudaStreamSynchronize(st) != cudaSuccess)
       return Status::kInternalError;
     for (int i = 0; i < k; ++i) {
       bool finite = true;
-      for (int c = 0; c < C; ++c)
-        finite = finite && std::isfinite(cur[static_cast<size_t>(i) * C + c]);
+      for (int j = 0; j < C; ++j)
+        finite = finite && std::isfinite(cur[static_cast<size_t>(i) * C + j]);
       if (finite)
         active |= 1u << i;
     }
   }
-  const bool adaptive = o.adaptive_linear_tolerance != 0 && host_.has_nonlinear;
+  c->adaptive = o.adaptive_linear_tolerance != 0 && host_.has_nonlinear;
   uint32_t warm_mask = warm ? active : 0u;
   if (warm && req.guard_warm && active) {
     // Equation residual ||K(A) A - b|| at the zero start and at the warm start; an item
@@ -611,7 +634,7 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
                               invalid_.get(), st) != cudaSuccess ||
           LaunchGatherValues(dev_, kp, ev_.get(), active, values_.get(), diag_.get(), invd_.get(),
                              invalid_.get(), st) != cudaSuccess ||
-          LaunchGatherRhs(dev_, kp, er_.get(), currents, hc, active, rhs_.get(), st) != cudaSuccess ||
+          LaunchGatherRhs(dev_, kp, er_.get(), c->currents, c->hc, active, rhs_.get(), st) != cudaSuccess ||
           LaunchStateToFree(dev_, kp, state_.get(), x0_.get(), st) != cudaSuccess ||
           LaunchEquationResidual(dev_, kp, values_.get(), rhs_.get(), x0_.get(), nullptr,
                                  norm_partials_.get(), norms_.get(), st) != cudaSuccess ||
@@ -632,127 +655,229 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
   if (LaunchInitState(dev_, kp, warm, k, warm_mask, state_.get(), st) != cudaSuccess)
     return Status::kInternalError;
   timing_.kernel_launches += 1;
-  std::vector<double> relax(k, 1.0), prev(k, std::numeric_limits<double>::infinity());
-  double *h = small_.get();
-  for (int iteration = 0; iteration < o.max_newton_iterations && active; ++iteration) {
-    double tol = std::numeric_limits<double>::infinity();
-    for (int i = 0; i < k; ++i)
-      if ((active >> i) & 1u)
-        tol = std::min(tol, NewtonLinearTolerance(o, adaptive, prev[i]));
-    // Iteration 0 of a cold start uses the cold secant; a warm start is Newton from the
-    // first iteration (nonlinear_solver.cu:698).
-    const uint32_t newton_mask = iteration > 0 ? active : (active & warm_mask);
+  c->active = active;
+  c->warm_mask = warm_mask;
+  c->relax.assign(k, 1.0);
+  c->prev.assign(k, std::numeric_limits<double>::infinity());
+  c->iteration = 0;
+  c->valid = true;
+  return Status::kOk;
+}
+
+// The inner tolerance of this Newton step: the tightest of the active items'
+// (BatchNewtonLinearTolerance, nonlinear_model.cpp:176-184).
+void Plan::ChunkTolerance(Chunk *c)
+{
+  const fg_solve_options &o = c->req->options;
+  c->tol = std::numeric_limits<double>::infinity();
+  for (int i = 0; i < c->k; ++i)
+    if ((c->active >> i) & 1u)
+      c->tol = std::min(c->tol, NewtonLinearTolerance(o, c->adaptive, c->prev[i]));
+}
+
+// Enqueues the Newton system of the active items at the current state.
+Status Plan::ChunkAssemble(Chunk *c)
+{
+  cudaStream_t st = c->req->stream;
+  const int kp = c->kp;
+  ChunkTolerance(c);
+  // Iteration 0 of a cold start uses the cold secant; a warm start is Newton from the
+  // first iteration (nonlinear_solver.cu:698).
+  const uint32_t newton_mask = c->iteration > 0 ? c->active : (c->active & c->warm_mask);
+  if (c->timed)
     cudaEventRecord(ev_start_, st);
-    if (cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) != cudaSuccess ||
-        LaunchElementKernel(dev_, kp, state_.get(), newton_mask, active, ev_.get(), er_.get(),
-                            invalid_.get(), st) != cudaSuccess ||
-        LaunchGatherValues(dev_, kp, ev_.get(), active, values_.get(), diag_.get(), invd_.get(),
-                           invalid_.get(), st) != cudaSuccess ||
-        LaunchGatherRhs(dev_, kp, er_.get(), currents, hc, active, rhs_.get(), st) != cudaSuccess)
-      return Status::kInternalError;
-    timing_.kernel_launches += 3;
+  if (cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) != cudaSuccess ||
+      LaunchElementKernel(dev_, kp, state_.get(), newton_mask, c->active, ev_.get(), er_.get(),
+                          invalid_.get(), st) != cudaSuccess ||
+      LaunchGatherValues(dev_, kp, ev_.get(), c->active, values_.get(), diag_.get(), invd_.get(),
+                         invalid_.get(), st) != cudaSuccess ||
+      LaunchGatherRhs(dev_, kp, er_.get(), c->currents, c->hc, c->active, rhs_.get(), st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 3;
+  if (c->timed)
     cudaEventRecord(ev_mid_, st);
-    double linfo[3 * kMaxItems];
-    s = LinearSolve(kp, k, active, tol, o.max_linear_iterations, st, linfo);
-    if (s != Status::kOk)
-      return s;
-    cudaEventRecord(ev_pcg_, st);
-    if (LaunchNewtonNorms(dev_, kp, x_.get(), state_.get(), norm_partials_.get(), norms_.get(), st) !=
-        cudaSuccess)
+  return Status::kOk;
+}
+
+bool Plan::ChunkPcgArgs(const Chunk &c, unsigned *barrier, int32_t *error, PcgArgs *out)
+{
+  if (options_.precision != FG_PRECISION_FP64 || block_size() != 0 || from_iterate_)
+    return false;
+  PcgArgs a{};
+  a.n = host_.n;
+  a.n_pad = host_.n_pad;
+  a.slices = host_.slices;
+  a.kp = c.kp;
+  a.items = c.k;
+  a.slice_off = slice_off_.get();
+  a.row_len = row_len_.get();
+  a.sell_col = sell_col_.get();
+  a.values = values_.get();
+  a.value_stride = c.kp;
+  a.value_item = 1;
+  a.diag = diag_.get();
+  a.invd = invd_.get();
+  a.diag_stride = c.kp;
+  a.diag_item = 1;
+  a.use_inverse = 1;
+  a.b = rhs_.get();
+  a.x = x_.get();
+  a.r = r_.get();
+  a.z = z_.get();
+  a.p0 = p0_.get();
+  a.p1 = p1_.get();
+  a.q = q_.get();
+  a.partials = pcg_partials_.get();
+  a.barrier = barrier;
+  a.error = error;
+  a.info = pcg_info_.get();
+  a.tolerance = c.tol;
+  a.max_iterations = c.req->options.max_linear_iterations;
+  a.active_mask = c.active;
+  a.timeout_ns = 5000000000LL;
+  *out = a;
+  return true;
+}
+
+Status Plan::ChunkLinear(Chunk *c)
+{
+  Status s = LinearSolve(c->kp, c->k, c->active, c->tol, c->req->options.max_linear_iterations,
+                         c->req->stream, c->linfo);
+  if (s == Status::kOk && c->timed)
+    cudaEventRecord(ev_pcg_, c->req->stream);
+  return s;
+}
+
+// Step norms and the small summary back to the host (asynchronously, into small_):
+// PCG info [3kp] (copied from the device when linfo_on_device), norms [2kp], assembly
+// flags, the PCG error flag.
+Status Plan::ChunkNorms(Chunk *c, bool linfo_on_device)
+{
+  cudaStream_t st = c->req->stream;
+  const int kp = c->kp;
+  double *h = small_.get();
+  if (LaunchNewtonNorms(dev_, kp, x_.get(), state_.get(), norm_partials_.get(), norms_.get(), st) !=
+      cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 2;
+  if (linfo_on_device) {
+    if (cudaMemcpyAsync(h, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess)
       return Status::kInternalError;
-    timing_.kernel_launches += 2;
-    // Small summary back to the host: norms [2kp], assembly flags, PCG error.
-    std::memcpy(h, linfo, sizeof(double) * 3 * kp);
-    if (cudaMemcpyAsync(h + 3 * kp, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 5 * kp), invalid_.get(), sizeof(int32_t) * kp,
-                        cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 6 * kp), error_.get(), sizeof(int32_t),
-                        cudaMemcpyDeviceToHost, st) != cudaSuccess)
-      return Status::kInternalError;
-    if (cudaStreamSynchronize(st) != cudaSuccess)
-      return Status::kInternalError;
+  } else {
+    std::memcpy(h, c->linfo, sizeof(double) * 3 * kp);
+  }
+  if (cudaMemcpyAsync(h + 3 * kp, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 5 * kp), invalid_.get(), sizeof(int32_t) * kp,
+                      cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(reinterpret_cast<int32_t *>(h + 6 * kp), error_.get(), sizeof(int32_t),
+                      cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return Status::kInternalError;
+  return Status::kOk;
+}
+
+// Host Newton policy after the summary has arrived: statuses, relaxation, the step gate.
+Status Plan::ChunkDecide(Chunk *c)
+{
+  const fg_solve_options &o = c->req->options;
+  const int kp = c->kp, k = c->k;
+  const double *h = small_.get();
+  if (c->timed) {
     timing_.assembly_ms += Elapsed(ev_start_, ev_mid_);
     timing_.pcg_ms += Elapsed(ev_mid_, ev_pcg_);
-    timing_.newton_iterations += 1;
-    const double *pinfo = h, *norms = h + 3 * kp;
-    const int32_t *invalid = reinterpret_cast<const int32_t *>(h + 5 * kp);
-    const int32_t pcg_error = *reinterpret_cast<const int32_t *>(h + 6 * kp);
-    if (pcg_error != 0)
-      return Status::kInternalError;
-    int max_its = 0;
-    ItemScalars rel{};
-    uint32_t update = 0;
-    const uint32_t was_active = active;
-    for (int i = 0; i < k; ++i) {
-      if (!((was_active >> i) & 1u))
-        continue;
-      fg_item_info &inf = req.info[first + i];
-      if (invalid[i]) {
-        inf.status = ToInt(Status::kAssemblyFailed);
-        active &= ~(1u << i);
-        continue;
-      }
-      const int pstatus = static_cast<int>(pinfo[3 * i]);
-      const int pits = static_cast<int>(pinfo[3 * i + 1]);
-      max_its = std::max(max_its, pits);
-      inf.linear_iterations += pits;
-      inf.last_linear_tolerance = tol;
-      if (pstatus != 0) {
-        inf.status = pstatus;
-        inf.iterations = pits;
-        inf.residual_l2 = pinfo[3 * i + 2];
-        active &= ~(1u << i);
-        continue;
-      }
-      const double dd = norms[i], cc = norms[kp + i];
-      const double residual =
-          std::sqrt(dd) / std::max(std::sqrt(cc), std::numeric_limits<double>::min());
-      inf.iterations = iteration + 1;
-      inf.residual_l2 = residual;
-      if (!std::isfinite(residual)) {
-        inf.status = ToInt(Status::kNumericalNonfinite);
-        active &= ~(1u << i);
-        continue;
-      }
-      if (iteration > 5) {
-        if (residual > prev[i] && relax[i] > 0.125)
-          relax[i] *= 0.5;
-        else
-          relax[i] += 0.1 * (1.0 - relax[i]);
-      }
-      rel.v[i] = relax[i];
-      update |= 1u << i;
-      if (iteration > 0 && residual < 100.0 * o.relative_tolerance &&
-          tol <= o.linear_relative_tolerance) {
-        inf.status = ToInt(Status::kOk);
-        active &= ~(1u << i);
-      } else {
-        prev[i] = residual;
-      }
-    }
-    timing_.pcg_iterations += max_its;
-    cudaEventRecord(ev_start_, st);
-    if (update && LaunchNewtonUpdate(dev_, kp, x_.get(), state_.get(), rel, update, st) != cudaSuccess)
-      return Status::kInternalError;
-    timing_.kernel_launches += update ? 1 : 0;
-    cudaEventRecord(ev_end_, st);
   }
+  timing_.newton_iterations += 1;
+  const double *pinfo = h, *norms = h + 3 * kp;
+  const int32_t *invalid = reinterpret_cast<const int32_t *>(h + 5 * kp);
+  const int32_t pcg_error = *reinterpret_cast<const int32_t *>(h + 6 * kp);
+  if (pcg_error != 0)
+    return Status::kInternalError;
+  int max_its = 0;
+  c->rel = ItemScalars{};
+  c->update = 0;
+  const uint32_t was_active = c->active;
+  for (int i = 0; i < k; ++i) {
+    if (!((was_active >> i) & 1u))
+      continue;
+    fg_item_info &inf = c->req->info[c->first + i];
+    if (invalid[i]) {
+      inf.status = ToInt(Status::kAssemblyFailed);
+      c->active &= ~(1u << i);
+      continue;
+    }
+    const int pstatus = static_cast<int>(pinfo[3 * i]);
+    const int pits = static_cast<int>(pinfo[3 * i + 1]);
+    max_its = std::max(max_its, pits);
+    inf.linear_iterations += pits;
+    inf.last_linear_tolerance = c->tol;
+    if (pstatus != 0) {
+      inf.status = pstatus;
+      inf.iterations = pits;
+      inf.residual_l2 = pinfo[3 * i + 2];
+      c->active &= ~(1u << i);
+      continue;
+    }
+    const double dd = norms[i], cc = norms[kp + i];
+    const double residual = std::sqrt(dd) / std::max(std::sqrt(cc), std::numeric_limits<double>::min());
+    inf.iterations = c->iteration + 1;
+    inf.residual_l2 = residual;
+    if (!std::isfinite(residual)) {
+      inf.status = ToInt(Status::kNumericalNonfinite);
+      c->active &= ~(1u << i);
+      continue;
+    }
+    if (c->iteration > 5) {
+      if (residual > c->prev[i] && c->relax[i] > 0.125)
+        c->relax[i] *= 0.5;
+      else
+        c->relax[i] += 0.1 * (1.0 - c->relax[i]);
+    }
+    c->rel.v[i] = c->relax[i];
+    c->update |= 1u << i;
+    if (c->iteration > 0 && residual < 100.0 * o.relative_tolerance && c->tol <= o.linear_relative_tolerance) {
+      inf.status = ToInt(Status::kOk);
+      c->active &= ~(1u << i);
+    } else {
+      c->prev[i] = residual;
+    }
+  }
+  timing_.pcg_iterations += max_its;
+  return Status::kOk;
+}
+
+Status Plan::ChunkUpdate(Chunk *c)
+{
+  cudaStream_t st = c->req->stream;
+  if (c->update && LaunchNewtonUpdate(dev_, c->kp, x_.get(), state_.get(), c->rel, c->update, st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += c->update ? 1 : 0;
+  ++c->iteration;
+  return Status::kOk;
+}
+
+Status Plan::ChunkFinish(Chunk *c)
+{
+  const SolveRequest &req = *c->req;
+  const int N = host_.N, E = host_.E, C = host_.C, k = c->k, first = c->first;
+  cudaStream_t st = req.stream;
   for (int i = 0; i < k; ++i)
-    if ((active >> i) & 1u)
+    if ((c->active >> i) & 1u)
       req.info[first + i].status = ToInt(Status::kNonlinearSolveNotConverged);
-  cudaEventRecord(ev_mid_, st);
+  if (c->timed)
+    cudaEventRecord(ev_mid_, st);
   const cudaError_t fe = LaunchFinalize(
-      dev_, kp, k, state_.get(), req.a_out ? req.a_out + static_cast<size_t>(first) * N : nullptr,
+      dev_, c->kp, k, state_.get(), req.a_out ? req.a_out + static_cast<size_t>(first) * N : nullptr,
       req.b1_out ? req.b1_out + static_cast<size_t>(first) * E : nullptr,
       req.b2_out ? req.b2_out + static_cast<size_t>(first) * E : nullptr,
       req.flux_out ? req.flux_out + static_cast<size_t>(first) * C : nullptr, st);
   if (fe != cudaSuccess)
     return Status::kInternalError;
   timing_.kernel_launches += 3;
-  cudaEventRecord(ev_pcg_, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess)
-    return Status::kInternalError;
-  timing_.finalize_ms += Elapsed(ev_mid_, ev_pcg_);
+  if (c->timed) {
+    cudaEventRecord(ev_pcg_, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.finalize_ms += Elapsed(ev_mid_, ev_pcg_);
+  }
   return Status::kOk;
 }
 

@@ -51,6 +51,37 @@ private:
   Status Upload();
   Status EnsureWorkspace(int kp);
   Status SolveChunk(const SolveRequest &request, int first, int count);
+
+public:
+  // One chunk's Newton solve as steps, so that several plans can advance together
+  // (MultiSolver): Begin, then per iteration Assemble, the linear solve (Linear, or the
+  // shared multi-plan PCG), Norms, a stream synchronisation, Decide and Update; Finish.
+  struct Chunk {
+    const SolveRequest *req = nullptr;
+    int first = 0, k = 0, kp = 0, iteration = 0;
+    bool valid = false, adaptive = false, timed = true;
+    uint32_t active = 0, warm_mask = 0, update = 0;
+    const double *currents = nullptr, *hc = nullptr;
+    double tol = 0.0;
+    std::vector<double> relax, prev;
+    double linfo[3 * kMaxItems];
+    ItemScalars rel{};
+  };
+  Status ChunkBegin(const SolveRequest &request, int first, int count, Chunk *c);
+  void ChunkTolerance(Chunk *c);
+  Status ChunkAssemble(Chunk *c);
+  Status ChunkLinear(Chunk *c);
+  Status ChunkNorms(Chunk *c, bool linfo_on_device);
+  Status ChunkDecide(Chunk *c);
+  Status ChunkUpdate(Chunk *c);
+  Status ChunkFinish(Chunk *c);
+  // The FP64 Jacobi PCG of this plan's current system for a multi-plan launch (barrier and
+  // error flag supplied by the caller); false when the plan's options need another kernel.
+  bool ChunkPcgArgs(const Chunk &c, unsigned *barrier, int32_t *error, PcgArgs *out);
+  fg_timing &mutable_timing() { return timing_; }
+
+private:
+  friend class MultiSolver;
   Status RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                 int value_stride, int value_item, int diag_stride, int diag_item, int use_inverse,
                 cudaStream_t stream, const double *blocks = nullptr, const double *b = nullptr,

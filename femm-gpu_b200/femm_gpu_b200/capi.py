@@ -42,6 +42,7 @@ EXPORTED = [
     "fg_mlp_set_parameters", "fg_mlp_forward", "fg_mlp_loss_gradient", "fg_mlp_train",
     "fg_warm_create", "fg_warm_destroy", "fg_warm_project", "fg_warm_project_device",
     "fg_warm_predict", "fg_solve_batch_learned",
+    "fg_multi_create", "fg_multi_destroy", "fg_multi_solve", "fg_multi_last_timing",
 ]
 
 
@@ -127,6 +128,7 @@ def lib():
         _LIB.fg_mlp_parameter_count.restype = C.c_int64
         _LIB.fg_mlp_destroy.restype = None
         _LIB.fg_warm_destroy.restype = None
+        _LIB.fg_multi_destroy.restype = None
     return _LIB
 
 
@@ -361,3 +363,53 @@ def bh_eval(b, h, slope, field_b):
     out = np.zeros(4)
     lib().fg_bh_eval(C.c_int32(b.size), _p(b), _p(h), _p(slope), C.c_double(field_b), _p(out))
     return out
+
+
+class FgMultiTiming(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("newton_steps", C.c_int64), ("pcg_launches", C.c_int64),
+                ("graph_launches", C.c_int64), ("graph_captures", C.c_int64),
+                ("kernel_launches", C.c_int64), ("max_ctas", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Multi:
+    """fg_multi: one sample on each of several plans (meshes of any size), solved together
+    with one multi-plan PCG launch per Newton step.  The plans must outlive this object."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p._h for p in self.plans])
+        self._h = C.c_void_p()
+        st = lib().fg_multi_create(arr, C.c_int32(len(self.plans)), C.byref(self._h))
+        if st:
+            self._h = None
+            raise FgError(st, "fg_multi_create")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_multi_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def solve(self, currents, options: Optional[FgSolveOptions] = None, outputs=True):
+        """currents: one vector per plan.  Returns (a, b1, b2, flux, info) lists."""
+        M = len(self.plans)
+        cur = [np.ascontiguousarray(np.asarray(c, np.float64).ravel()) for c in currents]
+        a = [np.zeros(p.N) for p in self.plans] if outputs else None
+        b1 = [np.zeros(p.E) for p in self.plans] if outputs is True else None
+        b2 = [np.zeros(p.E) for p in self.plans] if outputs is True else None
+        flux = [np.zeros(max(p.C, 1)) for p in self.plans] if outputs else None
+        ptrs = lambda xs: None if xs is None else (C.c_void_p * M)(*[x.ctypes.data for x in xs])  # noqa: E731
+        info = (FgItemInfo * M)()
+        opts = options if options is not None else production_options()
+        st = lib().fg_multi_solve(self._h, ptrs(cur), C.byref(opts), ptrs(a), ptrs(b1), ptrs(b2),
+                                  ptrs(flux), info)
+        if st:
+            raise FgError(st, "fg_multi_solve")
+        return a, b1, b2, flux, [info[i] for i in range(M)]
+
+    def last_timing(self) -> FgMultiTiming:
+        t = FgMultiTiming()
+        lib().fg_multi_last_timing(self._h, C.byref(t))
+        return t

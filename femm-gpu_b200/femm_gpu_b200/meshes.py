@@ -228,3 +228,69 @@ def periodic_strip(m: int = 16, antiperiodic: bool = False, current_a: float = 1
         circuit_count=1, depth_m=0.01, problem_type=PLANAR,
         name=f"{'anti' if antiperiodic else ''}periodic_strip_m{m}",
     )
+
+
+def annular_sector(nr: int = 160, nt: int = 250, hc: float = 9.0e5, turns: float = 20.0) -> Model:
+    """Rotor-stator quarter machine: r in [0.02, 0.06] m, a 90-degree sector with
+    anti-periodic edges (4 poles: one surface magnet per sector), 12 stator slots (3 per
+    sector), a 1 mm air gap.  Radially: rotor iron [0.020, 0.040) on the saturating B-H
+    table; surface magnet [0.040, 0.045) over the central 70 degrees of the pole
+    (mu_r 1.05, Hc = ``hc``, magnetised along the pole axis at 45 degrees), air between
+    magnets; air gap [0.045, 0.046); stator [0.046, 0.060] with three 15-degree slots
+    [0.047, 0.055) centred at 15, 45 and 75 degrees, each a coil of ``turns`` turns of one
+    series circuit (3 circuits), iron elsewhere.  A = 0 on the outer radius; the shaft
+    radius is a natural boundary.  nr x nt quads split into triangles on the polar grid;
+    nr = 160, nt = 250 gives 40,411 nodes / 80,000 triangles."""
+    r0, r1 = 0.02, 0.06
+    rs = np.linspace(r0, r1, nr + 1)
+    ts = np.linspace(0.0, 0.5 * np.pi, nt + 1)
+    T, R = np.meshgrid(ts, rs)  # row = r index, column = theta index: node = i * (nt + 1) + j
+    xy = np.stack([(R * np.cos(T)).ravel(), (R * np.sin(T)).ravel()], axis=1)
+    i, j = np.meshgrid(np.arange(nr), np.arange(nt), indexing="ij")
+    a = (i * (nt + 1) + j).ravel()  # (r_i, t_j)
+    b = a + 1                        # (r_i, t_j+1)
+    c = a + (nt + 1)                 # (r_i+1, t_j)
+    d = c + 1                        # (r_i+1, t_j+1)
+    tri = np.empty((2 * a.size, 3), dtype=np.int64)
+    # (r, theta) -> (x, y) preserves orientation for r > 0: (a, c, d) and (a, d, b) are CCW.
+    tri[0::2] = np.stack([a, c, d], axis=1)
+    tri[1::2] = np.stack([a, d, b], axis=1)
+    tri = tri.astype(np.int32)
+    cen = xy[tri].mean(axis=1)
+    rc = np.hypot(cen[:, 0], cen[:, 1])
+    tc = np.degrees(np.arctan2(cen[:, 1], cen[:, 0]))
+    mat = np.zeros(tri.shape[0], np.int32)  # 0 air
+    mat[rc < 0.040] = 1  # rotor iron
+    mat[(rc >= 0.040) & (rc < 0.045) & (np.abs(tc - 45.0) <= 35.0)] = 2  # magnet
+    stator = rc >= 0.046
+    mat[stator] = 3  # stator iron
+    for k, centre in enumerate((15.0, 45.0, 75.0)):
+        slot = stator & (rc >= 0.047) & (rc < 0.055) & (np.abs(tc - centre) <= 7.5)
+        mat[slot] = 4 + k
+    area = 0.5 * _signed_area2(xy, tri)
+    jpa = [turns / area[mat == 4 + k].sum() for k in range(3)]
+    nu_air = 1.0 / MU0
+    b_t, h = bh_table_saturating(24)
+    idx = np.arange(xy.shape[0])
+    ii, jj = idx // (nt + 1), idx % (nt + 1)
+    outer = idx[ii == nr].astype(np.int32)
+    left = idx[(jj == 0) & (ii < nr)]
+    right = idx[(jj == nt) & (ii < nr)]
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air, nu_air / 1.05, nu_air, nu_air, nu_air, nu_air],
+        alpha=np.zeros(7),
+        j_per_a=[0.0, 0.0, 0.0, 0.0, jpa[0], jpa[1], jpa[2]],
+        hc=[0.0, 0.0, hc, 0.0, 0.0, 0.0, 0.0],
+        mag_deg=[0.0, 0.0, 45.0, 0.0, 0.0, 0.0, 0.0],
+        curve_index=[-1, 0, -1, 0, -1, -1, -1],
+        circuit_index=[-1, -1, -1, -1, 0, 1, 2],
+        group=[0, 1, 2, 3, 4, 5, 6],
+        curves=[(b_t, h)],
+        dir_nodes=outer,
+        dir_values=np.zeros(outer.size),
+        con_a=left, con_b=right,
+        con_sign=np.full(left.size, -1, np.int8),
+        circuit_count=3, depth_m=0.05, problem_type=PLANAR,
+        name=f"annular_sector_{nr}x{nt}",
+    )

@@ -278,6 +278,38 @@ void fg_bh_eval(int32_t count, const double *b, const double *h, const double *s
                 double field_b, double *h_dh_nu_dnu);
 
 /* ------------------------------------------------------------------------------------
+ * Heterogeneous batches (no counterpart in the reference, which solves one operator per
+ * launch group).  Independent meshes -- one plan each, of any size -- are solved in
+ * lock-step, one sample per plan: per Newton iteration every active plan is assembled and
+ * all their PCG solves run in ONE cooperative launch, each on its own group of CTAs, with
+ * per-plan convergence; from the second iteration the assembly + PCG + norm sequence is a
+ * replayed CUDA graph.  An online tuner divides the CTAs by predicted cost (rows x
+ * iterations, from each plan's previous Newton step).  Plans must use the FP64 Jacobi
+ * form; they are borrowed and must outlive the fg_multi.
+ * ------------------------------------------------------------------------------------ */
+typedef struct fg_multi fg_multi;
+
+typedef struct fg_multi_timing {
+  double total_ms;          /* wall time of the last fg_multi_solve */
+  int64_t newton_steps;     /* lock-step Newton iterations */
+  int64_t pcg_launches;     /* multi-plan PCG launches */
+  int64_t graph_launches;   /* replays of captured iterations */
+  int64_t graph_captures;   /* (re)captures: once per distinct set of active plans */
+  int64_t kernel_launches;  /* launches outside graphs, plus captured kernels per replay */
+  int32_t max_ctas;         /* largest CTA count of one PCG launch */
+  int32_t reserved;
+} fg_multi_timing;
+
+int fg_multi_create(fg_plan *const *plans, int32_t count, fg_multi **multi);
+void fg_multi_destroy(fg_multi *multi);
+/* One sample per plan: currents[m] -> [C_m]; outputs per plan (host, each may be NULL):
+ * a_out[m] [N_m], b1_out[m] / b2_out[m] [E_m], flux_out[m] [C_m]; info [count]. */
+int fg_multi_solve(fg_multi *multi, const double *const *currents, const fg_solve_options *options,
+                   double *const *a_out, double *const *b1_out, double *const *b2_out,
+                   double *const *flux_out, fg_item_info *info);
+int fg_multi_last_timing(const fg_multi *multi, fg_multi_timing *timing);
+
+/* ------------------------------------------------------------------------------------
  * Learned warm start (no counterpart in the reference).  A reduced basis of A (mean +
  * rank orthonormal modes) whose coefficients a small MLP predicts from per-sample
  * features (circuit currents and magnet-angle terms, normalised by the caller's shift and

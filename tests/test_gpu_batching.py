@@ -1,0 +1,76 @@
+"""Batched forms on the GPU against the oracle.
+
+* Shared geometry with per-sample magnets (the rotor-stator sector, anti-periodic edges):
+  fg_solve_batch with per-item coercivity scales equals the oracle solving each sample's
+  own model (Hc scaled), item by item: same status and Newton iteration count, flux
+  linkage within 1e-8 (relative 2-norm), A within 5e-9, B within 5e-8 of max |B|.  These
+  bounds are looser than the other Newton tests' (A 1e-9, B 1e-8) because these samples
+  drive the iron to 2 T and take about 40 relaxed Newton iterations: each inner solve may
+  differ from the oracle's by cond(K) x 1e-10 and the relaxed iteration carries that
+  forward (measured: A 1.1e-9, B 1.3e-8 of max |B|).
+"""
+import numpy as np
+import pytest
+
+import femm_gpu_b200 as fg
+import oracle as O
+from femm_gpu_b200 import meshes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300)
+
+
+def test_shared_geometry_batch_with_per_sample_magnets(gpu):
+    model = meshes.annular_sector(nr=24, nt=36)
+    rng = np.random.default_rng(31)
+    k = 5
+    currents = rng.uniform(-15.0, 15.0, size=(k, 3))
+    hc = rng.uniform(8.5e5, 9.5e5, size=k)
+    plan = fg.Plan(model)
+    got = plan.solve(currents, hc_scale=hc / 9.0e5)
+    for i in range(k):
+        mi = meshes.annular_sector(nr=24, nt=36, hc=hc[i])
+        a, b1, b2, flux, info = O.solve_batch(mi, currents[i:i + 1])
+        assert got.info[i].status == info[0].status == 0
+        assert got.info[i].iterations == info[0].iterations
+        assert rel(got.a[i], a[0]) <= 5e-9
+        assert rel(got.flux[i], flux[0]) <= 1e-8
+        bmax = max(np.abs(b1[0]).max(), np.abs(b2[0]).max())
+        assert np.abs(got.b1[i] - b1[0]).max() <= 5e-8 * bmax
+    # the anti-periodic edges hold: A(theta = 90 deg) = -A(theta = 0)
+    pair = got.a[:, model.con_b] + got.a[:, model.con_a]
+    assert np.abs(pair).max() <= 1e-15 * np.abs(got.a).max()
+
+
+def test_heterogeneous_meshes_in_one_launch_match_single_solves(gpu):
+    """Independent jittered squares of different sizes, one sample each, solved together
+    (one multi-plan PCG launch per Newton step, graph replays after the first step): every
+    mesh's result equals the same sample solved alone on its plan (same status and Newton
+    iterations; flux within 1e-8, A within 5e-9: the multi launch gives a plan a different
+    CTA count, so its reductions round differently and the two answers may differ by
+    cond(K) x 1e-10, measured 1.03e-9) and the oracle's."""
+    sizes = [10, 37, 16, 52, 23, 8, 64]
+    models = [meshes.square_nonlinear(m=m, seed=100 + m) for m in sizes]
+    currents = [meshes.seeded_currents(1, 3, 20.0, seed=200 + m)[0] for m in sizes]
+    plans = [fg.Plan(mo) for mo in models]
+    multi = fg.Multi(plans)
+    a, b1, b2, flux, info = multi.solve(currents)
+    t = multi.last_timing()
+    assert t.pcg_launches == t.newton_steps >= max(i.iterations for i in info)
+    assert t.graph_launches >= 1 and t.graph_captures >= 1
+    for i, mo in enumerate(models):
+        alone = fg.Plan(mo).solve([currents[i]])
+        assert info[i].status == alone.info[0].status == 0
+        assert info[i].iterations == alone.info[0].iterations
+        assert rel(a[i], alone.a[0]) <= 5e-9
+        assert rel(flux[i][:3], alone.flux[0]) <= 1e-8
+        ao, _, _, fo, io = O.solve_batch(mo, currents[i][None, :])
+        assert io[0].status == 0 and rel(a[i], ao[0]) <= 5e-9
+    # a second solve on the same object replays its graphs again and matches the first
+    a2, _, _, flux2, info2 = multi.solve(currents)
+    for i in range(len(models)):
+        assert info2[i].iterations == info[i].iterations
+        assert rel(a2[i], a[i]) <= 1e-12

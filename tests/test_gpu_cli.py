@@ -108,16 +108,15 @@ def test_solver_options_mixed_block_jacobi(gpu, tmp_path):
 
 def test_postprocess_requests_are_refused_after_the_solve(gpu, tmp_path):
     # A legacy planar-DC artifact (no node constraints) with a force request.
-    src = json.load(open(os.path.join(GOLDEN, "axisymmetric_coil.gpu.json")))
+    from femm_gpu_b200 import meshes
+    text, _ = artifact.write_artifact(meshes.square_linear(m=12), [12.0])
+    src = json.loads(text)
     src["schema_version"] = "gpu_femm_planar_dc_mesh_v1"
     res = src["resolved"]
     del res["node_constraints"]
-    res["model"]["problem_type"] = "planar"
     for i, r in enumerate(res["regions"]):
         r["group_number"] = i  # distinct block-label groups for the force request
-    text = json.dumps(src)
-    model_text = artifact._loads(text)
-    src["canonical_identity_sha256"] = artifact.canonical_sha256(model_text["resolved"])
+    src["canonical_identity_sha256"] = artifact.canonical_sha256(artifact._loads(json.dumps(src))["resolved"])
     path = tmp_path / "legacy.gpu.json"
     path.write_text(json.dumps(src))
     groups = sorted({int(r["group_number"]) for r in res["regions"]})
