@@ -20,7 +20,10 @@ Forms (N = 1, rank 0; skipped with --no-forms): the same samples through block-J
 the FP32-inner mixed PCG (reliable updates) and the PCG started from the Newton iterate,
 each with solves/s, iterations and its error against the plain FP64 solutions; and the
 learned warm start on the axisymmetric plunger (about 100k nodes; --learned-train training
-solves, 256 held-out samples) against the plain zero start.
+solves, 256 held-out samples) against the plain zero start; the rotor-stator sector
+(--sector-samples samples sharing the mesh, per-sample currents and magnet strength); and
+--hetero-meshes independent meshes of 5k-200k nodes in one multi-plan launch per Newton
+step against solving them one plan at a time.
 
 Multi-GPU: replicas only -- every rank solves its own batch, no collective on the data
 path; ``value`` = all ranks' solves / max-over-ranks time (weak scaling).
@@ -56,6 +59,8 @@ def parse():
     p.add_argument("--no-forms", action="store_true", help="skip the mixed / block / learned forms")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm start form")
     p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
+    p.add_argument("--sector-samples", type=int, default=64, help="samples of the shared-geometry sector form")
+    p.add_argument("--hetero-meshes", type=int, default=64, help="meshes of the heterogeneous-batch form")
     return p.parse_args()
 
 
@@ -343,6 +348,68 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
                      "a_rel_err": err(a, ref_a), "flux_rel_err": err(f, ref_f),
                      "all_converged": all(i.status == 0 for i in info)}
         p.close()
+    # Shared geometry with per-sample magnets: the rotor-stator sector (40k nodes,
+    # anti-periodic edges), currents U[-15, 15] A and Hc U[8.5e5, 9.5e5] A/m per sample.
+    sector = meshes.annular_sector()
+    rng = np.random.default_rng(77)
+    ks = args.sector_samples
+    cur = rng.uniform(-15.0, 15.0, size=(ks, 3))
+    hcs = rng.uniform(8.5e5, 9.5e5, size=ks) / 9.0e5
+    res = {}
+    for name, kw in (("fp64_jacobi", {}),
+                     ("mixed_block8_from_iterate", dict(precision=1, preconditioner=1, block_size=8,
+                                                        from_iterate=True))):
+        p = fg.Plan(sector, **kw)
+        p.solve(cur[:8], hc_scale=hcs[:8], outputs="a")
+        t0 = time.perf_counter()
+        r = p.solve(cur, hc_scale=hcs, outputs="a")
+        dt = time.perf_counter() - t0
+        res[name] = {"solves_per_s_e2e": ks / dt,
+                     "newton_iterations_per_item": float(np.mean([i.iterations for i in r.info])),
+                     "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in r.info])),
+                     "all_converged": all(i.status == 0 for i in r.info), "a": r.a, "flux": r.flux}
+        p.close()
+    f = res["mixed_block8_from_iterate"]
+    f["a_rel_err"] = err(f["a"], res["fp64_jacobi"]["a"])
+    f["flux_rel_err"] = err(f["flux"], res["fp64_jacobi"]["flux"])
+    f["vs_fp64_jacobi"] = f["solves_per_s_e2e"] / res["fp64_jacobi"]["solves_per_s_e2e"]
+    for r_ in res.values():
+        r_.pop("a")
+        r_.pop("flux")
+    out["shared_geometry_sector"] = dict(
+        workload=f"rotor-stator sector, {sector.node_count} nodes, anti-periodic 90-degree edges, "
+                 f"{ks} samples with per-sample currents and magnet Hc; host-buffer API timing", **res)
+
+    # Heterogeneous meshes: jittered squares with node counts log-uniform in [5k, 200k],
+    # one sample each, in one multi-plan PCG launch per Newton step vs one plan at a time.
+    rng = np.random.default_rng(11)
+    count = args.hetero_meshes
+    ns = np.exp(rng.uniform(np.log(5e3), np.log(2e5), size=count))
+    models = [meshes.square_nonlinear(m=int(round(np.sqrt(n))) - 1, seed=1000 + i) for i, n in enumerate(ns)]
+    curs = [meshes.seeded_currents(1, 3, 20.0, seed=3000 + i)[0] for i in range(count)]
+    plans = [fg.Plan(mo) for mo in models]
+    multi = fg.Multi(plans)
+    multi.solve(curs, outputs=False)
+    t0 = time.perf_counter()
+    ma, _, _, mf, minfo = multi.solve(curs, outputs="a")
+    dt_multi = time.perf_counter() - t0
+    mt = multi.last_timing()
+    t0 = time.perf_counter()
+    single = [p.solve([c], outputs="a") for p, c in zip(plans, curs)]
+    dt_single = time.perf_counter() - t0
+    out["heterogeneous_meshes"] = {
+        "workload": f"{count} jittered squares, {sum(mo.node_count for mo in models)} nodes in all "
+                    "(5k-200k each, log-uniform), one sample each; host-buffer API timing",
+        "multi_solves_per_s": count / dt_multi, "one_plan_at_a_time_solves_per_s": count / dt_single,
+        "speedup": dt_single / dt_multi, "newton_steps": int(mt.newton_steps),
+        "pcg_launches": int(mt.pcg_launches), "graph_launches": int(mt.graph_launches),
+        "graph_captures": int(mt.graph_captures), "max_ctas": int(mt.max_ctas),
+        "all_converged": all(i.status == 0 for i in minfo),
+        "a_rel_err_vs_single": err(ma, [s_.a[0] for s_ in single])}
+    multi.close()
+    for p in plans:
+        p.close()
+
     if not args.no_learned:
         ax = meshes.axisymmetric_plunger()
         base = fg.Plan(ax)

@@ -233,14 +233,17 @@ def periodic_strip(m: int = 16, antiperiodic: bool = False, current_a: float = 1
 def annular_sector(nr: int = 160, nt: int = 250, hc: float = 9.0e5, turns: float = 20.0) -> Model:
     """Rotor-stator quarter machine: r in [0.02, 0.06] m, a 90-degree sector with
     anti-periodic edges (4 poles: one surface magnet per sector), 12 stator slots (3 per
-    sector), a 1 mm air gap.  Radially: rotor iron [0.020, 0.040) on the saturating B-H
-    table; surface magnet [0.040, 0.045) over the central 70 degrees of the pole
+    sector), a 1 mm air gap.  Radially: rotor iron [0.020, 0.043) on the saturating B-H
+    table; a 2 mm surface magnet [0.043, 0.045) over the central 60 degrees of the pole
     (mu_r 1.05, Hc = ``hc``, magnetised along the pole axis at 45 degrees), air between
     magnets; air gap [0.045, 0.046); stator [0.046, 0.060] with three 15-degree slots
-    [0.047, 0.055) centred at 15, 45 and 75 degrees, each a coil of ``turns`` turns of one
-    series circuit (3 circuits), iron elsewhere.  A = 0 on the outer radius; the shaft
-    radius is a natural boundary.  nr x nt quads split into triangles on the polar grid;
-    nr = 160, nt = 250 gives 40,411 nodes / 80,000 triangles."""
+    [0.046, 0.050), open at the gap, centred at 15, 45 and 75 degrees, each a coil of
+    ``turns`` turns of one series circuit (3 circuits), iron elsewhere.  The proportions
+    keep the 10 mm stator yoke near the knee of the B-H curve (about 1.8 T); the tooth
+    corners still reach 2 T, so Newton takes some 25-30 relaxed iterations.  A = 0 on the
+    outer radius; the shaft radius is a natural boundary.  nr x nt quads split into
+    triangles on the polar grid; nr = 160, nt = 250 gives 40,411 nodes / 80,000
+    triangles."""
     r0, r1 = 0.02, 0.06
     rs = np.linspace(r0, r1, nr + 1)
     ts = np.linspace(0.0, 0.5 * np.pi, nt + 1)
@@ -260,12 +263,12 @@ def annular_sector(nr: int = 160, nt: int = 250, hc: float = 9.0e5, turns: float
     rc = np.hypot(cen[:, 0], cen[:, 1])
     tc = np.degrees(np.arctan2(cen[:, 1], cen[:, 0]))
     mat = np.zeros(tri.shape[0], np.int32)  # 0 air
-    mat[rc < 0.040] = 1  # rotor iron
-    mat[(rc >= 0.040) & (rc < 0.045) & (np.abs(tc - 45.0) <= 35.0)] = 2  # magnet
+    mat[rc < 0.043] = 1  # rotor iron
+    mat[(rc >= 0.043) & (rc < 0.045) & (np.abs(tc - 45.0) <= 30.0)] = 2  # magnet
     stator = rc >= 0.046
     mat[stator] = 3  # stator iron
     for k, centre in enumerate((15.0, 45.0, 75.0)):
-        slot = stator & (rc >= 0.047) & (rc < 0.055) & (np.abs(tc - centre) <= 7.5)
+        slot = stator & (rc < 0.050) & (np.abs(tc - centre) <= 7.5)
         mat[slot] = 4 + k
     area = 0.5 * _signed_area2(xy, tri)
     jpa = [turns / area[mat == 4 + k].sum() for k in range(3)]
