@@ -236,6 +236,16 @@ def run_ours(args, world, rank, local):
     alg_bytes = item_its * per_item + pcg_its * shared
     achieved = alg_bytes / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
     peak, peak_kind = peaks()
+    # DRAM traffic of the PCG kernel from the committed ncu capture of this workload
+    # (profiles/pcg_square500_items8.md: bytes per CG iteration), per launch of this run.
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pcg_square500_items8.md")
+    if os.path.exists(prof) and args.mesh == MESH_M and k == 8:
+        import re
+        m_ = re.search(r"traffic_bytes_per_cg_iteration:\s*([0-9.eE+]+)", open(prof).read())
+        launches_timed = max(1, newton)
+        if m_:
+            traffic = float(m_.group(1)) * pcg_its / launches_timed
 
     # End to end through the host-buffer C ABI (H2D currents, D2H A / B / flux / info).
     host_in = [meshes.seeded_currents(k, Cc, 20.0, seed=777000 + 100000 * rank + s) for s in range(args.steps)]
@@ -265,7 +275,10 @@ def run_ours(args, world, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": "PcgKernel",
+                     "frac": achieved / peak, "traffic": traffic, "kernel": "PcgKernel",
+                     "traffic_source": "ncu capture of this workload, bytes per CG iteration x "
+                                       "iterations per launch (profiles/pcg_square500_items8.md)",
+                     "algorithmic_bytes_per_launch": alg_bytes / max(1, newton),
                      "peak_source": peak_kind, "pcg_ms": pcg_ms, "pcg_iterations": pcg_its,
                      "item_pcg_iterations": item_its},
         "newton_iterations": newton,
