@@ -132,6 +132,13 @@ cudaError_t LaunchNewtonUpdate(const DevicePlan &p, int kp, const double *x, dou
 // State = zero start (fixed values), or warm_item_major for items in warm_mask.
 cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm_item_major,
                             int items, uint32_t warm_mask, double *state, cudaStream_t stream);
+// Recovery: Armijo trial points, masked state copies and masked resets to the zero start
+// (items in mask only; nodal state arrays [N][kp]).
+cudaError_t LaunchTrial(const DevicePlan &p, int kp, const double *x, const double *saved,
+                        double *state, ItemScalars alpha, uint32_t mask, cudaStream_t stream);
+cudaError_t LaunchMaskedCopy(const DevicePlan &p, int kp, uint32_t mask, const double *from, double *to,
+                             cudaStream_t stream);
+cudaError_t LaunchResetState(const DevicePlan &p, int kp, uint32_t mask, double *state, cudaStream_t stream);
 // x[row][kp] = state[root node of row][kp] (free-row form of a nodal state; padding 0).
 cudaError_t LaunchStateToFree(const DevicePlan &p, int kp, const double *state, double *x,
                               cudaStream_t stream);

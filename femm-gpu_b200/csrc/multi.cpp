@@ -261,7 +261,9 @@ Status MultiSolver::Solve(const double *const *currents, const fg_solve_options 
   for (size_t m = 0; m < M; ++m) {
     if (!chunks_[m].valid)
       continue;
-    Status s = plans_[m]->ChunkFinish(&chunks_[m]);
+    Status s = plans_[m]->ChunkRecover(&chunks_[m]);
+    if (s == Status::kOk)
+      s = plans_[m]->ChunkFinish(&chunks_[m]);
     if (s != Status::kOk)
       return s;
   }

@@ -93,6 +93,40 @@ __global__ void UpdateKernel(DevicePlan p, const double *__restrict__ x, double 
   state[t] = s + relax.v[item] * (c - s);
 }
 
+// Recovery (SolveSafeguarded): state = saved + alpha (candidate - saved) for the items in
+// mask (an Armijo trial point), a masked copy, and a masked reset to the zero start.
+template <int KP>
+__global__ void TrialKernel(DevicePlan p, const double *__restrict__ x, const double *__restrict__ saved,
+                            double *__restrict__ state, ItemScalars alpha, uint32_t mask)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.N) * KP)
+    return;
+  const int node = static_cast<int>(t / KP), item = static_cast<int>(t % KP);
+  if (!((mask >> item) & 1u))
+    return;
+  const double c = Candidate(p, KP, x, node, item);
+  const double s = saved[t];
+  state[t] = s + alpha.v[item] * (c - s);
+}
+
+__global__ void MaskedCopyKernel(size_t count, int kp, uint32_t mask, const double *__restrict__ from,
+                                 double *__restrict__ to)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t < count && ((mask >> (t % kp)) & 1u))
+    to[t] = from[t];
+}
+
+__global__ void ResetStateKernel(DevicePlan p, int kp, uint32_t mask, double *__restrict__ state)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.N) * kp)
+    return;
+  if ((mask >> (t % kp)) & 1u)
+    state[t] = p.boundary[t / kp];
+}
+
 __global__ void InitStateKernel(DevicePlan p, int kp, const double *__restrict__ warm, int items,
                                 uint32_t warm_mask, double *__restrict__ state)
 {
@@ -325,6 +359,28 @@ cudaError_t LaunchInitState(const DevicePlan &p, int kp, const double *warm, int
 {
   InitStateKernel<<<Blocks(static_cast<size_t>(p.N) * kp), kThreads, 0, stream>>>(p, kp, warm, items,
                                                                                  warm_mask, state);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchTrial(const DevicePlan &p, int kp, const double *x, const double *saved,
+                        double *state, ItemScalars alpha, uint32_t mask, cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.N) * kp);
+  FG_DISPATCH_KP(kp, (TrialKernel<KP><<<blocks, kThreads, 0, stream>>>(p, x, saved, state, alpha, mask)));
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchMaskedCopy(const DevicePlan &p, int kp, uint32_t mask, const double *from, double *to,
+                             cudaStream_t stream)
+{
+  const size_t count = static_cast<size_t>(p.N) * kp;
+  MaskedCopyKernel<<<Blocks(count), kThreads, 0, stream>>>(count, kp, mask, from, to);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchResetState(const DevicePlan &p, int kp, uint32_t mask, double *state, cudaStream_t stream)
+{
+  ResetStateKernel<<<Blocks(static_cast<size_t>(p.N) * kp), kThreads, 0, stream>>>(p, kp, mask, state);
   return cudaGetLastError();
 }
 

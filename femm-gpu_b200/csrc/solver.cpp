@@ -227,8 +227,9 @@ Status Plan::EnsureWorkspace(int kp)
   FG_EN(barrier_, 1);
   FG_EN(error_, 1);
   FG_EN(invalid_, static_cast<size_t>(kp));
-  FG_EN(small_, static_cast<size_t>(10) * kp + 8);
+  FG_EN(small_, static_cast<size_t>(10) * kp + 8); // summary [0, 7kp), recovery [7kp, 10kp)
   FG_EN(x0_, vec);
+  FG_EN(saved_, static_cast<size_t>(h.N) * kp);
   FG_EN(d_, vec);
   FG_EN(item_tol_, static_cast<size_t>(kp));
   if (block_size() > 0) {
@@ -572,6 +573,8 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
     if ((s = ChunkDecide(&c)) != Status::kOk || (s = ChunkUpdate(&c)) != Status::kOk)
       return s;
   }
+  if ((s = ChunkRecover(&c)) != Status::kOk)
+    return s;
   return ChunkFinish(&c);
 }
 
@@ -852,6 +855,175 @@ Status Plan::ChunkUpdate(Chunk *c)
   timing_.kernel_launches += c->update ? 1 : 0;
   ++c->iteration;
   return Status::kOk;
+}
+
+// Equation residual ||J x0 - rhs|| and ||rhs|| of the items in mask at the current state
+// (the system must have been assembled there); res[i] receives the first, for all kp.
+Status Plan::EquationNorms(int kp, cudaStream_t st, double *res)
+{
+  if (LaunchStateToFree(dev_, kp, state_.get(), x0_.get(), st) != cudaSuccess ||
+      LaunchEquationResidual(dev_, kp, values_.get(), rhs_.get(), x0_.get(), nullptr, norm_partials_.get(),
+                             norms_.get(), st) != cudaSuccess ||
+      cudaMemcpyAsync(small_.get() + 8 * kp, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(reinterpret_cast<int32_t *>(small_.get() + 7 * kp), invalid_.get(), sizeof(int32_t) * kp,
+                      cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 3;
+  for (int i = 0; i < kp; ++i)
+    res[i] = std::sqrt(small_.get()[8 * kp + i]);
+  return Status::kOk;
+}
+
+// SolveSafeguarded (gpu_solver/src/solvers/nonlinear_solver.cu:534-659) for the items the
+// Newton loop exhausted, when the options ask for recovery (:515-530): from the zero start,
+// undamped Newton directions at the fixed linear tolerance, each accepted through Armijo
+// backtracking (at most 20 halvings, sufficient decrease 1e-4) on the equation residual
+// ||K(A) A - b||; done when the step is below 100 x relative_tolerance and the residual
+// has fallen by relative_tolerance.  The zero start already holds the expanded fixed
+// values, so the reference's root expansion before the first direction changes nothing.
+Status Plan::ChunkRecover(Chunk *c)
+{
+  const fg_solve_options &o = c->req->options;
+  const uint32_t rec = c->active;
+  if (!o.recover_nonconvergence || o.max_newton_iterations <= 0 || !rec)
+    return Status::kOk;
+  cudaStream_t st = c->req->stream;
+  const int kp = c->kp, k = c->k;
+  const double rel = o.relative_tolerance;
+  std::vector<int32_t> orig_its(k), orig_lin(k);
+  for (int i = 0; i < k; ++i) {
+    fg_item_info &inf = c->req->info[c->first + i];
+    orig_its[i] = inf.iterations;
+    orig_lin[i] = inf.linear_iterations;
+    if ((rec >> i) & 1u) {
+      inf.status = ToInt(Status::kNonlinearSolveNotConverged);
+      inf.iterations = 0;
+      inf.linear_iterations = 0;
+      inf.residual_l2 = std::numeric_limits<double>::infinity();
+    }
+  }
+  c->active &= ~rec;
+  auto assemble = [&](uint32_t mask) {
+    return cudaMemsetAsync(invalid_.get(), 0, sizeof(int32_t) * kp, st) == cudaSuccess &&
+           LaunchElementKernel(dev_, kp, state_.get(), mask, mask, ev_.get(), er_.get(), invalid_.get(), st) ==
+               cudaSuccess &&
+           LaunchGatherValues(dev_, kp, ev_.get(), mask, values_.get(), diag_.get(), invd_.get(), invalid_.get(),
+                              st) == cudaSuccess &&
+           LaunchGatherRhs(dev_, kp, er_.get(), c->currents, c->hc, mask, rhs_.get(), st) == cudaSuccess;
+  };
+  const int32_t *invalid = reinterpret_cast<const int32_t *>(small_.get() + 7 * kp);
+  std::vector<double> norm(kp, 0.0), scale(kp, 1.0), res(kp, 0.0);
+  if (LaunchResetState(dev_, kp, rec, state_.get(), st) != cudaSuccess || !assemble(rec))
+    return Status::kInternalError;
+  timing_.kernel_launches += 4;
+  Status s = EquationNorms(kp, st, res.data());
+  if (s != Status::kOk)
+    return s;
+  uint32_t run = rec;
+  for (int i = 0; i < k; ++i)
+    if ((rec >> i) & 1u) {
+      if (invalid[i]) {
+        c->req->info[c->first + i].status = ToInt(Status::kAssemblyFailed);
+        run &= ~(1u << i);
+      }
+      norm[i] = res[i];
+      scale[i] = std::max(norm[i], std::numeric_limits<double>::min());
+    }
+  for (int iteration = 0; iteration < o.max_newton_iterations && run; ++iteration) {
+    for (int i = 0; i < k; ++i)
+      if (((run >> i) & 1u) && !std::isfinite(norm[i])) {
+        c->req->info[c->first + i].status = ToInt(Status::kNumericalNonfinite);
+        run &= ~(1u << i);
+      }
+    if (!run)
+      break;
+    double linfo[3 * kMaxItems];
+    if ((s = LinearSolve(kp, k, run, o.linear_relative_tolerance, o.max_linear_iterations, st, linfo)) != Status::kOk)
+      return s;
+    double *h = small_.get();
+    if (LaunchNewtonNorms(dev_, kp, x_.get(), state_.get(), norm_partials_.get(), norms_.get(), st) != cudaSuccess ||
+        cudaMemcpyAsync(h, norms_.get(), sizeof(double) * 2 * kp, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 2;
+    timing_.newton_iterations += 1;
+    uint32_t trying = 0;
+    for (int i = 0; i < k; ++i) {
+      if (!((run >> i) & 1u))
+        continue;
+      fg_item_info &inf = c->req->info[c->first + i];
+      inf.linear_iterations += static_cast<int32_t>(linfo[3 * i + 1]);
+      inf.last_linear_tolerance = o.linear_relative_tolerance;
+      if (static_cast<int>(linfo[3 * i]) != 0) {
+        inf.status = static_cast<int>(linfo[3 * i]);
+        inf.iterations = static_cast<int32_t>(linfo[3 * i + 1]);
+        inf.residual_l2 = linfo[3 * i + 2];
+        continue;
+      }
+      const double step = std::sqrt(h[i]) / std::max(std::sqrt(h[kp + i]), std::numeric_limits<double>::min());
+      inf.iterations = iteration + 1;
+      inf.residual_l2 = step;
+      if (!std::isfinite(step)) {
+        inf.status = ToInt(Status::kNumericalNonfinite);
+        continue;
+      }
+      if (step < 100.0 * rel && norm[i] / scale[i] <= rel) {
+        inf.status = ToInt(Status::kOk);
+        continue;
+      }
+      trying |= 1u << i;
+    }
+    run = trying;
+    if (!trying)
+      break;
+    // Armijo backtracking from the saved state along the undamped direction.
+    if (LaunchMaskedCopy(dev_, kp, trying, state_.get(), saved_.get(), st) != cudaSuccess)
+      return Status::kInternalError;
+    ItemScalars alpha{};
+    for (int i = 0; i < k; ++i)
+      alpha.v[i] = 1.0;
+    uint32_t accepted = 0;
+    for (int backtrack = 0; backtrack < 20 && trying; ++backtrack) {
+      if (LaunchTrial(dev_, kp, x_.get(), saved_.get(), state_.get(), alpha, trying, st) != cudaSuccess ||
+          !assemble(trying))
+        return Status::kInternalError;
+      timing_.kernel_launches += 4;
+      if ((s = EquationNorms(kp, st, res.data())) != Status::kOk)
+        return s;
+      for (int i = 0; i < k; ++i) {
+        if (!((trying >> i) & 1u))
+          continue;
+        if (invalid[i]) {
+          c->req->info[c->first + i].status = ToInt(Status::kAssemblyFailed);
+          trying &= ~(1u << i);
+          run &= ~(1u << i);
+          continue;
+        }
+        const double trial = res[i];
+        if (std::isfinite(trial) &&
+            (trial <= (1.0 - 1e-4 * alpha.v[i]) * norm[i] || trial / scale[i] <= rel)) {
+          norm[i] = trial;
+          accepted |= 1u << i;
+          trying &= ~(1u << i);
+        } else {
+          alpha.v[i] *= 0.5;
+        }
+      }
+    }
+    // Not accepted after 20 halvings: back to the last accepted state; recovery stops.
+    if (trying && LaunchMaskedCopy(dev_, kp, trying, saved_.get(), state_.get(), st) != cudaSuccess)
+      return Status::kInternalError;
+    run = accepted;
+  }
+  for (int i = 0; i < k; ++i)
+    if ((rec >> i) & 1u) {
+      fg_item_info &inf = c->req->info[c->first + i];
+      inf.iterations += orig_its[i];
+      inf.linear_iterations += orig_lin[i];
+      inf.verified_equation_residual_relative = norm[i] / scale[i];
+    }
+  return cudaStreamSynchronize(st) == cudaSuccess ? Status::kOk : Status::kInternalError;
 }
 
 Status Plan::ChunkFinish(Chunk *c)

@@ -74,6 +74,8 @@ public:
   Status ChunkNorms(Chunk *c, bool linfo_on_device);
   Status ChunkDecide(Chunk *c);
   Status ChunkUpdate(Chunk *c);
+  // SolveSafeguarded for the items the Newton loop exhausted (recover_nonconvergence).
+  Status ChunkRecover(Chunk *c);
   Status ChunkFinish(Chunk *c);
   // The FP64 Jacobi PCG of this plan's current system for a multi-plan launch (barrier and
   // error flag supplied by the caller); false when the plan's options need another kernel.
@@ -129,6 +131,8 @@ private:
   DeviceArray<int32_t> block_fallbacks_;
   // PCG from the iterate: free-row state x0, defect d, per-item tolerances.
   DeviceArray<double> x0_, d_, item_tol_;
+  DeviceArray<double> saved_; // recovery: the last accepted state [N][KP]
+  Status EquationNorms(int kp, cudaStream_t st, double *res);
   DeviceArray<unsigned> barrier_;
   DeviceArray<unsigned long long> trace_;
   bool trace_enabled_ = false;

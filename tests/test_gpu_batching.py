@@ -74,3 +74,22 @@ def test_heterogeneous_meshes_in_one_launch_match_single_solves(gpu):
     for i in range(len(models)):
         assert info2[i].iterations == info[i].iterations
         assert rel(a2[i], a[i]) <= 1e-12
+
+
+@pytest.mark.parametrize("max_newton", [6, 10])
+def test_recovery_of_exhausted_items_matches_oracle(gpu, max_newton):
+    """SolveSafeguarded (nonlinear_solver.cu:534-659): items the relaxed Newton loop
+    exhausts are solved again from the zero start by Armijo-damped Newton; statuses, total
+    Newton iterations and the verified equation residual match the oracle's recovery, A
+    within the sector bound 5e-9."""
+    model = meshes.annular_sector(nr=24, nt=36)
+    cur = np.random.default_rng(5).uniform(-15, 15, size=(3, 3))
+    opts = fg.production_options(max_newton_iterations=max_newton)
+    got = fg.Plan(model).solve(cur, options=opts)
+    a, b1, b2, flux, info = O.solve_batch(model, cur, options=O.production_options(max_newton_iterations=max_newton))
+    for i in range(3):
+        assert got.info[i].status == info[i].status == 0
+        assert got.info[i].iterations == info[i].iterations > max_newton
+        assert got.info[i].verified_equation_residual_relative <= 1e-8
+        assert rel(got.a[i], a[i]) <= 5e-9
+        assert rel(got.flux[i], flux[i]) <= 1e-8
