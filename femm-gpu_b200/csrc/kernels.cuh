@@ -79,11 +79,15 @@ struct PcgArgs {
   double reliable_delta;
   const double *values64, *b64;
   double *x64;
-  // Column-index cache: host copy of slice_off (read by LaunchPcg only, never by the
-  // kernel) lets the launch size a shared-memory copy of each CTA's SELL column indices,
-  // loaded once per launch; col_cache / col_cache_offset are set by LaunchPcg.
+  // Column-index cache (opt-in, FG_PCG_COL_CACHE=1): host copy of slice_off (read by
+  // LaunchPcg only, never by the kernel) lets the launch size a shared-memory copy of each
+  // CTA's SELL column indices, loaded once per launch; col_cache / col_cache_offset are
+  // set by LaunchPcg.
   const int32_t *host_slice_off;
   int32_t col_cache, col_cache_offset;
+  // Value ring: the SpMV's operator values staged into shared memory by cp.async one chunk
+  // ahead of their use (set by LaunchPcg for 16-byte item vectors).
+  int32_t value_ring, value_ring_offset;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
   // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
   // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.

@@ -61,14 +61,26 @@ int KernelGrid(const void *kernel, size_t smem)
 
 // Dynamic shared memory a launch may use for staging plus the column cache: two CTAs of
 // 512 threads per SM must stay resident (228 KB per SM, about 12 KB static per CTA).
-constexpr size_t kColumnCacheBudget = 100 * 1024;
+constexpr size_t kColumnCacheBudget = 104 * 1024;
 
-// FG_PCG_COL_CACHE=0 in the environment turns the column cache off (for A/B timing).
+// FG_PCG_VALUE_RING=0 in the environment turns the cp.async value ring off (for A/B timing).
+bool ValueRingEnabled()
+{
+  static const bool enabled = [] {
+    const char *v = std::getenv("FG_PCG_VALUE_RING");
+    return !(v && v[0] == '0');
+  }();
+  return enabled;
+}
+
+// The column cache is off unless FG_PCG_COL_CACHE=1: beside the value ring its shared
+// memory shrinks L1 and costs the update phase more than the cached indices save
+// (measured on the 251k-node batch of 8: 69.9 us per CG iteration without, 73.2 with).
 bool ColumnCacheEnabled()
 {
   static const bool enabled = [] {
     const char *v = std::getenv("FG_PCG_COL_CACHE");
-    return !(v && v[0] == '0');
+    return v && v[0] == '1';
   }();
   return enabled;
 }
@@ -117,6 +129,20 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
     grid = max_grid;
   if (grid < 1)
     grid = 1;
+  // Value ring (16-byte item vectors, per-item operators): 2 stages x 4 entries x 32 lanes
+  // x 16 bytes per warp, after the block-Jacobi staging buffer.
+  args.value_ring = 0;
+  args.value_ring_offset = 0;
+  const bool ring_shape = (args.precision == 0 ? 8 : 4) * iv == 16 && args.value_item && ValueRingEnabled();
+  if (ring_shape) {
+    const size_t offset = (smem + 15) / 16 * 16;
+    const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 16;
+    if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
+      args.value_ring = 1;
+      args.value_ring_offset = static_cast<int32_t>(offset);
+      smem = total;
+    }
+  }
   // Column-index cache: the largest slice range any CTA's rows touch, if it fits in the
   // shared memory that still leaves the grid co-resident.
   args.col_cache = 0;

@@ -332,6 +332,27 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
 // One row's product for IV items: acc_j = sum_w a_rw,j * v_j(col_w), v = z (+ beta p),
 // in CSR order and in T arithmetic.  Column indices and values of a chunk of entries are
 // loaded before any gather so a thread keeps many independent loads in flight.
+// Asynchronous global -> shared copies (cp.async, sm_80+): 16 bytes per thread, L2
+// evict-first (the operator values are read once per iteration), grouped per chunk.
+__device__ __forceinline__ unsigned long long EvictFirstPolicy()
+{
+  unsigned long long pol;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+__device__ __forceinline__ void CpAsync16(void *smem, const void *gmem, unsigned long long pol)
+{
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const size_t g = __cvta_generic_to_global(gmem);
+  asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(g), "l"(pol)
+               : "memory");
+}
+__device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void CpAsyncWait()
+{
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // Column index of SELL position pos: from the CTA's shared-memory copy when cached.
 __device__ __forceinline__ int Column(const PcgArgs &a, const int32_t *colc, size_t cbase, size_t pos)
 {
@@ -807,12 +828,10 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         be[j] = static_cast<T>(ctl.beta[item0 + j]);
         any_mine = any_mine || on(j);
       }
-      if (any_mine) {
-        FG_ROWS_BEGIN
-        const int len = __ldg(a.row_len + r);
-        const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
-        T acc[IV], zr[IV], pr[IV], pnew[IV];
-        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
+      // Row epilogue: p_new of the row, q = acc, and p_new . q.
+      auto finish_row = [&](int r, const T (&acc)[IV]) {
+        const size_t ri = static_cast<size_t>(r) * KP + item0;
+        T zr[IV], pr[IV], pnew[IV];
         Load<T, IV>(Z + ri, zr);
         Load<T, IV>(pc + ri, pr);
 #pragma unroll
@@ -824,6 +843,99 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         for (int j = 0; j < IV; ++j)
           if (on(j))
             v[0][j] += static_cast<double>(pnew[j]) * static_cast<double>(acc[j]);
+      };
+      constexpr bool kRing = sizeof(T) * IV == 16;
+      if constexpr (kRing) {
+        if (any_mine && a.value_ring) {
+          // Software pipeline over this lane's (row, chunk) sequence: the values of the next
+          // chunk are copied to shared memory while the current chunk's gathers are in flight.
+          constexpr int U = 4;
+          T *ring = reinterpret_cast<T *>(fg_dynamic_smem + a.value_ring_offset) +
+                    static_cast<size_t>(warp) * 2 * U * 32 * IV;
+          const T *vals = static_cast<const T *>(a.values);
+          const unsigned long long pol = EvictFirstPolicy();
+          auto issue = [&](int stage, size_t base, int w0, int len) {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              if (w0 + u < len)
+                CpAsync16(ring + ((stage * U + u) * 32 + lane) * IV,
+                          vals + (base + 32 * static_cast<size_t>(w0 + u)) * a.value_stride + item0, pol);
+            CpAsyncCommit();
+          };
+          int ws = ws0 + warp, r = 0, len = 0, w0 = 0, stage = 0;
+          size_t base = 0;
+          auto row_at = [&](int w, int &rr, int &ll, size_t &bb) {
+            rr = w * S + lane / LR;
+            ll = __ldg(a.row_len + rr);
+            bb = static_cast<size_t>(__ldg(a.slice_off + (rr >> 5))) + (rr & 31);
+          };
+          if (ws < ws1) {
+            row_at(ws, r, len, base);
+            issue(0, base, 0, len);
+          }
+          T acc[IV];
+#pragma unroll
+          for (int j = 0; j < IV; ++j)
+            acc[j] = T(0);
+          while (ws < ws1) {
+            int nws = ws, nr = r, nlen = len, nw0 = w0 + U;
+            size_t nbase = base;
+            if (nw0 >= len) {
+              nws = ws + kPcgWarps;
+              nw0 = 0;
+              if (nws < ws1)
+                row_at(nws, nr, nlen, nbase);
+            }
+            if (nws < ws1)
+              issue(stage ^ 1, nbase, nw0, nlen);
+            else
+              CpAsyncCommit();
+            CpAsyncWait<1>(); // the current chunk's values have landed
+            int c[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              c[u] = w0 + u < len ? Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u)) : 0;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+              if (w0 + u < len) {
+                const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
+                T g[IV], pv[IV], vv[IV];
+                Load<T, IV>(Z + ci, g);
+                Load<T, IV>(pc + ci, pv);
+                Load<T, IV>(ring + ((stage * U + u) * 32 + lane) * IV, vv);
+#pragma unroll
+                for (int j = 0; j < IV; ++j) {
+                  if (fold[j])
+                    g[j] = Fma(be[j], pv[j], g[j]);
+                  acc[j] = Fma(vv[j], g[j], acc[j]);
+                }
+              }
+            }
+            if (w0 + U >= len) {
+              finish_row(r, acc);
+#pragma unroll
+              for (int j = 0; j < IV; ++j)
+                acc[j] = T(0);
+            }
+            ws = nws;
+            r = nr;
+            len = nlen;
+            w0 = nw0;
+            base = nbase;
+            stage ^= 1;
+          }
+          CpAsyncWait<0>();
+          any_mine = false; // done
+        }
+      }
+      if (any_mine) {
+        FG_ROWS_BEGIN
+        const int len = __ldg(a.row_len + r);
+        const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
+        T acc[IV];
+        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
+        (void)ri;
+        finish_row(r, acc);
         FG_ROWS_END
       }
       if (!GridReduce<KP, IV, 1, false>(a, gs, v, sm, epoch, buf, tr, 0))
