@@ -44,6 +44,7 @@ public:
                   double tolerance, int max_iterations, double *x, fg_linear_info *info);
 
   const HostPlan &host() const { return host_; }
+  const HostModel &model() const { return model_; }
   const fg_timing &timing() const { return timing_; }
   size_t DeviceBytes() const;
 

@@ -6,10 +6,10 @@
 * ``artifact`` -- the gpu_femm_magnetostatic_mesh_v1 JSON artifact writer
 """
 from . import meshes
-from .capi import (Plan, Multi, SolveResult, FgError, csr_pcg, lib, production_options, status_name,
-                   bh_build, bh_eval, LIB_PATH, STATUS_NAMES, EXPORTED)
+from .capi import (Plan, Multi, Postprocess, SolveResult, FgError, csr_pcg, lib, production_options,
+                   status_name, bh_build, bh_eval, LIB_PATH, STATUS_NAMES, EXPORTED)
 from .model import AXISYMMETRIC, MU0, PLANAR, Model
 
-__all__ = ["Model", "Plan", "Multi", "SolveResult", "FgError", "csr_pcg", "lib", "production_options",
-           "status_name", "bh_build", "bh_eval", "meshes", "LIB_PATH", "STATUS_NAMES", "EXPORTED",
+__all__ = ["Model", "Plan", "Multi", "Postprocess", "SolveResult", "FgError", "csr_pcg", "lib",
+           "production_options", "status_name", "bh_build", "bh_eval", "meshes", "LIB_PATH", "STATUS_NAMES", "EXPORTED",
            "PLANAR", "AXISYMMETRIC", "MU0"]

@@ -43,6 +43,9 @@ EXPORTED = [
     "fg_warm_create", "fg_warm_destroy", "fg_warm_project", "fg_warm_project_device",
     "fg_warm_predict", "fg_solve_batch_learned",
     "fg_multi_create", "fg_multi_destroy", "fg_multi_solve", "fg_multi_last_timing",
+    "fg_postprocess_default_options", "fg_postprocess_create", "fg_postprocess_destroy",
+    "fg_postprocess_probe_count", "fg_postprocess_mask", "fg_postprocess_compute",
+    "fg_postprocess_compute_device", "fg_postprocess_frozen",
 ]
 
 
@@ -129,6 +132,8 @@ def lib():
         _LIB.fg_mlp_destroy.restype = None
         _LIB.fg_warm_destroy.restype = None
         _LIB.fg_multi_destroy.restype = None
+        _LIB.fg_postprocess_destroy.restype = None
+        _LIB.fg_postprocess_default_options.restype = None
     return _LIB
 
 
@@ -413,3 +418,106 @@ class Multi:
         t = FgMultiTiming()
         lib().fg_multi_last_timing(self._h, C.byref(t))
         return t
+
+
+class FgPostprocessOptions(C.Structure):
+    _fields_ = [("selected_material_label", C.c_int32), ("air_material_label", C.c_int32),
+                ("selected_group_number", C.c_int32), ("air_group_number", C.c_int32),
+                ("airgap_radius_m", C.c_double), ("airgap_angle_count", C.c_int32),
+                ("airgap_angles_rad", C.c_void_p), ("max_mask_iterations", C.c_int32),
+                ("mask_relative_tolerance", C.c_double), ("symmetry_apex_count", C.c_int32),
+                ("symmetry_apex_nodes", C.c_void_p)]
+
+
+class FgPostprocessResult(C.Structure):
+    _fields_ = [("status", C.c_int32), ("reserved", C.c_int32), ("force_x_n", C.c_double),
+                ("force_y_n", C.c_double), ("torque_nm", C.c_double)]
+
+
+@dataclass
+class PostprocessResult:
+    status: np.ndarray       # [items]
+    force: np.ndarray        # [items, 2] (Fx, Fy) N
+    torque: np.ndarray       # [items] N m
+    radial_b: np.ndarray     # [items, probes] T
+
+
+class Postprocess:
+    """fg_postprocess: weighted-stress force / torque on a selected region and smoothed
+    radial air-gap B, reusable across the solutions of one plan.
+
+    selected / air: material label indices, or group numbers when selected_group /
+    air_group are >= 0.  mask (0 / 1 per node) skips the GPU mask solve."""
+
+    def __init__(self, plan: Plan, selected_label=1, air_label=3, selected_group=-1, air_group=-1,
+                 radius_m=0.0, angles_rad=(), max_mask_iterations=256, mask_tolerance=1e-12,
+                 apex_nodes=(), mask=None):
+        L = lib()
+        self._angles = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+        self._apex = np.ascontiguousarray(np.asarray(apex_nodes, np.int32).ravel())
+        o = FgPostprocessOptions()
+        L.fg_postprocess_default_options(C.byref(o))
+        o.selected_material_label, o.air_material_label = selected_label, air_label
+        o.selected_group_number, o.air_group_number = selected_group, air_group
+        o.airgap_radius_m = radius_m
+        o.airgap_angle_count = self._angles.size
+        o.airgap_angles_rad = self._angles.ctypes.data if self._angles.size else None
+        o.max_mask_iterations, o.mask_relative_tolerance = max_mask_iterations, mask_tolerance
+        o.symmetry_apex_count = self._apex.size
+        o.symmetry_apex_nodes = self._apex.ctypes.data if self._apex.size else None
+        self.options = o
+        self.plan = plan
+        m = None if mask is None else np.ascontiguousarray(np.asarray(mask, np.float64))
+        self._h = C.c_void_p()
+        st = L.fg_postprocess_create(plan._h, C.byref(o), None if m is None else _p(m), C.byref(self._h))
+        if st:
+            self._h = None
+            raise FgError(st, "fg_postprocess_create")
+        self.probes = int(L.fg_postprocess_probe_count(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fg_postprocess_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def mask(self) -> np.ndarray:
+        out = np.zeros(self.plan.N)
+        st = lib().fg_postprocess_mask(self._h, _p(out))
+        if st:
+            raise FgError(st, "fg_postprocess_mask")
+        return out
+
+    def _result(self, res, radial):
+        k = len(res)
+        return PostprocessResult(
+            status=np.array([res[i].status for i in range(k)]),
+            force=np.array([[res[i].force_x_n, res[i].force_y_n] for i in range(k)]).reshape(k, 2),
+            torque=np.array([res[i].torque_nm for i in range(k)]), radial_b=radial)
+
+    def compute(self, a, b1, b2) -> PostprocessResult:
+        """Host solutions: a [k, N], b1 / b2 [k, E]."""
+        a = np.ascontiguousarray(np.atleast_2d(a), np.float64)
+        b1 = np.ascontiguousarray(np.atleast_2d(b1), np.float64)
+        b2 = np.ascontiguousarray(np.atleast_2d(b2), np.float64)
+        k = a.shape[0]
+        res = (FgPostprocessResult * max(k, 1))()
+        radial = np.zeros((k, self.probes))
+        st = lib().fg_postprocess_compute(self._h, C.c_int32(k), _p(a), _p(b1), _p(b2), res,
+                                          _p(radial) if self.probes else None)
+        if st:
+            raise FgError(st, "fg_postprocess_compute")
+        return self._result([res[i] for i in range(k)], radial)
+
+    def compute_device(self, k, a_ptr, b1_ptr, b2_ptr, stream=0) -> PostprocessResult:
+        """Device solutions (item-major) by pointer, e.g. torch tensors' data_ptr()."""
+        res = (FgPostprocessResult * max(k, 1))()
+        radial = np.zeros((k, self.probes))
+        st = lib().fg_postprocess_compute_device(
+            self._h, C.c_int32(k), C.c_void_p(a_ptr), C.c_void_p(b1_ptr), C.c_void_p(b2_ptr), res,
+            _p(radial) if self.probes else None, C.c_void_p(stream))
+        if st:
+            raise FgError(st, "fg_postprocess_compute_device")
+        return self._result([res[i] for i in range(k)], radial)

@@ -2,9 +2,11 @@
 //
 //   femm_gpu [options] --solve REQUEST.json RESPONSE.json
 //   femm_gpu [options] --batch BATCH.json RESPONSE.json
+//   femm_gpu [options] --single-sample REQUEST.json RESPONSE.json
 //   femm_gpu --capabilities
 //   femm_gpu --describe-artifact ARTIFACT.json   (parsed model and plan sizes, as JSON)
 //   femm_gpu --sha256 FILE                        (the file-bytes SHA-256 a request names)
+//   femm_gpu --describe-femm-ans STEM CURVE_DIR   (the model --single-sample reads, as JSON)
 //   options: --preconditioner jacobi|block-jacobi  --block-size 8|32  --precision fp64|mixed
 //
 // --solve is the reference's `--solve` (PlanarDcSingleSampleAdapter, gpu_solver/src/app/
@@ -17,12 +19,21 @@
 // and validated once and solved together in fg_solve_batch launches of up to
 // max_items_per_chunk items; responses keep the input order.
 //
-// Force / torque and air-gap postprocessing (the reference's weighted-stress path) is not
-// served: a request that asks for it gets solve_status from the solve and
-// postprocess_status UNSUPPORTED_FEATURE, status FAIL.
+// A planar-DC request with compute_force_torque or air-gap angles gets the weighted-stress
+// force / torque on its force group (air = its stress-air group) and the FEMM-smoothed
+// radial B on the air-gap circle (ComputeFrozenPostprocess, sample_adapter.cpp:423-439:
+// mask PCG of at most 4096 iterations at 1e-12); items of a batch that share an artifact
+// and the same postprocess request share one mask.
+//
+// --single-sample is the reference's frozen FEMM adapter (SingleSampleAdapter,
+// gpu_solver/tests/native/reference_adapter.cu:63-124): a gpu_femm_single_sample_v1 request
+// naming a FEMM .ans nonlinear PM / coil solution, solved from scratch (relative tolerance
+// 1e-8, at most 128 Newton iterations, the other NonlinearOptions defaults), then
+// postprocessed on material label 1 with label 3 as air.
 //
 // Exit codes: 0 every response PASS, 1 a FAIL response or an I/O failure, 2 usage error.
 #include "artifact.h"
+#include "femm_ans.h"
 #include "femm_gpu.h"
 #include "json.h"
 #include "request.h"
@@ -50,6 +61,7 @@ using fgio::Artifact;
 using fgio::SampleRequest;
 
 constexpr double kTwoPi = 6.283185307179586476925286766559005768;
+constexpr double kPi = 3.141592653589793238462643383279502884;
 
 struct Options {
   fg_plan_options plan{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, 0};
@@ -111,6 +123,12 @@ struct Solved {
   double residual = 0.0;
 };
 
+// A postprocessed sample.
+struct Post {
+  double fx = 0.0, fy = 0.0, torque = 0.0;
+  std::vector<double> radial;
+};
+
 template <class V> void List(std::ostream &o, const V &v)
 {
   for (size_t i = 0; i < v.size(); ++i)
@@ -120,11 +138,12 @@ template <class V> void List(std::ostream &o, const V &v)
 // WritePlanarDcSampleResponse's layout (gpu_solver/src/app/sample_adapter.cpp:236-355).
 std::string SampleResponse(int status, int solve_status, bool post_requested, int post_status,
                            const SampleRequest *req, const Solved *sol, const std::string &diagnostic,
-                           const Artifact *art, const std::string &indent = "")
+                           const Artifact *art, const std::string &indent = "", const Post *post = nullptr)
 {
   std::ostringstream o;
   o << std::setprecision(17);
   const bool solved = solve_status == 0 && req && sol;
+  const bool postprocessed = solved && post_requested && post_status == 0 && post;
   const std::string protocol = req ? req->protocol : "gpu_femm_planar_dc_sample_v1";
   const bool generic = protocol == "gpu_femm_magnetostatic_sample_v1";
   const bool axi = art && art->problem_type == FG_AXISYMMETRIC;
@@ -142,16 +161,25 @@ std::string SampleResponse(int status, int solve_status, bool post_requested, in
     << in << "\"postprocess_status\": \""
     << (!post_requested ? "NOT_REQUESTED" : (solve_status == 0 ? StatusName(post_status) : "NOT_RUN")) << "\",\n"
     << in << "\"error_identifier\": \"" << (status == 0 ? "" : "GPU_FEMM_" + StatusName(status)) << "\",\n"
-    << in << "\"error_message\": \"" << fgio::Escape(message) << "\",\n"
-    << in << "\"Fx_N\": null,\n" << in << "\"Fy_N\": null,\n" << in << "\"torque_Nm\": null,\n"
-    << in << "\"actual_circuit_currents_A\": [";
+    << in << "\"error_message\": \"" << fgio::Escape(message) << "\",\n";
+  if (postprocessed && req->compute_force_torque)
+    o << in << "\"Fx_N\": " << post->fx << ",\n" << in << "\"Fy_N\": " << post->fy << ",\n"
+      << in << "\"torque_Nm\": " << post->torque << ",\n";
+  else
+    o << in << "\"Fx_N\": null,\n" << in << "\"Fy_N\": null,\n" << in << "\"torque_Nm\": null,\n";
+  o << in << "\"actual_circuit_currents_A\": [";
   if (solved)
     List(o, sol->currents);
   o << "],\n" << in << "\"circuit_flux_linkage_Wb\": [";
   if (solved)
     List(o, sol->flux);
-  o << "],\n" << in << "\"airgap_sample_angles_deg\": [],\n" << in << "\"airgap_radial_flux_density_T\": [],\n"
-    << in << "\"mesh_node_count\": " << (solved ? sol->a.size() : 0) << ",\n"
+  o << "],\n" << in << "\"airgap_sample_angles_deg\": [";
+  if (postprocessed)
+    List(o, req->airgap_angles_deg);
+  o << "],\n" << in << "\"airgap_radial_flux_density_T\": [";
+  if (postprocessed)
+    List(o, post->radial);
+  o << "],\n" << in << "\"mesh_node_count\": " << (solved ? sol->a.size() : 0) << ",\n"
     << in << "\"mesh_element_count\": " << (solved ? sol->b1.size() : 0) << ",\n";
   const bool field = solved && req->include_field_solution;
   o << in << "\"field_solution_included\": " << (field ? "true" : "false") << ",\n"
@@ -275,6 +303,69 @@ int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std:
   return 0;
 }
 
+// The postprocess options of a planar-DC request (sample_adapter.cpp:426-432).
+fg_postprocess_options PostOptions(const SampleRequest &r, std::vector<double> *angles)
+{
+  fg_postprocess_options o;
+  fg_postprocess_default_options(&o);
+  o.selected_group_number = r.force_group_number;
+  o.air_group_number = r.stress_air_group_number;
+  o.max_mask_iterations = 4096;
+  o.airgap_radius_m = r.airgap_radius_mm * 1e-3;
+  angles->clear();
+  for (double deg : r.airgap_angles_deg)
+    angles->push_back(deg * kPi / 180.0);
+  o.airgap_angle_count = static_cast<int32_t>(angles->size());
+  o.airgap_angles_rad = angles->data();
+  return o;
+}
+
+// Postprocesses one solved sample on `pp` (created for the same request options).
+int RunPost(fg_postprocess *pp, const Solved &s, Post *out)
+{
+  fg_postprocess_result r{};
+  out->radial.assign(static_cast<size_t>(fg_postprocess_probe_count(pp)), 0.0);
+  const int rc = fg_postprocess_compute(pp, 1, s.a.data(), s.b1.data(), s.b2.data(), &r, out->radial.data());
+  if (rc != 0)
+    return rc;
+  out->fx = r.force_x_n;
+  out->fy = r.force_y_n;
+  out->torque = r.torque_nm;
+  return r.status;
+}
+
+// Postprocess objects of one artifact's plan, one per distinct request (groups, circle).
+class PostCache
+{
+public:
+  ~PostCache()
+  {
+    for (auto &kv : cache_)
+      if (kv.second.second)
+        fg_postprocess_destroy(kv.second.second);
+  }
+  // Status of the postprocess plan; *pp valid when 0.
+  int Get(fg_plan *plan, const SampleRequest &r, fg_postprocess **pp)
+  {
+    std::vector<double> key{static_cast<double>(r.force_group_number),
+                            static_cast<double>(r.stress_air_group_number), r.airgap_radius_mm};
+    key.insert(key.end(), r.airgap_angles_deg.begin(), r.airgap_angles_deg.end());
+    auto it = cache_.find(key);
+    if (it == cache_.end()) {
+      std::vector<double> angles;
+      const fg_postprocess_options o = PostOptions(r, &angles);
+      fg_postprocess *p = nullptr;
+      const int rc = fg_postprocess_create(plan, &o, nullptr, &p);
+      it = cache_.emplace(key, std::make_pair(rc, p)).first;
+    }
+    *pp = it->second.second;
+    return it->second.first;
+  }
+
+private:
+  std::map<std::vector<double>, std::pair<int, fg_postprocess *>> cache_;
+};
+
 int Solve(const std::string &request_path, const std::string &response_path, const Options &opt)
 {
   if (SameFile(request_path, response_path)) {
@@ -323,13 +414,18 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   const int solve_status = status;
   const bool post = req.postprocess_requested();
   int post_status = 0;
+  Post result;
   if (solve_status == 0 && post) {
-    post_status = FG_UNSUPPORTED_FEATURE;
+    PostCache cache;
+    fg_postprocess *pp = nullptr;
+    post_status = cache.Get(p.plan, req, &pp);
+    if (post_status == 0)
+      post_status = RunPost(pp, sols[0], &result);
     status = post_status;
-    diagnostic = "force/torque and air-gap postprocessing are not served by this solver";
   }
   const std::string body = SampleResponse(status, solve_status, post, post_status, &req,
-                                          attempted ? &sols[0] : nullptr, diagnostic, &p.artifact);
+                                          attempted ? &sols[0] : nullptr, diagnostic, &p.artifact, "",
+                                          post_status == 0 ? &result : nullptr);
   if (!PublishAtomically(response_path, body + "\n")) {
     std::cerr << "FAIL magnetostatic solve: could not atomically publish response\n";
     return 1;
@@ -403,6 +499,7 @@ int Batch(const std::string &request_path, const std::string &response_path, con
       ready.clear();
     }
     const auto s0 = std::chrono::steady_clock::now();
+    PostCache cache;
     for (size_t first = 0; first < ready.size(); first += batch.max_items_per_chunk) {
       const size_t n = std::min<size_t>(batch.max_items_per_chunk, ready.size() - first);
       std::vector<const SampleRequest *> reqs;
@@ -418,14 +515,17 @@ int Batch(const std::string &request_path, const std::string &response_path, con
         int status = st[j];
         const int solve_status = status;
         int post_status = 0;
-        std::string diag;
+        Post result;
         if (solve_status == 0 && r.postprocess_requested()) {
-          post_status = FG_UNSUPPORTED_FEATURE;
+          fg_postprocess *pp = nullptr;
+          post_status = cache.Get(p.plan, r, &pp);
+          if (post_status == 0)
+            post_status = RunPost(pp, sols[j], &result);
           status = post_status;
-          diag = "force/torque and air-gap postprocessing are not served by this solver";
         }
         bodies[i] = SampleResponse(status, solve_status, r.postprocess_requested(), post_status, &r,
-                                   sols.empty() ? nullptr : &sols[j], diag, &p.artifact, "    ");
+                                   sols.empty() ? nullptr : &sols[j], "", &p.artifact, "    ",
+                                   post_status == 0 ? &result : nullptr);
         final_status[i] = status;
       }
     }
@@ -461,20 +561,125 @@ int Batch(const std::string &request_path, const std::string &response_path, con
   return pass ? 0 : 1;
 }
 
-// --describe-artifact: the parsed model as JSON (17 significant digits, exact round trip),
-// and its host-only plan's sizes -- for checking the parser against other readers.
-int DescribeArtifact(const std::string &path)
+// WriteSingleSampleResponse (gpu_solver/tests/native/reference_adapter.cu:16-61).
+std::string SingleSampleResponse(int status, const fgio::SingleSampleRequest *req, const Solved *sol,
+                                 const Post *post)
 {
-  std::string bytes, error;
-  Artifact a;
-  if (!ReadFile(path, &bytes)) {
-    std::cerr << "FAIL describe: cannot open mesh artifact\n";
+  std::ostringstream o;
+  o << std::setprecision(17) << "{\n  \"protocol\": \"gpu_femm_single_sample_v1\",\n"
+    << "  \"source_motor_fem_sha256\": \"" << (req ? req->source_motor_fem_sha256 : "") << "\",\n"
+    << "  \"status\": \"" << (status == 0 ? "PASS" : "FAIL") << "\",\n"
+    << "  \"solve_status\": \"" << (status == 0 ? "PASS" : "FAIL") << "\",\n"
+    << "  \"error_identifier\": \"" << (status == 0 ? "" : "GPU_FEMM_" + StatusName(status)) << "\",\n"
+    << "  \"error_message\": \"" << (status == 0 ? "" : StatusName(status)) << "\",\n";
+  if (status == 0 && req && sol && post) {
+    o << "  \"Fx_N\": " << post->fx << ",\n  \"Fy_N\": " << post->fy << ",\n  \"torque_Nm\": " << post->torque
+      << ",\n  \"actual_circuit_currents_A\": [" << req->current_a << "],\n  \"circuit_flux_linkage_Wb\": ["
+      << sol->flux[0] << "],\n  \"airgap_sample_angles_deg\": [";
+    List(o, req->airgap_angles_deg);
+    o << "],\n  \"airgap_radial_flux_density_T\": [";
+    List(o, post->radial);
+    o << "],\n  \"mesh_element_count\": " << sol->b1.size() << ",\n  \"convergence\": {\"iterations\": "
+      << sol->iterations << ", \"residual_l2\": " << sol->residual << "}\n";
+  } else {
+    o << "  \"Fx_N\": null,\n  \"Fy_N\": null,\n  \"torque_Nm\": null,\n"
+      << "  \"actual_circuit_currents_A\": [],\n  \"circuit_flux_linkage_Wb\": [],\n"
+      << "  \"airgap_sample_angles_deg\": [],\n  \"airgap_radial_flux_density_T\": [],\n"
+      << "  \"mesh_element_count\": 0,\n  \"convergence\": {\"iterations\": 0, \"residual_l2\": null}\n";
+  }
+  o << "}\n";
+  return o.str();
+}
+
+int SingleSample(const std::string &request_path, const std::string &response_path, const Options &opt)
+{
+  std::string text, error;
+  fgio::SingleSampleRequest req;
+  if (!ReadFile(request_path, &text) || !fgio::ParseSingleSampleRequestText(text, &req, &error)) {
+    if (!PublishAtomically(response_path, SingleSampleResponse(FG_INVALID_ARGUMENT, nullptr, nullptr, nullptr))) {
+      std::cerr << "FAIL single-sample response: cannot write " << response_path << '\n';
+      return 1;
+    }
+    std::cerr << "FAIL single-sample request: " << (error.empty() ? "cannot read request" : error) << '\n';
     return 1;
   }
-  if (!fgio::ParseArtifact(bytes, &a, &error)) {
-    std::cout << "{\"status\": \"FAIL\", \"error\": \"" << fgio::Escape(error) << "\"}\n";
+  Prepared p;
+  std::vector<double> femm_a;
+  bool loaded = fgio::ReadFemmNonlinear(req.stem, req.curve_directory, &p.artifact, &femm_a, &error);
+  if (loaded) {
+    // ValidateNonlinearModel belongs to the fixture reader: a host-only plan checks it.
+    fg_model m = p.artifact.Model();
+    fg_plan_options host = opt.plan;
+    host.flags |= FG_PLAN_HOST_ONLY;
+    fg_plan *check = nullptr;
+    loaded = fg_plan_create(&m, &host, &check) == 0;
+    if (check)
+      fg_plan_destroy(check);
+    if (!loaded)
+      error = "nonlinear frozen mesh validation failed";
+  }
+  if (!loaded) {
+    if (!PublishAtomically(response_path, SingleSampleResponse(FG_INPUT_IO, &req, nullptr, nullptr))) {
+      std::cerr << "FAIL single-sample response: cannot write " << response_path << '\n';
+      return 1;
+    }
+    std::cerr << "FAIL single-sample reference: " << error << '\n';
     return 1;
   }
+  int status = EnsurePlan(&p, opt);
+  Solved sol;
+  if (status == 0) {
+    const fg_model m = p.artifact.Model();
+    const size_t N = m.node_count, E = m.triangle_count;
+    sol.currents = {req.current_a};
+    sol.flux.assign(1, 0.0);
+    sol.a.assign(N, 0.0);
+    sol.b1.assign(E, 0.0);
+    sol.b2.assign(E, 0.0);
+    // NonlinearOptions defaults with relative tolerance 1e-8 and 128 Newton iterations.
+    const fg_solve_options o{1e-8, 128, 128, 1e-13, 0, 0};
+    fg_item_info info{};
+    status = fg_solve_batch(p.plan, 1, sol.currents.data(), nullptr, nullptr, &o, sol.a.data(), sol.b1.data(),
+                            sol.b2.data(), sol.flux.data(), &info);
+    if (status == 0)
+      status = info.status;
+    sol.iterations = info.iterations;
+    sol.residual = info.residual_l2;
+  }
+  Post post;
+  if (status == 0) {
+    std::vector<double> angles;
+    for (double deg : req.airgap_angles_deg)
+      angles.push_back(deg * kPi / 180.0);
+    fg_postprocess_options o;
+    fg_postprocess_default_options(&o);
+    o.selected_material_label = req.selected_material_label;
+    o.airgap_radius_m = req.airgap_radius_mm * 1e-3;
+    o.airgap_angle_count = static_cast<int32_t>(angles.size());
+    o.airgap_angles_rad = angles.data();
+    fg_postprocess *pp = nullptr;
+    status = fg_postprocess_create(p.plan, &o, nullptr, &pp);
+    if (status == 0) {
+      status = RunPost(pp, sol, &post);
+      fg_postprocess_destroy(pp);
+    }
+  }
+  if (!PublishAtomically(response_path, SingleSampleResponse(status, &req, status == 0 ? &sol : nullptr,
+                                                             status == 0 ? &post : nullptr))) {
+    std::cerr << "FAIL single-sample response: cannot write " << response_path << '\n';
+    return 1;
+  }
+  if (status != 0) {
+    std::cerr << "FAIL single-sample: " << StatusName(status) << '\n';
+    return 1;
+  }
+  return 0;
+}
+
+// The parsed model as JSON (17 significant digits, exact round trip) with its host-only
+// plan's sizes -- for checking the readers against the reference's.
+int DescribeModel(Artifact &a, const std::string &sha256)
+{
   fg_model m = a.Model();
   fg_plan_options po{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, FG_PLAN_HOST_ONLY};
   fg_plan *plan = nullptr;
@@ -484,7 +689,7 @@ int DescribeArtifact(const std::string &path)
     fg_plan_sizes_get(plan, &sz);
   std::ostringstream o;
   o << std::setprecision(17) << "{\"status\": \"PASS\", \"plan_status\": \"" << StatusName(rc)
-    << "\", \"schema_version\": \"" << a.schema_version << "\", \"sha256\": \"" << fgio::Sha256Hex(bytes)
+    << "\", \"schema_version\": \"" << a.schema_version << "\", \"sha256\": \"" << sha256
     << "\", \"canonical_identity_sha256\": \"" << a.canonical_identity_sha256
     << "\", \"problem_type\": " << a.problem_type << ", \"depth_m\": " << a.depth_m << ", \"xy\": [";
   List(o, a.xy);
@@ -523,11 +728,41 @@ int DescribeArtifact(const std::string &path)
   return rc == 0 ? 0 : 1;
 }
 
+// --describe-artifact ARTIFACT.json
+int DescribeArtifact(const std::string &path)
+{
+  std::string bytes, error;
+  Artifact a;
+  if (!ReadFile(path, &bytes)) {
+    std::cerr << "FAIL describe: cannot open mesh artifact\n";
+    return 1;
+  }
+  if (!fgio::ParseArtifact(bytes, &a, &error)) {
+    std::cout << "{\"status\": \"FAIL\", \"error\": \"" << fgio::Escape(error) << "\"}\n";
+    return 1;
+  }
+  return DescribeModel(a, fgio::Sha256Hex(bytes));
+}
+
+// --describe-femm-ans STEM CURVE_DIRECTORY: the model --single-sample solves.
+int DescribeFemmAns(const std::string &stem, const std::string &curves)
+{
+  std::string error;
+  Artifact a;
+  std::vector<double> femm_a;
+  if (!fgio::ReadFemmNonlinear(stem, curves, &a, &femm_a, &error)) {
+    std::cout << "{\"status\": \"FAIL\", \"error\": \"" << fgio::Escape(error) << "\"}\n";
+    return 1;
+  }
+  return DescribeModel(a, "");
+}
+
 int Usage()
 {
   std::cerr << "usage: femm_gpu [--preconditioner jacobi|block-jacobi] [--block-size 8|32] "
                "[--precision fp64|mixed] (--solve request.json response.json | "
-               "--batch batch.json response.json | --capabilities | --describe-artifact artifact.json)\n";
+               "--batch batch.json response.json | --single-sample request.json response.json | "
+               "--capabilities | --describe-artifact artifact.json)\n";
   return 2;
 }
 
@@ -569,7 +804,7 @@ int main(int argc, char **argv)
   const int rest = argc - next;
   if (rest == 1 && std::strcmp(argv[next], "--capabilities") == 0) {
     std::cout << "{\n  \"protocols\": [\"gpu_femm_planar_dc_sample_v1\", \"gpu_femm_magnetostatic_sample_v1\", "
-                 "\"gpu_femm_magnetostatic_batch_v1\"],\n"
+                 "\"gpu_femm_magnetostatic_batch_v1\", \"gpu_femm_single_sample_v1\"],\n"
               << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\"],\n"
               << "  \"preconditioners\": [\"jacobi\", \"block-jacobi\"],\n"
               << "  \"precisions\": [\"fp64\", \"mixed\"],\n"
@@ -587,9 +822,13 @@ int main(int argc, char **argv)
   }
   if (rest == 2 && std::strcmp(argv[next], "--describe-artifact") == 0)
     return DescribeArtifact(argv[next + 1]);
+  if (rest == 3 && std::strcmp(argv[next], "--describe-femm-ans") == 0)
+    return DescribeFemmAns(argv[next + 1], argv[next + 2]);
   if (rest == 3 && std::strcmp(argv[next], "--solve") == 0)
     return Solve(argv[next + 1], argv[next + 2], opt);
   if (rest == 3 && std::strcmp(argv[next], "--batch") == 0)
     return Batch(argv[next + 1], argv[next + 2], opt);
+  if (rest == 3 && std::strcmp(argv[next], "--single-sample") == 0)
+    return SingleSample(argv[next + 1], argv[next + 2], opt);
   return Usage();
 }

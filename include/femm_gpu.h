@@ -360,6 +360,76 @@ int fg_solve_batch_learned(fg_plan *plan, fg_warm *warm, int32_t items, const do
                            const fg_solve_options *options, double *a_out, double *b1_out,
                            double *b2_out, double *flux_out, fg_item_info *info);
 
+/* ---- Frozen-state postprocessing: weighted-stress force / torque and air-gap B ----
+ *
+ * ComputeFrozenPostprocess (gpu_solver/src/postprocess/field_postprocess.cpp:341-403) with
+ * its reusable FrozenPostprocessPlan (:205-339) and FEMM's weighted-stress mask
+ * (weighted_stress.cu:24-193): the mask is the sqrt(area)-weighted Laplace solution, 1 on
+ * the selected region, 0 on other non-air regions and on the Dirichlet nodes (symmetry
+ * apex nodes excepted), periodic across every node constraint whatever its magnetic sign,
+ * solved by the library's PCG on the GPU and thresholded at 0.5.  Planar plans only.
+ *
+ * Selection: selected_group_number >= 0 selects every label of that FEMM group, else the
+ * label index selected_material_label; likewise air. */
+typedef struct fg_postprocess_options {
+  int32_t selected_material_label; /* 1 */
+  int32_t air_material_label;      /* 3 */
+  int32_t selected_group_number;   /* -1 */
+  int32_t air_group_number;        /* -1 */
+  double airgap_radius_m;          /* probes at (r cos t, r sin t); each must fall in air */
+  int32_t airgap_angle_count;
+  const double *airgap_angles_rad;
+  int32_t max_mask_iterations;     /* 256 */
+  double mask_relative_tolerance;  /* 1e-12 */
+  int32_t symmetry_apex_count;     /* anti-periodic sector apex nodes: magnetic zero only */
+  const int32_t *symmetry_apex_nodes;
+} fg_postprocess_options;
+
+/* FrozenPostprocessResult minus the samples (written to a separate array). */
+typedef struct fg_postprocess_result {
+  int32_t status;
+  int32_t reserved;
+  double force_x_n;
+  double force_y_n;
+  double torque_nm;
+} fg_postprocess_result;
+
+typedef struct fg_postprocess fg_postprocess;
+
+/* The FrozenPostprocessOptions defaults (postprocess.h:20-33). */
+void fg_postprocess_default_options(fg_postprocess_options *options);
+/* Builds the reusable postprocess (mask, element geometry, probe elements) for the plan's
+ * model; mask [node_count] of 0 / 1 values, or NULL to solve it on the GPU.  Returns the
+ * plan status (FG_INVALID_MATERIAL for a selection that is absent or touches another
+ * non-air region, FG_BOUNDARY_INVALID for contradictory fixed mask values, FG_INVALID_ARGUMENT
+ * for bad options or a probe outside air, the mask PCG's status ...); *out is NULL unless
+ * FG_OK.  The postprocess copies what it needs and does not borrow the plan. */
+int fg_postprocess_create(const fg_plan *plan, const fg_postprocess_options *options,
+                          const double *mask, fg_postprocess **out);
+void fg_postprocess_destroy(fg_postprocess *postprocess);
+int32_t fg_postprocess_probe_count(const fg_postprocess *postprocess);
+/* The thresholded mask [node_count]. */
+int fg_postprocess_mask(const fg_postprocess *postprocess, double *mask);
+/* Force, torque and radial air-gap B of `items` solutions (host arrays, item-major:
+ * a [items][node_count], b1 / b2 [items][triangle_count]); results [items],
+ * airgap_radial_b_t [items][probe_count] (may be NULL when there are no probes).
+ * Per-item failures (FG_NUMERICAL_NONFINITE, FG_MESH_INVALID) are in results[i].status. */
+int fg_postprocess_compute(const fg_postprocess *postprocess, int32_t items, const double *a,
+                           const double *b1, const double *b2, fg_postprocess_result *results,
+                           double *airgap_radial_b_t);
+/* The same from DEVICE solutions (item-major, as above) on `stream` (a cudaStream_t): one
+ * deterministic reduction kernel for force and torque over all items, and a gather of
+ * the few values each probe's smoothing reads; results stay host memory. */
+int fg_postprocess_compute_device(fg_postprocess *postprocess, int32_t items,
+                                  const double *a, const double *b1, const double *b2,
+                                  fg_postprocess_result *results, double *airgap_radial_b_t,
+                                  void *stream);
+/* One-shot ComputeFrozenPostprocess: create, compute one item, destroy.  A plan failure is
+ * returned in result->status (the call itself returns FG_OK). */
+int fg_postprocess_frozen(const fg_plan *plan, const fg_postprocess_options *options,
+                          const double *a, const double *b1, const double *b2,
+                          fg_postprocess_result *result, double *airgap_radial_b_t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -359,3 +359,189 @@ class RefSession:
 
     def __del__(self):
         self.close()
+
+
+# ---- frozen postprocess (gpu_solver/src/postprocess/) ----
+
+def _ref_model(handle):
+    """The model behind a reference handle (ref_artifact_sizes / ref_artifact_copy)."""
+    from femm_gpu_b200.model import Model
+    r = ref()
+    sizes = np.zeros(8, np.int32)
+    depth, ptype = C.c_double(), C.c_int32()
+    r.ref_artifact_sizes(handle, _p(sizes), C.byref(depth), C.byref(ptype))
+    N, E, M, K, D, NC, NCIR, P = (int(v) for v in sizes)
+    xy, tri, tm = np.zeros(2 * N), np.zeros(3 * E, np.int32), np.zeros(E, np.int32)
+    md, mi = np.zeros(5 * M), np.zeros(3 * M, np.int32)
+    cb, ch, cs = np.zeros(max(P, 1)), np.zeros(max(P, 1)), np.zeros(max(P, 1))
+    dn, con, cu = np.zeros(max(D, 1), np.int32), np.zeros(3 * max(NC, 1), np.int32), np.zeros(max(NCIR, 1))
+    r.ref_artifact_copy(handle, _p(xy), _p(tri), _p(tm), _p(md), _p(mi), _p(cb), _p(ch), _p(cs),
+                        _p(dn), _p(con), _p(cu))
+    md, mi, con = md.reshape(-1, 5), mi.reshape(-1, 3), con[: 3 * NC].reshape(-1, 3)
+    # Curve boundaries: split the concatenated points where B restarts at the origin.
+    starts = [i for i in range(P) if cb[i] == 0.0 and ch[i] == 0.0] + [P]
+    curves = [(cb[starts[j]:starts[j + 1]].copy(), ch[starts[j]:starts[j + 1]].copy())
+              for j in range(len(starts) - 1)]
+    assert len(curves) == K
+    return Model(xy=xy.reshape(-1, 2), tri=tri.reshape(-1, 3), tri_mat=tm, nu0=md[:, 0], alpha=md[:, 1],
+                 j_per_a=md[:, 2], hc=md[:, 3], mag_deg=md[:, 4], curve_index=mi[:, 0],
+                 circuit_index=mi[:, 1], group=mi[:, 2], curves=curves, dir_nodes=dn[:D],
+                 dir_values=np.zeros(D), con_a=con[:, 0], con_b=con[:, 1], con_sign=con[:, 2],
+                 circuit_count=NCIR, depth_m=depth.value, problem_type=ptype.value), cu[:NCIR]
+
+
+class RefHandle:
+    """A reference model handle (ref_artifact) freed with the object."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if self.h and _REF is not None:
+            _REF.ref_artifact_free(self.h)
+            self.h = None
+
+
+def ref_femm_nonlinear(stem, curve_directory):
+    """ReadNonlinearFemmReference: (handle, model, FEMM's nodal A, FEMM's flux linkage)."""
+    r = ref()
+    h = C.c_void_p()
+    rc = r.ref_read_femm_nonlinear(stem.encode(), curve_directory.encode(), C.byref(h))
+    handle = RefHandle(h)
+    if rc:
+        raise RuntimeError(r.ref_artifact_error(h).decode())
+    model, _ = _ref_model(h)
+    a = np.zeros(model.node_count)
+    flux = C.c_double()
+    r.ref_femm_expected(h, _p(a), C.byref(flux))
+    return handle, model, a, flux.value
+
+
+def ref_model_handle(model):
+    """A reference handle of an oracle model, block-label groups included."""
+    r = ref()
+    view = ModelView(model)
+    h = C.c_void_p()
+    groups = np.ascontiguousarray(model.group, np.int32)
+    if r.ref_model_handle(view.ref(), _p(groups), C.byref(h)):
+        raise RuntimeError("reference model conversion failed")
+    return RefHandle(h)
+
+
+def ref_postprocess(handle, a, b1, b2, selected_label=1, air_label=3, selected_group=-1, air_group=-1,
+                    radius_m=0.0, angles_rad=(), max_mask_iterations=256, mask_tolerance=1e-12, mask=None,
+                    node_count=None):
+    """The reference's ComputeFrozenPostprocess (its mask through weighted_stress.cu with the
+    oracle's CPU PCG in place of the device solve, unless `mask` is given).
+    Returns (status, Fx, Fy, torque, radial [angles], mask [N])."""
+    r = ref()
+    a = np.ascontiguousarray(a, np.float64)
+    b1 = np.ascontiguousarray(b1, np.float64)
+    b2 = np.ascontiguousarray(b2, np.float64)
+    labels = np.array([selected_label, air_label, selected_group, air_group], np.int32)
+    angles = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+    out3 = np.full(3, np.nan)
+    radial = np.zeros(max(angles.size, 1))
+    mask_out = np.zeros(a.size)
+    m = None if mask is None else np.ascontiguousarray(mask, np.float64)
+    st = r.ref_postprocess(handle.h, _p(a), _p(b1), _p(b2), _p(labels), C.c_double(radius_m),
+                           C.c_int32(angles.size), _p(angles), C.c_int32(max_mask_iterations),
+                           C.c_double(mask_tolerance), None if m is None else _p(m), _p(out3), _p(radial),
+                           _p(mask_out))
+    return int(st), out3[0], out3[1], out3[2], radial[:angles.size], mask_out
+
+
+def ref_read_single_sample_request(path):
+    """ReadSingleSampleRequest: (True, fields dict) or (False, error)."""
+    r = ref()
+    bufs = [C.create_string_buffer(4096) for _ in range(4)]
+    cur, rad = C.c_double(), C.c_double()
+    sel, cnt = C.c_int32(), C.c_int32()
+    ang = np.zeros(64)
+    rc = r.ref_read_single_sample_request(str(path).encode(), bufs[0], bufs[1], bufs[2], C.byref(cur),
+                                          C.byref(sel), C.byref(rad), C.byref(cnt), _p(ang), bufs[3])
+    if rc:
+        return False, bufs[3].value.decode()
+    return True, dict(stem=bufs[0].value.decode(), curve_directory=bufs[1].value.decode(),
+                      source_motor_fem_sha256=bufs[2].value.decode(), current_A=cur.value,
+                      selected_material_label=sel.value, airgap_radius_mm=rad.value,
+                      airgap_angles_deg=list(ang[:cnt.value]))
+
+
+def weighted_stress_mask(model, selected, air, by_group=False, apex_nodes=()):
+    """Numpy restatement of the weighted-stress mask (weighted_stress.cu:24-183): the
+    sqrt(area)-weighted P1 Laplacian, fixed 1 on the selected region, 0 on other non-air
+    regions and non-apex Dirichlet nodes, periodic across every constraint pair (sign +1),
+    solved directly (scipy) and thresholded at 0.5.  None when the reference would refuse."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spla
+    N = model.node_count
+    key = model.group[model.tri_mat] if by_group else model.tri_mat
+    is_sel, is_air = key == selected, key == air
+    fixed = np.full(N, np.nan)
+    dn = np.asarray(model.dir_nodes)
+    dn = dn[~np.isin(dn, np.asarray(apex_nodes, np.int64))]
+    fixed[dn] = 0.0
+    for e in range(model.tri_count):
+        t = model.tri[e]
+        if is_sel[e]:
+            if np.any(np.isfinite(fixed[t]) & (fixed[t] != 1.0)):
+                return None
+            fixed[t] = 1.0
+        elif not is_air[e]:
+            fixed[t] = np.where(np.isfinite(fixed[t]), fixed[t], 0.0)
+    p = model.xy[model.tri]
+    det = ((p[:, 1, 0] - p[:, 0, 0]) * (p[:, 2, 1] - p[:, 0, 1])
+           - (p[:, 2, 0] - p[:, 0, 0]) * (p[:, 1, 1] - p[:, 0, 1]))
+    area = 0.5 * det
+    dx = np.stack([p[:, 1, 1] - p[:, 2, 1], p[:, 2, 1] - p[:, 0, 1], p[:, 0, 1] - p[:, 1, 1]], 1)
+    dy = np.stack([p[:, 2, 0] - p[:, 1, 0], p[:, 0, 0] - p[:, 2, 0], p[:, 1, 0] - p[:, 0, 0]], 1)
+    bx, by = dy / det[:, None], -dx / det[:, None]
+    ke = (np.sqrt(area) * area)[:, None, None] * (bx[:, :, None] * bx[:, None, :] + by[:, :, None] * by[:, None, :])
+    rows = np.repeat(model.tri, 3, axis=1).ravel()
+    cols = np.tile(model.tri, (1, 3)).ravel()
+    K = sp.csr_matrix((ke.ravel(), (rows, cols)), shape=(N, N))
+    # Periodic pairs: union-find roots, fixed values propagated through the pairs.
+    parent = np.arange(N)
+
+    def root(i):
+        while parent[i] != i:
+            parent[i] = parent[parent[i]]
+            i = parent[i]
+        return i
+    for a_, b_ in zip(model.con_a, model.con_b):
+        ra, rb = root(a_), root(b_)
+        if ra != rb:
+            parent[max(ra, rb)] = min(ra, rb)
+    roots = np.array([root(i) for i in range(N)])
+    root_val = np.full(N, np.nan)
+    for i in range(N):
+        if np.isfinite(fixed[i]):
+            if np.isfinite(root_val[roots[i]]) and root_val[roots[i]] != fixed[i]:
+                return None
+            root_val[roots[i]] = fixed[i]
+    free_roots = np.unique(roots[~np.isfinite(root_val[roots])])
+    value = root_val[roots]
+    if free_roots.size:
+        index = -np.ones(N, np.int64)
+        index[free_roots] = np.arange(free_roots.size)
+        P = sp.csr_matrix((np.ones(N), (np.arange(N), np.where(index[roots] >= 0, index[roots], 0))),
+                          shape=(N, free_roots.size))
+        P = P.multiply((index[roots] >= 0)[:, None]).tocsr()
+        fixed_part = np.where(np.isfinite(value), value, 0.0)
+        A = (P.T @ K @ P).tocsc()
+        rhs = -(P.T @ (K @ fixed_part))
+        x = spla.spsolve(A, rhs)
+        value = np.where(index[roots] >= 0, x[np.maximum(index[roots], 0)], value)
+    return (value > 0.5).astype(np.float64)
+
+
+def ref_artifact_handle(text: bytes):
+    """A reference handle of a mesh artifact parsed by the reference's own parser."""
+    r = ref()
+    h = C.c_void_p()
+    rc = r.ref_parse_artifact(text, C.c_size_t(len(text)), C.byref(h))
+    handle = RefHandle(h)
+    if rc:
+        raise RuntimeError(r.ref_artifact_error(h).decode())
+    return handle

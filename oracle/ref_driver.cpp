@@ -3,18 +3,25 @@
 // TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together with
 // FEMM-GPU's host translation units where they lie in the reference checkout
 // (gpu_solver/src/physics/{nonlinear_model,linear_model,nonlinear_topology}.cpp,
-// core/types.cpp, io/{strict_json,mesh_artifact}.cpp) into oracle/_ref/libfemm_ref.so.
+// core/types.cpp, io/{strict_json,mesh_artifact}.cpp, postprocess/{field_postprocess.cpp,
+// weighted_stress.cu} and the FEMM fixture reader tests/native/reference.cpp) into
+// oracle/_ref/libfemm_ref.so.  weighted_stress.cu is compiled as host C++ against
+// shim_cuda/solvers/csr_solver.cuh, a CPU stand-in for its one GPU linear solve.
 // Tests use it to pin the C restatement (femm_oracle.c) and the product's host
 // preparation to the reference bit for bit; nothing in the product loads it.
 #include "physics/nonlinear_model.h"
 #include "physics/nonlinear_topology.h"
 #include "io/mesh_artifact.h"
+#include "io/sample_request.h"
 #include "io/strict_json.h"
+#include "postprocess/postprocess.h"
 #include "signed_node_constraints.h"
+#include "../tests/native/reference.h"
 
 #include "femm_oracle.h"
 
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -90,6 +97,9 @@ struct ref_prepared {
 struct ref_artifact {
   GpuFemmMeshArtifact artifact;
   std::string error;
+  // FEMM fixtures read by ReadNonlinearFemmReference: FEMM's nodal A and flux linkage.
+  std::vector<double> expected_a;
+  double flux_linkage_wb = 0.0;
 };
 
 extern "C" {
@@ -351,6 +361,110 @@ int ref_canonical_sha256(const char *json, size_t length, char *hex65)
   const std::string hex = CanonicalJsonSha256(root);
   std::memcpy(hex65, hex.c_str(), 65);
   return 0;
+}
+
+// ReadSingleSampleRequest (io/sample_request.cpp:98-135).  Returns 0 and fills the fields
+// (strings into 4096-byte buffers, angles into [64]) or 1 and the error text in `error`.
+int ref_read_single_sample_request(const char *path, char *stem, char *curve_directory, char *sha,
+                                   double *current_a, int32_t *selected_label, double *radius_mm,
+                                   int32_t *angle_count, double *angles_deg, char *error)
+{
+  SingleSampleRequest r;
+  std::string e;
+  if (!ReadSingleSampleRequest(path, &r, &e)) {
+    std::snprintf(error, 4096, "%s", e.c_str());
+    return 1;
+  }
+  std::snprintf(stem, 4096, "%s", r.stem.c_str());
+  std::snprintf(curve_directory, 4096, "%s", r.curve_directory.c_str());
+  std::snprintf(sha, 4096, "%s", r.source_motor_fem_sha256.c_str());
+  *current_a = r.current_a;
+  *selected_label = r.selected_material_label;
+  *radius_mm = r.airgap_radius_mm;
+  *angle_count = static_cast<int32_t>(r.airgap_angles_deg.size());
+  for (size_t i = 0; i < r.airgap_angles_deg.size() && i < 64; ++i)
+    angles_deg[i] = r.airgap_angles_deg[i];
+  return 0;
+}
+
+// A model handle for ref_postprocess from an oracle model; groups [materials] or NULL.
+int ref_model_handle(const or_model *m, const int32_t *groups, ref_artifact **out)
+{
+  auto h = std::make_unique<ref_artifact>();
+  if (!ToModel(m, &h->artifact.model)) {
+    *out = h.release();
+    return 1;
+  }
+  if (groups)
+    for (size_t i = 0; i < h->artifact.model.materials.size(); ++i)
+      h->artifact.model.materials[i].group_number = groups[i];
+  *out = h.release();
+  return 0;
+}
+
+// ReadNonlinearFemmReference (tests/native/reference.cpp:229-379): a FEMM .ans solution
+// with the fixture's hard-wired materials, as a model handle for ref_artifact_sizes / copy.
+int ref_read_femm_nonlinear(const char *stem, const char *curve_directory, ref_artifact **out)
+{
+  auto h = std::make_unique<ref_artifact>();
+  NonlinearFemmReference reference;
+  if (!ReadNonlinearFemmReference(stem, curve_directory, &reference, &h->error)) {
+    *out = h.release();
+    return 1;
+  }
+  h->artifact.model = std::move(reference.model);
+  h->artifact.circuit_currents_a = {reference.current_a};
+  h->expected_a = std::move(reference.expected_a);
+  h->flux_linkage_wb = reference.flux_linkage_wb;
+  *out = h.release();
+  return 0;
+}
+
+void ref_femm_expected(const ref_artifact *h, double *a, double *flux_linkage_wb)
+{
+  std::copy(h->expected_a.begin(), h->expected_a.end(), a);
+  *flux_linkage_wb = h->flux_linkage_wb;
+}
+
+// ComputeFrozenPostprocess (field_postprocess.cpp:341-403) on a model handle and a given
+// solution.  mask [N] (0 / 1) selects BuildFrozenPostprocessPlanWithMask, NULL the full
+// BuildFrozenPostprocessPlan (mask through weighted_stress.cu); mask_out [N] may be NULL.
+// out3 = Fx, Fy, torque; radial [angles].  Returns the result status.
+int ref_postprocess(const ref_artifact *h, const double *a, const double *b1, const double *b2,
+                    const int32_t *labels /* selected, air, selected group, air group */,
+                    double radius_m, int32_t angle_count, const double *angles_rad,
+                    int32_t max_mask_iterations, double mask_tolerance, const double *mask,
+                    double *out3, double *radial, double *mask_out)
+{
+  const NonlinearModel &m = h->artifact.model;
+  FrozenPostprocessOptions o;
+  o.selected_material_label = labels[0];
+  o.air_material_label = labels[1];
+  o.selected_group_number = labels[2];
+  o.air_group_number = labels[3];
+  o.airgap_radius_m = radius_m;
+  o.airgap_angles_rad.assign(angles_rad, angles_rad + angle_count);
+  o.max_mask_iterations = max_mask_iterations;
+  o.mask_relative_tolerance = mask_tolerance;
+  NonlinearSolveResult solution;
+  solution.a_wb_per_m.assign(a, a + m.nodes.size());
+  solution.bx_t.assign(b1, b1 + m.triangles.size());
+  solution.by_t.assign(b2, b2 + m.triangles.size());
+  FrozenPostprocessPlan plan;
+  const Status ps = mask ? BuildFrozenPostprocessPlanWithMask(
+                               m, o, std::vector<double>(mask, mask + m.nodes.size()), &plan)
+                         : BuildFrozenPostprocessPlan(m, o, &plan);
+  if (ps != Status::kOk)
+    return static_cast<int>(ps);
+  if (mask_out)
+    std::copy(plan.mask.begin(), plan.mask.end(), mask_out);
+  const FrozenPostprocessResult r = ComputeFrozenPostprocess(m, solution, o, &plan);
+  out3[0] = r.force_x_n;
+  out3[1] = r.force_y_n;
+  out3[2] = r.torque_nm;
+  for (size_t i = 0; i < r.airgap_samples.size(); ++i)
+    radial[i] = r.airgap_samples[i].radial_b_t;
+  return static_cast<int>(r.status);
 }
 
 } // extern "C"

@@ -7,6 +7,10 @@ golden vectors for this path, copied byte for byte (gpu_solver/tests/fixtures/..
 * 35PN230.tab, reference_samples.txt, smoothing_reference.txt  (B-H spline / eval)
 * periodic_strip.gpu.json, antiperiodic_strip.gpu.json, axisymmetric_coil.gpu.json
   and their stock-FEMM *.summary.txt flux linkages (constraint folding, r-z element)
+* nonlinear_pm_coil_planar.{ans,summary.txt,postprocess.txt} and
+  nonlinear_pm_coil_single_sample_request.json: FEMM 4.2's own nonlinear PM / coil
+  solution with its weighted-stress force / torque and smoothed air-gap B samples
+  (the --single-sample fixture)
 
 plus expected.json: the stock-FEMM flux linkages parsed from the summaries.
 """
@@ -28,6 +32,11 @@ FILES = {
     "antiperiodic_strip_v1/antiperiodic_strip.summary.txt": "antiperiodic_strip.summary.txt",
     "axisymmetric_coil_v1/axisymmetric_coil.gpu.json": "axisymmetric_coil.gpu.json",
     "axisymmetric_coil_v1/axisymmetric_coil.summary.txt": "axisymmetric_coil.summary.txt",
+    "nonlinear_pm_coil_v1/nonlinear_pm_coil_planar.ans": "nonlinear_pm_coil_planar.ans",
+    "nonlinear_pm_coil_v1/nonlinear_pm_coil_planar.summary.txt": "nonlinear_pm_coil_planar.summary.txt",
+    "nonlinear_pm_coil_v1/nonlinear_pm_coil_planar.postprocess.txt":
+        "nonlinear_pm_coil_planar.postprocess.txt",
+    "nonlinear_pm_coil_v1/single_sample_request.json": "nonlinear_pm_coil_single_sample_request.json",
 }
 
 

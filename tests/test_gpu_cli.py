@@ -106,24 +106,9 @@ def test_solver_options_mixed_block_jacobi(gpu, tmp_path):
     assert abs(f - g) <= 1e-8 * abs(g)
 
 
-def test_postprocess_requests_are_refused_after_the_solve(gpu, tmp_path):
-    # A legacy planar-DC artifact (no node constraints) with a force request.
-    from femm_gpu_b200 import meshes
-    text, _ = artifact.write_artifact(meshes.square_linear(m=12), [12.0])
-    src = json.loads(text)
-    src["schema_version"] = "gpu_femm_planar_dc_mesh_v1"
-    res = src["resolved"]
-    del res["node_constraints"]
-    for i, r in enumerate(res["regions"]):
-        r["group_number"] = i  # distinct block-label groups for the force request
-    src["canonical_identity_sha256"] = artifact.canonical_sha256(artifact._loads(json.dumps(src))["resolved"])
-    path = tmp_path / "legacy.gpu.json"
-    path.write_text(json.dumps(src))
-    groups = sorted({int(r["group_number"]) for r in res["regions"]})
-    assert len(groups) >= 2
-    req = request(path, [12.0], protocol="gpu_femm_planar_dc_sample_v1", compute_force_torque=True,
-                  force_group_number=groups[0], stress_air_group_number=groups[1])
-    rc, body, _ = call(tmp_path, "--solve", req)
-    assert rc == 1 and body["status"] == "FAIL" and body["solve_status"] == "OK"
-    assert body["postprocess_status"] == "UNSUPPORTED_FEATURE" and body["Fx_N"] is None
-    assert len(body["circuit_flux_linkage_Wb"]) == 1
+def test_generic_protocol_refuses_postprocess_requests(gpu, tmp_path):
+    # The generic protocol exposes only the field solve (sample_adapter.cpp:199-205).
+    path = copy_fixture(tmp_path, "periodic_strip")
+    rc, body, _ = call(tmp_path, "--solve", request(path, [12.0], compute_force_torque=True))
+    assert rc == 1 and body["status"] == "FAIL" and body["solve_status"] == "INVALID_ARGUMENT"
+    assert body["postprocess_status"] == "NOT_RUN" and body["Fx_N"] is None
