@@ -393,6 +393,8 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
         workload=f"rotor-stator sector, {sector.node_count} nodes, anti-periodic 90-degree edges, "
                  f"{ks} samples with per-sample currents and magnet Hc; host-buffer API timing", **res)
 
+    out["postprocess_tangent_sector"] = postprocess_tangent_form(sector, cur, hcs, dev, stream, err)
+
     # Heterogeneous meshes: jittered squares with node counts log-uniform in [5k, 200k],
     # one sample each, in one multi-plan PCG launch per Newton step vs one plan at a time.
     rng = np.random.default_rng(11)
@@ -466,6 +468,104 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
             final_loss=float(ws.stats["final_loss"]), **res)
         fast.close()
         base.close()
+    return out
+
+
+def postprocess_tangent_form(sector, cur, hcs, dev, stream, err):
+    """Rotor torque, force and 45 smoothed air-gap B probes per sample of the sector
+    (weighted stress on the rotor iron + magnets against air, mask solved once on the GPU),
+    host form, device form (one launch for all samples) and the reference's own host
+    ComputeFrozenPostprocess with its reusable plan; then the 3-circuit tangent multi-RHS
+    at one operating point against central differences (6 nonlinear solves)."""
+    import torch
+    import femm_gpu_b200 as fg
+    import oracle as O
+    from femm_gpu_b200 import meshes
+
+    sec = meshes.annular_sector()
+    sec.group = np.array([0, 10, 10, 3, 4, 5, 6], np.int32)
+    p = fg.Plan(sec)
+    kk = 32
+    r = p.solve(cur[:kk], hc_scale=hcs[:kk])
+    ang = np.radians(np.linspace(1.0, 89.0, 45))
+    t0 = time.perf_counter()
+    pp = fg.Postprocess(p, selected_group=10, air_group=0, radius_m=0.0455, angles_rad=ang,
+                        max_mask_iterations=4096)
+    mask_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    host = pp.compute(r.a, r.b1, r.b2)
+    host_s = time.perf_counter() - t0
+    dev_in = [torch.from_numpy(x).to(dev).contiguous() for x in (r.a, r.b1, r.b2)]
+    torch.cuda.synchronize()
+    ptrs = [t_.data_ptr() for t_ in dev_in]
+    got = pp.compute_device(kk, *ptrs, stream=stream.cuda_stream)
+    reps = 50
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        pp.compute_device(kk, *ptrs, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    dev_us = 1e3 * e0.elapsed_time(e1) / reps
+    E = sec.tri_count
+    alg_bytes = E * (5 * 8 + kk * 2 * 8)
+    out = {"workload": f"sector {sec.node_count} nodes / {E} triangles, {kk} solved samples, rotor group "
+                       f"against air, {ang.size} probes at r = 45.5 mm",
+           "mask_build_s_gpu_pcg": mask_s,
+           "host_us_per_sample": 1e6 * host_s / kk,
+           "device_us_per_launch_all_samples": dev_us,
+           "device_us_per_sample": dev_us / kk,
+           "device_launch_includes": "reduction + probe gathers, one D2H of partials and gathers, host smoothing",
+           "device_achieved_gbs": alg_bytes / (dev_us * 1e-6) / 1e9,
+           "device_algorithmic_bytes": alg_bytes,
+           "device_vs_host_force_rel_err": err(got.force, host.force),
+           "device_vs_host_radial_equal": bool(np.array_equal(got.radial_b, host.radial_b)),
+           "all_ok": bool((host.status == 0).all() and (got.status == 0).all())}
+    if O.ref() is not None:
+        hs = O.ref_model_handle(sec)
+        mask = pp.mask()
+        nref = 4
+        t0 = time.perf_counter()
+        for i in range(nref):
+            st, fx, fy, tq, rad, _ = O.ref_postprocess(hs, r.a[i], r.b1[i], r.b2[i], selected_group=10,
+                                                       air_group=0, radius_m=0.0455, angles_rad=ang, mask=mask)
+        # ref_postprocess rebuilds the reusable plan (geometry, probes) for each call
+        out["reference_host_us_per_sample_incl_plan"] = 1e6 * (time.perf_counter() - t0) / nref
+        out["host_equals_reference"] = bool(host.force[nref - 1, 0] == fx and host.torque[nref - 1] == tq
+                                            and np.array_equal(host.radial_b[nref - 1], rad))
+    # Tangent: differential inductances and torque sensitivities at sample 0.
+    base = cur[0]
+    o = fg.production_options()
+    o.linear_relative_tolerance = 1e-13
+    o.max_linear_iterations = 4096
+    p_hc = fg.Plan(sec)  # the operating point without per-sample Hc: same magnets for +-h
+    b0 = p_hc.solve([base])
+    p_hc.solve_tangent(b0.a[0], base, np.eye(3), o)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    da, db1, db2, dflux, tinfo = p_hc.solve_tangent(b0.a[0], base, np.eye(3), o)
+    tan_s = time.perf_counter() - t0
+    h = 0.5
+    cd_in = np.concatenate([base + h * np.eye(3), base - h * np.eye(3)])
+    p_hc.solve(cd_in)
+    t0 = time.perf_counter()
+    cd = p_hc.solve(cd_in)
+    cd_s = time.perf_counter() - t0
+    L_cd = (cd.flux[:3] - cd.flux[3:]) / (2 * h)
+    pt = fg.Postprocess(p_hc, selected_group=10, air_group=0, radius_m=0.0455, angles_rad=ang,
+                        max_mask_iterations=4096)
+    tq = pt.tangent(b0.b1[0], b0.b2[0], da, db1, db2)
+    out["tangent"] = {"directions": 3, "tangent_ms_e2e": 1e3 * tan_s, "pcg_launches": 1,
+                      "pcg_iterations": [int(i.iterations) for i in tinfo],
+                      "central_difference_ms_e2e": 1e3 * cd_s, "speedup_vs_central_difference": cd_s / tan_s,
+                      "inductance_rel_err_vs_central_difference": err(dflux, L_cd),
+                      "dtorque_nm_per_a": [float(x) for x in tq.torque],
+                      "all_ok": bool(all(i.status == 0 for i in tinfo))}
+    pt.close()
+    pp.close()
+    p_hc.close()
+    p.close()
     return out
 
 

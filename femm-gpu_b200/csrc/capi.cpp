@@ -205,6 +205,20 @@ int fg_pcg_solve(fg_plan *plan, int32_t items, const double *values, int32_t val
                                    max_iterations, x, info));
 }
 
+int fg_solve_tangent(fg_plan *plan, const double *base_a, const double *base_currents, int32_t directions,
+                     const double *direction_currents, const fg_solve_options *options, double *da,
+                     double *db1, double *db2, double *dflux, fg_linear_info *info)
+{
+  if (!plan || !options)
+    return ToInt(Status::kInvalidArgument);
+  try {
+    return ToInt(plan->plan.SolveTangent(base_a, base_currents, directions, direction_currents, *options, da, db1,
+                                         db2, dflux, info));
+  } catch (...) {
+    return ToInt(Status::kInternalError);
+  }
+}
+
 int fg_solve_batch(fg_plan *plan, int32_t items, const double *currents, const double *hc_scale,
                    const double *warm_a, const fg_solve_options *options, double *a_out,
                    double *b1_out, double *b2_out, double *flux_out, fg_item_info *info)

@@ -154,6 +154,11 @@ cudaError_t LaunchEquationResidual(const DevicePlan &p, int kp, const double *va
 // x = x0 + (item in mask ? delta : 0) over [n_pad][kp].
 cudaError_t LaunchAddCorrection(const DevicePlan &p, int kp, uint32_t mask, const double *x0,
                                 const double *delta, double *x, cudaStream_t stream);
+// Tangent multi-RHS: circuit-derivative loads [n_pad][kp] and the nodal derivative state.
+cudaError_t LaunchTangentRhs(const DevicePlan &p, int kp, int items, const double *directions, double *rhs,
+                             cudaStream_t stream);
+cudaError_t LaunchDerivativeState(const DevicePlan &p, int kp, const double *x, double *state,
+                                  cudaStream_t stream);
 cudaError_t LaunchFinalize(const DevicePlan &p, int kp, int items, const double *state,
                            double *a_out, double *b1_out, double *b2_out, double *flux_out,
                            cudaStream_t stream);

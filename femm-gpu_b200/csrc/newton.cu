@@ -409,6 +409,56 @@ cudaError_t LaunchAddCorrection(const DevicePlan &p, int kp, uint32_t mask, cons
   return cudaGetLastError();
 }
 
+// Tangent right-hand sides (SolveTangentMultiRhs, nonlinear_solver.cu:131-144): for each
+// direction i, b_i = sum over circuits of dI_c / dI times the circuit's folded per-amp load;
+// no magnet or boundary terms.  Rows >= n and pad items are zero.
+template <int KP>
+__global__ void TangentRhsKernel(DevicePlan p, int items, const double *__restrict__ directions,
+                                 double *__restrict__ rhs)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.n_pad) * KP)
+    return;
+  const int r = static_cast<int>(t / KP), item = static_cast<int>(t % KP);
+  double sum = 0.0;
+  if (r < p.n && item < items)
+    for (int c = 0; c < p.C; ++c) {
+      const double scale = directions[item * p.C + c];
+      if (scale != 0.0)
+        sum += scale * p.circuit_rhs[static_cast<size_t>(c) * p.n + r];
+    }
+  rhs[t] = sum;
+}
+
+// The nodal derivative dA (ExpandAssemblyDerivative, nonlinear_model.cpp:412-422): the
+// signed free-row value, zero on fixed nodes.
+template <int KP>
+__global__ void DerivativeStateKernel(DevicePlan p, const double *__restrict__ x, double *__restrict__ state)
+{
+  const size_t t = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<size_t>(p.N) * KP)
+    return;
+  const int node = static_cast<int>(t / KP), item = static_cast<int>(t % KP);
+  const int row = p.node_to_free[node];
+  state[t] = row >= 0 ? static_cast<double>(p.node_sign[node]) * x[static_cast<size_t>(row) * KP + item] : 0.0;
+}
+
+cudaError_t LaunchTangentRhs(const DevicePlan &p, int kp, int items, const double *directions, double *rhs,
+                             cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.n_pad) * kp);
+  FG_DISPATCH_KP(kp, (TangentRhsKernel<KP><<<blocks, kThreads, 0, stream>>>(p, items, directions, rhs)));
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchDerivativeState(const DevicePlan &p, int kp, const double *x, double *state,
+                                  cudaStream_t stream)
+{
+  const unsigned blocks = Blocks(static_cast<size_t>(p.N) * kp);
+  FG_DISPATCH_KP(kp, (DerivativeStateKernel<KP><<<blocks, kThreads, 0, stream>>>(p, x, state)));
+  return cudaGetLastError();
+}
+
 cudaError_t LaunchFinalize(const DevicePlan &p, int kp, int items, const double *state,
                            double *a_out, double *b1_out, double *b2_out, double *flux_out,
                            cudaStream_t stream)

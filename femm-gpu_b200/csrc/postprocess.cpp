@@ -478,6 +478,32 @@ Status ComputePostprocess(const HostModel &m, const PostprocessPlan &plan, const
   return Status::kOk;
 }
 
+Status ComputeTangentPostprocess(const HostModel &m, const PostprocessPlan &plan, const double *b1,
+                                 const double *b2, const double *da, const double *db1, const double *db2,
+                                 fg_postprocess_result *res, double *radial_b)
+{
+  res->force_x_n = res->force_y_n = res->torque_nm = 0.0;
+  const int32_t E = m.triangles();
+  for (int32_t e = 0; e < E; ++e) {
+    const double hx = plan.hx[e], hy = plan.hy[e];
+    const double bx = b1[e], by = b2[e], dbx = db1[e], dby = db2[e];
+    const double dnormal = 2.0 * (bx * dbx - by * dby);
+    const double dshear = 2.0 * (dbx * by + bx * dby);
+    const double dfx = (dnormal * hx + dshear * hy) / (2.0 * kMu0);
+    const double dfy = (dshear * hx - dnormal * hy) / (2.0 * kMu0);
+    const double w = plan.weight[e];
+    res->force_x_n += w * dfx;
+    res->force_y_n += w * dfy;
+    res->torque_nm += w * (plan.cx[e] * dfy - plan.cy[e] * dfx);
+  }
+  auto at = [](const double *v) { return [v](int32_t i) { return v[i]; }; };
+  if (!Samples(m, plan, at(da), at(db1), at(db2), radial_b))
+    return Status::kMeshInvalid;
+  if (!std::isfinite(res->force_x_n) || !std::isfinite(res->force_y_n) || !std::isfinite(res->torque_nm))
+    return Status::kNumericalNonfinite;
+  return Status::kOk;
+}
+
 } // namespace fg
 
 using fg::Status;
@@ -658,6 +684,22 @@ int fg_postprocess_compute_device(fg_postprocess *pp, int32_t items, const doubl
         (!std::isfinite(r.force_x_n) || !std::isfinite(r.force_y_n) || !std::isfinite(r.torque_nm)))
       st = Status::kNumericalNonfinite;
     r.status = ToInt(st);
+  }
+  return ToInt(Status::kOk);
+}
+
+int fg_postprocess_tangent(const fg_postprocess *pp, int32_t m, const double *b1, const double *b2, const double *da,
+                           const double *db1, const double *db2, fg_postprocess_result *results, double *radial)
+{
+  const size_t P = pp ? pp->plan.probes.size() : 0;
+  if (!pp || m < 0 || (m > 0 && (!b1 || !b2 || !da || !db1 || !db2 || !results || (P > 0 && !radial))))
+    return ToInt(Status::kInvalidArgument);
+  const size_t N = pp->model.nodes(), E = pp->model.triangles();
+  for (int32_t i = 0; i < m; ++i) {
+    fg_postprocess_result &r = results[i];
+    r = fg_postprocess_result{};
+    r.status = ToInt(fg::ComputeTangentPostprocess(pp->model, pp->plan, b1, b2, da + i * N, db1 + i * E,
+                                                   db2 + i * E, &r, P ? radial + i * P : nullptr));
   }
   return ToInt(Status::kOk);
 }

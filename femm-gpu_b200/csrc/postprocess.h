@@ -46,6 +46,12 @@ Status ComputePostprocess(const HostModel &model, const PostprocessPlan &plan, c
                           const double *b1, const double *b2, fg_postprocess_result *result,
                           double *radial_b);
 
+// ComputeFrozenTangentPostprocess (field_postprocess.cpp:405-520) with the reusable plan:
+// force / torque / radial B derivatives of one tangent solution about base B.
+Status ComputeTangentPostprocess(const HostModel &model, const PostprocessPlan &plan, const double *base_b1,
+                                 const double *base_b2, const double *da, const double *db1,
+                                 const double *db2, fg_postprocess_result *result, double *radial_b);
+
 // Device form: force / torque partial sums per CTA and the probe gathers in one launch.
 struct PostprocessDevice {
   const double *hx, *hy, *weight, *cx, *cy; // [E]

@@ -1229,4 +1229,100 @@ Status Plan::PcgSolve(int items, const double *values, int values_per_item, cons
   return Status::kOk;
 }
 
+Status Plan::SolveTangent(const double *base_a, const double *base_currents, int m, const double *directions,
+                          const fg_solve_options &o, double *da, double *db1, double *db2, double *dflux,
+                          fg_linear_info *info)
+{
+  if (host_only_)
+    return Status::kGpuUnavailable;
+  if (m <= 0 || !base_a || !directions || !info || (!base_currents && host_.C > 0))
+    return Status::kInvalidArgument;
+  const size_t N = host_.N, E = host_.E, C = host_.C;
+  for (int i = 0; i < m; ++i)
+    info[i] = fg_linear_info{ToInt(Status::kInvalidArgument), 0, std::numeric_limits<double>::infinity()};
+  // The reference's argument checks (nonlinear_solver.cu:96-104) fail every direction.
+  bool valid = o.linear_relative_tolerance > 0.0 && o.linear_relative_tolerance < 1.0 &&
+               std::isfinite(o.linear_relative_tolerance) && o.max_linear_iterations >= 0;
+  for (size_t i = 0; valid && i < N; ++i)
+    valid = std::isfinite(base_a[i]);
+  for (size_t i = 0; valid && i < m * C; ++i)
+    valid = std::isfinite(directions[i]);
+  if (!valid)
+    return Status::kOk;
+  timing_ = fg_timing{};
+  const int cap = std::min(chunk_cap_, kMaxItems);
+  const int kp_max = PadItems(std::min(m, cap));
+  Status s = EnsureWorkspace(kp_max);
+  if (s != Status::kOk)
+    return s;
+  if ((s = in_warm_.upload(base_a, N)) != Status::kOk || (s = in_currents_.upload(directions, m * C)) != Status::kOk ||
+      (da && (s = out_a_.ensure(m * N)) != Status::kOk) || (db1 && (s = out_b1_.ensure(m * E)) != Status::kOk) ||
+      (db2 && (s = out_b2_.ensure(m * E)) != Status::kOk) ||
+      (dflux && C > 0 && (s = out_flux_.ensure(m * C)) != Status::kOk))
+    return s;
+  // The consistent Newton Jacobian at the base field, one operator (item 0 of a kp = 1 layout).
+  int32_t invalid = 0;
+  if (LaunchInterleave(1, 1, static_cast<int>(N), static_cast<int>(N), in_warm_.get(), state_.get(), nullptr) !=
+          cudaSuccess ||
+      cudaMemset(invalid_.get(), 0, sizeof(int32_t)) != cudaSuccess ||
+      LaunchElementKernel(dev_, 1, state_.get(), 1u, 1u, ev_.get(), er_.get(), invalid_.get(), nullptr) != cudaSuccess ||
+      LaunchGatherValues(dev_, 1, ev_.get(), 1u, values_.get(), diag_.get(), invd_.get(), invalid_.get(), nullptr) !=
+          cudaSuccess ||
+      cudaMemcpy(&invalid, invalid_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return Status::kInternalError;
+  timing_.kernel_launches += 3;
+  if (invalid) {
+    for (int i = 0; i < m; ++i)
+      info[i].status = ToInt(Status::kAssemblyFailed);
+    return Status::kOk;
+  }
+  if (block_size() && cudaMemset(block_fallbacks_.get(), 0, sizeof(int32_t)) != cudaSuccess)
+    return Status::kInternalError;
+  if ((s = BuildBlocks(1, 1, false, false, nullptr)) != Status::kOk)
+    return s;
+  for (int first = 0; first < m; first += cap) {
+    const int k = std::min(cap, m - first), kp = PadItems(k);
+    const uint32_t mask = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+    if (LaunchTangentRhs(dev_, kp, k, in_currents_.get() + static_cast<size_t>(first) * C, rhs_.get(), nullptr) !=
+        cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 1;
+    if ((s = RunPcg(kp, k, mask, o.linear_relative_tolerance, o.max_linear_iterations, 1, 0, 1, 0, 1, nullptr,
+                    block_size() ? blocks64_.get() : nullptr)) != Status::kOk)
+      return s;
+    double pinfo[3 * kMaxItems];
+    int32_t err = 0;
+    if (cudaMemcpy(pinfo, pcg_info_.get(), sizeof(double) * 3 * kp, cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(&err, error_.get(), sizeof(int32_t), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return Status::kInternalError;
+    if (err)
+      return Status::kInternalError;
+    if (LaunchDerivativeState(dev_, kp, x_.get(), state_.get(), nullptr) != cudaSuccess ||
+        LaunchFinalize(dev_, kp, k, state_.get(), da ? out_a_.get() + static_cast<size_t>(first) * N : nullptr,
+                       db1 ? out_b1_.get() + static_cast<size_t>(first) * E : nullptr,
+                       db2 ? out_b2_.get() + static_cast<size_t>(first) * E : nullptr,
+                       dflux && C > 0 ? out_flux_.get() + static_cast<size_t>(first) * C : nullptr,
+                       nullptr) != cudaSuccess)
+      return Status::kInternalError;
+    timing_.kernel_launches += 4;
+    for (int i = 0; i < k; ++i) {
+      info[first + i].status = static_cast<int32_t>(pinfo[3 * i]);
+      info[first + i].iterations = static_cast<int32_t>(pinfo[3 * i + 1]);
+      info[first + i].residual_l2 = pinfo[3 * i + 2];
+    }
+  }
+  if ((da && cudaMemcpy(da, out_a_.get(), m * N * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (db1 && cudaMemcpy(db1, out_b1_.get(), m * E * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (db2 && cudaMemcpy(db2, out_b2_.get(), m * E * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess) ||
+      (dflux && C > 0 && cudaMemcpy(dflux, out_flux_.get(), m * C * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess))
+    return Status::kInternalError;
+  // A derivative whose B or flux is not finite fails like FinalizeResult's check.
+  if (dflux)
+    for (int i = 0; i < m; ++i)
+      for (size_t c = 0; c < C; ++c)
+        if (info[i].status == 0 && !std::isfinite(dflux[i * C + c]))
+          info[i].status = ToInt(Status::kNumericalNonfinite);
+  return Status::kOk;
+}
+
 } // namespace fg

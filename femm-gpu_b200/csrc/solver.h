@@ -42,6 +42,12 @@ public:
                   const int32_t *use_newton, double *values, double *diagonal, double *rhs);
   Status PcgSolve(int items, const double *values, int values_per_item, const double *rhs,
                   double tolerance, int max_iterations, double *x, fg_linear_info *info);
+  // SolveTangentMultiRhs: the consistent Newton Jacobian at base_a [N] and the circuit-
+  // derivative solutions of `directions` [m][C] through one shared-operator PCG launch per
+  // chunk; host arrays out (each may be NULL): da [m][N], db1 / db2 [m][E], dflux [m][C].
+  Status SolveTangent(const double *base_a, const double *base_currents, int m, const double *directions,
+                      const fg_solve_options &options, double *da, double *db1, double *db2,
+                      double *dflux, fg_linear_info *info);
 
   const HostPlan &host() const { return host_; }
   const HostModel &model() const { return model_; }

@@ -45,7 +45,8 @@ EXPORTED = [
     "fg_multi_create", "fg_multi_destroy", "fg_multi_solve", "fg_multi_last_timing",
     "fg_postprocess_default_options", "fg_postprocess_create", "fg_postprocess_destroy",
     "fg_postprocess_probe_count", "fg_postprocess_mask", "fg_postprocess_compute",
-    "fg_postprocess_compute_device", "fg_postprocess_frozen",
+    "fg_postprocess_compute_device", "fg_postprocess_frozen", "fg_postprocess_tangent",
+    "fg_solve_tangent",
 ]
 
 
@@ -311,6 +312,23 @@ class Plan:
             raise FgError(status, "fg_solve_batch_device")
         return [info[i] for i in range(items)]
 
+    def solve_tangent(self, base_a, base_currents, directions, options: Optional[FgSolveOptions] = None):
+        """Tangent multi-RHS at a converged field: returns (da [m, N], db1, db2 [m, E],
+        dflux [m, C], info list)."""
+        base_a = np.ascontiguousarray(base_a, np.float64).ravel()
+        cur = np.ascontiguousarray(base_currents, np.float64).ravel()
+        d = np.ascontiguousarray(np.atleast_2d(directions), np.float64)
+        m = d.shape[0]
+        opts = options if options is not None else production_options()
+        da, db1, db2 = np.zeros((m, self.N)), np.zeros((m, self.E)), np.zeros((m, self.E))
+        dflux = np.zeros((m, max(self.C, 1)))
+        info = (FgLinearInfo * m)()
+        st = lib().fg_solve_tangent(self._h, _p(base_a), _p(cur), C.c_int32(m), _p(d), C.byref(opts), _p(da),
+                                    _p(db1), _p(db2), _p(dflux), info)
+        if st:
+            raise FgError(st, "fg_solve_tangent")
+        return da, db1, db2, dflux[:, : self.C], [info[i] for i in range(m)]
+
     def last_timing(self) -> FgTiming:
         t = FgTiming()
         lib().fg_plan_last_timing(self._h, C.byref(t))
@@ -510,6 +528,22 @@ class Postprocess:
         if st:
             raise FgError(st, "fg_postprocess_compute")
         return self._result([res[i] for i in range(k)], radial)
+
+    def tangent(self, base_b1, base_b2, da, db1, db2) -> PostprocessResult:
+        """Derivatives about base B of tangent solutions da [m, N], db1 / db2 [m, E]."""
+        b1 = np.ascontiguousarray(base_b1, np.float64).ravel()
+        b2 = np.ascontiguousarray(base_b2, np.float64).ravel()
+        da = np.ascontiguousarray(np.atleast_2d(da), np.float64)
+        db1 = np.ascontiguousarray(np.atleast_2d(db1), np.float64)
+        db2 = np.ascontiguousarray(np.atleast_2d(db2), np.float64)
+        m = da.shape[0]
+        res = (FgPostprocessResult * max(m, 1))()
+        radial = np.zeros((m, self.probes))
+        st = lib().fg_postprocess_tangent(self._h, C.c_int32(m), _p(b1), _p(b2), _p(da), _p(db1), _p(db2), res,
+                                          _p(radial) if self.probes else None)
+        if st:
+            raise FgError(st, "fg_postprocess_tangent")
+        return self._result([res[i] for i in range(m)], radial)
 
     def compute_device(self, k, a_ptr, b1_ptr, b2_ptr, stream=0) -> PostprocessResult:
         """Device solutions (item-major) by pointer, e.g. torch tensors' data_ptr()."""

@@ -267,6 +267,22 @@ int fg_solve_batch_device(fg_plan *plan, int32_t items, const double *currents,
                           const fg_solve_options *options, double *a_out, double *b1_out,
                           double *b2_out, double *flux_out, fg_item_info *info, void *stream);
 
+/* First-order response about a converged operating point (SolveTangentMultiRhs,
+ * gpu_solver/src/solvers/nonlinear_solver.cu:85-172): the consistent Newton Jacobian J is
+ * assembled once at base_a [node_count] (base_currents [circuit_count] name the operating
+ * point), and J dA_i = S_i is solved for every direction i -- S_i = sum over circuits of
+ * directions[i][c] times the circuit's per-amp source load, no magnet or boundary terms --
+ * in shared-operator PCG launches of up to 32 directions (16 with 32-row blocks), at
+ * options->linear_relative_tolerance within options->max_linear_iterations.  Outputs are host
+ * arrays and may be NULL: da [m][node_count] (zero on fixed nodes), db1 / db2
+ * [m][triangle_count], dflux [m][circuit_count] (the differential inductances for unit
+ * directions).  info[i] carries each direction's PCG status, iterations and residual;
+ * invalid arguments (non-finite base or directions, a bad tolerance) set every info[i] to
+ * FG_INVALID_ARGUMENT as the reference does. */
+int fg_solve_tangent(fg_plan *plan, const double *base_a, const double *base_currents, int32_t directions,
+                     const double *direction_currents, const fg_solve_options *options, double *da,
+                     double *db1, double *db2, double *dflux, fg_linear_info *info);
+
 /* Timing and launch counters of the last solve on this plan. */
 int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing);
 
@@ -424,6 +440,14 @@ int fg_postprocess_compute_device(fg_postprocess *postprocess, int32_t items,
                                   const double *a, const double *b1, const double *b2,
                                   fg_postprocess_result *results, double *airgap_radial_b_t,
                                   void *stream);
+/* Force / torque / air-gap derivatives of `directions` tangent solutions about the base
+ * field (ComputeFrozenTangentPostprocess, field_postprocess.cpp:405-520): the bilinear cross
+ * term of the weighted-stress density between base B (base_b1 / base_b2 [triangle_count])
+ * and each dB, and the smoothed radial dB at the probes.  da [m][node_count], db1 / db2
+ * [m][triangle_count]; results [m] (N/A, N m/A), airgap_radial_b_t [m][probe_count] (T/A). */
+int fg_postprocess_tangent(const fg_postprocess *postprocess, int32_t directions, const double *base_b1,
+                           const double *base_b2, const double *da, const double *db1, const double *db2,
+                           fg_postprocess_result *results, double *airgap_radial_b_t);
 /* One-shot ComputeFrozenPostprocess: create, compute one item, destroy.  A plan failure is
  * returned in result->status (the call itself returns FG_OK). */
 int fg_postprocess_frozen(const fg_plan *plan, const fg_postprocess_options *options,

@@ -545,3 +545,56 @@ def ref_artifact_handle(text: bytes):
     if rc:
         raise RuntimeError(r.ref_artifact_error(h).decode())
     return handle
+
+
+def finalize(model, a):
+    """B and flux linkage of a nodal solution (or_finalize, nonlinear_solver.cu:16-83)."""
+    view = ModelView(model)
+    a = np.ascontiguousarray(a, np.float64)
+    b1, b2 = np.zeros(model.tri_count), np.zeros(model.tri_count)
+    flux = np.zeros(max(model.circuit_count, 1))
+    st = lib().or_finalize(view.ref(), _p(a), _p(b1), _p(b2), _p(flux))
+    if st:
+        raise RuntimeError(f"oracle finalize status {st}")
+    return b1, b2, flux[: model.circuit_count]
+
+
+def tangent(model, base_a, base_currents, directions, tol=1e-13, maxit=16384):
+    """Restatement of SolveTangentMultiRhs (nonlinear_solver.cu:85-172): the consistent
+    Newton system at base_a (the oracle assembler), S_i = sum_c d_ic * (signed per-amp
+    circuit load), the oracle PCG per direction, dA = signed free values (0 on fixed
+    nodes), then B and flux of dA.  Returns (da [m, N], db1, db2 [m, E], dflux [m, C],
+    [(status, iterations, residual)])."""
+    s = assemble(model, base_a, base_currents, 1)
+    d = np.atleast_2d(np.asarray(directions, np.float64))
+    N = model.node_count
+    out_a, out_b1, out_b2, out_f, infos = [], [], [], [], []
+    for row in d:
+        rhs = np.zeros(s.rows)
+        for c, scale in enumerate(row):
+            if scale != 0.0:
+                rhs += scale * s.sources[c]
+        st, x, its, res = pcg(s, rhs, tol=tol, maxit=maxit)
+        da = np.where(s.node_to_free >= 0, s.node_sign * x[np.maximum(s.node_to_free, 0)], 0.0)
+        b1, b2, fl = finalize(model, da)
+        out_a.append(da)
+        out_b1.append(b1)
+        out_b2.append(b2)
+        out_f.append(fl)
+        infos.append((st, its, res))
+    return np.array(out_a), np.array(out_b1), np.array(out_b2), np.array(out_f), infos
+
+
+def ref_tangent_postprocess(handle, a, b1, b2, da, db1, db2, mask, selected_label=1, air_label=3,
+                            selected_group=-1, air_group=-1, radius_m=0.0, angles_rad=()):
+    """The reference's ComputeFrozenTangentPostprocess with the plan of `mask`.
+    Returns (status, dFx, dFy, dtorque, radial [angles])."""
+    r = ref()
+    arrs = [np.ascontiguousarray(x, np.float64) for x in (a, b1, b2, da, db1, db2, mask)]
+    labels = np.array([selected_label, air_label, selected_group, air_group], np.int32)
+    angles = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+    out3 = np.full(3, np.nan)
+    radial = np.zeros(max(angles.size, 1))
+    st = r.ref_tangent_postprocess(handle.h, *[_p(x) for x in arrs[:6]], _p(labels), C.c_double(radius_m),
+                                   C.c_int32(angles.size), _p(angles), _p(arrs[6]), _p(out3), _p(radial))
+    return int(st), out3[0], out3[1], out3[2], radial[:angles.size]

@@ -467,4 +467,40 @@ int ref_postprocess(const ref_artifact *h, const double *a, const double *b1, co
   return static_cast<int>(r.status);
 }
 
+// ComputeFrozenTangentPostprocess (field_postprocess.cpp:405-520) with the reusable plan
+// built from `mask`: out3 = dFx, dFy, dtorque per amp; radial [angles].  Returns the status.
+int ref_tangent_postprocess(const ref_artifact *h, const double *a, const double *b1, const double *b2,
+                            const double *da, const double *db1, const double *db2, const int32_t *labels,
+                            double radius_m, int32_t angle_count, const double *angles_rad, const double *mask,
+                            double *out3, double *radial)
+{
+  const NonlinearModel &m = h->artifact.model;
+  FrozenPostprocessOptions o;
+  o.selected_material_label = labels[0];
+  o.air_material_label = labels[1];
+  o.selected_group_number = labels[2];
+  o.air_group_number = labels[3];
+  o.airgap_radius_m = radius_m;
+  o.airgap_angles_rad.assign(angles_rad, angles_rad + angle_count);
+  const std::vector<double> mk(mask, mask + m.nodes.size());
+  FrozenPostprocessPlan plan;
+  const Status ps = BuildFrozenPostprocessPlanWithMask(m, o, mk, &plan);
+  if (ps != Status::kOk)
+    return static_cast<int>(ps);
+  NonlinearSolveResult base, derivative;
+  base.a_wb_per_m.assign(a, a + m.nodes.size());
+  base.bx_t.assign(b1, b1 + m.triangles.size());
+  base.by_t.assign(b2, b2 + m.triangles.size());
+  derivative.a_wb_per_m.assign(da, da + m.nodes.size());
+  derivative.bx_t.assign(db1, db1 + m.triangles.size());
+  derivative.by_t.assign(db2, db2 + m.triangles.size());
+  const TangentPostprocessResult r = ComputeFrozenTangentPostprocess(m, base, derivative, o, mk, &plan);
+  out3[0] = r.force_x_n_per_a;
+  out3[1] = r.force_y_n_per_a;
+  out3[2] = r.torque_nm_per_a;
+  for (size_t i = 0; i < r.airgap_radial_flux_density_t_per_a.size(); ++i)
+    radial[i] = r.airgap_radial_flux_density_t_per_a[i];
+  return static_cast<int>(r.status);
+}
+
 } // extern "C"
