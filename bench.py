@@ -537,8 +537,6 @@ def postprocess_tangent_form(sector, cur, hcs, dev, stream, err):
     # Tangent: differential inductances and torque sensitivities at sample 0.
     base = cur[0]
     o = fg.production_options()
-    o.linear_relative_tolerance = 1e-13
-    o.max_linear_iterations = 4096
     p_hc = fg.Plan(sec)  # the operating point without per-sample Hc: same magnets for +-h
     b0 = p_hc.solve([base])
     p_hc.solve_tangent(b0.a[0], base, np.eye(3), o)

@@ -192,17 +192,6 @@ bool Barycentric(const HostModel &m, int32_t e, double x, double y, double lam[3
   return std::isfinite(lam[0]) && std::isfinite(lam[1]) && std::isfinite(lam[2]);
 }
 
-// Sorted-id lookup into a gathered array.
-struct Gathered {
-  const std::vector<int32_t> *ids;
-  const double *values;
-  double operator()(int32_t id) const
-  {
-    const auto it = std::lower_bound(ids->begin(), ids->end(), id);
-    return values[it - ids->begin()];
-  }
-};
-
 } // namespace
 
 Status WeightedStressMask(const HostModel &m, const fg_postprocess_options &o, std::vector<double> *mask)
@@ -344,6 +333,125 @@ Status WeightedStressMask(const HostModel &m, const fg_postprocess_options &o, s
   return Status::kOk;
 }
 
+namespace
+{
+
+// The recipe NodalB follows at corner l of `element` (same control flow, nothing read from
+// a solution), appended to plan->corners and the term arrays.
+void BuildCorner(const HostModel &m, int32_t element, int l, PostprocessPlan *plan)
+{
+  const int32_t *tri = m.tri.data();
+  const double *xy = m.xy.data();
+  const int32_t mat = m.tri_mat[element];
+  const int32_t node = tri[3 * element + l];
+  const std::vector<int32_t> &around = plan->incident[node];
+  CornerStencil c{};
+  c.first = static_cast<int32_t>(plan->term_elem.size());
+  c.element = element;
+  c.node = node;
+  auto term = [&](int32_t e, int32_t other, double w, double tx, double ty, double len) {
+    plan->term_elem.push_back(e);
+    plan->term_node.push_back(other);
+    plan->term_w.push_back(w);
+    plan->term_tx.push_back(tx);
+    plan->term_ty.push_back(ty);
+    plan->term_len.push_back(len);
+  };
+  auto truncate = [&] {
+    plan->term_elem.resize(c.first);
+    plan->term_node.resize(c.first);
+    plan->term_w.resize(c.first);
+    plan->term_tx.resize(c.first);
+    plan->term_ty.resize(c.first);
+    plan->term_len.resize(c.first);
+  };
+  auto finish = [&](int kind) {
+    c.kind = kind;
+    c.count = static_cast<int32_t>(plan->term_elem.size()) - c.first;
+    plan->corners.push_back(c);
+  };
+  bool same = true;
+  for (int32_t e : around)
+    same = same && m.tri_mat[e] == mat;
+  if (same) {
+    double wsum = 0.0;
+    for (int32_t e : around) {
+      const int32_t *t = &tri[3 * e];
+      const double cx = (xy[2 * t[0]] + xy[2 * t[1]] + xy[2 * t[2]]) / 3.0;
+      const double cy = (xy[2 * t[0] + 1] + xy[2 * t[1] + 1] + xy[2 * t[2] + 1]) / 3.0;
+      const double w = 1.0 / std::hypot(xy[2 * node] - cx, xy[2 * node + 1] - cy);
+      if (!(w > 0.0) || !std::isfinite(w))
+        return finish(-1);
+      wsum += w;
+      term(e, -1, w, 0.0, 0.0, 0.0);
+    }
+    c.wsum = wsum;
+    return finish(0);
+  }
+  auto position = [&](int32_t e) {
+    for (int i = 0; i < 3; ++i)
+      if (tri[3 * e + i] == node)
+        return i;
+    return -1;
+  };
+  auto across = [&](int32_t current, int32_t other) {
+    for (int32_t e : around) {
+      if (e == current)
+        continue;
+      for (int i = 0; i < 3; ++i)
+        if (tri[3 * e + i] == other)
+          return e;
+    }
+    return static_cast<int32_t>(-1);
+  };
+  double wsum = 0.0, t1[2] = {0.0, 0.0}, t2[2] = {0.0, 0.0};
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    int32_t current = element;
+    for (size_t step = 0; step < around.size(); ++step) {
+      const int i = position(current);
+      if (i < 0)
+        return finish(-1);
+      const int32_t other = tri[3 * current + (sweep == 0 ? (i + 2) % 3 : (i + 1) % 3)];
+      const int32_t next = across(current, other);
+      if (next < 0) {
+        truncate();
+        c.element = current;
+        return finish(2);
+      }
+      if (m.tri_mat[next] != mat) {
+        const double dx = xy[2 * other] - xy[2 * node], dy = xy[2 * other + 1] - xy[2 * node + 1];
+        const double len = std::hypot(dx, dy);
+        if (!(len > 0.0))
+          return finish(-1);
+        const double w = 0.5 / len;
+        term(current, other, w, dx / len, dy / len, len);
+        wsum += w;
+        const double len2 = std::hypot(xy[2 * other] - xy[2 * node], xy[2 * other + 1] - xy[2 * node + 1]);
+        double *t = sweep == 0 ? t1 : t2;
+        t[0] = (xy[2 * other] - xy[2 * node]) / len2;
+        t[1] = (xy[2 * other + 1] - xy[2 * node + 1]) / len2;
+        break;
+      }
+      current = next;
+    }
+  }
+  if (!(wsum > 0.0))
+    return finish(-1);
+  c.wsum = wsum;
+  const bool simple = std::hypot(t1[0], t1[1]) < 0.9 || std::hypot(t2[0], t2[1]) < 0.9 ||
+                      (-t1[0] * t2[0] - t1[1] * t2[1]) > 0.985;
+  if (simple)
+    return finish(1);
+  // The fallback reads only |B| of the corner's same-label elements and B of the element.
+  truncate();
+  for (int32_t e : around)
+    if (m.tri_mat[e] == mat)
+      term(e, -1, 0.0, 0.0, 0.0, 0.0);
+  return finish(3);
+}
+
+} // namespace
+
 Status BuildPostprocessPlan(const HostModel &m, const fg_postprocess_options &o, std::vector<double> mask,
                             PostprocessPlan *plan)
 {
@@ -418,15 +526,7 @@ Status BuildPostprocessPlan(const HostModel &m, const fg_postprocess_options &o,
   }
   for (const AirgapProbe &p : plan->probes)
     for (int l = 0; l < 3; ++l)
-      for (int32_t e : plan->incident[m.tri[3 * p.element + l]]) {
-        plan->gather_elements.push_back(e);
-        for (int j = 0; j < 3; ++j)
-          plan->gather_nodes.push_back(m.tri[3 * e + j]);
-      }
-  for (std::vector<int32_t> *ids : {&plan->gather_elements, &plan->gather_nodes}) {
-    std::sort(ids->begin(), ids->end());
-    ids->erase(std::unique(ids->begin(), ids->end()), ids->end());
-  }
+      BuildCorner(m, p.element, l, plan);
   return Status::kOk;
 }
 
@@ -612,19 +712,35 @@ int fg_postprocess_compute_device(fg_postprocess *pp, int32_t items, const doubl
   cudaStream_t stream = static_cast<cudaStream_t>(stream_ptr);
   const fg::PostprocessPlan &pl = pp->plan;
   const int32_t E = pp->model.triangles(), N = pp->model.nodes();
-  const int32_t ge = static_cast<int32_t>(pl.gather_elements.size());
-  const int32_t gn = static_cast<int32_t>(pl.gather_nodes.size());
+  const int32_t Pn = static_cast<int32_t>(P), T = static_cast<int32_t>(pl.term_elem.size());
+  for (const fg::CornerStencil &c : pl.corners)
+    if (c.kind < 0) {
+      for (int32_t i = 0; i < items; ++i) {
+        results[i] = fg_postprocess_result{};
+        results[i].status = ToInt(Status::kMeshInvalid);
+      }
+      return ToInt(Status::kOk);
+    }
   Status s = Status::kOk;
   if (pp->geometry.capacity() == 0) {
     std::vector<double> g;
-    g.reserve(5 * static_cast<size_t>(E));
+    g.reserve(5 * static_cast<size_t>(E) + 5 * P + 4 * static_cast<size_t>(T));
     for (const std::vector<double> *v : {&pl.hx, &pl.hy, &pl.weight, &pl.cx, &pl.cy})
       g.insert(g.end(), v->begin(), v->end());
-    std::vector<int32_t> ids(pl.gather_elements);
-    ids.insert(ids.end(), pl.gather_nodes.begin(), pl.gather_nodes.end());
+    for (const fg::AirgapProbe &p : pl.probes) {
+      g.insert(g.end(), p.lambda, p.lambda + 3);
+      g.push_back(p.cosine);
+      g.push_back(p.sine);
+    }
+    for (const std::vector<double> *v : {&pl.term_w, &pl.term_tx, &pl.term_ty, &pl.term_len})
+      g.insert(g.end(), v->begin(), v->end());
+    std::vector<int32_t> ids(pl.term_elem);
+    ids.insert(ids.end(), pl.term_node.begin(), pl.term_node.end());
     s = pp->geometry.upload(g.data(), g.size(), stream);
     if (s == Status::kOk)
-      s = pp->gathers.upload(ids.data(), ids.size(), stream);
+      s = pp->terms.upload(ids.data(), ids.size(), stream);
+    if (s == Status::kOk)
+      s = pp->corners.upload(pl.corners.data(), pl.corners.size(), stream);
     // The uploads read pageable host vectors that die here.
     if (s == Status::kOk && cudaStreamSynchronize(stream) != cudaSuccess)
       s = Status::kInternalError;
@@ -635,29 +751,34 @@ int fg_postprocess_compute_device(fg_postprocess *pp, int32_t items, const doubl
   }
   const int ctas = fg::PostprocessCtas(E);
   const size_t partial_count = static_cast<size_t>(ctas) * items * 3;
-  const size_t per_item = 2 * static_cast<size_t>(ge) + gn;
-  const size_t total = partial_count + per_item * items;
+  const size_t total = partial_count + P * items;
   if ((s = pp->out.ensure(total)) != Status::kOk || (s = pp->host_out.ensure(total)) != Status::kOk)
     return ToInt(s);
   fg::PostprocessDevice d{};
-  d.hx = pp->geometry.get();
-  d.hy = d.hx + E;
-  d.weight = d.hy + E;
-  d.cx = d.weight + E;
-  d.cy = d.cx + E;
-  d.gather_elements = pp->gathers.get();
-  d.gather_nodes = d.gather_elements + ge;
+  const double *g = pp->geometry.get();
+  d.hx = g;
+  d.hy = g + E;
+  d.weight = g + 2 * static_cast<size_t>(E);
+  d.cx = g + 3 * static_cast<size_t>(E);
+  d.cy = g + 4 * static_cast<size_t>(E);
+  d.probe = g + 5 * static_cast<size_t>(E);
+  d.term_w = d.probe + 5 * P;
+  d.term_tx = d.term_w + T;
+  d.term_ty = d.term_tx + T;
+  d.term_len = d.term_ty + T;
+  d.term_elem = pp->terms.get();
+  d.term_node = d.term_elem + T;
+  d.corners = pp->corners.get();
   d.E = E;
   d.N = N;
   d.items = items;
   d.ctas = ctas;
-  d.gather_e = ge;
-  d.gather_n = gn;
+  d.probes = Pn;
   d.a = a;
   d.b1 = b1;
   d.b2 = b2;
   d.partials = pp->out.get();
-  d.gathered = d.partials + partial_count;
+  d.radial = d.partials + partial_count;
   if (fg::LaunchPostprocess(d, stream) != cudaSuccess ||
       cudaMemcpyAsync(pp->host_out.get(), pp->out.get(), total * sizeof(double), cudaMemcpyDeviceToHost,
                       stream) != cudaSuccess ||
@@ -675,15 +796,11 @@ int fg_postprocess_compute_device(fg_postprocess *pp, int32_t items, const doubl
       r.force_y_n += q[1];
       r.torque_nm += q[2];
     }
-    const double *g = h + partial_count + per_item * i;
-    const fg::Gathered gb1{&pl.gather_elements, g}, gb2{&pl.gather_elements, g + ge};
-    const fg::Gathered ga{&pl.gather_nodes, g + 2 * ge};
-    Status st = fg::Samples(pp->model, pl, ga, gb1, gb2, P ? radial + i * P : nullptr) ? Status::kOk
-                                                                                        : Status::kMeshInvalid;
-    if (st == Status::kOk &&
-        (!std::isfinite(r.force_x_n) || !std::isfinite(r.force_y_n) || !std::isfinite(r.torque_nm)))
-      st = Status::kNumericalNonfinite;
-    r.status = ToInt(st);
+    if (P)
+      std::copy(h + partial_count + P * i, h + partial_count + P * (i + 1), radial + P * i);
+    r.status = ToInt(std::isfinite(r.force_x_n) && std::isfinite(r.force_y_n) && std::isfinite(r.torque_nm)
+                         ? Status::kOk
+                         : Status::kNumericalNonfinite);
   }
   return ToInt(Status::kOk);
 }

@@ -105,8 +105,10 @@ def test_sector_torque_derivative_equals_reference(gpu):
     base = np.array([6.0, -3.0, -3.0])
     sol = plan.solve([base])
     assert sol.info[0].status == 0
-    da, db1, db2, dflux, info = plan.solve_tangent(sol.a[0], base, np.eye(3), options())
-    assert all(i.status == 0 for i in info)
+    # The reference's motor options (linear tolerance 1e-10): 1e-13 is below the FP64 floor
+    # of the saturated sector's Jacobian (the oracle's PCG stalls near 1e-12 as well).
+    da, db1, db2, dflux, info = plan.solve_tangent(sol.a[0], base, np.eye(3), fg.production_options())
+    assert all(i.status == 0 for i in info), [(i.status, i.iterations, i.residual_l2) for i in info]
     ang = np.radians(np.linspace(2.0, 88.0, 12))
     pp = fg.Postprocess(plan, selected_group=10, air_group=0, radius_m=0.0455, angles_rad=ang,
                         max_mask_iterations=4096)
