@@ -9,8 +9,10 @@ Tolerances:
 * the mask: equal to the reference's (0 / 1 per node, no tolerance);
 * the library's host postprocess of a GPU solution: equal bit for bit to the reference's
   ComputeFrozenPostprocess on the same solution and mask;
-* the device form against the host form: radial B bit for bit (the same smoothing code on
-  gathered values); force and torque to 1e-12 relative of the largest partial magnitude
+* the device form against the host form: radial B to 1e-13 relative of the largest sample
+  (the same operations in the same order with explicit rounding, except that FEMM's
+  sharp-corner fallback takes |B| from the device hypot, which may differ from the host's
+  in the last bits); force and torque to 1e-12 relative of the largest partial magnitude
   (per-CTA partial sums instead of one sequential sum).
 """
 import hashlib
@@ -112,7 +114,8 @@ def test_device_postprocess_matches_host_form(gpu):
     torch.cuda.synchronize()
     got = pp.compute_device(6, dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr())
     assert (got.status == 0).all() and (host.status == 0).all()
-    assert np.array_equal(got.radial_b, host.radial_b)
+    scale_b = np.abs(host.radial_b).max()
+    np.testing.assert_allclose(got.radial_b, host.radial_b, rtol=0, atol=1e-13 * scale_b)
     scale = np.abs(host.force).max() + np.abs(host.torque).max() / 0.05
     np.testing.assert_allclose(got.force, host.force, rtol=0, atol=1e-12 * scale)
     np.testing.assert_allclose(got.torque, host.torque, rtol=0, atol=1e-12 * scale * 0.05)
