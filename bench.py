@@ -514,9 +514,10 @@ def postprocess_tangent_form(sector, cur, hcs, dev, stream, err):
                        f"against air, {ang.size} probes at r = 45.5 mm",
            "mask_build_s_gpu_pcg": mask_s,
            "host_us_per_sample": 1e6 * host_s / kk,
-           "device_us_per_launch_all_samples": dev_us,
-           "device_us_per_sample": dev_us / kk,
-           "device_launch_includes": "reduction + probe gathers, one D2H of partials and gathers, host smoothing",
+           "device_api_us_per_call_all_samples": dev_us,
+           "device_api_us_per_sample": dev_us / kk,
+           "device_call_includes": "one kernel (force/torque partials + probe smoothing), one D2H of "
+                                   "partials and samples, the ctypes call",
            "device_achieved_gbs": alg_bytes / (dev_us * 1e-6) / 1e9,
            "device_algorithmic_bytes": alg_bytes,
            "device_vs_host_force_rel_err": err(got.force, host.force),
