@@ -395,6 +395,8 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
 
     out["postprocess_tangent_sector"] = postprocess_tangent_form(sector, cur, hcs, dev, stream, err)
 
+    out["streaming_worker"] = worker_form()
+
     # Heterogeneous meshes: jittered squares with node counts log-uniform in [5k, 200k],
     # one sample each, in one multi-plan PCG launch per Newton step vs one plan at a time.
     rng = np.random.default_rng(11)
@@ -567,6 +569,61 @@ def postprocess_tangent_form(sector, cur, hcs, dev, stream, err):
     p_hc.close()
     p.close()
     return out
+
+
+def worker_form(jobs=8, items=8):
+    """The JSON boundary as a service: `jobs` batch files of `items` samples on one 40,401-node
+    artifact, streamed through one `femm_gpu --worker` (plans resident across jobs, the next
+    job prepared while the GPU solves) against one `femm_gpu --batch` process per file."""
+    import hashlib
+    import subprocess
+    import tempfile
+    from femm_gpu_b200 import artifact, meshes
+
+    cli = os.path.join(ROOT, "femm-gpu_b200", "bin", "femm_gpu")
+    tmp = tempfile.mkdtemp(prefix="fg_worker_")
+    model = meshes.square_nonlinear(m=200, seed=2)
+    text, _ = artifact.write_artifact(model, [10.0, -5.0, 3.0])
+    art = os.path.join(tmp, "mesh.gpu.json")
+    open(art, "w").write(text)
+    digest = hashlib.sha256(text.encode()).hexdigest()
+    files = []
+    for j in range(jobs):
+        cur = meshes.seeded_currents(items, 3, 20.0, seed=9000 + j)
+        body = {"protocol": "gpu_femm_magnetostatic_batch_v1", "max_items_per_chunk": items,
+                "items": [{"task_id": f"j{j}i{i}", "request": {
+                    "protocol": "gpu_femm_magnetostatic_sample_v1", "mesh_artifact_path": art,
+                    "mesh_artifact_sha256": digest, "circuit_currents_A": [float(x) for x in cur[i]],
+                    "force_group_number": -1, "stress_air_group_number": -1, "airgap_radius_mm": 0,
+                    "airgap_angles_deg": [], "sliding_band_angle_deg": 0, "compute_force_torque": False,
+                    "include_field_solution": False}} for i in range(items)]}
+        f = os.path.join(tmp, f"b{j}.json")
+        open(f, "w").write(json.dumps(body))
+        files.append(f)
+    session = hashlib.sha256(b"bench").hexdigest()
+    lines = [json.dumps({"session": session, "sequence": j + 1, "request_path": f,
+                         "response_path": os.path.join(tmp, f"w{j}.json"),
+                         "request_sha256": hashlib.sha256(open(f, "rb").read()).hexdigest()})
+             for j, f in enumerate(files)]
+    t0 = time.perf_counter()
+    r = subprocess.run([cli, "--worker"], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                       timeout=900)
+    worker_s = time.perf_counter() - t0
+    status = [json.loads(x) for x in r.stdout.strip().splitlines()]
+    t0 = time.perf_counter()
+    rcs = [subprocess.run([cli, "--batch", f, os.path.join(tmp, f"o{j}.json")], capture_output=True,
+                          timeout=900).returncode for j, f in enumerate(files)]
+    oneshot_s = time.perf_counter() - t0
+    same = all(json.load(open(os.path.join(tmp, f"w{j}.json")))["items"][0]["response"]["circuit_flux_linkage_Wb"]
+               == json.load(open(os.path.join(tmp, f"o{j}.json")))["items"][0]["response"]["circuit_flux_linkage_Wb"]
+               for j in range(jobs))
+    return {"workload": f"{jobs} batch files x {items} samples, one {model.node_count}-node artifact "
+                        f"({len(text) / 1e6:.1f} MB JSON), wall clock including process start",
+            "worker_solves_per_s": jobs * items / worker_s, "one_shot_solves_per_s": jobs * items / oneshot_s,
+            "speedup": oneshot_s / worker_s,
+            "worker_prepare_seconds": [round(s_["prepare_seconds"], 4) for s_ in status],
+            "all_pass": all(s_["exit_code"] == 0 for s_ in status) and all(rc == 0 for rc in rcs),
+            "responses_equal": bool(same)}
 
 
 def run_reference(args, world, rank, local):

@@ -205,6 +205,17 @@ int fg_pcg_solve(fg_plan *plan, int32_t items, const double *values, int32_t val
                                    max_iterations, x, info));
 }
 
+int fg_plan_attach_device(fg_plan *plan)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  try {
+    return ToInt(plan->plan.AttachDevice());
+  } catch (...) {
+    return ToInt(Status::kInternalError);
+  }
+}
+
 int fg_solve_tangent(fg_plan *plan, const double *base_a, const double *base_currents, int32_t directions,
                      const double *direction_currents, const fg_solve_options *options, double *da,
                      double *db1, double *db2, double *dflux, fg_linear_info *info)

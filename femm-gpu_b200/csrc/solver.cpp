@@ -89,6 +89,24 @@ Status Plan::Create(HostModel model, const fg_plan_options &options)
   from_iterate_ = (options_.flags & FG_PLAN_PCG_FROM_ITERATE) != 0;
   if (host_only_)
     return Status::kOk;
+  return DeviceInit();
+}
+
+Status Plan::AttachDevice()
+{
+  if (!host_only_)
+    return Status::kOk;
+  const Status s = DeviceInit();
+  if (s == Status::kOk) {
+    host_only_ = false;
+    options_.flags &= ~FG_PLAN_HOST_ONLY;
+  }
+  return s;
+}
+
+Status Plan::DeviceInit()
+{
+  Status s = Status::kOk;
   int devices = 0;
   if (cudaGetDeviceCount(&devices) != cudaSuccess || devices < 1) {
     cudaGetLastError();

@@ -31,6 +31,8 @@ class Plan
 {
 public:
   Status Create(HostModel model, const fg_plan_options &options);
+  // Gives a host-only plan its device side (upload, events); no-op on a device plan.
+  Status AttachDevice();
   Status SolveDevice(const SolveRequest &request);
   // Host buffers in and out.  warm_device (device [items * N], used instead of the host
   // `warm`) and guard_warm serve the learned warm start.
@@ -55,6 +57,7 @@ public:
   size_t DeviceBytes() const;
 
 private:
+  Status DeviceInit();
   Status Upload();
   Status EnsureWorkspace(int kp);
   Status SolveChunk(const SolveRequest &request, int first, int count);

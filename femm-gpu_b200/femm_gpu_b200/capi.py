@@ -46,7 +46,7 @@ EXPORTED = [
     "fg_postprocess_default_options", "fg_postprocess_create", "fg_postprocess_destroy",
     "fg_postprocess_probe_count", "fg_postprocess_mask", "fg_postprocess_compute",
     "fg_postprocess_compute_device", "fg_postprocess_frozen", "fg_postprocess_tangent",
-    "fg_solve_tangent",
+    "fg_solve_tangent", "fg_plan_attach_device",
 ]
 
 

@@ -3,6 +3,7 @@
 //   femm_gpu [options] --solve REQUEST.json RESPONSE.json
 //   femm_gpu [options] --batch BATCH.json RESPONSE.json
 //   femm_gpu [options] --single-sample REQUEST.json RESPONSE.json
+//   femm_gpu [options] --worker        (job envelopes on stdin, one status line per job)
 //   femm_gpu --capabilities
 //   femm_gpu --describe-artifact ARTIFACT.json   (parsed model and plan sizes, as JSON)
 //   femm_gpu --sha256 FILE                        (the file-bytes SHA-256 a request names)
@@ -41,6 +42,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -50,6 +52,13 @@
 #include <iomanip>
 #include <iostream>
 #include <map>
+#include <memory>
+#include <mutex>
+#include <condition_variable>
+#include <thread>
+#include <atomic>
+#include <set>
+#include <list>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -228,81 +237,6 @@ bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
   return r.sliding_band_angle_deg == 0.0 && (!post || groups);
 }
 
-// A verified, parsed artifact and its plan.
-struct Prepared {
-  int status = 0;
-  std::string error;
-  Artifact artifact;
-  fg_plan *plan = nullptr;
-  ~Prepared()
-  {
-    if (plan)
-      fg_plan_destroy(plan);
-  }
-};
-
-void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
-{
-  std::string bytes;
-  if (!ReadFile(path, &bytes)) {
-    p->status = FG_INPUT_IO;
-    p->error = "cannot open mesh artifact";
-  } else if (fgio::Sha256Hex(bytes) != sha) {
-    p->status = FG_INVALID_ARGUMENT;
-    p->error = "mesh artifact SHA mismatch";
-  } else if (!fgio::ParseArtifact(bytes, &p->artifact, &p->error)) {
-    p->status = FG_INVALID_ARGUMENT;
-  }
-}
-
-// The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
-int EnsurePlan(Prepared *p, const Options &opt)
-{
-  if (p->plan)
-    return 0;
-  fg_model m = p->artifact.Model();
-  const int rc = fg_plan_create(&m, &opt.plan, &p->plan);
-  if (rc != 0)
-    p->plan = nullptr;
-  return rc;
-}
-
-// Solves k samples on a prepared plan; statuses[i] = per-item status.
-int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std::vector<Solved> *out,
-               std::vector<int> *statuses, int *launches)
-{
-  const fg_model m = p.artifact.Model();
-  const size_t k = reqs.size(), N = m.node_count, E = m.triangle_count, C = m.circuit_count;
-  std::vector<double> cur(k * C), a(k * N), b1(k * E), b2(k * E), flux(k * (C ? C : 1));
-  for (size_t i = 0; i < k; ++i)
-    for (size_t c = 0; c < C; ++c)
-      cur[i * C + c] = reqs[i]->circuit_currents_a[c];
-  std::vector<fg_item_info> info(k);
-  fg_solve_options o;
-  fg_production_options(&o);
-  const int rc = fg_solve_batch(p.plan, static_cast<int32_t>(k), cur.data(), nullptr, nullptr, &o, a.data(),
-                                b1.data(), b2.data(), flux.data(), info.data());
-  fg_timing t{};
-  fg_plan_last_timing(p.plan, &t);
-  *launches += static_cast<int>(t.pcg_launches);
-  out->assign(k, Solved{});
-  statuses->assign(k, rc);
-  if (rc != 0)
-    return rc;
-  for (size_t i = 0; i < k; ++i) {
-    Solved &s = (*out)[i];
-    s.currents.assign(cur.begin() + i * C, cur.begin() + (i + 1) * C);
-    s.flux.assign(flux.begin() + i * C, flux.begin() + i * C + C);
-    s.a.assign(a.begin() + i * N, a.begin() + (i + 1) * N);
-    s.b1.assign(b1.begin() + i * E, b1.begin() + (i + 1) * E);
-    s.b2.assign(b2.begin() + i * E, b2.begin() + (i + 1) * E);
-    s.iterations = info[i].iterations;
-    s.residual = info[i].residual_l2;
-    (*statuses)[i] = info[i].status;
-  }
-  return 0;
-}
-
 // The postprocess options of a planar-DC request (sample_adapter.cpp:426-432).
 fg_postprocess_options PostOptions(const SampleRequest &r, std::vector<double> *angles)
 {
@@ -366,6 +300,107 @@ private:
   std::map<std::vector<double>, std::pair<int, fg_postprocess *>> cache_;
 };
 
+// A verified, parsed artifact and its plan.
+struct Prepared {
+  int status = 0;
+  std::string error;
+  Artifact artifact;
+  fg_plan *plan = nullptr;
+  int plan_status = -1;   // -1 not attempted, else the fg_plan_create status
+  bool host_only = false; // a host-only plan still to be given its device side
+  PostCache post;         // postprocess masks of this artifact, per request options
+  ~Prepared()
+  {
+    if (plan)
+      fg_plan_destroy(plan);
+  }
+};
+
+void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
+{
+  std::string bytes;
+  if (!ReadFile(path, &bytes)) {
+    p->status = FG_INPUT_IO;
+    p->error = "cannot open mesh artifact";
+  } else if (fgio::Sha256Hex(bytes) != sha) {
+    p->status = FG_INVALID_ARGUMENT;
+    p->error = "mesh artifact SHA mismatch";
+  } else if (!fgio::ParseArtifact(bytes, &p->artifact, &p->error)) {
+    p->status = FG_INVALID_ARGUMENT;
+  }
+}
+
+// Builds the host side of the plan ahead of the GPU work (the streaming worker's prefetch).
+void PreparePlanOnHost(Prepared *p, const Options &opt)
+{
+  if (p->status != 0 || p->plan_status >= 0)
+    return;
+  fg_model m = p->artifact.Model();
+  fg_plan_options o = opt.plan;
+  o.flags |= FG_PLAN_HOST_ONLY;
+  p->plan_status = fg_plan_create(&m, &o, &p->plan);
+  if (p->plan_status != 0)
+    p->plan = nullptr;
+  p->host_only = p->plan_status == 0;
+}
+
+// The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
+int EnsurePlan(Prepared *p, const Options &opt)
+{
+  if (p->plan && p->host_only) {
+    const int rc = fg_plan_attach_device(p->plan);
+    if (rc != 0)
+      return rc;
+    p->host_only = false;
+  }
+  if (p->plan)
+    return 0;
+  if (p->plan_status > 0)
+    return p->plan_status;
+  fg_model m = p->artifact.Model();
+  const int rc = fg_plan_create(&m, &opt.plan, &p->plan);
+  if (rc != 0)
+    p->plan = nullptr;
+  p->plan_status = rc;
+  return rc;
+}
+
+// Solves k samples on a prepared plan; statuses[i] = per-item status.
+int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std::vector<Solved> *out,
+               std::vector<int> *statuses, int *launches)
+{
+  const fg_model m = p.artifact.Model();
+  const size_t k = reqs.size(), N = m.node_count, E = m.triangle_count, C = m.circuit_count;
+  std::vector<double> cur(k * C), a(k * N), b1(k * E), b2(k * E), flux(k * (C ? C : 1));
+  for (size_t i = 0; i < k; ++i)
+    for (size_t c = 0; c < C; ++c)
+      cur[i * C + c] = reqs[i]->circuit_currents_a[c];
+  std::vector<fg_item_info> info(k);
+  fg_solve_options o;
+  fg_production_options(&o);
+  const int rc = fg_solve_batch(p.plan, static_cast<int32_t>(k), cur.data(), nullptr, nullptr, &o, a.data(),
+                                b1.data(), b2.data(), flux.data(), info.data());
+  fg_timing t{};
+  fg_plan_last_timing(p.plan, &t);
+  *launches += static_cast<int>(t.pcg_launches);
+  out->assign(k, Solved{});
+  statuses->assign(k, rc);
+  if (rc != 0)
+    return rc;
+  for (size_t i = 0; i < k; ++i) {
+    Solved &s = (*out)[i];
+    s.currents.assign(cur.begin() + i * C, cur.begin() + (i + 1) * C);
+    s.flux.assign(flux.begin() + i * C, flux.begin() + i * C + C);
+    s.a.assign(a.begin() + i * N, a.begin() + (i + 1) * N);
+    s.b1.assign(b1.begin() + i * E, b1.begin() + (i + 1) * E);
+    s.b2.assign(b2.begin() + i * E, b2.begin() + (i + 1) * E);
+    s.iterations = info[i].iterations;
+    s.residual = info[i].residual_l2;
+    (*statuses)[i] = info[i].status;
+  }
+  return 0;
+}
+
 int Solve(const std::string &request_path, const std::string &response_path, const Options &opt)
 {
   if (SameFile(request_path, response_path)) {
@@ -416,9 +451,8 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   int post_status = 0;
   Post result;
   if (solve_status == 0 && post) {
-    PostCache cache;
     fg_postprocess *pp = nullptr;
-    post_status = cache.Get(p.plan, req, &pp);
+    post_status = p.post.Get(p.plan, req, &pp);
     if (post_status == 0)
       post_status = RunPost(pp, sols[0], &result);
     status = post_status;
@@ -437,31 +471,20 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   return 0;
 }
 
-int Batch(const std::string &request_path, const std::string &response_path, const Options &opt)
+using ArtifactKey = std::pair<std::string, std::string>; // path, SHA-256
+using ArtifactCache = std::map<ArtifactKey, std::shared_ptr<Prepared>>;
+
+// Solves a parsed batch and returns the response text.  Items naming the same artifact are
+// solved together; `artifacts` supplies prepared artifacts (and keeps the ones prepared
+// here), so a caller that keeps it keeps plans and postprocess masks across batches.
+std::string RunBatch(const fgio::BatchRequest &batch, const Options &opt, ArtifactCache *artifacts,
+                     std::chrono::steady_clock::time_point t0, bool *all_pass)
 {
-  if (SameFile(request_path, response_path)) {
-    std::cerr << "FAIL magnetostatic batch: response must not overwrite request\n";
-    return 1;
-  }
-  const auto t0 = std::chrono::steady_clock::now();
-  std::string text, error;
-  fgio::BatchRequest batch;
-  if (!ReadFile(request_path, &text) || !fgio::ParseBatchRequestText(text, &batch, &error)) {
-    std::ostringstream o;
-    o << "{\n  \"protocol\": \"gpu_femm_magnetostatic_batch_v1\",\n  \"status\": \"FAIL\",\n"
-      << "  \"solve_status\": \"" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
-      << "  \"error_identifier\": \"GPU_FEMM_" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
-      << "  \"error_message\": \"" << fgio::Escape(error.empty() ? "cannot read request" : error)
-      << "\",\n  \"items\": []\n}\n";
-    PublishAtomically(response_path, o.str());
-    std::cerr << "FAIL magnetostatic batch request: " << error << '\n';
-    return 1;
-  }
   const size_t k = batch.items.size();
   std::vector<std::string> bodies(k);
   std::vector<int> final_status(k, FG_INTERNAL_ERROR);
   // Items grouped by artifact (path + SHA): each artifact read, verified and planned once.
-  std::map<std::pair<std::string, std::string>, std::vector<size_t>> groups;
+  std::map<ArtifactKey, std::vector<size_t>> groups;
   for (size_t i = 0; i < k; ++i)
     groups[{batch.items[i].request.mesh_artifact_path, batch.items[i].request.mesh_artifact_sha256}].push_back(i);
   int chunks = 0, launches = 0, cache_hits = 0;
@@ -469,8 +492,12 @@ int Batch(const std::string &request_path, const std::string &response_path, con
   for (auto &g : groups) {
     cache_hits += static_cast<int>(g.second.size()) - 1;
     const auto a0 = std::chrono::steady_clock::now();
-    Prepared p;
-    Prepare(g.first.first, g.first.second, opt, &p);
+    std::shared_ptr<Prepared> &slot = (*artifacts)[g.first];
+    if (!slot) {
+      slot = std::make_shared<Prepared>();
+      Prepare(g.first.first, g.first.second, opt, slot.get());
+    }
+    Prepared &p = *slot;
     artifact_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - a0).count();
     std::vector<size_t> ready;
     for (size_t i : g.second) {
@@ -499,7 +526,6 @@ int Batch(const std::string &request_path, const std::string &response_path, con
       ready.clear();
     }
     const auto s0 = std::chrono::steady_clock::now();
-    PostCache cache;
     for (size_t first = 0; first < ready.size(); first += batch.max_items_per_chunk) {
       const size_t n = std::min<size_t>(batch.max_items_per_chunk, ready.size() - first);
       std::vector<const SampleRequest *> reqs;
@@ -518,7 +544,7 @@ int Batch(const std::string &request_path, const std::string &response_path, con
         Post result;
         if (solve_status == 0 && r.postprocess_requested()) {
           fg_postprocess *pp = nullptr;
-          post_status = cache.Get(p.plan, r, &pp);
+          post_status = p.post.Get(p.plan, r, &pp);
           if (post_status == 0)
             post_status = RunPost(pp, sols[j], &result);
           status = post_status;
@@ -531,7 +557,8 @@ int Batch(const std::string &request_path, const std::string &response_path, con
     }
     solve_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
   }
-  bool pass = true;
+  bool &pass = *all_pass;
+  pass = true;
   for (int s : final_status)
     pass = pass && s == 0;
   std::ostringstream o;
@@ -552,13 +579,292 @@ int Batch(const std::string &request_path, const std::string &response_path, con
     o << "    {\"task_id\": \"" << batch.items[i].task_id << "\", \"response\": " << bodies[i]
       << (i + 1 < k ? "},\n" : "}\n");
   o << "  ]\n}\n";
-  if (!PublishAtomically(response_path, o.str())) {
+  return o.str();
+}
+
+int Batch(const std::string &request_path, const std::string &response_path, const Options &opt)
+{
+  if (SameFile(request_path, response_path)) {
+    std::cerr << "FAIL magnetostatic batch: response must not overwrite request\n";
+    return 1;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  std::string text, error;
+  fgio::BatchRequest batch;
+  if (!ReadFile(request_path, &text) || !fgio::ParseBatchRequestText(text, &batch, &error)) {
+    std::ostringstream o;
+    o << "{\n  \"protocol\": \"gpu_femm_magnetostatic_batch_v1\",\n  \"status\": \"FAIL\",\n"
+      << "  \"solve_status\": \"" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
+      << "  \"error_identifier\": \"GPU_FEMM_" << StatusName(FG_INVALID_ARGUMENT) << "\",\n"
+      << "  \"error_message\": \"" << fgio::Escape(error.empty() ? "cannot read request" : error)
+      << "\",\n  \"items\": []\n}\n";
+    PublishAtomically(response_path, o.str());
+    std::cerr << "FAIL magnetostatic batch request: " << error << '\n';
+    return 1;
+  }
+  ArtifactCache artifacts;
+  bool pass = false;
+  const std::string text_out = RunBatch(batch, opt, &artifacts, t0, &pass);
+  if (!PublishAtomically(response_path, text_out)) {
     std::cerr << "FAIL magnetostatic batch: could not atomically publish response\n";
     return 1;
   }
   if (!pass)
     std::cerr << "FAIL magnetostatic batch: one or more batch items failed\n";
   return pass ? 0 : 1;
+}
+
+// ---- --worker: the streaming batch worker (MotorBatchWorker, gpu_solver/src/app/
+// motor_worker.cpp:24-191) over the neutral batch protocol.
+//
+// Standard input carries one job envelope per line, {"session", "sequence", "request_path",
+// "response_path", "request_sha256"}; one thread prepares the next job (envelope, request
+// bytes and SHA-256, batch parse, the artifacts it names read, verified, parsed and their
+// plans built on the host by up to 4 threads) while the GPU solves the current one, with at
+// most one prepared job waiting.  Jobs of one session must come in sequence (1, 2, ...); a
+// refused job still consumes its number.  After each job one status line goes to standard
+// output.  Unlike the one-shot --batch, prepared artifacts -- device plans and postprocess
+// masks -- stay resident across jobs (at most kWorkerArtifacts, least recently used out);
+// an artifact file is still read and hashed for every job that names it, so a changed file
+// fails exactly as it would for --batch.
+constexpr size_t kWorkerArtifacts = 32;
+
+struct WorkerJob {
+  std::string session, request_path, response_path, request_sha256, error;
+  int32_t sequence = 0;
+  fgio::BatchRequest batch;
+  ArtifactCache staged; // artifacts read for this job that the resident set lacks or must replace
+  double prepare_seconds = 0.0;
+  std::chrono::steady_clock::time_point prepare_begin, prepare_end;
+};
+
+// The resident artifacts: the consumer owns the map, the producer asks which keys exist.
+struct WorkerArtifacts {
+  std::mutex mutex;
+  std::set<ArtifactKey> keys;
+  ArtifactCache map;
+  std::list<ArtifactKey> order; // most recently used first
+};
+
+std::unique_ptr<WorkerJob> PrepareWorkerJob(const std::string &line, const std::string &executable,
+                                            const Options &opt, WorkerArtifacts *resident)
+{
+  auto job = std::make_unique<WorkerJob>();
+  const auto started = std::chrono::steady_clock::now();
+  job->prepare_begin = started;
+  try {
+    fgio::Json root;
+    std::string error;
+    if (!fgio::ParseJson(line, &root, &error) ||
+        !fgio::HasExactly(root, {"session", "sequence", "request_path", "response_path", "request_sha256"},
+                          &error))
+      throw std::runtime_error("invalid stream job envelope");
+    using K = fgio::Json::Kind;
+    const fgio::Json *session = root.get("session", K::String, &error);
+    const fgio::Json *sequence = root.get("sequence", K::Number, &error);
+    const fgio::Json *request = root.get("request_path", K::String, &error);
+    const fgio::Json *response = root.get("response_path", K::String, &error);
+    const fgio::Json *hash = root.get("request_sha256", K::String, &error);
+    if (!session || !sequence || !request || !response || !hash || !fgio::IsSha256Hex(session->text) ||
+        !fgio::IsSha256Hex(hash->text) || !fgio::AsInt32(*sequence, &job->sequence) || job->sequence < 1)
+      throw std::runtime_error("invalid stream job identity");
+    job->session = session->text;
+    job->request_path = request->text;
+    job->response_path = response->text;
+    job->request_sha256 = hash->text;
+    if (job->request_path.empty() || job->response_path.empty() ||
+        SameFile(job->response_path, job->request_path) || SameFile(job->response_path, executable))
+      throw std::runtime_error("unsafe stream output path");
+    std::string bytes;
+    if (!ReadFile(job->request_path, &bytes) || fgio::Sha256Hex(bytes) != job->request_sha256)
+      throw std::runtime_error("stream request SHA-256 mismatch");
+    if (!fgio::ParseBatchRequestText(bytes, &job->batch, &error))
+      throw std::runtime_error(error);
+    // A transaction is bounded independently of the number of submissions.
+    if (job->batch.items.size() > 32)
+      throw std::runtime_error("stream transaction exceeds 32 items");
+    std::vector<ArtifactKey> keys;
+    for (const fgio::BatchItem &item : job->batch.items) {
+      const ArtifactKey key{item.request.mesh_artifact_path, item.request.mesh_artifact_sha256};
+      if (std::find(keys.begin(), keys.end(), key) == keys.end())
+        keys.push_back(key);
+    }
+    for (const ArtifactKey &key : keys)
+      if (SameFile(job->response_path, key.first))
+        throw std::runtime_error("stream response would overwrite an artifact");
+    std::set<ArtifactKey> have;
+    {
+      std::lock_guard<std::mutex> lock(resident->mutex);
+      have = resident->keys;
+    }
+    std::vector<std::shared_ptr<Prepared>> loads(keys.size());
+    std::atomic<size_t> next{0};
+    auto load = [&] {
+      for (;;) {
+        const size_t slot = next.fetch_add(1, std::memory_order_relaxed);
+        if (slot >= keys.size())
+          return;
+        const ArtifactKey &key = keys[slot];
+        if (have.count(key)) {
+          // Resident: the file must still hold the bytes that were verified.
+          std::string art;
+          auto check = std::make_shared<Prepared>();
+          if (!ReadFile(key.first, &art)) {
+            check->status = FG_INPUT_IO;
+            check->error = "cannot open mesh artifact";
+          } else if (fgio::Sha256Hex(art) != key.second) {
+            check->status = FG_INVALID_ARGUMENT;
+            check->error = "mesh artifact SHA mismatch";
+          } else {
+            continue;
+          }
+          loads[slot] = check;
+          continue;
+        }
+        auto p = std::make_shared<Prepared>();
+        Prepare(key.first, key.second, opt, p.get());
+        PreparePlanOnHost(p.get(), opt);
+        loads[slot] = p;
+      }
+    };
+    std::vector<std::thread> loaders;
+    const size_t width = std::min<size_t>(4, keys.size());
+    for (size_t i = 1; i < width; ++i) {
+      try {
+        loaders.emplace_back(load);
+      } catch (const std::system_error &) {
+        break;
+      }
+    }
+    load();
+    for (std::thread &t : loaders)
+      t.join();
+    for (size_t i = 0; i < keys.size(); ++i)
+      if (loads[i])
+        job->staged[keys[i]] = loads[i];
+  } catch (const std::exception &e) {
+    job->error = e.what();
+  }
+  job->prepare_end = std::chrono::steady_clock::now();
+  job->prepare_seconds = std::chrono::duration<double>(job->prepare_end - started).count();
+  return job;
+}
+
+// Runs a prepared job against the resident artifacts; the exit code of --batch.
+int RunWorkerJob(WorkerJob *job, const Options &opt, WorkerArtifacts *resident)
+{
+  ArtifactCache view;
+  {
+    std::lock_guard<std::mutex> lock(resident->mutex);
+    for (auto &kv : job->staged) {
+      const bool failed = kv.second->status != 0;
+      if (failed) {
+        view[kv.first] = kv.second; // a stale or unreadable file: fail this job only
+        continue;
+      }
+      resident->map[kv.first] = kv.second;
+      resident->keys.insert(kv.first);
+    }
+    for (const fgio::BatchItem &item : job->batch.items) {
+      const ArtifactKey key{item.request.mesh_artifact_path, item.request.mesh_artifact_sha256};
+      if (view.count(key))
+        continue;
+      auto it = resident->map.find(key);
+      if (it != resident->map.end()) {
+        view[key] = it->second;
+        resident->order.remove(key);
+        resident->order.push_front(key);
+      }
+    }
+    while (resident->order.size() > kWorkerArtifacts) {
+      const ArtifactKey old = resident->order.back();
+      resident->order.pop_back();
+      if (!view.count(old)) {
+        resident->map.erase(old);
+        resident->keys.erase(old);
+      }
+    }
+  }
+  bool pass = false;
+  const std::string text = RunBatch(job->batch, opt, &view, job->prepare_begin, &pass);
+  if (!PublishAtomically(job->response_path, text)) {
+    job->error = "could not atomically publish response";
+    return 1;
+  }
+  return pass ? 0 : 1;
+}
+
+int Worker(const Options &opt, const std::string &executable)
+{
+  const auto worker_start = std::chrono::steady_clock::now();
+  WorkerArtifacts resident;
+  std::mutex mutex;
+  std::condition_variable changed;
+  std::unique_ptr<WorkerJob> ready;
+  bool eof = false;
+  std::thread producer([&] {
+    for (;;) {
+      // Wait before reading: at most one prepared job besides the one on the GPU.
+      std::unique_lock<std::mutex> lock(mutex);
+      changed.wait(lock, [&] { return !ready; });
+      lock.unlock();
+      std::string line;
+      if (!std::getline(std::cin, line))
+        break;
+      auto job = PrepareWorkerJob(line, executable, opt, &resident);
+      lock.lock();
+      ready = std::move(job);
+      changed.notify_all();
+    }
+    std::lock_guard<std::mutex> lock(mutex);
+    eof = true;
+    changed.notify_all();
+  });
+  std::string session;
+  int32_t previous = 0;
+  for (;;) {
+    std::unique_lock<std::mutex> lock(mutex);
+    changed.wait(lock, [&] { return ready || eof; });
+    if (!ready)
+      break;
+    std::unique_ptr<WorkerJob> job = std::move(ready);
+    changed.notify_all();
+    lock.unlock();
+    int result = 1;
+    const auto solve_begin = std::chrono::steady_clock::now();
+    const bool in_sequence = (session.empty() || session == job->session) && job->sequence == previous + 1;
+    if (job->error.empty()) {
+      if (in_sequence) {
+        session = job->session;
+        previous = job->sequence;
+        try {
+          result = RunWorkerJob(job.get(), opt, &resident);
+        } catch (const std::exception &e) {
+          job->error = e.what();
+        }
+      } else {
+        job->error = "stream session or submission sequence mismatch";
+      }
+    } else if (in_sequence) {
+      // A refused request still consumes its envelope number, not GPU work.
+      session = job->session;
+      previous = job->sequence;
+    }
+    const auto solve_end = std::chrono::steady_clock::now();
+    auto since = [&](std::chrono::steady_clock::time_point t) {
+      return std::chrono::duration<double>(t - worker_start).count();
+    };
+    std::cout << std::setprecision(17) << "{\"session\":\"" << fgio::Escape(job->session)
+              << "\",\"sequence\":" << job->sequence << ",\"request_sha256\":\"" << job->request_sha256
+              << "\",\"exit_code\":" << result << ",\"prepare_seconds\":" << job->prepare_seconds
+              << ",\"prepare_begin_seconds\":" << since(job->prepare_begin)
+              << ",\"prepare_end_seconds\":" << since(job->prepare_end)
+              << ",\"solve_begin_seconds\":" << since(solve_begin)
+              << ",\"solve_end_seconds\":" << since(solve_end) << ",\"error\":\"" << fgio::Escape(job->error)
+              << "\"}" << std::endl;
+  }
+  producer.join();
+  return 0;
 }
 
 // WriteSingleSampleResponse (gpu_solver/tests/native/reference_adapter.cu:16-61).
@@ -761,7 +1067,7 @@ int Usage()
 {
   std::cerr << "usage: femm_gpu [--preconditioner jacobi|block-jacobi] [--block-size 8|32] "
                "[--precision fp64|mixed] (--solve request.json response.json | "
-               "--batch batch.json response.json | --single-sample request.json response.json | "
+               "--batch batch.json response.json | --single-sample request.json response.json | --worker | "
                "--capabilities | --describe-artifact artifact.json)\n";
   return 2;
 }
@@ -828,6 +1134,8 @@ int main(int argc, char **argv)
     return Solve(argv[next + 1], argv[next + 2], opt);
   if (rest == 3 && std::strcmp(argv[next], "--batch") == 0)
     return Batch(argv[next + 1], argv[next + 2], opt);
+  if (rest == 1 && std::strcmp(argv[next], "--worker") == 0)
+    return Worker(opt, argv[0]);
   if (rest == 3 && std::strcmp(argv[next], "--single-sample") == 0)
     return SingleSample(argv[next + 1], argv[next + 2], opt);
   return Usage();

@@ -283,6 +283,12 @@ int fg_solve_tangent(fg_plan *plan, const double *base_a, const double *base_cur
                      const double *direction_currents, const fg_solve_options *options, double *da,
                      double *db1, double *db2, double *dflux, fg_linear_info *info);
 
+/* Gives a host-only plan (FG_PLAN_HOST_ONLY) its device side -- the uploads and set-up
+ * fg_plan_create does for a device plan -- so that the host preparation (validation,
+ * splines, signed folding, symbolic CSR, gather plan) can run on another thread, ahead of
+ * the GPU work.  FG_OK on a plan that already has it; FG_GPU_UNAVAILABLE without a GPU. */
+int fg_plan_attach_device(fg_plan *plan);
+
 /* Timing and launch counters of the last solve on this plan. */
 int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing);
 
