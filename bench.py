@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
     p.add_argument("--sector-samples", type=int, default=64, help="samples of the shared-geometry sector form")
     p.add_argument("--hetero-meshes", type=int, default=64, help="meshes of the heterogeneous-batch form")
+    p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker"],
+                   help="run one form alone and print its JSON (profiling)")
     return p.parse_args()
 
 
@@ -697,8 +699,32 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line))
 
 
+def only_form(args):
+    import torch
+
+    from femm_gpu_b200 import meshes
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    if args.only_form == "streaming_worker":
+        out = worker_form()
+    else:
+        rng = np.random.default_rng(77)
+        cur = rng.uniform(-15.0, 15.0, size=(args.sector_samples, 3))
+        hcs = rng.uniform(8.5e5, 9.5e5, size=args.sector_samples) / 9.0e5
+
+        def err(a, b):
+            return float(max(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i]) for i in range(len(b))))
+        out = postprocess_tangent_form(meshes.annular_sector(), cur, hcs, dev, stream, err)
+    print(json.dumps({"form": args.only_form, **out}))
+
+
 def main():
     args = parse()
+    if args.only_form:
+        only_form(args)
+        return
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank, local)
