@@ -34,6 +34,7 @@
 //
 // Exit codes: 0 every response PASS, 1 a FAIL response or an I/O failure, 2 usage error.
 #include "artifact.h"
+#include "cli_common.h"
 #include "femm_ans.h"
 #include "femm_gpu.h"
 #include "json.h"
@@ -66,83 +67,9 @@
 namespace
 {
 
+using namespace fgcli;
 using fgio::Artifact;
 using fgio::SampleRequest;
-
-constexpr double kTwoPi = 6.283185307179586476925286766559005768;
-constexpr double kPi = 3.141592653589793238462643383279502884;
-
-struct Options {
-  fg_plan_options plan{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, 0};
-};
-
-std::string StatusName(int s) { return fg_status_name(s); }
-
-bool ReadFile(const std::string &path, std::string *out)
-{
-  std::ifstream f(path, std::ios::binary);
-  if (!f)
-    return false;
-  std::stringstream ss;
-  ss << f.rdbuf();
-  *out = ss.str();
-  return static_cast<bool>(f) || f.eof();
-}
-
-// Same file (by device and inode when both exist, else by resolved path).
-bool SameFile(const std::string &a, const std::string &b)
-{
-  struct stat sa {}, sb {};
-  if (stat(a.c_str(), &sa) == 0 && stat(b.c_str(), &sb) == 0)
-    return sa.st_dev == sb.st_dev && sa.st_ino == sb.st_ino;
-  char ra[4096], rb[4096];
-  const char *pa = realpath(a.c_str(), ra), *pb = realpath(b.c_str(), rb);
-  return std::string(pa ? pa : a.c_str()) == std::string(pb ? pb : b.c_str());
-}
-
-// Writes `text` to path.tmp.<clock>.<n> and renames it over `path`.
-bool PublishAtomically(const std::string &path, const std::string &text)
-{
-  static std::atomic<uint64_t> sequence{0};
-  const std::string tmp = path + ".tmp." +
-                          std::to_string(std::chrono::steady_clock::now().time_since_epoch().count()) +
-                          "." + std::to_string(sequence.fetch_add(1));
-  {
-    std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
-    if (!f)
-      return false;
-    f << text;
-    f.flush();
-    if (!f) {
-      std::remove(tmp.c_str());
-      return false;
-    }
-  }
-  if (std::rename(tmp.c_str(), path.c_str()) != 0) {
-    std::remove(tmp.c_str());
-    return false;
-  }
-  return true;
-}
-
-// What one solved sample returns.
-struct Solved {
-  std::vector<double> currents, flux, a, b1, b2;
-  int32_t iterations = 0;
-  double residual = 0.0;
-};
-
-// A postprocessed sample.
-struct Post {
-  double fx = 0.0, fy = 0.0, torque = 0.0;
-  std::vector<double> radial;
-};
-
-template <class V> void List(std::ostream &o, const V &v)
-{
-  for (size_t i = 0; i < v.size(); ++i)
-    o << (i ? ", " : "") << v[i];
-}
 
 // WritePlanarDcSampleResponse's layout (gpu_solver/src/app/sample_adapter.cpp:236-355).
 std::string SampleResponse(int status, int solve_status, bool post_requested, int post_status,
@@ -237,134 +164,6 @@ bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
   return r.sliding_band_angle_deg == 0.0 && (!post || groups);
 }
 
-// The postprocess options of a planar-DC request (sample_adapter.cpp:426-432).
-fg_postprocess_options PostOptions(const SampleRequest &r, std::vector<double> *angles)
-{
-  fg_postprocess_options o;
-  fg_postprocess_default_options(&o);
-  o.selected_group_number = r.force_group_number;
-  o.air_group_number = r.stress_air_group_number;
-  o.max_mask_iterations = 4096;
-  o.airgap_radius_m = r.airgap_radius_mm * 1e-3;
-  angles->clear();
-  for (double deg : r.airgap_angles_deg)
-    angles->push_back(deg * kPi / 180.0);
-  o.airgap_angle_count = static_cast<int32_t>(angles->size());
-  o.airgap_angles_rad = angles->data();
-  return o;
-}
-
-// Postprocesses one solved sample on `pp` (created for the same request options).
-int RunPost(fg_postprocess *pp, const Solved &s, Post *out)
-{
-  fg_postprocess_result r{};
-  out->radial.assign(static_cast<size_t>(fg_postprocess_probe_count(pp)), 0.0);
-  const int rc = fg_postprocess_compute(pp, 1, s.a.data(), s.b1.data(), s.b2.data(), &r, out->radial.data());
-  if (rc != 0)
-    return rc;
-  out->fx = r.force_x_n;
-  out->fy = r.force_y_n;
-  out->torque = r.torque_nm;
-  return r.status;
-}
-
-// Postprocess objects of one artifact's plan, one per distinct request (groups, circle).
-class PostCache
-{
-public:
-  ~PostCache()
-  {
-    for (auto &kv : cache_)
-      if (kv.second.second)
-        fg_postprocess_destroy(kv.second.second);
-  }
-  // Status of the postprocess plan; *pp valid when 0.
-  int Get(fg_plan *plan, const SampleRequest &r, fg_postprocess **pp)
-  {
-    std::vector<double> key{static_cast<double>(r.force_group_number),
-                            static_cast<double>(r.stress_air_group_number), r.airgap_radius_mm};
-    key.insert(key.end(), r.airgap_angles_deg.begin(), r.airgap_angles_deg.end());
-    auto it = cache_.find(key);
-    if (it == cache_.end()) {
-      std::vector<double> angles;
-      const fg_postprocess_options o = PostOptions(r, &angles);
-      fg_postprocess *p = nullptr;
-      const int rc = fg_postprocess_create(plan, &o, nullptr, &p);
-      it = cache_.emplace(key, std::make_pair(rc, p)).first;
-    }
-    *pp = it->second.second;
-    return it->second.first;
-  }
-
-private:
-  std::map<std::vector<double>, std::pair<int, fg_postprocess *>> cache_;
-};
-
-// A verified, parsed artifact and its plan.
-struct Prepared {
-  int status = 0;
-  std::string error;
-  Artifact artifact;
-  fg_plan *plan = nullptr;
-  int plan_status = -1;   // -1 not attempted, else the fg_plan_create status
-  bool host_only = false; // a host-only plan still to be given its device side
-  PostCache post;         // postprocess masks of this artifact, per request options
-  ~Prepared()
-  {
-    if (plan)
-      fg_plan_destroy(plan);
-  }
-};
-
-void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
-{
-  std::string bytes;
-  if (!ReadFile(path, &bytes)) {
-    p->status = FG_INPUT_IO;
-    p->error = "cannot open mesh artifact";
-  } else if (fgio::Sha256Hex(bytes) != sha) {
-    p->status = FG_INVALID_ARGUMENT;
-    p->error = "mesh artifact SHA mismatch";
-  } else if (!fgio::ParseArtifact(bytes, &p->artifact, &p->error)) {
-    p->status = FG_INVALID_ARGUMENT;
-  }
-}
-
-// Builds the host side of the plan ahead of the GPU work (the streaming worker's prefetch).
-void PreparePlanOnHost(Prepared *p, const Options &opt)
-{
-  if (p->status != 0 || p->plan_status >= 0)
-    return;
-  fg_model m = p->artifact.Model();
-  fg_plan_options o = opt.plan;
-  o.flags |= FG_PLAN_HOST_ONLY;
-  p->plan_status = fg_plan_create(&m, &o, &p->plan);
-  if (p->plan_status != 0)
-    p->plan = nullptr;
-  p->host_only = p->plan_status == 0;
-}
-
-// The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
-int EnsurePlan(Prepared *p, const Options &opt)
-{
-  if (p->plan && p->host_only) {
-    const int rc = fg_plan_attach_device(p->plan);
-    if (rc != 0)
-      return rc;
-    p->host_only = false;
-  }
-  if (p->plan)
-    return 0;
-  if (p->plan_status > 0)
-    return p->plan_status;
-  fg_model m = p->artifact.Model();
-  const int rc = fg_plan_create(&m, &opt.plan, &p->plan);
-  if (rc != 0)
-    p->plan = nullptr;
-  p->plan_status = rc;
-  return rc;
-}
-
 // Solves k samples on a prepared plan; statuses[i] = per-item status.
 int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std::vector<Solved> *out,
                std::vector<int> *statuses, int *launches)
@@ -452,7 +251,8 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   Post result;
   if (solve_status == 0 && post) {
     fg_postprocess *pp = nullptr;
-    post_status = p.post.Get(p.plan, req, &pp);
+    post_status = p.post.Get(p.plan, req.force_group_number, req.stress_air_group_number, req.airgap_radius_mm,
+                             req.airgap_angles_deg, &pp);
     if (post_status == 0)
       post_status = RunPost(pp, sols[0], &result);
     status = post_status;
@@ -470,9 +270,6 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   }
   return 0;
 }
-
-using ArtifactKey = std::pair<std::string, std::string>; // path, SHA-256
-using ArtifactCache = std::map<ArtifactKey, std::shared_ptr<Prepared>>;
 
 // Solves a parsed batch and returns the response text.  Items naming the same artifact are
 // solved together; `artifacts` supplies prepared artifacts (and keeps the ones prepared
@@ -544,7 +341,8 @@ std::string RunBatch(const fgio::BatchRequest &batch, const Options &opt, Artifa
         Post result;
         if (solve_status == 0 && r.postprocess_requested()) {
           fg_postprocess *pp = nullptr;
-          post_status = p.post.Get(p.plan, r, &pp);
+          post_status = p.post.Get(p.plan, r.force_group_number, r.stress_air_group_number, r.airgap_radius_mm,
+                                   r.airgap_angles_deg, &pp);
           if (post_status == 0)
             post_status = RunPost(pp, sols[j], &result);
           status = post_status;

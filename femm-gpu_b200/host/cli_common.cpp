@@ -1,0 +1,144 @@
+// cli_common.cpp -- pieces shared by the femm_gpu adapters.
+#include "cli_common.h"
+
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <atomic>
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <sstream>
+
+namespace fgcli
+{
+
+std::string StatusName(int s) { return fg_status_name(s); }
+
+bool ReadFile(const std::string &path, std::string *out)
+{
+  std::ifstream f(path, std::ios::binary);
+  if (!f)
+    return false;
+  std::stringstream ss;
+  ss << f.rdbuf();
+  *out = ss.str();
+  return static_cast<bool>(f) || f.eof();
+}
+
+bool SameFile(const std::string &a, const std::string &b)
+{
+  struct stat sa {}, sb {};
+  if (stat(a.c_str(), &sa) == 0 && stat(b.c_str(), &sb) == 0)
+    return sa.st_dev == sb.st_dev && sa.st_ino == sb.st_ino;
+  char ra[4096], rb[4096];
+  const char *pa = realpath(a.c_str(), ra), *pb = realpath(b.c_str(), rb);
+  return std::string(pa ? pa : a.c_str()) == std::string(pb ? pb : b.c_str());
+}
+
+bool PublishAtomically(const std::string &path, const std::string &text)
+{
+  static std::atomic<uint64_t> sequence{0};
+  const std::string tmp = path + ".tmp." +
+                          std::to_string(std::chrono::steady_clock::now().time_since_epoch().count()) +
+                          "." + std::to_string(sequence.fetch_add(1));
+  {
+    std::ofstream f(tmp, std::ios::binary | std::ios::trunc);
+    if (!f)
+      return false;
+    f << text;
+    f.flush();
+    if (!f) {
+      std::remove(tmp.c_str());
+      return false;
+    }
+  }
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+    std::remove(tmp.c_str());
+    return false;
+  }
+  return true;
+}
+
+// The postprocess options of an adapter request (sample_adapter.cpp:51-58, :426-432):
+// group selection, a mask PCG of at most 4096 iterations, the circle in metres and radians.
+fg_postprocess_options PostOptions(int32_t selected_group, int32_t air_group, double radius_mm,
+                                   const std::vector<double> &angles_deg, std::vector<double> *angles)
+{
+  fg_postprocess_options o;
+  fg_postprocess_default_options(&o);
+  o.selected_group_number = selected_group;
+  o.air_group_number = air_group;
+  o.max_mask_iterations = 4096;
+  o.airgap_radius_m = radius_mm * 1e-3;
+  angles->clear();
+  for (double deg : angles_deg)
+    angles->push_back(deg * kPi / 180.0);
+  o.airgap_angle_count = static_cast<int32_t>(angles->size());
+  o.airgap_angles_rad = angles->data();
+  return o;
+}
+
+int RunPost(fg_postprocess *pp, const Solved &s, Post *out)
+{
+  fg_postprocess_result r{};
+  out->radial.assign(static_cast<size_t>(fg_postprocess_probe_count(pp)), 0.0);
+  const int rc = fg_postprocess_compute(pp, 1, s.a.data(), s.b1.data(), s.b2.data(), &r, out->radial.data());
+  if (rc != 0)
+    return rc;
+  out->fx = r.force_x_n;
+  out->fy = r.force_y_n;
+  out->torque = r.torque_nm;
+  return r.status;
+}
+
+void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
+{
+  std::string bytes;
+  if (!ReadFile(path, &bytes)) {
+    p->status = FG_INPUT_IO;
+    p->error = "cannot open mesh artifact";
+  } else if (fgio::Sha256Hex(bytes) != sha) {
+    p->status = FG_INVALID_ARGUMENT;
+    p->error = "mesh artifact SHA mismatch";
+  } else if (!fgio::ParseArtifact(bytes, &p->artifact, &p->error)) {
+    p->status = FG_INVALID_ARGUMENT;
+  }
+}
+
+void PreparePlanOnHost(Prepared *p, const Options &opt)
+{
+  if (p->status != 0 || p->plan_status >= 0)
+    return;
+  fg_model m = p->artifact.Model();
+  fg_plan_options o = opt.plan;
+  o.flags |= FG_PLAN_HOST_ONLY;
+  p->plan_status = fg_plan_create(&m, &o, &p->plan);
+  if (p->plan_status != 0)
+    p->plan = nullptr;
+  p->host_only = p->plan_status == 0;
+}
+
+int EnsurePlan(Prepared *p, const Options &opt)
+{
+  if (p->plan && p->host_only) {
+    const int rc = fg_plan_attach_device(p->plan);
+    if (rc != 0)
+      return rc;
+    p->host_only = false;
+  }
+  if (p->plan)
+    return 0;
+  if (p->plan_status > 0)
+    return p->plan_status;
+  fg_model m = p->artifact.Model();
+  const int rc = fg_plan_create(&m, &opt.plan, &p->plan);
+  if (rc != 0)
+    p->plan = nullptr;
+  p->plan_status = rc;
+  return rc;
+}
+
+} // namespace fgcli

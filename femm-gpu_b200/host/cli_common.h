@@ -1,0 +1,116 @@
+// cli_common.h -- pieces shared by the femm_gpu adapters: file I/O with atomic publication,
+// prepared (read, verified, parsed, planned) artifacts, solved samples and their
+// postprocess.
+#pragma once
+
+#include "artifact.h"
+#include "femm_gpu.h"
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <ostream>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace fgcli
+{
+
+constexpr double kTwoPi = 6.283185307179586476925286766559005768;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+struct Options {
+  fg_plan_options plan{FG_PRECOND_JACOBI, 8, FG_PRECISION_FP64, 0};
+};
+
+std::string StatusName(int s);
+bool ReadFile(const std::string &path, std::string *out);
+// Same file (by device and inode when both exist, else by resolved path).
+bool SameFile(const std::string &a, const std::string &b);
+// Writes `text` to path.tmp.<clock>.<n> and renames it over `path`.
+bool PublishAtomically(const std::string &path, const std::string &text);
+
+// What one solved sample returns.
+struct Solved {
+  std::vector<double> currents, flux, a, b1, b2;
+  int32_t iterations = 0;
+  double residual = 0.0;
+};
+
+// A postprocessed sample.
+struct Post {
+  double fx = 0.0, fy = 0.0, torque = 0.0;
+  std::vector<double> radial;
+};
+
+template <class V> void List(std::ostream &o, const V &v)
+{
+  for (size_t i = 0; i < v.size(); ++i)
+    o << (i ? ", " : "") << v[i];
+}
+
+fg_postprocess_options PostOptions(int32_t selected_group, int32_t air_group, double radius_mm,
+                                   const std::vector<double> &angles_deg, std::vector<double> *angles);
+// Postprocesses one solved sample on `pp` (created for the same request options).
+int RunPost(fg_postprocess *pp, const Solved &s, Post *out);
+
+// Postprocess objects of one artifact's plan, one per distinct request (groups, circle).
+class PostCache
+{
+public:
+  ~PostCache()
+  {
+    for (auto &kv : cache_)
+      if (kv.second.second)
+        fg_postprocess_destroy(kv.second.second);
+  }
+  // Status of the postprocess plan of (selected group, air group, circle); *pp valid when 0.
+  int Get(fg_plan *plan, int32_t selected_group, int32_t air_group, double radius_mm,
+          const std::vector<double> &angles_deg, fg_postprocess **pp)
+  {
+    std::vector<double> key{static_cast<double>(selected_group), static_cast<double>(air_group), radius_mm};
+    key.insert(key.end(), angles_deg.begin(), angles_deg.end());
+    auto it = cache_.find(key);
+    if (it == cache_.end()) {
+      std::vector<double> angles;
+      const fg_postprocess_options o = PostOptions(selected_group, air_group, radius_mm, angles_deg, &angles);
+      fg_postprocess *p = nullptr;
+      const int rc = fg_postprocess_create(plan, &o, nullptr, &p);
+      it = cache_.emplace(key, std::make_pair(rc, p)).first;
+    }
+    *pp = it->second.second;
+    return it->second.first;
+  }
+
+private:
+  std::map<std::vector<double>, std::pair<int, fg_postprocess *>> cache_;
+};
+
+// A verified, parsed artifact and its plan.
+struct Prepared {
+  int status = 0;
+  std::string error;
+  fgio::Artifact artifact;
+  fg_plan *plan = nullptr;
+  int plan_status = -1;   // -1 not attempted, else the fg_plan_create status
+  bool host_only = false; // a host-only plan still to be given its device side
+  PostCache post;         // postprocess masks of this artifact, per request options
+  ~Prepared()
+  {
+    if (plan)
+      fg_plan_destroy(plan);
+  }
+};
+
+// Reads the artifact, checks its SHA-256 and parses it (the adapters' artifact gate).
+void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p);
+// Builds the host side of the plan ahead of the GPU work (the streaming worker's prefetch).
+void PreparePlanOnHost(Prepared *p, const Options &opt);
+// The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
+int EnsurePlan(Prepared *p, const Options &opt);
+
+using ArtifactKey = std::pair<std::string, std::string>; // path, SHA-256
+using ArtifactCache = std::map<ArtifactKey, std::shared_ptr<Prepared>>;
+
+} // namespace fgcli
