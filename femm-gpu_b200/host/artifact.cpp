@@ -59,32 +59,54 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
     return false;
   const bool planar_dc = schema->text == "gpu_femm_planar_dc_mesh_v1";
   const bool generic = schema->text == "gpu_femm_magnetostatic_mesh_v1";
-  if (!planar_dc && !generic) {
-    *error = "unsupported mesh artifact schema (motor artifacts are not served here)";
+  const bool neutral = planar_dc || generic;
+  const bool motor = schema->text == "gpu_femm_mesh_v1";
+  if (schema->text == "gpu_femm_mesh_v2" || schema->text == "gpu_femm_mesh_v3" ||
+      schema->text == "gpu_femm_mesh_v4") {
+    *error = "unsupported mesh artifact schema (native air-gap element and sector artifacts are not served "
+             "here)";
     return false;
   }
-  if (!HasExactly(root, {"schema_version", "source_fem_sha256", "canonical_identity_sha256", "resolved"}, error))
+  if (!neutral && !motor) {
+    *error = "unsupported mesh artifact schema";
     return false;
+  }
+  if (!(neutral ? HasExactly(root, {"schema_version", "source_fem_sha256", "canonical_identity_sha256", "resolved"},
+                             error)
+                : HasExactly(root, {"schema_version", "base_motor_fem_sha256", "source_fem_sha256",
+                                    "canonical_identity_sha256", "resolved"},
+                             error)))
+    return false;
+  // Neutral schemas bind lower-case digests and the canonical identity; the motor schema
+  // accepts any-case digests and carries no identity check (mesh_artifact.cpp:42-85).
+  const bool lower = neutral;
   const Json *source = root.get("source_fem_sha256", K::String, error);
+  const Json *root_base = neutral ? source : root.get("base_motor_fem_sha256", K::String, error);
   const Json *identity = root.get("canonical_identity_sha256", K::String, error);
   const Json *res = root.get("resolved", K::Object, error);
   const bool header_ok =
-      source && identity && res && IsSha256Hex(source->text) && IsSha256Hex(identity->text) &&
+      source && root_base && identity && res && IsSha256Hex(root_base->text, lower) &&
+      IsSha256Hex(source->text, lower) && IsSha256Hex(identity->text, lower) &&
       (generic ? HasExactly(*res, {"source_fem_sha256", "model", "nodes_mm", "triangles", "regions",
                                    "materials", "circuits", "outer_dirichlet", "node_constraints"}, error)
-               : HasExactly(*res, {"source_fem_sha256", "model", "nodes_mm", "triangles", "regions",
-                                   "materials", "circuits", "outer_dirichlet"}, error));
+               : planar_dc ? HasExactly(*res, {"source_fem_sha256", "model", "nodes_mm", "triangles", "regions",
+                                               "materials", "circuits", "outer_dirichlet"}, error)
+                           : HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
+                                               "nodes_mm", "triangles", "regions", "materials", "circuits",
+                                               "outer_dirichlet"}, error));
   if (!header_ok) {
     if (error->empty())
       *error = "invalid GPU FEMM mesh artifact header";
     return false;
   }
-  if (Sha256Hex(Canonical(*res)) != identity->text) {
+  if (neutral && Sha256Hex(Canonical(*res)) != identity->text) {
     *error = "canonical artifact identity mismatch";
     return false;
   }
   const Json *rsource = res->get("source_fem_sha256", K::String, error);
+  const Json *rbase = neutral ? rsource : res->get("base_motor_fem_sha256", K::String, error);
   const Json *model = res->get("model", K::Object, error);
+  const Json *pose = neutral ? nullptr : res->get("pose", K::Object, error);
   const Json *nodes = res->get("nodes_mm", K::Array, error);
   const Json *triangles = res->get("triangles", K::Object, error);
   const Json *regions = res->get("regions", K::Array, error);
@@ -92,8 +114,9 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const Json *circuits = res->get("circuits", K::Array, error);
   const Json *boundary = res->get("outer_dirichlet", K::Object, error);
   const Json *constraints = generic ? res->get("node_constraints", K::Array, error) : nullptr;
-  if (!rsource || !model || !nodes || !triangles || !regions || !materials || !circuits || !boundary ||
-      (generic && !constraints) || !IsSha256Hex(rsource->text) || rsource->text != source->text) {
+  if (!rsource || !rbase || !model || (!neutral && !pose) || !nodes || !triangles || !regions || !materials ||
+      !circuits || !boundary || (generic && !constraints) || !IsSha256Hex(rsource->text, lower) ||
+      !IsSha256Hex(rbase->text, lower) || rsource->text != source->text || rbase->text != root_base->text) {
     if (error->empty())
       *error = "source FEM SHA mismatch";
     return false;
@@ -105,10 +128,22 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const Json *freq = model->get("frequency_hz", K::Number, error);
   const bool planar = type && type->text == "planar";
   const bool axi = type && type->text == "axisymmetric";
-  if (!depth || !type || !freq || !(depth->number > 0.0) || freq->number != 0.0 ||
-      (planar_dc && !planar) || (generic && !planar && !axi)) {
+  if (!depth || !type || !freq || !(depth->number > 0.0) || freq->number != 0.0 || (!generic && !planar) ||
+      (generic && !planar && !axi)) {
     *error = "unsupported model physics";
     return false;
+  }
+  const Json *rotor = nullptr, *displacement = nullptr;
+  if (!neutral) {
+    if (!HasExactly(*pose, {"rotor_angle_deg", "displacement_mm"}, error))
+      return false;
+    rotor = pose->get("rotor_angle_deg", K::Number, error);
+    displacement = pose->get("displacement_mm", K::Array, error);
+    if (!rotor || !displacement || displacement->items.size() != 2 || !displacement->items[0].is(K::Number) ||
+        !displacement->items[1].is(K::Number)) {
+      *error = "invalid pose";
+      return false;
+    }
   }
   if (nodes->items.size() < 3 || materials->items.empty() || regions->items.empty()) {
     *error = "empty mesh/material input";
@@ -116,6 +151,11 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   }
   Artifact a;
   a.schema_version = schema->text;
+  a.motor = motor;
+  a.base_motor_fem_sha256 = root_base->text;
+  a.rotor_angle_deg = motor ? rotor->number : 0.0;
+  a.displacement_mm[0] = motor ? displacement->items[0].number : 0.0;
+  a.displacement_mm[1] = motor ? displacement->items[1].number : 0.0;
   a.source_fem_sha256 = source->text;
   a.canonical_identity_sha256 = identity->text;
   a.problem_type = axi ? FG_AXISYMMETRIC : FG_PLANAR;

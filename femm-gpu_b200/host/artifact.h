@@ -13,6 +13,10 @@ namespace fgio
 // A parsed artifact owning every array an fg_model points at.
 struct Artifact {
   std::string schema_version, source_fem_sha256, canonical_identity_sha256;
+  // Motor schema (gpu_femm_mesh_v1): the base motor identity and the mesh's pose.
+  bool motor = false;
+  std::string base_motor_fem_sha256;
+  double rotor_angle_deg = 0.0, displacement_mm[2] = {0.0, 0.0};
   int32_t problem_type = FG_PLANAR;
   double depth_m = 0.0;
   std::vector<double> xy;
@@ -32,10 +36,11 @@ struct Artifact {
 };
 
 // ParseGpuFemmMeshArtifactJson (gpu_solver/src/io/mesh_artifact.cpp:14-715) for the two
-// neutral schemas: the same acceptance rules and the same mapping -- millimetres to metres,
-// nu0 = 1 / (mu0 mu_x), one label material per region appended after the base materials
-// (group, circuit, magnet angle, J = turns / region area), zero outer Dirichlet values,
-// signed node constraints.  Motor schemas (gpu_femm_mesh_v1..v4) are refused.
+// neutral schemas and the conforming posed motor schema gpu_femm_mesh_v1: the same
+// acceptance rules and the same mapping -- millimetres to metres, nu0 = 1 / (mu0 mu_x), one
+// label material per region appended after the base materials (group, circuit, magnet
+// angle, J = turns / region area), zero outer Dirichlet values, signed node constraints.
+// The native air-gap element and sector schemas (gpu_femm_mesh_v2..v4) are refused.
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error);
 
 } // namespace fgio

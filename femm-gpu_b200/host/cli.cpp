@@ -3,7 +3,9 @@
 //   femm_gpu [options] --solve REQUEST.json RESPONSE.json
 //   femm_gpu [options] --batch BATCH.json RESPONSE.json
 //   femm_gpu [options] --single-sample REQUEST.json RESPONSE.json
-//   femm_gpu [options] --worker        (job envelopes on stdin, one status line per job)
+//   femm_gpu [options] --worker        (job envelopes on stdin, one status line per job; also --motor-worker)
+//   femm_gpu [options] --motor-single-sample REQUEST.json RESPONSE.json
+//   femm_gpu [options] --motor-batch[-profile] BATCH.json RESPONSE.json
 //   femm_gpu --capabilities
 //   femm_gpu --describe-artifact ARTIFACT.json   (parsed model and plan sizes, as JSON)
 //   femm_gpu --sha256 FILE                        (the file-bytes SHA-256 a request names)
@@ -35,6 +37,7 @@
 // Exit codes: 0 every response PASS, 1 a FAIL response or an I/O failure, 2 usage error.
 #include "artifact.h"
 #include "cli_common.h"
+#include "motor.h"
 #include "femm_ans.h"
 #include "femm_gpu.h"
 #include "json.h"
@@ -168,36 +171,10 @@ bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
 int SolveItems(Prepared &p, const std::vector<const SampleRequest *> &reqs, std::vector<Solved> *out,
                std::vector<int> *statuses, int *launches)
 {
-  const fg_model m = p.artifact.Model();
-  const size_t k = reqs.size(), N = m.node_count, E = m.triangle_count, C = m.circuit_count;
-  std::vector<double> cur(k * C), a(k * N), b1(k * E), b2(k * E), flux(k * (C ? C : 1));
-  for (size_t i = 0; i < k; ++i)
-    for (size_t c = 0; c < C; ++c)
-      cur[i * C + c] = reqs[i]->circuit_currents_a[c];
-  std::vector<fg_item_info> info(k);
-  fg_solve_options o;
-  fg_production_options(&o);
-  const int rc = fg_solve_batch(p.plan, static_cast<int32_t>(k), cur.data(), nullptr, nullptr, &o, a.data(),
-                                b1.data(), b2.data(), flux.data(), info.data());
-  fg_timing t{};
-  fg_plan_last_timing(p.plan, &t);
-  *launches += static_cast<int>(t.pcg_launches);
-  out->assign(k, Solved{});
-  statuses->assign(k, rc);
-  if (rc != 0)
-    return rc;
-  for (size_t i = 0; i < k; ++i) {
-    Solved &s = (*out)[i];
-    s.currents.assign(cur.begin() + i * C, cur.begin() + (i + 1) * C);
-    s.flux.assign(flux.begin() + i * C, flux.begin() + i * C + C);
-    s.a.assign(a.begin() + i * N, a.begin() + (i + 1) * N);
-    s.b1.assign(b1.begin() + i * E, b1.begin() + (i + 1) * E);
-    s.b2.assign(b2.begin() + i * E, b2.begin() + (i + 1) * E);
-    s.iterations = info[i].iterations;
-    s.residual = info[i].residual_l2;
-    (*statuses)[i] = info[i].status;
-  }
-  return 0;
+  std::vector<const std::vector<double> *> currents;
+  for (const SampleRequest *r : reqs)
+    currents.push_back(&r->circuit_currents_a);
+  return SolveCurrents(p, currents, out, statuses, launches);
 }
 
 int Solve(const std::string &request_path, const std::string &response_path, const Options &opt)
@@ -431,6 +408,8 @@ struct WorkerJob {
   std::string session, request_path, response_path, request_sha256, error;
   int32_t sequence = 0;
   fgio::BatchRequest batch;
+  bool motor = false; // a gpu_femm_motor_batch_v* transaction
+  fgio::MotorBatchRequest motor_batch;
   ArtifactCache staged; // artifacts read for this job that the resident set lacks or must replace
   double prepare_seconds = 0.0;
   std::chrono::steady_clock::time_point prepare_begin, prepare_end;
@@ -476,17 +455,34 @@ std::unique_ptr<WorkerJob> PrepareWorkerJob(const std::string &line, const std::
     std::string bytes;
     if (!ReadFile(job->request_path, &bytes) || fgio::Sha256Hex(bytes) != job->request_sha256)
       throw std::runtime_error("stream request SHA-256 mismatch");
-    if (!fgio::ParseBatchRequestText(bytes, &job->batch, &error))
+    {
+      // Motor transactions name a gpu_femm_motor_batch_v* protocol; the rest take the neutral reader.
+      fgio::Json probe;
+      std::string ignored;
+      if (fgio::ParseJson(bytes, &probe, &ignored) && probe.is(fgio::Json::Kind::Object)) {
+        auto it = probe.members.find("protocol");
+        job->motor = it != probe.members.end() && it->second.is(fgio::Json::Kind::String) &&
+                     it->second.text.rfind("gpu_femm_motor_batch_v", 0) == 0;
+      }
+    }
+    if (job->motor ? !fgio::ParseMotorBatchRequestText(bytes, &job->motor_batch, &error)
+                   : !fgio::ParseBatchRequestText(bytes, &job->batch, &error))
       throw std::runtime_error(error);
     // A transaction is bounded independently of the number of submissions.
-    if (job->batch.items.size() > 32)
+    if ((job->motor ? job->motor_batch.items.size() : job->batch.items.size()) > 32)
       throw std::runtime_error("stream transaction exceeds 32 items");
     std::vector<ArtifactKey> keys;
-    for (const fgio::BatchItem &item : job->batch.items) {
-      const ArtifactKey key{item.request.mesh_artifact_path, item.request.mesh_artifact_sha256};
+    auto add_key = [&](const std::string &path, const std::string &sha) {
+      const ArtifactKey key{path, sha};
       if (std::find(keys.begin(), keys.end(), key) == keys.end())
         keys.push_back(key);
-    }
+    };
+    if (job->motor)
+      for (const fgio::MotorBatchItem &item : job->motor_batch.items)
+        add_key(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
+    else
+      for (const fgio::BatchItem &item : job->batch.items)
+        add_key(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
     for (const ArtifactKey &key : keys)
       if (SameFile(job->response_path, key.first))
         throw std::runtime_error("stream response would overwrite an artifact");
@@ -563,8 +559,14 @@ int RunWorkerJob(WorkerJob *job, const Options &opt, WorkerArtifacts *resident)
       resident->map[kv.first] = kv.second;
       resident->keys.insert(kv.first);
     }
-    for (const fgio::BatchItem &item : job->batch.items) {
-      const ArtifactKey key{item.request.mesh_artifact_path, item.request.mesh_artifact_sha256};
+    std::vector<ArtifactKey> keys;
+    if (job->motor)
+      for (const fgio::MotorBatchItem &item : job->motor_batch.items)
+        keys.emplace_back(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
+    else
+      for (const fgio::BatchItem &item : job->batch.items)
+        keys.emplace_back(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
+    for (const ArtifactKey &key : keys) {
       if (view.count(key))
         continue;
       auto it = resident->map.find(key);
@@ -584,7 +586,9 @@ int RunWorkerJob(WorkerJob *job, const Options &opt, WorkerArtifacts *resident)
     }
   }
   bool pass = false;
-  const std::string text = RunBatch(job->batch, opt, &view, job->prepare_begin, &pass);
+  // Motor transactions carry the reference worker's timing block.
+  const std::string text = job->motor ? RunMotorBatch(job->motor_batch, opt, &view, true, job->prepare_begin, &pass)
+                                      : RunBatch(job->batch, opt, &view, job->prepare_begin, &pass);
   if (!PublishAtomically(job->response_path, text)) {
     job->error = "could not atomically publish response";
     return 1;
@@ -698,6 +702,19 @@ std::string SingleSampleResponse(int status, const fgio::SingleSampleRequest *re
 int SingleSample(const std::string &request_path, const std::string &response_path, const Options &opt)
 {
   std::string text, error;
+  // A strict-JSON gpu_femm_motor_sample_v1 request goes to the motor adapter
+  // (SingleSampleAdapter, reference_adapter.cu:63-78).
+  {
+    fgio::Json root;
+    std::string ignored;
+    if (ReadFile(request_path, &text) && fgio::ParseJson(text, &root, &ignored) && root.is(fgio::Json::Kind::Object)) {
+      auto it = root.members.find("protocol");
+      if (it != root.members.end() && it->second.is(fgio::Json::Kind::String) &&
+          it->second.text == "gpu_femm_motor_sample_v1")
+        return MotorSingleSample(request_path, response_path, opt);
+    }
+    text.clear();
+  }
   fgio::SingleSampleRequest req;
   if (!ReadFile(request_path, &text) || !fgio::ParseSingleSampleRequestText(text, &req, &error)) {
     if (!PublishAtomically(response_path, SingleSampleResponse(FG_INVALID_ARGUMENT, nullptr, nullptr, nullptr))) {
@@ -866,6 +883,7 @@ int Usage()
   std::cerr << "usage: femm_gpu [--preconditioner jacobi|block-jacobi] [--block-size 8|32] "
                "[--precision fp64|mixed] (--solve request.json response.json | "
                "--batch batch.json response.json | --single-sample request.json response.json | --worker | "
+               "--motor-single-sample request.json response.json | --motor-batch[-profile] batch.json response.json | "
                "--capabilities | --describe-artifact artifact.json)\n";
   return 2;
 }
@@ -908,8 +926,10 @@ int main(int argc, char **argv)
   const int rest = argc - next;
   if (rest == 1 && std::strcmp(argv[next], "--capabilities") == 0) {
     std::cout << "{\n  \"protocols\": [\"gpu_femm_planar_dc_sample_v1\", \"gpu_femm_magnetostatic_sample_v1\", "
-                 "\"gpu_femm_magnetostatic_batch_v1\", \"gpu_femm_single_sample_v1\"],\n"
-              << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\"],\n"
+                 "\"gpu_femm_magnetostatic_batch_v1\", \"gpu_femm_single_sample_v1\", \"gpu_femm_motor_sample_v1\", "
+                 "\"gpu_femm_motor_sample_v2\", \"gpu_femm_motor_batch_v1\", \"gpu_femm_motor_batch_v2\"],\n"
+              << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\", "
+                 "\"gpu_femm_mesh_v1\"],\n"
               << "  \"preconditioners\": [\"jacobi\", \"block-jacobi\"],\n"
               << "  \"precisions\": [\"fp64\", \"mixed\"],\n"
               << "  \"abi_version\": " << fg_abi_version() << "\n}\n";
@@ -932,8 +952,14 @@ int main(int argc, char **argv)
     return Solve(argv[next + 1], argv[next + 2], opt);
   if (rest == 3 && std::strcmp(argv[next], "--batch") == 0)
     return Batch(argv[next + 1], argv[next + 2], opt);
-  if (rest == 1 && std::strcmp(argv[next], "--worker") == 0)
+  if (rest == 1 && (std::strcmp(argv[next], "--worker") == 0 || std::strcmp(argv[next], "--motor-worker") == 0))
     return Worker(opt, argv[0]);
+  if (rest == 3 && std::strcmp(argv[next], "--motor-single-sample") == 0)
+    return MotorSingleSample(argv[next + 1], argv[next + 2], opt);
+  if (rest == 3 && std::strcmp(argv[next], "--motor-batch") == 0)
+    return MotorBatch(argv[next + 1], argv[next + 2], opt, false);
+  if (rest == 3 && std::strcmp(argv[next], "--motor-batch-profile") == 0)
+    return MotorBatch(argv[next + 1], argv[next + 2], opt, true);
   if (rest == 3 && std::strcmp(argv[next], "--single-sample") == 0)
     return SingleSample(argv[next + 1], argv[next + 2], opt);
   return Usage();

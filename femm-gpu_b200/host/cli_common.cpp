@@ -141,4 +141,39 @@ int EnsurePlan(Prepared *p, const Options &opt)
   return rc;
 }
 
+int SolveCurrents(Prepared &p, const std::vector<const std::vector<double> *> &currents, std::vector<Solved> *out,
+                  std::vector<int> *statuses, int *launches)
+{
+  const fg_model m = p.artifact.Model();
+  const size_t k = currents.size(), N = m.node_count, E = m.triangle_count, C = m.circuit_count;
+  std::vector<double> cur(k * C), a(k * N), b1(k * E), b2(k * E), flux(k * (C ? C : 1));
+  for (size_t i = 0; i < k; ++i)
+    for (size_t c = 0; c < C; ++c)
+      cur[i * C + c] = (*currents[i])[c];
+  std::vector<fg_item_info> info(k);
+  fg_solve_options o;
+  fg_production_options(&o);
+  const int rc = fg_solve_batch(p.plan, static_cast<int32_t>(k), cur.data(), nullptr, nullptr, &o, a.data(),
+                                b1.data(), b2.data(), flux.data(), info.data());
+  fg_timing t{};
+  fg_plan_last_timing(p.plan, &t);
+  *launches += static_cast<int>(t.pcg_launches);
+  out->assign(k, Solved{});
+  statuses->assign(k, rc);
+  if (rc != 0)
+    return rc;
+  for (size_t i = 0; i < k; ++i) {
+    Solved &s = (*out)[i];
+    s.currents.assign(cur.begin() + i * C, cur.begin() + (i + 1) * C);
+    s.flux.assign(flux.begin() + i * C, flux.begin() + i * C + C);
+    s.a.assign(a.begin() + i * N, a.begin() + (i + 1) * N);
+    s.b1.assign(b1.begin() + i * E, b1.begin() + (i + 1) * E);
+    s.b2.assign(b2.begin() + i * E, b2.begin() + (i + 1) * E);
+    s.iterations = info[i].iterations;
+    s.residual = info[i].residual_l2;
+    (*statuses)[i] = info[i].status;
+  }
+  return 0;
+}
+
 } // namespace fgcli

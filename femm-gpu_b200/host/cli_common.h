@@ -110,6 +110,11 @@ void PreparePlanOnHost(Prepared *p, const Options &opt);
 // The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
 int EnsurePlan(Prepared *p, const Options &opt);
 
+// Solves k samples (their circuit currents) on a prepared plan with the reference's
+// production options (ProductionSampleOptions); statuses[i] = the item's status.
+int SolveCurrents(Prepared &p, const std::vector<const std::vector<double> *> &currents, std::vector<Solved> *out,
+                  std::vector<int> *statuses, int *launches);
+
 using ArtifactKey = std::pair<std::string, std::string>; // path, SHA-256
 using ArtifactCache = std::map<ArtifactKey, std::shared_ptr<Prepared>>;
 

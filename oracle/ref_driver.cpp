@@ -503,4 +503,16 @@ int ref_tangent_postprocess(const ref_artifact *h, const double *a, const double
   return static_cast<int>(r.status);
 }
 
+// ReadMotorSampleRequestJson (io/sample_request.cpp:212-391) and ReadMotorBatchRequestJson
+// (app/batch_prepare.cpp:73-129) are not compiled here (the batch reader sits in a CUDA
+// translation unit's neighbourhood); the sample reader is: 0 accepted, 1 refused (error).
+int ref_read_motor_sample_request(const char *text, size_t length, char *error)
+{
+  MotorSampleRequest r;
+  std::string e;
+  const bool ok = ReadMotorSampleRequestJson(std::string(text, length), &r, &e);
+  std::snprintf(error, 4096, "%s", e.c_str());
+  return ok ? 0 : 1;
+}
+
 } // extern "C"

@@ -11,6 +11,7 @@ golden vectors for this path, copied byte for byte (gpu_solver/tests/fixtures/..
   nonlinear_pm_coil_single_sample_request.json: FEMM 4.2's own nonlinear PM / coil
   solution with its weighted-stress force / torque and smoothed air-gap B samples
   (the --single-sample fixture)
+* motor_mesh_v1.gpu.json: the reference's posed motor artifact fixture (gpu_femm_mesh_v1)
 
 plus expected.json: the stock-FEMM flux linkages parsed from the summaries.
 """
@@ -37,6 +38,7 @@ FILES = {
     "nonlinear_pm_coil_v1/nonlinear_pm_coil_planar.postprocess.txt":
         "nonlinear_pm_coil_planar.postprocess.txt",
     "nonlinear_pm_coil_v1/single_sample_request.json": "nonlinear_pm_coil_single_sample_request.json",
+    "stream_worker_v1/mesh.json": "motor_mesh_v1.gpu.json",
 }
 
 
