@@ -749,7 +749,7 @@ int fg_postprocess_compute_device(fg_postprocess *pp, int32_t items, const doubl
       return ToInt(s);
     }
   }
-  const int ctas = fg::PostprocessCtas(E);
+  const int ctas = fg::PostprocessCtas(E, items);
   const size_t partial_count = static_cast<size_t>(ctas) * items * 3;
   const size_t total = partial_count + P * items;
   if ((s = pp->out.ensure(total)) != Status::kOk || (s = pp->host_out.ensure(total)) != Status::kOk)

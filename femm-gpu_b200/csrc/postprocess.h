@@ -78,7 +78,7 @@ struct PostprocessDevice {
   double *partials;          // [ctas][items][3]
   double *radial;            // [items][probes]
 };
-int PostprocessCtas(int32_t E);
+int PostprocessCtas(int32_t E, int32_t items);
 cudaError_t LaunchPostprocess(const PostprocessDevice &p, cudaStream_t stream);
 
 } // namespace fg

@@ -13,9 +13,10 @@ namespace
 {
 
 constexpr int kThreads = 256;
-constexpr int kMaxCtas = 148;
-constexpr int kPerThread = 16; // elements per thread of the force reduction
-constexpr double kTwoMu0 = 2.0 * 4.0e-7 * 3.141592653589793238462643383279502884;
+constexpr int kSms = 148;
+constexpr int kMaxCtas = 3 * kSms;
+constexpr int kPerThread = 8; // elements per thread of the force reduction, at least
+constexpr double kInvTwoMu0 = 1.0 / (2.0 * 4.0e-7 * 3.141592653589793238462643383279502884);
 
 // Sum over the block in a fixed order: warp trees, then warp 0 over the warp totals.
 __device__ double BlockSum(double v, double *scratch)
@@ -100,10 +101,12 @@ __device__ void Corner(const PostprocessDevice &p, const CornerStencil &c, const
 }
 
 // Force / torque partial sums: CTA (blockIdx.x, item blockIdx.y) over a contiguous element
-// range of kPerThread elements per thread.
-__global__ void __launch_bounds__(kThreads) ForceKernel(PostprocessDevice p)
+// range.  Each thread takes its elements three at a time and issues all 21 loads of a group
+// before using any, so that a warp keeps enough bytes in flight to cover the HBM latency.
+__global__ void __launch_bounds__(kThreads, 3) ForceKernel(PostprocessDevice p)
 {
   __shared__ double scratch[kThreads / 32];
+  constexpr int G = 3;
   const int item = blockIdx.y;
   const int64_t chunk = (static_cast<int64_t>(p.E) + p.ctas - 1) / p.ctas;
   const int64_t first = chunk * blockIdx.x;
@@ -111,16 +114,28 @@ __global__ void __launch_bounds__(kThreads) ForceKernel(PostprocessDevice p)
   const double *b1 = p.b1 + static_cast<int64_t>(item) * p.E;
   const double *b2 = p.b2 + static_cast<int64_t>(item) * p.E;
   double fx = 0.0, fy = 0.0, tq = 0.0;
-#pragma unroll 4
-  for (int64_t e = first + threadIdx.x; e < last; e += kThreads) {
-    const double hx = p.hx[e], hy = p.hy[e];
-    const double bx = __ldcs(b1 + e), by = __ldcs(b2 + e);
-    const double fxd = ((bx * bx - by * by) * hx + 2.0 * bx * by * hy) / kTwoMu0;
-    const double fyd = (2.0 * bx * by * hx + (by * by - bx * bx) * hy) / kTwoMu0;
-    const double w = p.weight[e];
-    fx += w * fxd;
-    fy += w * fyd;
-    tq += w * (p.cx[e] * fyd - p.cy[e] * fxd);
+  for (int64_t base = first + threadIdx.x; base < last; base += G * kThreads) {
+    double hx[G], hy[G], w[G], cx[G], cy[G], bx[G], by[G];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int64_t e = base + g * kThreads;
+      const bool in = e < last;
+      hx[g] = in ? p.hx[e] : 0.0;
+      hy[g] = in ? p.hy[e] : 0.0;
+      w[g] = in ? p.weight[e] : 0.0;
+      cx[g] = in ? p.cx[e] : 0.0;
+      cy[g] = in ? p.cy[e] : 0.0;
+      bx[g] = in ? __ldcs(b1 + e) : 0.0;
+      by[g] = in ? __ldcs(b2 + e) : 0.0;
+    }
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const double fxd = ((bx[g] * bx[g] - by[g] * by[g]) * hx[g] + 2.0 * bx[g] * by[g] * hy[g]) * kInvTwoMu0;
+      const double fyd = (2.0 * bx[g] * by[g] * hx[g] + (by[g] * by[g] - bx[g] * bx[g]) * hy[g]) * kInvTwoMu0;
+      fx += w[g] * fxd;
+      fy += w[g] * fyd;
+      tq += w[g] * (cx[g] * fyd - cy[g] * fxd);
+    }
   }
   fx = BlockSum(fx, scratch);
   fy = BlockSum(fy, scratch);
@@ -170,9 +185,13 @@ __global__ void __launch_bounds__(kThreads) ProbeKernel(PostprocessDevice p)
 
 } // namespace
 
-int PostprocessCtas(int32_t E)
+int PostprocessCtas(int32_t E, int32_t items)
 {
-  const int64_t want = (static_cast<int64_t>(E) + kPerThread * kThreads - 1) / (kPerThread * kThreads);
+  // One wave: at most three resident CTAs per SM over all (range, item) CTAs, and at least
+  // kPerThread elements per thread.
+  const int64_t by_size = (static_cast<int64_t>(E) + kPerThread * kThreads - 1) / (kPerThread * kThreads);
+  const int64_t by_wave = (3 * kSms) / (items > 0 ? items : 1);
+  int64_t want = by_size > by_wave ? by_wave : by_size;
   return static_cast<int>(want < 1 ? 1 : (want > kMaxCtas ? kMaxCtas : want));
 }
 
