@@ -297,3 +297,89 @@ def annular_sector(nr: int = 160, nt: int = 250, hc: float = 9.0e5, turns: float
         circuit_count=3, depth_m=0.05, problem_type=PLANAR,
         name=f"annular_sector_{nr}x{nt}",
     )
+
+
+def two_pole_machine(nr: int = 40, nt: int = 120, full: bool = False, hc: float = 9.0e5,
+                     turns: float = 20.0) -> Model:
+    """A two-pole surface-magnet machine, as the 180-degree sector [0, 180] degrees with
+    antiperiodic edges (``full=False``) or the full 360-degree annulus (``full=True``, the
+    sector and its 180-degree rotation, equal node numbering on the shared edges).
+
+    r in [0.02, 0.06] m: rotor iron to 0.043 on the saturating B-H table, a 2 mm magnet
+    [0.043, 0.045) over the central 120 degrees of the pole magnetised along +y (mu_r 1.05,
+    Hc = ``hc``; the other pole's magnet points along +y too, an antiperiodic field), a 1 mm
+    air gap, a stator with three 20-degree slots [0.046, 0.050) at 30, 90 and 150 degrees
+    (circuits 0, 1, 2, ``turns`` turns each; the rotated copies in the full machine belong to
+    the same circuits wound the other way).  Groups: air 50, rotor iron and magnets 20,
+    stator 30, slots 40-42.  A = 0 on the outer radius."""
+    r0, r1 = 0.02, 0.06
+    span = 2.0 * np.pi if full else np.pi
+    ntt = 2 * nt if full else nt
+    rs = np.linspace(r0, r1, nr + 1)
+    ts = np.linspace(0.0, span, ntt + 1)
+    if full:
+        ts = ts[:-1]  # the 360-degree seam closes on the first column
+    cols = ts.size
+    T, R = np.meshgrid(ts, rs)
+    xy = np.stack([(R * np.cos(T)).ravel(), (R * np.sin(T)).ravel()], axis=1)
+    if not full:
+        xy[np.arange(nr + 1) * cols + (cols - 1), 1] = 0.0  # the 180-degree edge on y = 0 exactly
+    else:
+        # (-x, -y) partners exactly: the second half is the rotation of the first.
+        half = nt
+        for i in range(nr + 1):
+            for j in range(half, cols):
+                k, m = i * cols + j, i * cols + (j - half)
+                xy[k] = -xy[m]
+    i, j = np.meshgrid(np.arange(nr), np.arange(ntt), indexing="ij")
+    jn = (j + 1) % cols if full else j + 1
+    a = (i * cols + j).ravel()
+    b = (i * cols + jn).ravel()
+    c = ((i + 1) * cols + j).ravel()
+    d = ((i + 1) * cols + jn).ravel()
+    tri = np.empty((2 * a.size, 3), dtype=np.int64)
+    tri[0::2] = np.stack([a, c, d], axis=1)
+    tri[1::2] = np.stack([a, d, b], axis=1)
+    tri = tri.astype(np.int32)
+    cen = xy[tri].mean(axis=1)
+    rc = np.hypot(cen[:, 0], cen[:, 1])
+    tc = np.degrees(np.arctan2(cen[:, 1], cen[:, 0])) % 360.0
+    upper = tc < 180.0
+    tl = np.where(upper, tc, tc - 180.0)  # angle within its half
+    mat = np.zeros(tri.shape[0], np.int32)  # 0 air
+    mat[rc < 0.043] = 1
+    mat[(rc >= 0.043) & (rc < 0.045) & (np.abs(tl - 90.0) <= 60.0)] = 2
+    stator = rc >= 0.046
+    mat[stator] = 3
+    for k, centre in enumerate((30.0, 90.0, 150.0)):
+        slot = stator & (rc < 0.050) & (np.abs(tl - centre) <= 10.0)
+        mat[slot & upper] = 4 + k
+        mat[slot & ~upper] = 7 + k
+    area = 0.5 * _signed_area2(xy, tri)
+    jpa = [turns / area[mat == 4 + k].sum() for k in range(3)]
+    nu_air = 1.0 / MU0
+    b_t, h = bh_table_saturating(24)
+    idx = np.arange(xy.shape[0])
+    ii, jj = idx // cols, idx % cols
+    outer = idx[ii == nr].astype(np.int32)
+    left = idx[(jj == 0) & (ii < nr)]
+    right = idx[(jj == cols - 1) & (ii < nr)]
+    M = 10 if full else 7  # the sector has no rotated slot copies
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=([nu_air, nu_air, nu_air / 1.05, nu_air] + [nu_air] * 6)[:M],
+        alpha=np.zeros(M),
+        j_per_a=([0.0, 0.0, 0.0, 0.0] + jpa + [-v for v in jpa])[:M],
+        hc=([0.0, 0.0, hc] + [0.0] * 7)[:M],
+        mag_deg=([0.0, 0.0, 90.0] + [0.0] * 7)[:M],
+        curve_index=([-1, 0, -1, 0] + [-1] * 6)[:M],
+        circuit_index=[-1, -1, -1, -1, 0, 1, 2, 0, 1, 2][:M],
+        group=[50, 20, 20, 30, 40, 41, 42, 40, 41, 42][:M],
+        curves=[(b_t, h)],
+        dir_nodes=outer,
+        dir_values=np.zeros(outer.size),
+        con_a=np.zeros(0, np.int32) if full else left, con_b=np.zeros(0, np.int32) if full else right,
+        con_sign=np.zeros(0, np.int8) if full else np.full(left.size, -1, np.int8),
+        circuit_count=3, depth_m=0.05, problem_type=PLANAR,
+        name=f"two_pole_{'full' if full else 'sector'}_{nr}x{nt}",
+    )

@@ -1,7 +1,9 @@
 // artifact.cpp -- neutral mesh artifact parser (see artifact.h).
 #include "artifact.h"
 
+#include <algorithm>
 #include <cmath>
+#include <limits>
 #include <map>
 
 namespace fgio
@@ -49,6 +51,123 @@ fg_model Artifact::Model()
   return m;
 }
 
+// The 180-degree sector metadata of gpu_femm_mesh_v3 (mesh_artifact.cpp:441-608): p pole
+// pairs, the p + 1 suspension order, the boundary relation of the pole-pair parity, every
+// constraint pair related by an exact 180-degree rotation and carrying that relation,
+// apex self-pairs at the origin, a circuit partner map that closes after two copies with
+// positive orientation.  An antiperiodic sector fixes its apex nodes to zero.
+bool ParseSector(const Json &sec, Artifact *a, std::string *error)
+{
+  if (!HasExactly(sec, {"schema_version", "sector_start_angle_deg", "angle_deg", "full_machine_sector_count",
+                        "electrical_pole_pairs", "suspension_spatial_order", "boundary_relation",
+                        "circuit_partner_indices", "circuit_partner_orientations", "apex_self_pair_nodes",
+                        "model_invariance_certificate_sha256"},
+                  error))
+    return false;
+  const Json *schema = sec.get("schema_version", K::String, error);
+  const Json *start = sec.get("sector_start_angle_deg", K::Number, error);
+  const Json *angle = sec.get("angle_deg", K::Number, error);
+  const Json *repeats = sec.get("full_machine_sector_count", K::Number, error);
+  const Json *pole_pairs = sec.get("electrical_pole_pairs", K::Number, error);
+  const Json *order = sec.get("suspension_spatial_order", K::Number, error);
+  const Json *relation = sec.get("boundary_relation", K::String, error);
+  const Json *partners = sec.get("circuit_partner_indices", K::Array, error);
+  const Json *orientations = sec.get("circuit_partner_orientations", K::Array, error);
+  const Json *apex = sec.get("apex_self_pair_nodes", K::Array, error);
+  const Json *cert = sec.get("model_invariance_certificate_sha256", K::String, error);
+  int32_t k = 0, p = 0, n = 0;
+  const size_t C = a->circuit_currents.size();
+  if (!schema || !start || !std::isfinite(start->number) || !angle || !repeats || !pole_pairs || !order ||
+      !relation || !partners || !orientations || !apex || !cert || !IsSha256Hex(cert->text) ||
+      schema->text != "gpu_femm_motor_sector_v1" || !(angle->number > 0.0) || !AsInt32(*repeats, &k) || k < 2 ||
+      !AsInt32(*pole_pairs, &p) || p <= 0 || !AsInt32(*order, &n) || n != p + 1 ||
+      (relation->text != "periodic" && relation->text != "antiperiodic") || partners->items.size() != C ||
+      orientations->items.size() != C) {
+    *error = "motor sector requires positive k, p and p+1 harmonic metadata";
+    return false;
+  }
+  if (angle->number != 180.0 || k != 2) {
+    *error = "motor sector angle/count are inconsistent";
+    return false;
+  }
+  a->sector = true;
+  a->sector_start_angle_deg = start->number;
+  a->sector_angle_deg = angle->number;
+  a->full_machine_sector_count = k;
+  a->electrical_pole_pairs = p;
+  a->suspension_spatial_order = n;
+  a->sector_boundary_sign = relation->text == "periodic" ? 1 : -1;
+  a->model_invariance_certificate_sha256 = cert->text;
+  const size_t N = a->xy.size() / 2;
+  double radius = 1e-3;
+  for (size_t i = 0; i < N; ++i)
+    radius = std::max(radius, std::hypot(a->xy[2 * i], a->xy[2 * i + 1]));
+  const double tol = std::max(1e-10 * radius, 64.0 * std::numeric_limits<double>::epsilon() * radius);
+  for (size_t c = 0; c < a->con_signs.size(); ++c) {
+    const double *pa = &a->xy[2 * a->con_nodes[2 * c]], *pb = &a->xy[2 * a->con_nodes[2 * c + 1]];
+    if (std::hypot(pa[0] + pb[0], pa[1] + pb[1]) > tol) {
+      *error = "motor sector non-self constraint nodes must be related by an exact 180-degree rotation";
+      return false;
+    }
+  }
+  std::vector<bool> seen(N, false);
+  for (const Json &x : apex->items) {
+    int32_t node = -1;
+    bool bad = !AsInt32(x, &node) || node < 0 || static_cast<size_t>(node) >= N;
+    bad = bad || seen[node] || std::hypot(a->xy[2 * node], a->xy[2 * node + 1]) > tol;
+    for (size_t c = 0; !bad && c < a->con_nodes.size(); ++c)
+      bad = a->con_nodes[c] == node;
+    bad = bad || std::find(a->dir_nodes.begin(), a->dir_nodes.end(), node) != a->dir_nodes.end();
+    if (bad) {
+      *error = "motor sector apex self-pair nodes must be unique origin nodes separate from physical boundaries "
+               "and non-self constraints";
+      return false;
+    }
+    seen[node] = true;
+    a->apex_nodes.push_back(node);
+  }
+  std::vector<bool> used(C, false);
+  for (size_t c = 0; c < C; ++c) {
+    int32_t partner = -1, orientation = 0;
+    if (!AsInt32(partners->items[c], &partner) || !AsInt32(orientations->items[c], &orientation) || partner < 0 ||
+        static_cast<size_t>(partner) >= C || used[partner] || (orientation != -1 && orientation != 1)) {
+      *error = "invalid motor sector circuit partner mapping";
+      return false;
+    }
+    used[partner] = true;
+    a->circuit_partners.push_back(partner);
+    a->circuit_orientations.push_back(static_cast<int8_t>(orientation));
+  }
+  for (size_t c = 0; c < C; ++c) {
+    int32_t at = static_cast<int32_t>(c);
+    int sign = 1;
+    for (int32_t copy = 0; copy < k; ++copy) {
+      sign *= a->circuit_orientations[at];
+      at = a->circuit_partners[at];
+    }
+    if (at != static_cast<int32_t>(c) || sign != 1) {
+      *error = "motor sector circuit generator must close after k copies with positive orientation";
+      return false;
+    }
+  }
+  if (a->con_signs.empty() ||
+      !std::all_of(a->con_signs.begin(), a->con_signs.end(), [&](int8_t s) { return s == a->sector_boundary_sign; })) {
+    *error = "motor sector node constraints do not match boundary_relation";
+    return false;
+  }
+  const int base_sign = p % 2 == 0 ? 1 : -1;
+  if (a->sector_boundary_sign != base_sign) {
+    *error = "motor sector boundary_relation does not match electrical pole-pair parity";
+    return false;
+  }
+  if (base_sign < 0)
+    for (int32_t node : a->apex_nodes) {
+      a->dir_nodes.push_back(node);
+      a->dir_values.push_back(0.0);
+    }
+  return true;
+}
+
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
 {
   Json root;
@@ -60,11 +179,11 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const bool planar_dc = schema->text == "gpu_femm_planar_dc_mesh_v1";
   const bool generic = schema->text == "gpu_femm_magnetostatic_mesh_v1";
   const bool neutral = planar_dc || generic;
-  const bool motor = schema->text == "gpu_femm_mesh_v1";
-  if (schema->text == "gpu_femm_mesh_v2" || schema->text == "gpu_femm_mesh_v3" ||
-      schema->text == "gpu_femm_mesh_v4") {
-    *error = "unsupported mesh artifact schema (native air-gap element and sector artifacts are not served "
-             "here)";
+  const bool motor_v1 = schema->text == "gpu_femm_mesh_v1";
+  const bool sector = schema->text == "gpu_femm_mesh_v3";
+  const bool motor = motor_v1 || sector;
+  if (schema->text == "gpu_femm_mesh_v2" || schema->text == "gpu_femm_mesh_v4") {
+    *error = "unsupported mesh artifact schema (native air-gap element artifacts are not served here)";
     return false;
   }
   if (!neutral && !motor) {
@@ -91,9 +210,13 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
                                    "materials", "circuits", "outer_dirichlet", "node_constraints"}, error)
                : planar_dc ? HasExactly(*res, {"source_fem_sha256", "model", "nodes_mm", "triangles", "regions",
                                                "materials", "circuits", "outer_dirichlet"}, error)
-                           : HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
-                                               "nodes_mm", "triangles", "regions", "materials", "circuits",
-                                               "outer_dirichlet"}, error));
+               : motor_v1 ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
+                                              "nodes_mm", "triangles", "regions", "materials", "circuits",
+                                              "outer_dirichlet"}, error)
+                          : HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
+                                              "nodes_mm", "triangles", "regions", "materials", "circuits",
+                                              "outer_dirichlet", "air_gap_elements", "node_constraints",
+                                              "sector"}, error));
   if (!header_ok) {
     if (error->empty())
       *error = "invalid GPU FEMM mesh artifact header";
@@ -113,9 +236,11 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const Json *materials = res->get("materials", K::Array, error);
   const Json *circuits = res->get("circuits", K::Array, error);
   const Json *boundary = res->get("outer_dirichlet", K::Object, error);
-  const Json *constraints = generic ? res->get("node_constraints", K::Array, error) : nullptr;
+  const Json *constraints = (generic || sector) ? res->get("node_constraints", K::Array, error) : nullptr;
+  const Json *sector_meta = sector ? res->get("sector", K::Object, error) : nullptr;
   if (!rsource || !rbase || !model || (!neutral && !pose) || !nodes || !triangles || !regions || !materials ||
-      !circuits || !boundary || (generic && !constraints) || !IsSha256Hex(rsource->text, lower) ||
+      !circuits || !boundary || ((generic || sector) && !constraints) || (sector && !sector_meta) ||
+      !IsSha256Hex(rsource->text, lower) ||
       !IsSha256Hex(rbase->text, lower) || rsource->text != source->text || rbase->text != root_base->text) {
     if (error->empty())
       *error = "source FEM SHA mismatch";
@@ -148,6 +273,14 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   if (nodes->items.size() < 3 || materials->items.empty() || regions->items.empty()) {
     *error = "empty mesh/material input";
     return false;
+  }
+  if (sector) {
+    // gpu_femm_mesh_v3 is a conforming posed sector: its air-gap element list must be empty.
+    const auto ages = res->members.find("air_gap_elements");
+    if (ages == res->members.end() || !ages->second.is(K::Array) || !ages->second.items.empty()) {
+      *error = "gpu_femm_mesh_v3 requires a conforming posed sector mesh; native AGE sectors are not supported";
+      return false;
+    }
   }
   Artifact a;
   a.schema_version = schema->text;
@@ -339,7 +472,7 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
     a.dir_nodes.push_back(node);
     a.dir_values.push_back(0.0);
   }
-  if (generic) {
+  if (generic || sector) {
     for (const Json &c : constraints->items) {
       if (!HasExactly(c, {"node_a", "node_b", "relation"}, error))
         return false;
@@ -358,6 +491,8 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
       a.con_signs.push_back(rel->text == "periodic" ? 1 : -1);
     }
   }
+  if (sector && !ParseSector(*sector_meta, &a, error))
+    return false;
   *out = std::move(a);
   return true;
 }

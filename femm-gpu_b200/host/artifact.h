@@ -17,6 +17,15 @@ struct Artifact {
   bool motor = false;
   std::string base_motor_fem_sha256;
   double rotor_angle_deg = 0.0, displacement_mm[2] = {0.0, 0.0};
+  // gpu_femm_mesh_v3: a conforming 180-degree sector and how the full machine follows.
+  bool sector = false;
+  double sector_start_angle_deg = 0.0, sector_angle_deg = 0.0;
+  int32_t full_machine_sector_count = 0, electrical_pole_pairs = 0, suspension_spatial_order = 0;
+  int32_t sector_boundary_sign = 1;
+  std::string model_invariance_certificate_sha256;
+  std::vector<int32_t> apex_nodes; // rotational apex self-pairs (origin nodes)
+  std::vector<int32_t> circuit_partners;
+  std::vector<int8_t> circuit_orientations;
   int32_t problem_type = FG_PLANAR;
   double depth_m = 0.0;
   std::vector<double> xy;
@@ -40,7 +49,8 @@ struct Artifact {
 // acceptance rules and the same mapping -- millimetres to metres, nu0 = 1 / (mu0 mu_x), one
 // label material per region appended after the base materials (group, circuit, magnet
 // angle, J = turns / region area), zero outer Dirichlet values, signed node constraints.
-// The native air-gap element and sector schemas (gpu_femm_mesh_v2..v4) are refused.
+// and its conforming 180-degree sector gpu_femm_mesh_v3 (sector metadata, apex self-pairs,
+// circuit partners).  The native air-gap element schemas (gpu_femm_mesh_v2, v4) are refused.
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error);
 
 } // namespace fgio

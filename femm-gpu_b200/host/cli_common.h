@@ -66,15 +66,28 @@ public:
         fg_postprocess_destroy(kv.second.second);
   }
   // Status of the postprocess plan of (selected group, air group, circle); *pp valid when 0.
+  // angles_rad replaces the converted angles (sector probes folded into the representative
+  // sector); apex lists the symmetry apex nodes the mask does not fix.
   int Get(fg_plan *plan, int32_t selected_group, int32_t air_group, double radius_mm,
-          const std::vector<double> &angles_deg, fg_postprocess **pp)
+          const std::vector<double> &angles_deg, fg_postprocess **pp,
+          const std::vector<double> *angles_rad = nullptr, const std::vector<int32_t> *apex = nullptr)
   {
-    std::vector<double> key{static_cast<double>(selected_group), static_cast<double>(air_group), radius_mm};
+    std::vector<double> key{static_cast<double>(selected_group), static_cast<double>(air_group), radius_mm,
+                            angles_rad ? 1.0 : 0.0};
     key.insert(key.end(), angles_deg.begin(), angles_deg.end());
     auto it = cache_.find(key);
     if (it == cache_.end()) {
       std::vector<double> angles;
-      const fg_postprocess_options o = PostOptions(selected_group, air_group, radius_mm, angles_deg, &angles);
+      fg_postprocess_options o = PostOptions(selected_group, air_group, radius_mm, angles_deg, &angles);
+      if (angles_rad) {
+        angles = *angles_rad;
+        o.airgap_angles_rad = angles.data();
+        o.airgap_angle_count = static_cast<int32_t>(angles.size());
+      }
+      if (apex && !apex->empty()) {
+        o.symmetry_apex_count = static_cast<int32_t>(apex->size());
+        o.symmetry_apex_nodes = apex->data();
+      }
       fg_postprocess *p = nullptr;
       const int rc = fg_postprocess_create(plan, &o, nullptr, &p);
       it = cache_.emplace(key, std::make_pair(rc, p)).first;
@@ -96,6 +109,10 @@ struct Prepared {
   int plan_status = -1;   // -1 not attempted, else the fg_plan_create status
   bool host_only = false; // a host-only plan still to be given its device side
   PostCache post;         // postprocess masks of this artifact, per request options
+  // A v3 sector's tangent operator: the same mesh with the suspension order's boundary
+  // relation (MakeMotorSectorTangentModel), built on first use.
+  std::shared_ptr<Prepared> sector_tangent;
+  bool sector_tangent_tried = false;
   ~Prepared()
   {
     if (plan)

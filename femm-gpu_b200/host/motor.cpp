@@ -44,7 +44,84 @@ struct MotorItem {
   size_t elements = 0;
   int tangent_status = FG_OK;
   std::vector<TangentRhs> rhs;
+  // gpu_femm_motor_sample_v3 on a sector: the full-machine reconstruction.
+  bool sector = false;
+  int sector_status = FG_OK;
+  int base_sign = 1, tangent_sign = 1;
+  double base_torque_multiplier = 2.0, tangent_force_multiplier = 0.0, tangent_torque_multiplier = 0.0;
+  size_t evidence_operators = 0, evidence_uploads = 0, evidence_rhs = 0, evidence_operator_bytes = 0,
+         evidence_rhs_bytes = 0;
 };
+
+// MapSectorAirgapAnglesToRepresentative (sample_request.cpp:531-558): probes folded into the
+// half-turn that starts at the sector start; odd copies take the repeat sign.
+std::vector<int> FoldSectorAngles(double start_rad, int repeat_sign, std::vector<double> *angles)
+{
+  std::vector<int> signs;
+  for (double &angle : *angles) {
+    int64_t copy = static_cast<int64_t>(std::floor((angle - start_rad) / kPi));
+    angle -= static_cast<double>(copy) * kPi;
+    const double tol = 64.0 * std::numeric_limits<double>::epsilon() *
+                       std::max({1.0, std::abs(angle), std::abs(start_rad)});
+    if (angle < start_rad - tol) {
+      angle += kPi;
+      --copy;
+    } else if (angle >= start_rad + kPi - tol) {
+      angle -= kPi;
+      ++copy;
+    }
+    if (std::abs(angle - start_rad) <= tol)
+      angle = start_rad;
+    signs.push_back(std::abs(copy) % 2 != 0 ? repeat_sign : 1);
+  }
+  return signs;
+}
+
+// ReconstructSectorCircuitFluxLinkage (batch_response.cpp:20-35): each circuit's flux plus its
+// partner copy's, oriented and signed by the field's repeat relation.
+std::vector<double> ReconstructFlux(const std::vector<double> &sector, const fgio::Artifact &a, int sign)
+{
+  if (sector.size() != a.circuit_partners.size())
+    return {};
+  std::vector<double> full = sector;
+  for (size_t c = 0; c < sector.size(); ++c)
+    full[a.circuit_partners[c]] += static_cast<double>(a.circuit_orientations[c] * sign) * sector[c];
+  return full;
+}
+
+// MakeMotorSectorTangentModel (sample_request.cpp:499-529): the suspension order's boundary
+// relation on every pair; apex nodes fixed to zero only when that relation is antiperiodic.
+int SectorTangentPlan(Prepared &p, const Options &opt)
+{
+  if (p.sector_tangent_tried)
+    return p.sector_tangent ? p.sector_tangent->plan_status : FG_INVALID_ARGUMENT;
+  p.sector_tangent_tried = true;
+  auto t = std::make_shared<Prepared>();
+  t->artifact = p.artifact;
+  fgio::Artifact &a = t->artifact;
+  const int sign = a.suspension_spatial_order % 2 == 0 ? 1 : -1;
+  for (int32_t apex : a.apex_nodes)
+    for (size_t i = 0; i < a.dir_nodes.size();) {
+      if (a.dir_nodes[i] == apex) {
+        a.dir_nodes.erase(a.dir_nodes.begin() + i);
+        a.dir_values.erase(a.dir_values.begin() + i);
+      } else {
+        ++i;
+      }
+    }
+  if (sign < 0)
+    for (int32_t apex : a.apex_nodes) {
+      a.dir_nodes.push_back(apex);
+      a.dir_values.push_back(0.0);
+    }
+  for (int8_t &s : a.con_signs)
+    s = static_cast<int8_t>(sign);
+  const int rc = EnsurePlan(t.get(), opt);
+  if (rc != 0)
+    return FG_INVALID_ARGUMENT; // the tangent model failed validation
+  p.sector_tangent = t;
+  return 0;
+}
 
 template <class V> void Csv(std::ostream &o, const V &v)
 {
@@ -97,8 +174,40 @@ std::string SingleResponse(int status, const MotorSampleRequest *req, const Solv
   return o.str();
 }
 
+// The sector_reconstruction member (batch_response.cpp:164-222), conforming sectors.
+void SectorBlock(std::ostream &o, const MotorItem &d, const fgio::Artifact &a)
+{
+  o << "  \"sector_reconstruction\": {\"schema_version\": \"gpu_femm_motor_sector_reconstruction_response_v1\", "
+    << "\"status\": \"" << (d.sector_status == 0 ? "PASS" : "FAIL") << "\", \"error_identifier\": \""
+    << (d.sector_status == 0 ? "" : "GPU_FEMM_SECTOR_" + StatusName(d.sector_status))
+    << "\", \"sector_start_angle_deg\": " << a.sector_start_angle_deg << ", \"sector_angle_deg\": " << a.sector_angle_deg
+    << ", \"full_machine_sector_count\": " << a.full_machine_sector_count
+    << ", \"electrical_pole_pairs\": " << a.electrical_pole_pairs
+    << ", \"suspension_spatial_order\": " << a.suspension_spatial_order << ", \"base_boundary_relation\": \""
+    << (d.base_sign > 0 ? "periodic" : "antiperiodic") << "\", \"tangent_boundary_relation\": \""
+    << (d.tangent_sign > 0 ? "periodic" : "antiperiodic") << "\", \"base_field_repeat_sign\": " << d.base_sign
+    << ", \"tangent_field_repeat_sign\": " << d.tangent_sign << ", \"output_normalization\": \"full_machine\""
+    << ", \"load_extraction_method\": \"weighted_stress_tensor_periodic_pair_mask\""
+    << ", \"periodic_pair_aware_weighted_stress_mask\": true, \"constraint_source\": \"cropped_sector_artifact\""
+    << ", \"operator_construction\": \"same_topology_dual_signed_reduction\""
+    << ", \"tangent_operator_storage\": \"shared_single_upload\", \"tangent_physical_operator_count\": "
+    << d.evidence_operators << ", \"tangent_operator_upload_count\": " << d.evidence_uploads
+    << ", \"tangent_rhs_count\": " << d.evidence_rhs << ", \"tangent_operator_bytes\": " << d.evidence_operator_bytes
+    << ", \"tangent_rhs_workspace_bytes\": " << d.evidence_rhs_bytes
+    << ", \"base_force_rule\": \"sum_rotated_sector_vectors\", \"base_torque_multiplier\": "
+    << d.base_torque_multiplier << ", \"tangent_force_multiplier\": " << d.tangent_force_multiplier
+    << ", \"tangent_torque_multiplier\": " << d.tangent_torque_multiplier << ", \"circuit_partner_indices\": [";
+  Csv(o, a.circuit_partners);
+  o << "], \"circuit_partner_orientations\": [";
+  for (size_t i = 0; i < a.circuit_orientations.size(); ++i)
+    o << (i ? ", " : "") << static_cast<int>(a.circuit_orientations[i]);
+  o << "], \"apex_self_pair_nodes\": [";
+  Csv(o, a.apex_nodes);
+  o << "], \"model_invariance_certificate_sha256\": \"" << a.model_invariance_certificate_sha256 << "\"},\n";
+}
+
 // WriteMotorBatchItemResponseJson (batch_response.cpp:124-281), conforming artifacts.
-void ItemResponse(std::ostream &o, const MotorSampleRequest &req, const MotorItem &d)
+void ItemResponse(std::ostream &o, const MotorSampleRequest &req, const MotorItem &d, const fgio::Artifact *art)
 {
   o << std::setprecision(17) << "{\n  \"protocol\": \"" << req.protocol << "\",\n"
     << "  \"mesh_artifact_sha256\": \"" << req.mesh_artifact_sha256 << "\",\n"
@@ -119,6 +228,8 @@ void ItemResponse(std::ostream &o, const MotorSampleRequest &req, const MotorIte
     o << "],\n  \"airgap_radial_flux_density_T\": [";
     Csv(o, d.radial);
     o << "],\n  \"mesh_element_count\": " << d.elements << ",\n";
+    if (d.sector && art)
+      SectorBlock(o, d, *art);
     if (d.tangent_requested) {
       o << "  \"tangent_multi_rhs\": {\"schema_version\": \"gpu_femm_tangent_multi_rhs_response_v1\", \"status\": \""
         << (d.tangent_status == 0 ? "PASS" : "FAIL") << "\", \"solve_status\": \"" << StatusName(d.tangent_status)
@@ -155,8 +266,8 @@ void ItemResponse(std::ostream &o, const MotorSampleRequest &req, const MotorIte
 }
 
 // The tangent block of one solved, postprocessed item (motor_postprocess.cpp:84-183).
-void Tangent(Prepared &p, fg_postprocess *pp, const MotorSampleRequest &req, const Solved &sol, MotorItem *d,
-             int *launches)
+void Tangent(fg_plan *plan, fg_postprocess *pp, const MotorSampleRequest &req, const Solved &sol, MotorItem *d,
+             int *launches, const std::vector<int> *radial_signs = nullptr)
 {
   const size_t m = req.tangent_rhs.size(), N = sol.a.size(), E = sol.b1.size(), C = sol.currents.size();
   std::vector<double> dirs;
@@ -166,10 +277,10 @@ void Tangent(Prepared &p, fg_postprocess *pp, const MotorSampleRequest &req, con
   std::vector<fg_linear_info> info(m);
   fg_solve_options o;
   fg_production_options(&o);
-  int rc = fg_solve_tangent(p.plan, sol.a.data(), sol.currents.data(), static_cast<int32_t>(m), dirs.data(), &o,
+  int rc = fg_solve_tangent(plan, sol.a.data(), sol.currents.data(), static_cast<int32_t>(m), dirs.data(), &o,
                             da.data(), db1.data(), db2.data(), dflux.data(), info.data());
   fg_timing t{};
-  fg_plan_last_timing(p.plan, &t);
+  fg_plan_last_timing(plan, &t);
   *launches += static_cast<int>(t.pcg_launches);
   if (rc != 0) {
     d->tangent_status = rc;
@@ -201,6 +312,9 @@ void Tangent(Prepared &p, fg_postprocess *pp, const MotorSampleRequest &req, con
     r.dtorque = res[k].torque_nm;
     r.dflux.assign(dflux.begin() + k * C, dflux.begin() + (k + 1) * C);
     r.dradial.assign(radial.begin() + k * P, radial.begin() + (k + 1) * P);
+    if (radial_signs)
+      for (size_t j = 0; j < P && j < radial_signs->size(); ++j)
+        r.dradial[j] *= (*radial_signs)[j];
     r.iterations = info[k].iterations;
     r.residual = info[k].residual_l2;
     d->rhs.push_back(std::move(r));
@@ -243,7 +357,7 @@ int MotorSingleSample(const std::string &request_path, const std::string &respon
     if (status == 0) {
       fg_postprocess *pp = nullptr;
       status = p.post.Get(p.plan, req.selected_group_number, req.air_group_number, req.airgap_radius_mm,
-                          req.airgap_angles_deg, &pp);
+                          req.airgap_angles_deg, &pp, nullptr, &p.artifact.apex_nodes);
       if (status == 0)
         status = RunPost(pp, sols[0], &post);
     }
@@ -345,26 +459,88 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
         const auto p0 = Clock::now();
         fg_postprocess *pp = nullptr;
         Post post;
+        const bool sector = r.sector_performance && p.artifact.sector;
+        std::vector<int> base_signs, tangent_signs;
+        std::vector<double> folded;
+        if (sector) {
+          for (double deg : r.airgap_angles_deg)
+            folded.push_back(deg * kPi / 180.0);
+          std::vector<double> tangent_folded = folded;
+          const double start = p.artifact.sector_start_angle_deg * kPi / 180.0;
+          d.base_sign = p.artifact.sector_boundary_sign;
+          d.tangent_sign = p.artifact.suspension_spatial_order % 2 == 0 ? 1 : -1;
+          base_signs = FoldSectorAngles(start, d.base_sign, &folded);
+          tangent_signs = FoldSectorAngles(start, d.tangent_sign, &tangent_folded);
+        }
         d.status = p.post.Get(p.plan, r.selected_group_number, r.air_group_number, r.airgap_radius_mm,
-                              r.airgap_angles_deg, &pp);
+                              r.airgap_angles_deg, &pp, sector ? &folded : nullptr, &p.artifact.apex_nodes);
         if (d.status == 0)
           d.status = RunPost(pp, sols[j], &post);
         post_s += seconds(p0);
-        if (d.status != 0)
-          continue;
-        d.fx = post.fx;
-        d.fy = post.fy;
-        d.torque = post.torque;
-        d.flux = sols[j].flux;
-        d.angles = r.airgap_angles_deg;
-        d.radial = post.radial;
-        d.elements = sols[j].b1.size();
-        if (r.tangent_requested) {
-          const auto q0 = Clock::now();
-          Tangent(p, pp, r, sols[j], &d, &launches);
-          tangent_s += seconds(q0);
-          ++symbolic_hits; // the tangent operator reuses the plan's symbolic CSR
+        if (d.status == 0 && sector)
+          for (size_t k = 0; k < post.radial.size() && k < base_signs.size(); ++k)
+            post.radial[k] *= base_signs[k];
+        if (d.status == 0) {
+          d.fx = post.fx;
+          d.fy = post.fy;
+          d.torque = post.torque;
+          d.flux = sols[j].flux;
+          d.angles = r.airgap_angles_deg;
+          d.radial = post.radial;
+          d.elements = sols[j].b1.size();
         }
+        if (sector) {
+          // ApplyBaseSectorReconstruction (batch_response.cpp:56-99): the orbit cancels the
+          // force, doubles the torque, and the partner circuits complete the flux.
+          d.sector = true;
+          const int cross = d.base_sign * d.tangent_sign;
+          d.tangent_force_multiplier = 1.0 - cross;
+          d.tangent_torque_multiplier = 1.0 + cross;
+          if (d.status == 0) {
+            d.fx = 0.0;
+            d.fy = 0.0;
+            d.torque *= d.base_torque_multiplier;
+            d.flux = ReconstructFlux(d.flux, p.artifact, d.base_sign);
+            if (d.flux.empty())
+              d.status = FG_INTERNAL_ERROR;
+          }
+          d.sector_status = d.status;
+        }
+        if (d.status != 0 || !r.tangent_requested)
+          continue;
+        const auto q0 = Clock::now();
+        d.tangent_status = 0;
+        fg_plan *tangent_plan = p.plan;
+        if (sector) {
+          d.tangent_status = SectorTangentPlan(p, opt);
+          tangent_plan = d.tangent_status == 0 ? p.sector_tangent->plan : nullptr;
+        }
+        if (d.tangent_status == 0) {
+          Tangent(tangent_plan, pp, r, sols[j], &d, &launches, sector ? &tangent_signs : nullptr);
+          ++symbolic_hits; // the tangent operator reuses a resident symbolic CSR
+          if (sector) {
+            fg_plan_sizes z{};
+            fg_plan_sizes_get(tangent_plan, &z);
+            const size_t m = r.tangent_rhs.size();
+            d.evidence_operators = d.evidence_uploads = 1;
+            d.evidence_rhs = m;
+            d.evidence_operator_bytes = static_cast<size_t>(z.nnz + 2 * z.rows) * sizeof(double);
+            d.evidence_rhs_bytes = m * static_cast<size_t>(z.rows) * 7 * sizeof(double) + m * sizeof(fg_linear_info);
+          }
+        }
+        if (sector) {
+          // ApplyTangentSectorReconstruction (batch_response.cpp:101-113).
+          for (TangentRhs &t : d.rhs) {
+            t.dfx *= d.tangent_force_multiplier;
+            t.dfy *= d.tangent_force_multiplier;
+            t.dtorque *= d.tangent_torque_multiplier;
+            t.dflux = ReconstructFlux(t.dflux, p.artifact, d.tangent_sign);
+            if (t.dflux.empty())
+              d.tangent_status = FG_INTERNAL_ERROR;
+          }
+          d.sector_status = d.tangent_status;
+        }
+        tangent_s += seconds(q0);
       }
     }
   }
@@ -410,7 +586,9 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
   o << "  \"items\": [\n";
   for (size_t i = 0; i < n; ++i) {
     o << "    {\"task_id\": \"" << batch.items[i].task_id << "\", \"response\": ";
-    ItemResponse(o, batch.items[i].request, out[i]);
+    const MotorSampleRequest &r = batch.items[i].request;
+    auto it = artifacts->find({r.mesh_artifact_path, r.mesh_artifact_sha256});
+    ItemResponse(o, r, out[i], it != artifacts->end() && it->second ? &it->second->artifact : nullptr);
     o << "}" << (i + 1 == n ? "\n" : ",\n");
   }
   o << "  ]\n}\n";

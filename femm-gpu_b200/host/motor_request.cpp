@@ -172,8 +172,16 @@ bool ParseMotorSampleRequestText(const std::string &text, MotorSampleRequest *ou
 
 bool MotorRequestMatchesArtifact(const MotorSampleRequest &r, const Artifact &a)
 {
-  // Neutral artifacts carry their source digest as the base identity and a zero pose.
-  if (r.protocol == "gpu_femm_motor_sample_v3" || r.protocol == "gpu_femm_motor_sample_v4")
+  // Neutral artifacts carry their source digest as the base identity and a zero pose; native
+  // air-gap element sectors (v4) are not served.
+  const bool sector_request = r.protocol == "gpu_femm_motor_sample_v3";
+  if (r.protocol == "gpu_femm_motor_sample_v4" || sector_request != a.sector)
+    return false;
+  if (sector_request &&
+      (a.schema_version != "gpu_femm_mesh_v3" || a.sector_angle_deg != 180.0 || a.full_machine_sector_count != 2 ||
+       a.electrical_pole_pairs <= 0 || a.suspension_spatial_order != a.electrical_pole_pairs + 1 ||
+       a.sector_boundary_sign != (a.electrical_pole_pairs % 2 == 0 ? 1 : -1) || !r.sector_performance ||
+       r.model_invariance_certificate_sha256 != a.model_invariance_certificate_sha256))
     return false;
   return r.base_motor_fem_sha256 == a.base_motor_fem_sha256 && r.source_fem_sha256 == a.source_fem_sha256 &&
          r.rotor_angle_deg == a.rotor_angle_deg && r.displacement_mm[0] == a.displacement_mm[0] &&

@@ -34,9 +34,10 @@ bool ParseMotorSampleRequest(const Json &root, MotorSampleRequest *out, std::str
 bool ParseMotorSampleRequestText(const std::string &text, MotorSampleRequest *out, std::string *error);
 
 // RequestMatchesArtifact (sample_request.cpp:393-446) for the conforming artifacts served
-// here: the request's identities, pose and circuit count against the artifact's.  Sector
-// (v3) and native air-gap sector (v4) requests need artifacts that are not served, so
-// they never match.
+// here: the request's identities, pose and circuit count against the artifact's; a v3
+// request needs a v3 sector artifact with consistent harmonic metadata and the same model
+// invariance certificate.  Native air-gap element sectors (v4) are not served and never
+// match.
 bool MotorRequestMatchesArtifact(const MotorSampleRequest &r, const Artifact &a);
 
 // ReadMotorBatchRequestJson (gpu_solver/src/app/batch_prepare.cpp:73-129).

@@ -72,13 +72,79 @@ def test_motor_artifact_refusals_follow_the_reference(tmp_path):
     p = tmp_path / "upper.json"
     p.write_text(json.dumps(ok))
     assert describe(str(p))[0] == 0 and ref_parse(json.dumps(ok).encode())[0] is not None
-    # The native air-gap element schemas are refused (not served).
+    # The native air-gap element schemas are refused (not served); v3 needs its sector fields.
     for schema in ("gpu_femm_mesh_v2", "gpu_femm_mesh_v3", "gpu_femm_mesh_v4"):
         v = copy.deepcopy(root)
         v["schema_version"] = schema
         p.write_text(json.dumps(v))
         rc, d = describe(str(p))
-        assert rc == 1 and "not served" in d["error"]
+        ref, ref_err = ref_parse(json.dumps(v).encode())
+        assert rc == 1 and ref is None
+        assert "not served" in d["error"] if schema != "gpu_femm_mesh_v3" else d["error"] == ref_err
+
+
+def sector_artifact_text(model, base=BASE, source=SOURCE, cert="d" * 64, **sector):
+    """A gpu_femm_mesh_v3 artifact of a 180-degree sector model (two_pole_machine)."""
+    from femm_gpu_b200 import artifact
+    text, _ = artifact.write_artifact(model, [0.0] * model.circuit_count, source_sha256=source)
+    root = json.loads(text)
+    root["schema_version"] = "gpu_femm_mesh_v3"
+    root["base_motor_fem_sha256"] = base
+    res = root["resolved"]
+    res["base_motor_fem_sha256"] = base
+    res["pose"] = {"rotor_angle_deg": 0, "displacement_mm": [0, 0]}
+    res["air_gap_elements"] = []
+    meta = {"schema_version": "gpu_femm_motor_sector_v1", "sector_start_angle_deg": 0, "angle_deg": 180,
+            "full_machine_sector_count": 2, "electrical_pole_pairs": 1, "suspension_spatial_order": 2,
+            "boundary_relation": "antiperiodic", "circuit_partner_indices": list(range(model.circuit_count)),
+            "circuit_partner_orientations": [-1] * model.circuit_count, "apex_self_pair_nodes": [],
+            "model_invariance_certificate_sha256": cert}
+    meta.update(sector)
+    res["sector"] = meta
+    return json.dumps(root)
+
+
+@needs_ref
+def test_sector_artifact_parses_like_the_reference(tmp_path):
+    from femm_gpu_b200 import meshes
+    model = meshes.two_pole_machine(nr=12, nt=24)
+    good = sector_artifact_text(model)
+    p = tmp_path / "s.json"
+    p.write_text(good)
+    rc, d = describe(str(p))
+    ref, err = ref_parse(good.encode())
+    assert rc == 0 and ref is not None, (d, err)
+    assert np.array_equal(np.array(d["xy"]), ref["xy"]) and np.array_equal(np.array(d["tri_mat"]), ref["tm"])
+    assert np.array_equal(np.array(d["dirichlet_nodes"]), ref["dn"])
+    nc = ref["sizes"][5]
+    con = ref["con"][: 3 * nc].reshape(-1, 3)
+    assert np.array_equal(np.array(d["constraint_signs"]), con[:, 2])
+    variants = {
+        "angle": dict(angle_deg=90),
+        "count": dict(full_machine_sector_count=3),
+        "order": dict(suspension_spatial_order=3),
+        "relation parity": dict(boundary_relation="periodic"),
+        "partner": dict(circuit_partner_indices=[0, 0, 2]),
+        "orientation": dict(circuit_partner_orientations=[2, -1, -1]),
+        "apex off origin": dict(apex_self_pair_nodes=[5]),
+        "certificate": dict(model_invariance_certificate_sha256="D" * 64),
+        "schema": dict(schema_version="gpu_femm_motor_sector_v2"),
+    }
+    for label, kw in variants.items():
+        text = sector_artifact_text(model, **kw)
+        p.write_text(text)
+        rc, d = describe(str(p))
+        ref, ref_err = ref_parse(text.encode())
+        assert ref is None and rc == 1, label
+        assert d["error"] == ref_err, (label, d["error"], ref_err)
+    # a constraint pair that is not a 180-degree rotation
+    root = json.loads(good)
+    root["resolved"]["nodes_mm"][int(model.con_b[3])][0] += 0.5
+    text = json.dumps(root)
+    p.write_text(text)
+    rc, d = describe(str(p))
+    ref, ref_err = ref_parse(text.encode())
+    assert ref is None and rc == 1 and d["error"] == ref_err
 
 
 def motor_request(protocol="gpu_femm_motor_sample_v1", **kw):
