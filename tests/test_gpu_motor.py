@@ -142,3 +142,76 @@ def test_motor_transaction_in_worker(gpu, tmp_path):
     assert rc == 0 and "timing" in got and "timing" in ref
     assert [i["response"] for i in got["items"]] == [i["response"] for i in ref["items"]]
     assert got["cache"] == ref["cache"]
+
+
+def test_sector_batch_reconstructs_the_full_machine(gpu, tmp_path):
+    """A v3 sector batch (half of a two-pole machine, antiperiodic) reports the full
+    machine: its torque, flux linkages and air-gap samples equal a solve of the full
+    360-degree mesh within 1e-6 (two discretisations of one field that agree up to the
+    Newton and PCG tolerances); its force is zero by the orbit rule and the full machine's
+    is zero to roundoff.  The tangent block follows the reference's reconstruction rules on
+    the library's tangent of the periodic (suspension-order) operator."""
+    from femm_gpu_b200 import meshes
+    from test_motor_cli import sector_artifact_text
+    sector = meshes.two_pole_machine(nr=24, nt=72)
+    full = meshes.two_pole_machine(nr=24, nt=72, full=True)
+    source = "f" * 64
+    path = tmp_path / "sector.gpu.json"
+    path.write_text(sector_artifact_text(sector, base=BASE, source=source))
+    digest = hashlib.sha256(open(path, "rb").read()).hexdigest()
+    angles = [10.0, 100.0, 190.0, 280.0, 350.0]
+    tangent = {"schema_version": "gpu_femm_tangent_multi_rhs_v1",
+               "rhs": [{"name": "a", "circuit_current_derivative_A_per_A": [1.0, 0.0, 0.0]}]}
+    currents = [[6.0, -3.0, -3.0], [0.0, 4.0, -4.0]]
+    items = []
+    for i, cur in enumerate(currents):
+        items.append({"task_id": f"s{i}", "request": {
+            "protocol": "gpu_femm_motor_sample_v3", "mesh_artifact_path": str(path), "mesh_artifact_sha256": digest,
+            "base_motor_fem_sha256": BASE, "source_fem_sha256": source, "circuit_currents_A": cur,
+            "selected_group_number": 20, "air_group_number": 50, "airgap_radius_mm": 45.5,
+            "airgap_angles_deg": angles, "rotor_angle_deg": 0, "displacement_mm": [0, 0],
+            "tangent_multi_rhs": tangent,
+            "sector_performance": {"schema_version": "gpu_femm_motor_sector_performance_v1",
+                                   "model_invariance_certificate_sha256": "d" * 64}}})
+    body = {"protocol": "gpu_femm_motor_batch_v3", "max_items_per_chunk": 4, "items": items}
+    rc, b, err = call(tmp_path, "--motor-batch", body, name="sector.json")
+    assert rc == 0 and b["status"] == "PASS", err
+    fplan = fg.Plan(full)
+    fsol = fplan.solve(currents)
+    fpp = fg.Postprocess(fplan, selected_group=20, air_group=50, radius_m=0.0455,
+                         angles_rad=np.radians(angles), max_mask_iterations=4096)
+    fres = fpp.compute(fsol.a, fsol.b1, fsol.b2)
+    # the library's tangent of the suspension-order (periodic) operator at the sector base
+    tmodel = meshes.two_pole_machine(nr=24, nt=72)
+    tmodel.con_sign[:] = 1
+    tplan, splan = fg.Plan(tmodel), fg.Plan(sector)
+    spp = fg.Postprocess(splan, selected_group=20, air_group=50, radius_m=0.0455,
+                         angles_rad=np.radians([10.0, 100.0, 10.0, 100.0, 170.0]), max_mask_iterations=4096)
+    for i, item in enumerate(b["items"]):
+        r = item["response"]
+        sr = r["sector_reconstruction"]
+        assert sr["status"] == "PASS" and sr["base_torque_multiplier"] == 2 and sr["base_field_repeat_sign"] == -1
+        assert sr["tangent_field_repeat_sign"] == 1 and sr["tangent_force_multiplier"] == 2
+        assert sr["tangent_torque_multiplier"] == 0 and sr["tangent_rhs_count"] == 1
+        assert r["Fx_N"] == 0.0 and r["Fy_N"] == 0.0
+        scale = max(abs(fres.torque[i]), 1e-9)
+        assert abs(r["torque_Nm"] - fres.torque[i]) <= 1e-6 * scale, (r["torque_Nm"], fres.torque[i])
+        assert np.abs(fres.force[i]).max() <= 1e-6 * max(1.0, np.abs(fres.torque[i]) / 0.05)
+        np.testing.assert_allclose(r["circuit_flux_linkage_Wb"], fsol.flux[i], rtol=1e-6,
+                                   atol=1e-6 * np.abs(fsol.flux[i]).max())
+        np.testing.assert_allclose(r["airgap_radial_flux_density_T"], fres.radial_b[i], rtol=0,
+                                   atol=1e-6 * np.abs(fres.radial_b[i]).max())
+        assert r["airgap_sample_angles_deg"] == angles
+        # tangent block: library tangent on the periodic operator, reconstruction rules
+        ssol = splan.solve([currents[i]])
+        da, db1, db2, dflux, info = tplan.solve_tangent(ssol.a[0], currents[i], [[1.0, 0.0, 0.0]])
+        t = spp.tangent(ssol.b1[0], ssol.b2[0], da, db1, db2)
+        rhs = r["tangent_multi_rhs"]["rhs"][0]
+        assert r["tangent_multi_rhs"]["status"] == "PASS"
+        for got, want in ((rhs["dFx_N_per_A"], 2 * t.force[0, 0]), (rhs["dFy_N_per_A"], 2 * t.force[0, 1])):
+            assert abs(got - want) <= 1e-6 * max(abs(want), 1e-9), (got, want)
+        assert rhs["dtorque_Nm_per_A"] == 0.0
+        part = np.array(dflux[0]) + (-1) * np.array(dflux[0])  # partner orientation -1, repeat sign +1
+        np.testing.assert_allclose(rhs["circuit_flux_linkage_derivative_Wb_per_A"], part, atol=1e-12)
+        np.testing.assert_allclose(rhs["airgap_radial_flux_density_derivative_T_per_A"], t.radial_b[0], rtol=0,
+                                   atol=1e-6 * np.abs(t.radial_b[0]).max())
