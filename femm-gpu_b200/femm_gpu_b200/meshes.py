@@ -299,7 +299,7 @@ def annular_sector(nr: int = 160, nt: int = 250, hc: float = 9.0e5, turns: float
     )
 
 
-def two_pole_machine(nr: int = 40, nt: int = 120, full: bool = False, hc: float = 9.0e5,
+def two_pole_machine(nr: int = 160, nt: int = 120, full: bool = False, hc: float = 9.0e5,
                      turns: float = 20.0) -> Model:
     """A two-pole surface-magnet machine, as the 180-degree sector [0, 180] degrees with
     antiperiodic edges (``full=False``) or the full 360-degree annulus (``full=True``, the

@@ -145,7 +145,8 @@ def test_motor_transaction_in_worker(gpu, tmp_path):
 
 
 def test_sector_batch_reconstructs_the_full_machine(gpu, tmp_path):
-    """A v3 sector batch (half of a two-pole machine, antiperiodic) reports the full
+    """A v3 sector batch (half of a two-pole machine, antiperiodic; 0.25 mm radial cells so
+    that the air gap holds free mask nodes) reports the full
     machine: its torque, flux linkages and air-gap samples equal a solve of the full
     360-degree mesh within 1e-6 (two discretisations of one field that agree up to the
     Newton and PCG tolerances); its force is zero by the orbit rule and the full machine's
@@ -153,8 +154,8 @@ def test_sector_batch_reconstructs_the_full_machine(gpu, tmp_path):
     the library's tangent of the periodic (suspension-order) operator."""
     from femm_gpu_b200 import meshes
     from test_motor_cli import sector_artifact_text
-    sector = meshes.two_pole_machine(nr=24, nt=72)
-    full = meshes.two_pole_machine(nr=24, nt=72, full=True)
+    sector = meshes.two_pole_machine(nr=160, nt=72)
+    full = meshes.two_pole_machine(nr=160, nt=72, full=True)
     source = "f" * 64
     path = tmp_path / "sector.gpu.json"
     path.write_text(sector_artifact_text(sector, base=BASE, source=source))
@@ -175,14 +176,15 @@ def test_sector_batch_reconstructs_the_full_machine(gpu, tmp_path):
                                    "model_invariance_certificate_sha256": "d" * 64}}})
     body = {"protocol": "gpu_femm_motor_batch_v3", "max_items_per_chunk": 4, "items": items}
     rc, b, err = call(tmp_path, "--motor-batch", body, name="sector.json")
-    assert rc == 0 and b["status"] == "PASS", err
+    assert rc == 0 and b["status"] == "PASS", (err, [(i["response"]["solve_status"],
+                                                      i["response"]["convergence"]) for i in b["items"]])
     fplan = fg.Plan(full)
     fsol = fplan.solve(currents)
     fpp = fg.Postprocess(fplan, selected_group=20, air_group=50, radius_m=0.0455,
                          angles_rad=np.radians(angles), max_mask_iterations=4096)
     fres = fpp.compute(fsol.a, fsol.b1, fsol.b2)
     # the library's tangent of the suspension-order (periodic) operator at the sector base
-    tmodel = meshes.two_pole_machine(nr=24, nt=72)
+    tmodel = meshes.two_pole_machine(nr=160, nt=72)
     tmodel.con_sign[:] = 1
     tplan, splan = fg.Plan(tmodel), fg.Plan(sector)
     spp = fg.Postprocess(splan, selected_group=20, air_group=50, radius_m=0.0455,
