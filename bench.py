@@ -124,6 +124,23 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def max_over_ranks(x, world, device):
+    """The slowest rank's figure (replicas: every rank times its own batch), then a barrier."""
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.barrier()
+    return float(t.item())
+
+
+def weak_value(world, items, steps, seconds):
+    """Whole-job solves/s: every rank solves `items` samples per step."""
+    return world * items * steps / seconds
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -222,14 +239,8 @@ def run_ours(args, world, rank, local):
             item_its += sum(x.linear_iterations for x in info)
             statuses += [x.status for x in info]
         torch.cuda.synchronize()
-    ms = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dist.barrier()
-        ms = float(tt.item())
-    value = world * k * args.steps / (ms / 1e3)
+    ms = max_over_ranks(sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1)), world, dev)
+    value = weak_value(world, k, args.steps, ms / 1e3)
 
     # Roofline of the dominant kernel (the cooperative PCG).
     n, nnz = plan.rows, plan.nnz
@@ -256,13 +267,8 @@ def run_ours(args, world, rank, local):
     t0 = time.perf_counter()
     for s in range(args.steps):
         plan.solve(host_in[s])
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": world * k * args.steps / e2e_s, "unit": "solves/s",
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e = {"value": weak_value(world, k, args.steps, e2e_s), "unit": "solves/s",
            "h2d_bytes_per_step": k * Cc * 8,
            "d2h_bytes_per_step": k * (N + 2 * E + Cc) * 8 + k * 40}
 
