@@ -308,9 +308,22 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
     return false;
   TraceMark(a, gs, tr, 2 * phase + 1);
   for (int t = warp; t < QK; t += kPcgWarps) {
+    // Lane-strided partials in CTA order; eight loads issued before their adds (the add
+    // order, and so the result, is that of the one-at-a-time loop).
+    const double *pt = part + static_cast<size_t>(t) * G;
     double s = 0.0;
-    for (int g = lane; g < G; g += 32) {
-      const double y = __ldcg(part + static_cast<size_t>(t) * G + g);
+    int g = lane;
+    for (; g + 32 * 7 < G; g += 32 * 8) {
+      double y[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        y[u] = __ldcg(pt + g + 32 * u);
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        s = kMax ? fmax(s, y[u]) : s + y[u];
+    }
+    for (; g < G; g += 32) {
+      const double y = __ldcg(pt + g);
       s = kMax ? fmax(s, y) : s + y;
     }
 #pragma unroll
