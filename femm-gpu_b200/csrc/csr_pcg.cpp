@@ -103,7 +103,7 @@ Status CsrPcg(int32_t n, const int32_t *ro, const int32_t *col, const double *va
       b[static_cast<size_t>(r) * kp + i] = rhs[static_cast<size_t>(i) * n + r];
 
   DeviceArray<int32_t> d_len, d_off, d_col, d_err;
-  DeviceArray<double> d_val, d_diag, d_inv, d_b, d_x, d_r, d_z, d_p0, d_q, d_part, d_info;
+  DeviceArray<double> d_val, d_diag, d_inv, d_b, d_x, d_r, d_z, d_p0, d_p1, d_q, d_part, d_info;
   DeviceArray<unsigned> d_bar;
   const size_t vec = static_cast<size_t>(n_pad) * kp;
   const int grid_cap = fg::PcgMaxGrid(kp);
@@ -117,8 +117,8 @@ Status CsrPcg(int32_t n, const int32_t *ro, const int32_t *col, const double *va
       (s = d_diag.upload(d.data(), d.size())) != Status::kOk ||
       (s = d_inv.upload(inv.data(), inv.size())) != Status::kOk ||
       (s = d_b.upload(b.data(), b.size())) != Status::kOk || (s = d_x.ensure(vec)) != Status::kOk ||
-      (s = d_r.ensure(vec)) != Status::kOk || (s = d_z.ensure(2 * vec)) != Status::kOk ||
-      (s = d_p0.ensure(2 * vec)) != Status::kOk ||
+      (s = d_r.ensure(vec)) != Status::kOk || (s = d_z.ensure(vec)) != Status::kOk ||
+      (s = d_p0.ensure(vec)) != Status::kOk || (s = d_p1.ensure(vec)) != Status::kOk ||
       (s = d_q.ensure(vec)) != Status::kOk ||
       (s = d_part.ensure(static_cast<size_t>(2) * 64 * grid_cap)) != Status::kOk ||
       (s = d_info.ensure(3 * static_cast<size_t>(kp))) != Status::kOk ||
@@ -146,7 +146,7 @@ Status CsrPcg(int32_t n, const int32_t *ro, const int32_t *col, const double *va
   a.r = d_r.get();
   a.z = d_z.get();
   a.p0 = d_p0.get();
-  a.p1 = nullptr;
+  a.p1 = d_p1.get();
   a.q = d_q.get();
   a.partials = d_part.get();
   a.barrier = d_bar.get();

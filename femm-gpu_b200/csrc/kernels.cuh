@@ -57,8 +57,6 @@ struct PcgArgs {
   const void *blocks;
   int32_t block_size, block_stride, block_item;
   const void *b;
-  // z and p: [n_pad][2 KP] rows (z of the row's items, then p) in two buffers z and p0,
-  // swapped every iteration; p1 is unused.
   void *x, *r, *z, *p0, *p1, *q;
   double *partials;   // [2][64][grid]
   unsigned int *barrier;

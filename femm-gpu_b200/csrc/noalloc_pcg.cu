@@ -54,9 +54,10 @@ constexpr size_t kOffInvd = kOffDiag + kVec;
 constexpr size_t kOffB = kOffInvd + kVec;
 constexpr size_t kOffX = kOffB + kVec;
 constexpr size_t kOffR = kOffX + kVec;
-constexpr size_t kOffZ = kOffR + kVec;    // z | p rows, current buffer
-constexpr size_t kOffP0 = kOffZ + 2 * kVec; // z | p rows, the other buffer
-constexpr size_t kOffQ = kOffP0 + 2 * kVec;
+constexpr size_t kOffZ = kOffR + kVec;
+constexpr size_t kOffP0 = kOffZ + kVec;
+constexpr size_t kOffP1 = kOffP0 + kVec;
+constexpr size_t kOffQ = kOffP1 + kVec;
 constexpr size_t kOffPartials = kOffQ + kVec;
 constexpr size_t kOffControl = kOffPartials + Align(sizeof(double) * 2 * 64 * kNoallocMaxGrid);
 constexpr size_t kScratchBytes = kOffControl + 256;
@@ -259,7 +260,7 @@ Status NoallocPcg(int32_t n, const int32_t *ro, const int32_t *col, const double
   a.r = reinterpret_cast<double *>(scratch + kOffR);
   a.z = reinterpret_cast<double *>(scratch + kOffZ);
   a.p0 = reinterpret_cast<double *>(scratch + kOffP0);
-  a.p1 = nullptr;
+  a.p1 = reinterpret_cast<double *>(scratch + kOffP1);
   a.q = reinterpret_cast<double *>(scratch + kOffQ);
   a.partials = reinterpret_cast<double *>(scratch + kOffPartials);
   Control *dctl = reinterpret_cast<Control *>(scratch + kOffControl);

@@ -375,8 +375,7 @@ __device__ __forceinline__ int Column(const PcgArgs &a, const int32_t *colc, siz
 template <typename T, int KP, int IV, bool kFold>
 __device__ __forceinline__ void RowProduct(const PcgArgs &a, const int32_t *colc, size_t cbase,
                                            size_t base, int len, int item0, const T *z, const T *p,
-                                           size_t stride, const bool (&fold)[IV], const T (&beta)[IV],
-                                           T (&acc)[IV])
+                                           const bool (&fold)[IV], const T (&beta)[IV], T (&acc)[IV])
 {
   const T *vals = static_cast<const T *>(a.values);
 #pragma unroll
@@ -401,7 +400,7 @@ __device__ __forceinline__ void RowProduct(const PcgArgs &a, const int32_t *colc
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       if (w0 + u < len) {
-        const size_t ci = static_cast<size_t>(c[u]) * stride + item0;
+        const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
         T g[IV];
         Load<T, IV>(z + ci, g);
         if constexpr (kFold) {
@@ -484,11 +483,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
   const T *IDG = static_cast<const T *>(a.invd);
   T *X = static_cast<T *>(a.x);
   T *R = static_cast<T *>(a.r);
-  // z and p of a row side by side, [n_pad][2 KP] (z | p), in two buffers: the current one
-  // holds z_i and p_i (gathered by the SpMV), the other receives p_i+1 and then z_i+1.
-  T *ZP[2] = {static_cast<T *>(a.z), static_cast<T *>(a.p0)};
-  int cur = 0;
-  auto zrow = [&](int b, int r) { return ZP[b] + static_cast<size_t>(r) * (2 * KP) + item0; };
+  T *Z = static_cast<T *>(a.z);
   T *Qv = static_cast<T *>(a.q);
 
   if (threadIdx.x < KP) {
@@ -672,7 +667,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
     const bool nofold[IV] = {};
     const T nobeta[IV] = {};
     T acc[IV];
-    RowProduct<T, KP, IV, false>(a, colc, cbase, base, len, item0, X, nullptr, KP, nofold, nobeta, acc);
+    RowProduct<T, KP, IV, false>(a, colc, cbase, base, len, item0, X, nullptr, nofold, nobeta, acc);
 #pragma unroll
     for (int j = 0; j < IV; ++j)
       t[j] = bd[j] / sc[j] - static_cast<double>(acc[j]);
@@ -761,7 +756,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
       }
       precond(rv, r, zv);
       Store<T, IV>(R + ri, rt);
-      Store<T, IV>(zrow(cur, r), zv);
+      Store<T, IV>(Z + ri, zv);
 #pragma unroll
       for (int j = 0; j < IV; ++j)
         if (on(j)) {
@@ -794,7 +789,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           double rv[IV];
           T zv[IV];
           block_row(wu, u, rv, zv);
-          Store<T, IV>(zrow(cur, sub_row(wu, u)), zv);
+          Store<T, IV>(Z + static_cast<size_t>(sub_row(wu, u)) * KP + item0, zv);
 #pragma unroll
           for (int j = 0; j < IV; ++j)
             if (on(j))
@@ -824,6 +819,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
     __syncthreads();
   }
 
+  T *pc = static_cast<T *>(a.p0), *pn = static_cast<T *>(a.p1);
   for (int iteration = 0; iteration < a.max_iterations; ++iteration) {
     bool any = false;
 #pragma unroll
@@ -849,13 +845,12 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
       auto finish_row = [&](int r, const T (&acc)[IV]) {
         const size_t ri = static_cast<size_t>(r) * KP + item0;
         T zr[IV], pr[IV], pnew[IV];
-        const T *own = zrow(cur, r);
-        Load<T, IV>(own, zr);
-        Load<T, IV>(own + KP, pr);
+        Load<T, IV>(Z + ri, zr);
+        Load<T, IV>(pc + ri, pr);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
           pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
-        Store<T, IV>(zrow(cur ^ 1, r) + KP, pnew);
+        Store<T, IV>(pn + ri, pnew);
         Store<T, IV>(Qv + ri, acc);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
@@ -916,10 +911,10 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
-                const T *zc = zrow(cur, c[u]);
+                const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
                 T g[IV], pv[IV], vv[IV];
-                Load<T, IV>(zc, g);
-                Load<T, IV>(zc + KP, pv);
+                Load<T, IV>(Z + ci, g);
+                Load<T, IV>(pc + ci, pv);
                 Load<T, IV>(ring + ((stage * U + u) * 32 + lane) * IV, vv);
 #pragma unroll
                 for (int j = 0; j < IV; ++j) {
@@ -951,8 +946,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         const int len = __ldg(a.row_len + r);
         const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
         T acc[IV];
-        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, ZP[cur], ZP[cur] + KP, 2 * KP, fold, be,
-                                    acc);
+        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
         (void)ri;
         finish_row(r, acc);
         FG_ROWS_END
@@ -975,7 +969,9 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         }
       }
       __syncthreads();
-      cur ^= 1; // the buffer holding p_i+1 becomes current; phase B adds z_i+1 to it
+      T *t = pc;
+      pc = pn;
+      pn = t;
     }
 
     // Phase B: x += alpha p, r -= alpha q, z = M^-1 r, r.r and r.z
@@ -996,7 +992,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             for (int u = 0; u < SUB; ++u) {
               const size_t ri = static_cast<size_t>(sub_row(wu, u)) * KP + item0;
               Load<T, IV>(X + ri, xo[u]);
-              Load<T, IV>(zrow(cur, sub_row(wu, u)) + KP, po[u]);
+              Load<T, IV>(pc + ri, po[u]);
               Load<T, IV>(R + ri, ro[u]);
               Load<T, IV>(Qv + ri, qo[u]);
             }
@@ -1022,7 +1018,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
               double rn[IV];
               T zn[IV];
               block_row(wu, u, rn, zn);
-              Store<T, IV>(zrow(cur, sub_row(wu, u)), zn);
+              Store<T, IV>(Z + static_cast<size_t>(sub_row(wu, u)) * KP + item0, zn);
 #pragma unroll
               for (int j = 0; j < IV; ++j)
                 if (on(j)) {
@@ -1041,12 +1037,12 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           const size_t i1 = static_cast<size_t>(r1) * KP + item0;
           T x0[IV], p0[IV], rv0[IV], q0[IV], x1[IV], p1[IV], rv1[IV], q1[IV];
           Load<T, IV>(X + i0, x0);
-          Load<T, IV>(zrow(cur, r0) + KP, p0);
+          Load<T, IV>(pc + i0, p0);
           Load<T, IV>(R + i0, rv0);
           Load<T, IV>(Qv + i0, q0);
           if (two) {
             Load<T, IV>(X + i1, x1);
-            Load<T, IV>(zrow(cur, r1) + KP, p1);
+            Load<T, IV>(pc + i1, p1);
             Load<T, IV>(R + i1, rv1);
             Load<T, IV>(Qv + i1, q1);
           }
@@ -1064,7 +1060,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           precond(rn, r0, zn);
           Store<T, IV>(X + i0, xn);
           Store<T, IV>(R + i0, rt);
-          Store<T, IV>(zrow(cur, r0), zn);
+          Store<T, IV>(Z + i0, zn);
 #pragma unroll
           for (int j = 0; j < IV; ++j)
             if (on(j)) {
@@ -1084,7 +1080,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             precond(rn, r1, zn);
             Store<T, IV>(X + i1, xn);
             Store<T, IV>(R + i1, rt);
-            Store<T, IV>(zrow(cur, r1), zn);
+            Store<T, IV>(Z + i1, zn);
 #pragma unroll
             for (int j = 0; j < IV; ++j)
               if (on(j)) {
@@ -1210,7 +1206,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
               T zv[IV], zo[IV];
               double rd[IV];
               settle_x(ri, f, s, v[1]);
-              Load<T, IV>(zrow(cur, sub_row(wu, u)), zo);
+              Load<T, IV>(Z + ri, zo);
               block_row(wu, u, rd, zv);
 #pragma unroll
               for (int j = 0; j < IV; ++j) {
@@ -1219,7 +1215,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
                 else
                   zv[j] = zo[j];
               }
-              Store<T, IV>(zrow(cur, sub_row(wu, u)), zv);
+              Store<T, IV>(Z + ri, zv);
             }
             __syncwarp();
           }
@@ -1229,7 +1225,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         double rd[IV];
         settle_x(ri, f, s, v[1]);
         Load<T, IV>(R + ri, rv);
-        Load<T, IV>(zrow(cur, r), zo);
+        Load<T, IV>(Z + ri, zo);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
           rd[j] = rv[j];
@@ -1241,7 +1237,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           else
             zv[j] = zo[j];
         }
-        Store<T, IV>(zrow(cur, r), zv);
+        Store<T, IV>(Z + ri, zv);
         FG_ROWS_END
       }
       if (!GridReduce<KP, IV, 2, false>(a, gs, v, sm, epoch, buf, tr, 2))

@@ -62,7 +62,7 @@ size_t Plan::DeviceBytes() const
        circuit_rhs_.bytes() + elem_geo_.bytes() + boundary_.bytes();
   b += state_.bytes() + ev_.bytes() + er_.bytes() + values_.bytes() + diag_.bytes() +
        invd_.bytes() + rhs_.bytes() + x_.bytes() + r_.bytes() + z_.bytes() + p0_.bytes() +
-       q_.bytes() + pcg_partials_.bytes() + staging_.bytes();
+       p1_.bytes() + q_.bytes() + pcg_partials_.bytes() + staging_.bytes();
   b += in_currents_.bytes() + in_hc_.bytes() + in_warm_.bytes() + out_a_.bytes() + out_b1_.bytes() +
        out_b2_.bytes() + out_flux_.bytes();
   return b;
@@ -234,9 +234,9 @@ Status Plan::EnsureWorkspace(int kp)
   FG_EN(rhs_, vec);
   FG_EN(x_, vec);
   FG_EN(r_, vec);
-  // z and p interleaved per row in two buffers ([n_pad][2 KP] each, PcgArgs::z / p0).
-  FG_EN(z_, 2 * vec);
-  FG_EN(p0_, 2 * vec);
+  FG_EN(z_, vec);
+  FG_EN(p0_, vec);
+  FG_EN(p1_, vec);
   FG_EN(q_, vec);
   FG_EN(norm_partials_, static_cast<size_t>(2) * kp * 256);
   FG_EN(norms_, static_cast<size_t>(2) * kp);
@@ -262,8 +262,9 @@ Status Plan::EnsureWorkspace(int kp)
     FG_EN(i32_, vec);
     FG_EN(x32_, vec);
     FG_EN(r32_, vec);
-    FG_EN(z32_, 2 * vec);
-    FG_EN(p032_, 2 * vec);
+    FG_EN(z32_, vec);
+    FG_EN(p032_, vec);
+    FG_EN(p132_, vec);
     FG_EN(q32_, vec);
   }
 #undef FG_EN
@@ -310,7 +311,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.r = r_.get();
   a.z = z_.get();
   a.p0 = p0_.get();
-  a.p1 = nullptr;
+  a.p1 = p1_.get();
   a.q = q_.get();
   a.partials = pcg_partials_.get();
   a.barrier = barrier_.get();
@@ -471,7 +472,7 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   a.r = r32_.get();
   a.z = z32_.get();
   a.p0 = p032_.get();
-  a.p1 = nullptr;
+  a.p1 = p132_.get();
   a.q = q32_.get();
   a.reliable = 1;
   a.reliable_delta = kReliableDelta;
@@ -745,7 +746,7 @@ bool Plan::ChunkPcgArgs(const Chunk &c, unsigned *barrier, int32_t *error, PcgAr
   a.r = r_.get();
   a.z = z_.get();
   a.p0 = p0_.get();
-  a.p1 = nullptr;
+  a.p1 = p1_.get();
   a.q = q_.get();
   a.partials = pcg_partials_.get();
   a.barrier = barrier;

@@ -131,10 +131,10 @@ private:
   DeviceArray<double> pm_rhs_, circuit_rhs_, elem_geo_, mat_nu0_, mat_alpha_, mat_cold_, mat_jpa_,
       curve_b_, curve_h_, curve_slope_, boundary_;
   // Batch workspace.
-  DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, q_; // z_, p0_: z | p rows
+  DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, p1_, q_;
   DeviceArray<double> norm_partials_, norms_, pcg_partials_, pcg_info_, staging_;
   // Mixed-precision form: FP32 operator, preconditioner and inner-solve vectors.
-  DeviceArray<float> v32_, d32_, i32_, x32_, r32_, z32_, p032_, q32_;
+  DeviceArray<float> v32_, d32_, i32_, x32_, r32_, z32_, p032_, p132_, q32_;
   // Block-Jacobi inverses [n_pad * bs][KP] (FP64; FP32 for the mixed form's inner solve).
   DeviceArray<double> blocks64_;
   DeviceArray<float> blocks32_;
