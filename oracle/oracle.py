@@ -417,14 +417,18 @@ def ref_femm_nonlinear(stem, curve_directory):
     return handle, model, a, flux.value
 
 
-def ref_model_handle(model):
-    """A reference handle of an oracle model, block-label groups included."""
+def ref_model_handle(model, apex_nodes=()):
+    """A reference handle of an oracle model, block-label groups included; apex_nodes become
+    the model's symmetry_apex_nodes (physics/nonlinear_model.h:96)."""
     r = ref()
     view = ModelView(model)
     h = C.c_void_p()
     groups = np.ascontiguousarray(model.group, np.int32)
     if r.ref_model_handle(view.ref(), _p(groups), C.byref(h)):
         raise RuntimeError("reference model conversion failed")
+    apex = np.ascontiguousarray(np.asarray(apex_nodes, np.int32).ravel())
+    if apex.size:
+        r.ref_model_set_apex(h, C.c_int32(apex.size), _p(apex))
     return RefHandle(h)
 
 

@@ -402,6 +402,13 @@ int ref_model_handle(const or_model *m, const int32_t *groups, ref_artifact **ou
   return 0;
 }
 
+// NonlinearModel::symmetry_apex_nodes (physics/nonlinear_model.h:96) of a model handle: the
+// Dirichlet nodes the weighted-stress mask does not hold at 0 (weighted_stress.cu:80-84).
+void ref_model_set_apex(ref_artifact *h, int32_t count, const int32_t *nodes)
+{
+  h->artifact.model.symmetry_apex_nodes.assign(nodes, nodes + count);
+}
+
 // ReadNonlinearFemmReference (tests/native/reference.cpp:229-379): a FEMM .ans solution
 // with the fixture's hard-wired materials, as a model handle for ref_artifact_sizes / copy.
 int ref_read_femm_nonlinear(const char *stem, const char *curve_directory, ref_artifact **out)

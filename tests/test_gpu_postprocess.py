@@ -28,7 +28,7 @@ import oracle as O
 from conftest import GOLDEN, ROOT
 from femm_gpu_b200 import artifact, meshes
 from test_postprocess_host import (STEM, describe_femm, element_b, frozen_reference, model_from_description,
-                                   sector_model)
+                                   paired_mask_model, sector_model)
 
 pytestmark = pytest.mark.gpu
 CLI = os.path.join(ROOT, "femm-gpu_b200", "bin", "femm_gpu")
@@ -98,6 +98,25 @@ def test_periodic_sector_mask_on_gpu_equals_reference(gpu):
                                          max_mask_iterations=4096)
     assert st == 0 and np.array_equal(pp.mask(), ref_mask)
     assert np.array_equal(O.weighted_stress_mask(sec, 10, 0, by_group=True), ref_mask)
+
+
+@needs_ref
+def test_gpu_mask_with_apex_node_and_antiperiodic_pair_equals_reference(gpu):
+    """physics_regression.cu:225-251: the apex node's Dirichlet zero is no mask boundary and
+    the anti-periodic pair is tied with sign +1; without the apex entry both refuse alike."""
+    model, apex = paired_mask_model()
+    z_n, z_e = np.zeros(model.node_count), np.zeros(model.tri_count)
+    st, *_, ref_mask = O.ref_postprocess(O.ref_model_handle(model, apex_nodes=apex), z_n, z_e, z_e,
+                                         selected_label=1, air_label=0)
+    assert st == 0
+    plan = fg.Plan(model)
+    pp = fg.Postprocess(plan, selected_label=1, air_label=0, apex_nodes=apex)
+    got = pp.mask()
+    assert np.array_equal(got, ref_mask) and got[6] == got[8] and got[12] == 1.0
+    st_plain, *_ = O.ref_postprocess(O.ref_model_handle(model), z_n, z_e, z_e, selected_label=1, air_label=0)
+    with pytest.raises(fg.FgError) as e:
+        fg.Postprocess(plan, selected_label=1, air_label=0)
+    assert st_plain != 0 and e.value.status == st_plain
 
 
 def test_device_postprocess_matches_host_form(gpu):

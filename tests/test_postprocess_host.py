@@ -108,6 +108,49 @@ def test_numpy_mask_restatement_equals_reference_mask():
     assert 0 < mask.sum() < sec.node_count
 
 
+def paired_mask_model():
+    """The reference's paired-mask case (tests/native/physics_regression.cu:225-251 on
+    LargeStructuredMaskFixture(4), tests/native/fixtures.cpp:47-84): a 5 x 5 node grid, 1 m
+    cells, the selected label 1 on the one triangle (12, 13, 18), label 0 elsewhere (the
+    air), the outer ring held at 0, an anti-periodic pair 6 ~ 8 and node 12 Dirichlet too.
+    Returns (model, apex_nodes)."""
+    side = 5
+    xy = np.array([(x, y) for y in range(side) for x in range(side)], np.float64)
+    tri, mat = [], []
+    for y in range(side - 1):
+        for x in range(side - 1):
+            ll = y * side + x
+            lr, ul = ll + 1, ll + side
+            ur = ul + 1
+            tri += [(ll, lr, ur), (ll, ur, ul)]
+            mat += [1 if ll == 12 else 0, 0]
+    ring = [y * side + x for y in range(side) for x in range(side)
+            if x in (0, side - 1) or y in (0, side - 1)]
+    dirichlet = ring + [12]
+    nu = 1.0 / meshes.MU0
+    model = fg.Model(xy=xy, tri=tri, tri_mat=mat, nu0=[nu, nu], alpha=[0.0, 0.0], j_per_a=[0.0, 0.0],
+                     hc=[0.0, 0.0], mag_deg=[0.0, 0.0], curve_index=[-1, -1], circuit_index=[-1, -1],
+                     group=[0, 1], curves=[], dir_nodes=dirichlet, dir_values=np.zeros(len(dirichlet)),
+                     con_a=[6], con_b=[8], con_sign=[-1], circuit_count=1)
+    return model, [12]
+
+
+@needs_ref
+def test_mask_ignores_apex_zero_and_ties_periodic_pairs_like_the_reference():
+    model, apex = paired_mask_model()
+    st, *_, mask = O.ref_postprocess(O.ref_model_handle(model, apex_nodes=apex), np.zeros(25), np.zeros(32),
+                                     np.zeros(32), selected_label=1, air_label=0)
+    assert st == 0 and mask[6] == mask[8] and mask[12] == 1.0
+    assert np.array_equal(O.weighted_stress_mask(model, 1, 0, apex_nodes=apex), mask)
+    # without the apex entry node 12 is both Dirichlet 0 and selected 1: the reference refuses
+    st_plain, *_ = O.ref_postprocess(O.ref_model_handle(model), np.zeros(25), np.zeros(32), np.zeros(32),
+                                     selected_label=1, air_label=0)
+    assert st_plain != 0 and O.weighted_stress_mask(model, 1, 0) is None
+    with pytest.raises(fg.FgError) as e:  # refused before any GPU work
+        fg.Postprocess(fg.Plan(model, host_only=True), selected_label=1, air_label=0)
+    assert e.value.status == st_plain
+
+
 def sector_model(nr=48, nt=72):
     m = meshes.annular_sector(nr=nr, nt=nt)
     m.group = np.array([0, 10, 10, 3, 4, 5, 6], np.int32)
