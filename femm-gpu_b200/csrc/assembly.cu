@@ -223,6 +223,9 @@ __global__ void __launch_bounds__(kThreads)
       const double v = ev[((code >> 1) & 7) * stride + static_cast<size_t>(code >> 4) * KP + item];
       sum += (code & 1) ? -v : v;
     }
+    // The air-gap stiffness joins after every triangle, as the reference orders it.
+    if (p.age_val)
+      sum += p.age_val[s];
     val[(base + 32 * static_cast<size_t>(w)) * KP + item] = sum;
     if (p.columns[s] == r) {
       diag[static_cast<size_t>(r) * KP + item] = sum;
@@ -252,6 +255,8 @@ __global__ void __launch_bounds__(kThreads)
   if (!((active_mask >> item) & 1u))
     return;
   double sum = hc_scale ? p.pm_rhs[r] * hc_scale[item] : p.pm_rhs[r];
+  if (p.age_rhs)
+    sum += p.age_rhs[r];
   for (int c = 0; c < p.C; ++c)
     sum += currents[item * p.C + c] * p.circuit_rhs[static_cast<size_t>(c) * p.n + r];
   const size_t stride = static_cast<size_t>(p.E) * KP;

@@ -66,6 +66,25 @@ Status ToHostModel(const fg_model *m, fg::HostModel *out)
   }
   h.circuit_count = m->circuit_count;
   h.depth_m = m->depth_m;
+  if (m->air_gap_count < 0 || (m->air_gap_count > 0 && !m->air_gap_elements))
+    return Status::kInvalidArgument;
+  for (int i = 0; i < m->air_gap_count; ++i) {
+    const fg_air_gap_element &src = m->air_gap_elements[i];
+    if (src.point_count < 0 || (src.point_count > 0 && (!src.nodes || !src.weights)))
+      return Status::kInvalidArgument;
+    fg::AirGap g;
+    g.antiperiodic = src.antiperiodic != 0;
+    g.cx = src.center_x_m;
+    g.cy = src.center_y_m;
+    g.ri = src.inner_radius_m;
+    g.ro = src.outer_radius_m;
+    g.arc_deg = src.arc_length_deg;
+    g.inner_shift = src.inner_shift;
+    g.outer_shift = src.outer_shift;
+    g.node.assign(src.nodes, src.nodes + 4 * static_cast<size_t>(src.point_count));
+    g.weight.assign(src.weights, src.weights + 4 * static_cast<size_t>(src.point_count));
+    h.ages.push_back(std::move(g));
+  }
   *out = std::move(h);
   return Status::kOk;
 }
@@ -165,6 +184,26 @@ int fg_plan_contributors(const fg_plan *plan, int32_t *slot_offsets, int32_t *sl
     std::copy(h.pm_rhs.begin(), h.pm_rhs.end(), pm_rhs);
   if (circuit_rhs)
     std::copy(h.circuit_rhs.begin(), h.circuit_rhs.end(), circuit_rhs);
+  return 0;
+}
+
+int fg_plan_air_gap(const fg_plan *plan, double *values, double *rhs)
+{
+  if (!plan)
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostPlan &h = plan->plan.host();
+  if (values) {
+    if (h.age_val.empty())
+      std::fill(values, values + h.nnz, 0.0);
+    else
+      std::copy(h.age_val.begin(), h.age_val.end(), values);
+  }
+  if (rhs) {
+    if (h.age_rhs.empty())
+      std::fill(rhs, rhs + h.n, 0.0);
+    else
+      std::copy(h.age_rhs.begin(), h.age_rhs.end(), rhs);
+  }
   return 0;
 }
 

@@ -20,6 +20,7 @@ struct DevicePlan {
   const int32_t *row_offsets, *columns, *row_len, *slice_off, *sell_col;
   const int32_t *contrib_off, *contrib, *rhs_off, *rhs_contrib;
   const double *pm_rhs, *circuit_rhs;
+  const double *age_val, *age_rhs; // air-gap stiffness [nnz] and load [n]; null without
   const int32_t *elem_nodes, *elem_mat;
   const double *elem_geo;
   const double *mat_nu0, *mat_alpha, *mat_cold, *mat_jpa;

@@ -269,6 +269,20 @@ Status ValidateModel(const HostModel &m)
     if (!ElementTerms(p0, p1, p2, &area, bx, by))
       return Status::kMeshInvalid;
   }
+  for (const AirGap &g : m.ages) {
+    if (m.problem_type != 0)
+      return Status::kUnsupportedFeature;
+    if (g.points() < 3 || g.weight.size() != g.node.size() || g.node.size() % 4 != 0 || !(g.ri > 0.0) ||
+        !(g.ro > g.ri) || !(g.arc_deg > 0.0) || !std::isfinite(g.cx) || !std::isfinite(g.cy) ||
+        !std::isfinite(g.inner_shift) || !std::isfinite(g.outer_shift))
+      return Status::kMeshInvalid;
+    for (size_t l = 0; l < g.node.size(); ++l)
+      if (g.node[l] < 0 || g.node[l] >= N || !std::isfinite(g.weight[l]))
+        return Status::kMeshInvalid;
+    const double dt = g.arc_deg / static_cast<double>(g.arcs());
+    if (!(dt > 0.0) || !std::isfinite(dt))
+      return Status::kMeshInvalid;
+  }
   SignedDofs dofs;
   if (BuildSignedDofs(m, &dofs) != 0 || dofs.free_roots.empty())
     return Status::kBoundaryInvalid;
@@ -399,6 +413,23 @@ Status BuildHostPlan(const HostModel &m, HostPlan *plan)
         if (n2f[m.tri[3 * e + j]] >= 0)
           ++cand_off[r + 1];
     }
+  // Air-gap couples: every (free, free) pair of each arc's ten-node stencil.
+  auto for_each_age_entry = [&m](auto &&visit) {
+    for (const AirGap &g : m.ages)
+      for (int32_t k = 0; k < g.arcs(); ++k) {
+        int32_t node[10];
+        double weight[10];
+        AirGapStencil(g, k, node, weight);
+        for (int i = 0; i < 10; ++i)
+          for (int j = 0; j < 10; ++j)
+            visit(g, k, i, j, node, weight);
+      }
+  };
+  for_each_age_entry([&](const AirGap &, int32_t, int i, int j, const int32_t *node, const double *) {
+    const int32_t r = n2f[node[i]];
+    if (r >= 0 && n2f[node[j]] >= 0)
+      ++cand_off[r + 1];
+  });
   for (int32_t r = 0; r < n; ++r)
     cand_off[r + 1] += cand_off[r];
   std::vector<int32_t> cand(cand_off[n]), cfill(cand_off.begin(), cand_off.end() - 1);
@@ -413,6 +444,11 @@ Status BuildHostPlan(const HostModel &m, HostPlan *plan)
           cand[cfill[r]++] = c;
       }
     }
+  for_each_age_entry([&](const AirGap &, int32_t, int i, int j, const int32_t *node, const double *) {
+    const int32_t r = n2f[node[i]], c = n2f[node[j]];
+    if (r >= 0 && c >= 0)
+      cand[cfill[r]++] = c;
+  });
   p.row_offsets.assign(n + 1, 0);
   p.diag_slot.assign(n, -1);
   for (int32_t r = 0; r < n; ++r) {
@@ -551,6 +587,35 @@ Status BuildHostPlan(const HostModel &m, HostPlan *plan)
       if (mt.circuit >= 0)
         p.circuit_rhs[static_cast<size_t>(mt.circuit) * n + r] += static_cast<double>(sgn[tn[i]]) * coil[i];
     }
+  }
+
+  // Air-gap stiffness (relative-reluctivity element matrix times 1/mu0) and the load of
+  // its fixed nodes, in band / arc / i / j order.
+  if (!m.ages.empty()) {
+    p.age_val.assign(p.nnz, 0.0);
+    p.age_rhs.assign(n, 0.0);
+    const std::vector<double> &fixed = p.dofs.boundary;
+    double mg[10][10];
+    const AirGap *current = nullptr;
+    bool ok = true;
+    for_each_age_entry([&](const AirGap &g, int32_t, int i, int j, const int32_t *node,
+                           const double *weight) {
+      if (current != &g) {
+        const AirGapTerms t = AirGapBandTerms(g);
+        ok = ok && AirGapElementMatrix(t.K, t.Ki, t.ci, t.co, mg);
+        current = &g;
+      }
+      if (!ok)
+        return;
+      const double value = mg[i][j] * weight[i] * weight[j] * (1.0 / kMu0);
+      const int32_t r = n2f[node[i]], c = n2f[node[j]];
+      if (r >= 0 && c >= 0)
+        p.age_val[find_slot(r, c)] += static_cast<double>(sgn[node[i]] * sgn[node[j]]) * value;
+      else if (r >= 0)
+        p.age_rhs[r] -= static_cast<double>(sgn[node[i]]) * value * fixed[node[j]];
+    });
+    if (!ok)
+      return Status::kMeshInvalid;
   }
 
   // SELL-32 layout of the symbolic pattern.

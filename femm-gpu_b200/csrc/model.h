@@ -2,6 +2,7 @@
 // device assembly plan topology.
 #pragma once
 
+#include "air_gap.h"
 #include "common.h"
 
 #include <cstdint>
@@ -39,6 +40,7 @@ struct HostModel {
   std::vector<int8_t> con_sign;
   int32_t circuit_count = 1;
   double depth_m = 0.0;
+  std::vector<AirGap> ages; // native air-gap elements (planar only)
 
   int32_t nodes() const { return static_cast<int32_t>(xy.size() / 2); }
   int32_t triangles() const { return static_cast<int32_t>(tri_mat.size()); }
@@ -54,7 +56,7 @@ void EvaluateBh(const BhCurve &curve, double field_b, double out[4]);
 bool ElementTerms(const double *p0, const double *p1, const double *p2, double *area,
                   double bx[3], double by[3]);
 
-// ValidateNonlinearModel (nonlinear_model.cpp:223-319), air-gap elements excluded.
+// ValidateNonlinearModel (nonlinear_model.cpp:223-319).
 Status ValidateModel(const HostModel &model);
 
 // Signed DOF map (signed_node_constraints.h:33-106).
@@ -83,6 +85,11 @@ struct HostPlan {
   std::vector<int32_t> rhs_off, rhs_contrib;
   std::vector<double> pm_rhs;      // [n]
   std::vector<double> circuit_rhs; // [C * n]
+  // Air-gap elements: their fixed stiffness per CSR slot and the load their fixed nodes put
+  // on free rows, each summed in band / arc / i / j order (nonlinear_topology.cpp:180-232);
+  // empty without air-gap elements.
+  std::vector<double> age_val;     // [nnz]
+  std::vector<double> age_rhs;     // [n]
   // Element data: node ids, material, planar area and curl basis.
   std::vector<int32_t> elem_nodes; // [3E]
   std::vector<int32_t> elem_mat;   // [E]

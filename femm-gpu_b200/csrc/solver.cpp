@@ -162,6 +162,10 @@ Status Plan::Upload()
   FG_UP(curve_h_, h.curve_h);
   FG_UP(curve_slope_, h.curve_slope);
   FG_UP(boundary_, h.dofs.boundary);
+  if (!h.age_val.empty()) {
+    FG_UP(age_val_, h.age_val);
+    FG_UP(age_rhs_, h.age_rhs);
+  }
 #undef FG_UP
   if (s != Status::kOk)
     return s;
@@ -188,6 +192,8 @@ Status Plan::Upload()
   d.rhs_contrib = rhs_contrib_.get();
   d.pm_rhs = pm_rhs_.get();
   d.circuit_rhs = circuit_rhs_.get();
+  d.age_val = h.age_val.empty() ? nullptr : age_val_.get();
+  d.age_rhs = h.age_val.empty() ? nullptr : age_rhs_.get();
   d.elem_nodes = elem_nodes_.get();
   d.elem_mat = elem_mat_.get();
   d.elem_geo = elem_geo_.get();

@@ -128,6 +128,7 @@ private:
       contrib_, rhs_off_, rhs_contrib_, elem_nodes_, elem_mat_, mat_curve_off_, mat_curve_cnt_,
       mat_circuit_, node_to_free_, free_roots_, circuit_elem_off_, circuit_elems_;
   DeviceArray<int8_t> node_sign_;
+  DeviceArray<double> age_val_, age_rhs_; // allocated only with air-gap elements
   DeviceArray<double> pm_rhs_, circuit_rhs_, elem_geo_, mat_nu0_, mat_alpha_, mat_cold_, mat_jpa_,
       curve_b_, curve_h_, curve_slope_, boundary_;
   // Batch workspace.

@@ -8,8 +8,8 @@
 from . import meshes
 from .capi import (Plan, Multi, Postprocess, SolveResult, FgError, csr_pcg, lib, production_options,
                    status_name, bh_build, bh_eval, LIB_PATH, STATUS_NAMES, EXPORTED)
-from .model import AXISYMMETRIC, MU0, PLANAR, Model
+from .model import AXISYMMETRIC, MU0, PLANAR, AirGap, Model
 
-__all__ = ["Model", "Plan", "Multi", "Postprocess", "SolveResult", "FgError", "csr_pcg", "lib",
+__all__ = ["Model", "AirGap", "Plan", "Multi", "Postprocess", "SolveResult", "FgError", "csr_pcg", "lib",
            "production_options", "status_name", "bh_build", "bh_eval", "meshes", "LIB_PATH", "STATUS_NAMES", "EXPORTED",
            "PLANAR", "AXISYMMETRIC", "MU0"]

@@ -37,7 +37,7 @@ EXPORTED = [
     "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
     "fg_plan_destroy", "fg_plan_sizes_get", "fg_plan_symbolic", "fg_assemble", "fg_pcg_solve",
     "fg_csr_pcg", "fg_solve_batch", "fg_solve_batch_device", "fg_plan_last_timing",
-    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_csr_pcg_noalloc",
+    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_plan_air_gap", "fg_csr_pcg_noalloc",
     "fg_mlp_create", "fg_mlp_destroy", "fg_mlp_parameter_count", "fg_mlp_get_parameters",
     "fg_mlp_set_parameters", "fg_mlp_forward", "fg_mlp_loss_gradient", "fg_mlp_train",
     "fg_warm_create", "fg_warm_destroy", "fg_warm_project", "fg_warm_project_device",
@@ -71,7 +71,30 @@ class FgModel(C.Structure):
         ("dirichlet_values", C.c_void_p), ("constraint_count", C.c_int32),
         ("constraint_nodes", C.c_void_p), ("constraint_signs", C.c_void_p),
         ("circuit_count", C.c_int32), ("depth_m", C.c_double),
+        ("air_gap_count", C.c_int32), ("air_gap_elements", C.c_void_p),
     ]
+
+
+class FgAirGap(C.Structure):
+    _fields_ = [
+        ("antiperiodic", C.c_int32), ("point_count", C.c_int32), ("center_x_m", C.c_double),
+        ("center_y_m", C.c_double), ("inner_radius_m", C.c_double), ("outer_radius_m", C.c_double),
+        ("arc_length_deg", C.c_double), ("inner_shift", C.c_double), ("outer_shift", C.c_double),
+        ("nodes", C.c_void_p), ("weights", C.c_void_p),
+    ]
+
+
+def air_gap_array(ages):
+    """ctypes fg_air_gap_element[] of Model.ages (None when there are none)."""
+    if not ages:
+        return None
+    arr = (FgAirGap * len(ages))()
+    for i, g in enumerate(ages):
+        arr[i] = FgAirGap(int(bool(g.antiperiodic)), int(g.nodes.shape[0]), float(g.center_m[0]),
+                          float(g.center_m[1]), float(g.inner_radius_m), float(g.outer_radius_m),
+                          float(g.arc_length_deg), float(g.inner_shift), float(g.outer_shift),
+                          _p(g.nodes), _p(g.weights))
+    return arr
 
 
 class FgPlanOptions(C.Structure):
@@ -202,6 +225,10 @@ class Plan:
             constraint_count=int(model.con_a.size), constraint_nodes=_p(con),
             constraint_signs=_p(model.con_sign), circuit_count=model.circuit_count,
             depth_m=model.depth_m)
+        ages = air_gap_array(model.ages)
+        if ages is not None:
+            self._keep.append(ages)
+            fm.air_gap_count, fm.air_gap_elements = len(model.ages), C.cast(ages, C.c_void_p)
         flags = (PLAN_HOST_ONLY if host_only else 0) | (PLAN_PCG_FROM_ITERATE if from_iterate else 0)
         opts = FgPlanOptions(preconditioner, block_size, precision, flags)
         self._h = C.c_void_p()
@@ -250,6 +277,14 @@ class Plan:
         cr = np.zeros(max(self.C, 1) * self.rows)
         lib().fg_plan_contributors(self._h, _p(so), _p(se), _p(ro), _p(re), _p(pm), _p(cr))
         return so, se, ro, re, pm, cr[: self.C * self.rows].reshape(self.C, self.rows)
+
+    def air_gap(self):
+        """The fixed air-gap element terms: stiffness per CSR slot [nnz], load per row [rows]."""
+        vals, rhs = np.zeros(self.nnz), np.zeros(self.rows)
+        st = lib().fg_plan_air_gap(self._h, _p(vals), _p(rhs))
+        if st:
+            raise FgError(st, "fg_plan_air_gap")
+        return vals, rhs
 
     def assemble(self, states, currents, use_newton):
         states = np.ascontiguousarray(np.atleast_2d(states), np.float64)

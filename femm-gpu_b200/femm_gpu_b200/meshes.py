@@ -25,7 +25,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from .model import AXISYMMETRIC, MU0, PLANAR, Model
+from .model import AXISYMMETRIC, MU0, PLANAR, AirGap, Model
 
 SIDE_M = 0.1
 
@@ -382,4 +382,94 @@ def two_pole_machine(nr: int = 160, nt: int = 120, full: bool = False, hc: float
         con_sign=np.zeros(0, np.int8) if full else np.full(left.size, -1, np.int8),
         circuit_count=3, depth_m=0.05, problem_type=PLANAR,
         name=f"two_pole_{'full' if full else 'sector'}_{nr}x{nt}",
+    )
+
+
+def sliding_band_machine(nr: int = 160, nt: int = 120, rotor_deg: float = 0.0, hc: float = 9.0e5,
+                         turns: float = 20.0) -> Model:
+    """The full two-pole machine of ``two_pole_machine(full=True)`` with its 1 mm air gap
+    [0.045, 0.046] m left untriangulated and spanned by one periodic native air-gap
+    element (FEMM's AGE).  The rotor (r <= 0.045, iron, magnets and the air between them)
+    and the stator (r >= 0.046) are meshed separately on polar grids of the same radial
+    step 0.04 / ``nr`` and 2 ``nt`` uniform columns; the rotor mesh, magnets included, is
+    turned by ``rotor_deg``.  The band's records follow FEMM's preprocessor: each ring
+    sorted by angle in [0, 360), point p bracketed by ring entries p - 1 and p (weights +1),
+    and each ring's shift = the angle of its first entry in units of one column.  Groups:
+    air 50, rotor 20, stator 30, slots 40-42.  A = 0 on the outer radius."""
+    h = 0.04 / nr
+    rows_r, rows_s = int(round(0.025 / h)), int(round(0.014 / h))
+    if abs(rows_r * h - 0.025) > 1e-12 or abs(rows_s * h - 0.014) > 1e-12:
+        raise ValueError("nr must put the gap radii 0.045 and 0.046 m on grid rows")
+    cols = 2 * nt
+    dt = 360.0 / cols
+    rot = np.radians(rotor_deg)
+
+    def polar(r_in, r_out, rows, turn):
+        rs = np.linspace(r_in, r_out, rows + 1)
+        ts = np.radians(np.arange(cols) * dt) + turn
+        T, R = np.meshgrid(ts, rs)
+        xy = np.stack([(R * np.cos(T)).ravel(), (R * np.sin(T)).ravel()], axis=1)
+        i, j = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+        a = (i * cols + j).ravel()
+        b = (i * cols + (j + 1) % cols).ravel()
+        c = a + cols
+        d = b + cols
+        tri = np.empty((2 * a.size, 3), np.int64)
+        tri[0::2] = np.stack([a, c, d], axis=1)
+        tri[1::2] = np.stack([a, d, b], axis=1)
+        return xy, tri
+
+    xy_r, tri_r = polar(0.02, 0.045, rows_r, rot)
+    xy_s, tri_s = polar(0.046, 0.06, rows_s, 0.0)
+    off = xy_r.shape[0]
+    xy = np.concatenate([xy_r, xy_s])
+    tri = np.concatenate([tri_r, tri_s + off]).astype(np.int32)
+    cen = xy[tri].mean(axis=1)
+    rc = np.hypot(cen[:, 0], cen[:, 1])
+    tc = np.degrees(np.arctan2(cen[:, 1], cen[:, 0]))
+    rotor = np.arange(tri.shape[0]) < tri_r.shape[0]
+    body = np.where(rotor, tc - rotor_deg, tc) % 360.0  # rotor parts move with the rotor
+    upper = body < 180.0
+    tl = np.where(upper, body, body - 180.0)
+    mat = np.zeros(tri.shape[0], np.int32)
+    mat[rotor & (rc < 0.043)] = 1
+    mat[rotor & (rc >= 0.043) & (np.abs(tl - 90.0) <= 60.0)] = 2
+    stator = ~rotor
+    mat[stator] = 3
+    for k, centre in enumerate((30.0, 90.0, 150.0)):
+        slot = stator & (rc < 0.050) & (np.abs(tl - centre) <= 10.0)
+        mat[slot & upper] = 4 + k
+        mat[slot & ~upper] = 7 + k
+    area = 0.5 * _signed_area2(xy, tri)
+    jpa = [turns / area[mat == 4 + k].sum() for k in range(3)]
+    nu_air = 1.0 / MU0
+    b_t, hh = bh_table_saturating(24)
+    outer = (off + rows_s * cols + np.arange(cols)).astype(np.int32)
+
+    def ring(first, shift_deg):
+        ang = (np.arange(cols) * dt + shift_deg) % 360.0
+        order = np.argsort(ang, kind="stable")
+        return first + order, ang[order[0]] / dt
+
+    inner_nodes, inner_shift = ring(rows_r * cols, rotor_deg)
+    outer_nodes, outer_shift = ring(off, 0.0)
+    p = np.arange(cols + 1)
+    p1, p0 = p % cols, (p - 1) % cols
+    nodes = np.stack([inner_nodes[p0], inner_nodes[p1], outer_nodes[p0], outer_nodes[p1]], axis=1)
+    band = AirGap(nodes=nodes, weights=np.ones(nodes.shape), inner_radius_m=0.045, outer_radius_m=0.046,
+                  arc_length_deg=360.0, inner_shift=float(inner_shift), outer_shift=float(outer_shift))
+    return Model(
+        xy=xy, tri=tri, tri_mat=mat,
+        nu0=[nu_air, nu_air, nu_air / 1.05, nu_air] + [nu_air] * 6,
+        alpha=np.zeros(10),
+        j_per_a=[0.0, 0.0, 0.0, 0.0] + jpa + [-v for v in jpa],
+        hc=[0.0, 0.0, hc] + [0.0] * 7,
+        mag_deg=[0.0, 0.0, 90.0 + rotor_deg] + [0.0] * 7,
+        curve_index=[-1, 0, -1, 0] + [-1] * 6,
+        circuit_index=[-1, -1, -1, -1, 0, 1, 2, 0, 1, 2],
+        group=[50, 20, 20, 30, 40, 41, 42, 40, 41, 42],
+        curves=[(b_t, hh)],
+        dir_nodes=outer, dir_values=np.zeros(outer.size),
+        circuit_count=3, depth_m=0.05, problem_type=PLANAR,
+        name=f"sliding_band_{nr}x{nt}_{rotor_deg:g}deg", ages=[band],
     )

@@ -21,6 +21,27 @@ AXISYMMETRIC = 1
 
 
 @dataclass
+class AirGap:
+    """FEMM's native air-gap element (fg_air_gap_element): an untriangulated annular band.
+    nodes / weights [points, 4]: per band point the inner-ring nodes n0, n1 bracketing it
+    and the outer-ring ones n2, n3, each weight the +1 / -1 sign of the ring copy;
+    inner_shift / outer_shift place each ring's first node in units of one arc."""
+    nodes: np.ndarray
+    weights: np.ndarray
+    inner_radius_m: float
+    outer_radius_m: float
+    arc_length_deg: float
+    inner_shift: float = 0.0
+    outer_shift: float = 0.0
+    antiperiodic: bool = False
+    center_m: Tuple[float, float] = (0.0, 0.0)
+
+    def __post_init__(self):
+        self.nodes = np.ascontiguousarray(self.nodes, dtype=np.int32).reshape(-1, 4)
+        self.weights = np.ascontiguousarray(self.weights, dtype=np.float64).reshape(-1, 4)
+
+
+@dataclass
 class Model:
     xy: np.ndarray  # [N, 2] float64, metres (x, y) or (r, z)
     tri: np.ndarray  # [E, 3] int32, CCW
@@ -43,6 +64,7 @@ class Model:
     depth_m: float = 1.0
     problem_type: int = PLANAR
     name: str = "model"
+    ages: List[AirGap] = field(default_factory=list)
 
     def __post_init__(self):
         self.xy = np.ascontiguousarray(self.xy, dtype=np.float64).reshape(-1, 2)

@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define FG_ABI_VERSION 1
+#define FG_ABI_VERSION 2
 
 /* Status codes (gpu_solver/src/core/types.h:11-28). */
 enum {
@@ -69,6 +69,24 @@ typedef struct fg_bh_curve {
   const double *h_a_per_m;
 } fg_bh_curve;
 
+/* FEMM's native air-gap element (AirGapElement, gpu_solver/src/physics/nonlinear_model.h:
+ * 63-81): an annular air band ri < r < ro that is not triangulated.  The band is split
+ * into point_count - 1 equal arcs over arc_length_deg; each point carries four (node,
+ * weight) pairs -- n0 / n1 the inner-ring nodes that bracket it, n2 / n3 the outer-ring
+ * ones, each weight the +1 / -1 sign of the ring copy the node comes from.  inner_shift /
+ * outer_shift place the first ring node of each side, in units of one arc.  The band adds
+ * a fixed linear stiffness (planar models only). */
+typedef struct fg_air_gap_element {
+  int32_t antiperiodic;     /* 0 periodic, 1 anti-periodic closure of the band */
+  int32_t point_count;      /* arcs + 1, at least 3 */
+  double center_x_m, center_y_m;
+  double inner_radius_m, outer_radius_m;
+  double arc_length_deg;    /* angle the band spans */
+  double inner_shift, outer_shift;
+  const int32_t *nodes;     /* [4 * point_count]: n0, n1, n2, n3 per point */
+  const double *weights;    /* [4 * point_count]: w0, w1, w2, w3 per point */
+} fg_air_gap_element;
+
 /* The model (NonlinearModel, gpu_solver/src/physics/nonlinear_model.h:83-100). */
 typedef struct fg_model {
   int32_t problem_type; /* FG_PLANAR or FG_AXISYMMETRIC (x = r, y = z) */
@@ -89,6 +107,9 @@ typedef struct fg_model {
   const int8_t *constraint_signs;  /* [constraint_count], +1 periodic / -1 anti-periodic */
   int32_t circuit_count;
   double depth_m;
+  /* Appended in ABI version 2; zero them (or zero-initialise the struct) for none. */
+  int32_t air_gap_count;
+  const fg_air_gap_element *air_gap_elements;
 } fg_model;
 
 typedef struct fg_plan_options {
@@ -204,6 +225,12 @@ int fg_plan_symbolic(const fg_plan *plan, int32_t *row_offsets, int32_t *columns
 int fg_plan_contributors(const fg_plan *plan, int32_t *slot_offsets, int32_t *slot_entries,
                          int32_t *row_offsets, int32_t *row_entries, double *pm_rhs,
                          double *circuit_rhs);
+
+/* The fixed air-gap element terms of the plan (PreparedNonlinearAssembly::age_values /
+ * age_rhs, nonlinear_topology.cpp:180-262): values [nnz] the band stiffness per CSR slot,
+ * rhs [rows] the load that fixed ring nodes put on free rows.  Zeros when the model has no
+ * air-gap element.  Either pointer may be NULL. */
+int fg_plan_air_gap(const fg_plan *plan, double *values, double *rhs);
 
 /* Device Newton assembly at given nodal states (DeviceNonlinearAssemblyPlan::Assemble,
  * nonlinear_assembly.cu:229-309).  states [items * N]; currents [items * C];

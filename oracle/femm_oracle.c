@@ -398,6 +398,8 @@ int or_validate(const or_model *m)
       (m->problem_type == 0 && (!(m->depth_m > 0.0) || !isfinite(m->depth_m))) ||
       m->circuit_count < 0 || m->dir_count <= 0)
     return OR_INVALID_ARGUMENT;
+  if (m->age_count != 0)
+    return OR_UNSUPPORTED; /* air-gap elements: checked against the reference build only */
   char *bnd = calloc((size_t)m->node_count, 1);
   for (int i = 0; i < m->dir_count; ++i) {
     const int node = m->dir_nodes[i];

@@ -39,6 +39,17 @@ typedef struct {
   int32_t smoothing_passes;
 } or_curve;
 
+/* A native air-gap element, laid out as fg_air_gap_element.  The restatement does not
+ * assemble these (models carrying them are refused with OR_UNSUPPORTED); the
+ * reference build (ref_driver.cpp) maps them onto AirGapElement. */
+typedef struct {
+  int32_t antiperiodic, point_count;
+  double center_x_m, center_y_m, inner_radius_m, outer_radius_m, arc_length_deg;
+  double inner_shift, outer_shift;
+  const int32_t *nodes;  /* [4 * point_count] */
+  const double *weights; /* [4 * point_count] */
+} or_air_gap;
+
 typedef struct {
   int32_t problem_type; /* 0 planar, 1 axisymmetric (x = r, y = z) */
   int32_t node_count;
@@ -60,6 +71,8 @@ typedef struct {
   const int8_t *con_sign;
   int32_t circuit_count;
   double depth_m;
+  int32_t age_count;
+  const or_air_gap *ages;
 } or_model;
 
 typedef struct {

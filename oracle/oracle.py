@@ -34,7 +34,16 @@ class OrModel(C.Structure):
         ("curve_h", C.c_void_p), ("dir_count", C.c_int32), ("dir_nodes", C.c_void_p),
         ("dir_values", C.c_void_p), ("con_count", C.c_int32), ("con_a", C.c_void_p),
         ("con_b", C.c_void_p), ("con_sign", C.c_void_p), ("circuit_count", C.c_int32),
-        ("depth_m", C.c_double),
+        ("depth_m", C.c_double), ("age_count", C.c_int32), ("ages", C.c_void_p),
+    ]
+
+
+class OrAirGap(C.Structure):
+    _fields_ = [
+        ("antiperiodic", C.c_int32), ("point_count", C.c_int32), ("center_x_m", C.c_double),
+        ("center_y_m", C.c_double), ("inner_radius_m", C.c_double), ("outer_radius_m", C.c_double),
+        ("arc_length_deg", C.c_double), ("inner_shift", C.c_double), ("outer_shift", C.c_double),
+        ("nodes", C.c_void_p), ("weights", C.c_void_p),
     ]
 
 
@@ -117,6 +126,16 @@ class ModelView:
             dir_values=_p(model.dir_values), con_count=int(model.con_a.size),
             con_a=_p(model.con_a), con_b=_p(model.con_b), con_sign=_p(model.con_sign),
             circuit_count=model.circuit_count, depth_m=model.depth_m)
+        ages = getattr(model, "ages", None) or []
+        if ages:
+            arr = (OrAirGap * len(ages))()
+            for i, g in enumerate(ages):
+                arr[i] = OrAirGap(int(bool(g.antiperiodic)), int(g.nodes.shape[0]), float(g.center_m[0]),
+                                  float(g.center_m[1]), float(g.inner_radius_m), float(g.outer_radius_m),
+                                  float(g.arc_length_deg), float(g.inner_shift), float(g.outer_shift),
+                                  _p(g.nodes), _p(g.weights))
+            self.keep.append(arr)
+            self.s.age_count, self.s.ages = len(ages), C.cast(arr, C.c_void_p)
 
     def ref(self):
         return C.byref(self.s)
@@ -602,3 +621,41 @@ def ref_tangent_postprocess(handle, a, b1, b2, da, db1, db2, mask, selected_labe
     st = r.ref_tangent_postprocess(handle.h, *[_p(x) for x in arrs[:6]], _p(labels), C.c_double(radius_m),
                                    C.c_int32(angles.size), _p(angles), _p(arrs[6]), _p(out3), _p(radial))
     return int(st), out3[0], out3[1], out3[2], radial[:angles.size]
+
+
+def age_matrix(K, Ki, ci, co):
+    """Numpy restatement of FEMM's native air-gap element matrix (BuildNativeFemmAirGapMatrix,
+    native_airgap_matrix.cpp:5-22, its expanded polynomials from fkn/prob1big.cpp:158-213)
+    as T^T Q T: corner values by Catmull-Rom interpolation of four ring nodes at t = 1 - c,
+    Q the four-corner form K (5a^2 + 2ab + 5b^2)/12 + Ki (5a'^2 + 2a'b' + 5b'^2)/12."""
+    def cr(t):
+        return np.array([0.5 * (-t ** 3 + 2 * t ** 2 - t), 0.5 * (3 * t ** 3 - 5 * t ** 2 + 2),
+                         0.5 * (-3 * t ** 3 + 4 * t ** 2 + t), 0.5 * (t ** 3 - t ** 2)])
+    T = np.zeros((4, 10))
+    wi, wo = cr(1.0 - ci), cr(1.0 - co)
+    T[0, 0:4], T[1, 1:5], T[2, 5:9], T[3, 6:10] = wi, wi, wo, wo
+    d, al, ac, dg = 5 * (K + Ki), Ki - 5 * K, K - 5 * Ki, -(K + Ki)
+    Q = np.array([[d, al, ac, dg], [al, d, dg, ac], [ac, dg, d, al], [dg, ac, al, d]]) / 12.0
+    return T.T @ Q @ T
+
+
+def ref_age_matrix(K, Ki, ci, co):
+    """The reference's BuildNativeFemmAirGapMatrix (oracle/_ref), or None if it refuses."""
+    out = np.zeros(100)
+    if ref().ref_age_matrix(C.c_double(K), C.c_double(Ki), C.c_double(ci), C.c_double(co), _p(out)):
+        return None
+    return out.reshape(10, 10)
+
+
+def ref_prepared_age(model):
+    """PreparedNonlinearAssembly's (status, age_values [nnz], age_rhs [rows]) of a model."""
+    r = ref()
+    view = ModelView(model)
+    h = C.c_void_p()
+    st = r.ref_prepare(view.ref(), C.byref(h))
+    if st:
+        return st, None, None
+    vals, rhs = np.zeros(r.ref_prepared_nnz(h)), np.zeros(r.ref_prepared_rows(h))
+    r.ref_prepared_age(h, _p(vals), _p(rhs))
+    r.ref_prepared_free(h)
+    return 0, vals, rhs

@@ -34,56 +34,12 @@ using namespace gpu_femm;
 extern "C" {
 int ref_validate(const or_model *m);
 }
+bool RefModelFromOracle(const or_model *m, NonlinearModel *out); // ref_driver.cpp
 
 namespace
 {
 
-bool BuildModel(const or_model *m, NonlinearModel *out)
-{
-  NonlinearModel model;
-  model.problem_type =
-      m->problem_type == 1 ? MagneticProblemType::kAxisymmetric : MagneticProblemType::kPlanar;
-  model.depth_m = m->depth_m;
-  model.circuit_count = m->circuit_count;
-  for (int i = 0; i < m->node_count; ++i)
-    model.nodes.push_back({m->xy[2 * i], m->xy[2 * i + 1]});
-  for (int c = 0; c < m->curve_count; ++c) {
-    NonlinearBhCurve curve;
-    for (int k = m->curve_offsets[c]; k < m->curve_offsets[c + 1]; ++k) {
-      curve.b_t.push_back(m->curve_b[k]);
-      curve.h_a_per_m.push_back(m->curve_h[k]);
-    }
-    if (!BuildNonlinearBhSpline(&curve))
-      return false;
-    model.bh_curves.push_back(curve);
-  }
-  for (int i = 0; i < m->mat_count; ++i) {
-    NonlinearMaterial material;
-    material.reluctivity_zero_m_per_h = m->nu0[i];
-    material.alpha_per_t2 = m->alpha[i];
-    material.source_j_per_a = m->j_per_a[i];
-    material.h_c_a_per_m = m->hc[i];
-    material.magnetization_deg = m->mag_deg[i];
-    material.bh_curve_index = m->curve_index[i];
-    material.circuit_index = m->circuit_index[i];
-    model.materials.push_back(material);
-  }
-  for (int e = 0; e < m->tri_count; ++e)
-    model.triangles.push_back({{m->tri[3 * e], m->tri[3 * e + 1], m->tri[3 * e + 2]}, m->tri_mat[e]});
-  for (int i = 0; i < m->dir_count; ++i) {
-    model.dirichlet_nodes.push_back(m->dir_nodes[i]);
-    model.dirichlet_a_wb_per_m.push_back(m->dir_values[i]);
-  }
-  for (int i = 0; i < m->con_count; ++i) {
-    SignedNodeConstraint constraint;
-    constraint.node_a = m->con_a[i];
-    constraint.node_b = m->con_b[i];
-    constraint.sign = m->con_sign[i];
-    model.node_constraints.push_back(constraint);
-  }
-  *out = std::move(model);
-  return true;
-}
+bool BuildModel(const or_model *m, NonlinearModel *out) { return RefModelFromOracle(m, out); }
 
 double TrueResidual(const Assembly &a, const std::vector<double> &rhs, const double *x)
 {

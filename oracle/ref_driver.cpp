@@ -29,10 +29,9 @@
 
 using namespace gpu_femm;
 
-// The native air-gap element matrix comes from code the reference generates at
-// build time from FEMM's fkn sources.  No model built by these tests carries an
-// air-gap element, so this definition only reports "unsupported".
-bool BuildNativeFemmAirGapMatrix(double, double, double, double, double[10][10]) { return false; }
+// FEMM's native air-gap element matrix (native_airgap_matrix.cpp, its body cut from
+// fkn/prob1big.cpp by the Makefile as the reference's own build does).
+bool BuildNativeFemmAirGapMatrix(double K, double Ki, double ci, double co, double matrix[10][10]);
 
 namespace
 {
@@ -80,11 +79,35 @@ bool ToModel(const or_model *m, NonlinearModel *out)
     constraint.sign = m->con_sign[i];
     model.node_constraints.push_back(constraint);
   }
+  for (int i = 0; i < m->age_count; ++i) {
+    const or_air_gap &src = m->ages[i];
+    AirGapElement age;
+    age.antiperiodic = src.antiperiodic != 0;
+    age.center_x_m = src.center_x_m;
+    age.center_y_m = src.center_y_m;
+    age.inner_radius_m = src.inner_radius_m;
+    age.outer_radius_m = src.outer_radius_m;
+    age.arc_length_deg = src.arc_length_deg;
+    age.inner_shift = src.inner_shift;
+    age.outer_shift = src.outer_shift;
+    for (int p = 0; p < src.point_count; ++p) {
+      AirGapQuadPoint point;
+      for (int l = 0; l < 4; ++l) {
+        point.node[l] = src.nodes[4 * p + l];
+        point.weight[l] = src.weights[4 * p + l];
+      }
+      age.quad_points.push_back(point);
+    }
+    model.air_gap_elements.push_back(std::move(age));
+  }
   *out = std::move(model);
   return true;
 }
 
 } // namespace
+
+// The one oracle-model -> NonlinearModel conversion, shared with ref_cpu_baseline.cpp.
+bool RefModelFromOracle(const or_model *m, NonlinearModel *out) { return ToModel(m, out); }
 
 struct ref_system {
   Assembly assembly;
@@ -235,6 +258,13 @@ void ref_prepared_copy(const ref_prepared *p, int32_t *row_offsets, int32_t *col
   std::memcpy(pm_rhs, q.pm_rhs.data(), sizeof(double) * q.pm_rhs.size());
   std::memcpy(circuit_rhs, q.circuit_rhs.data(), sizeof(double) * q.circuit_rhs.size());
   std::memcpy(diagonal_slots, q.diagonal_slots.data(), sizeof(int32_t) * q.diagonal_slots.size());
+}
+
+// PreparedNonlinearAssembly::age_values [nnz] / age_rhs [rows] (nonlinear_topology.cpp:180-262).
+void ref_prepared_age(const ref_prepared *p, double *age_values, double *age_rhs)
+{
+  std::memcpy(age_values, p->prepared.age_values.data(), sizeof(double) * p->prepared.age_values.size());
+  std::memcpy(age_rhs, p->prepared.age_rhs.data(), sizeof(double) * p->prepared.age_rhs.size());
 }
 
 void ref_prepared_free(ref_prepared *p) { delete p; }
@@ -523,3 +553,13 @@ int ref_read_motor_sample_request(const char *text, size_t length, char *error)
 }
 
 } // extern "C"
+
+// BuildNativeFemmAirGapMatrix (native_airgap_matrix.cpp:5-22) as a flat [10][10].
+extern "C" int ref_age_matrix(double K, double Ki, double ci, double co, double *out)
+{
+  double m[10][10];
+  if (!BuildNativeFemmAirGapMatrix(K, Ki, ci, co, m))
+    return 1;
+  std::memcpy(out, m, sizeof(m));
+  return 0;
+}

@@ -162,7 +162,7 @@ def test_library_exports_every_header_symbol():
     missing = [name for name in sorted(declared) if not hasattr(lib, name)]
     assert not missing, missing
     assert set(fg.EXPORTED) <= declared
-    assert fg.lib().fg_abi_version() == 1
+    assert fg.lib().fg_abi_version() == 2
     assert fg.status_name(14) == "NONLINEAR_SOLVE_NOT_CONVERGED"
 
 
