@@ -107,4 +107,172 @@ void AirGapStencil(const AirGap &band, int32_t k, int32_t node[10], double weigh
   }
 }
 
+bool AirGapArcFields(const AirGap &band, const double *a, std::vector<double> *br, std::vector<double> *bt)
+{
+  const int32_t arcs = band.arcs();
+  const double dt = (kPi / 180.0) * band.arc_deg / static_cast<double>(arcs);
+  const double radius = 0.5 * (band.ri + band.ro), dr = band.ro - band.ri;
+  double wi[4], wo[4];
+  CatmullRom(1.0 - band.inner_shift, wi);
+  CatmullRom(1.0 - band.outer_shift, wo);
+  br->assign(arcs, 0.0);
+  bt->assign(arcs, 0.0);
+  for (int32_t k = 0; k < arcs; ++k) {
+    int32_t node[10];
+    double weight[10], v[10];
+    AirGapStencil(band, k, node, weight);
+    for (int i = 0; i < 10; ++i)
+      v[i] = a[node[i]] * weight[i];
+    double il = 0.0, ir = 0.0, ol = 0.0, orr = 0.0;
+    for (int l = 0; l < 4; ++l) {
+      il += wi[l] * v[l];
+      ir += wi[l] * v[l + 1];
+      ol += wo[l] * v[5 + l];
+      orr += wo[l] * v[6 + l];
+    }
+    (*br)[k] = ((ir - il) + (orr - ol)) / (2.0 * dt * radius);
+    (*bt)[k] = ((il + ir) - (ol + orr)) / (2.0 * dr);
+    if (!std::isfinite((*br)[k]) || !std::isfinite((*bt)[k]))
+      return false;
+  }
+  return true;
+}
+
+double AirGapSeries::At(double theta) const
+{
+  double v = 0.0;
+  for (size_t h = 0; h < order.size(); ++h) {
+    const double phase = static_cast<double>(order[h]) * theta;
+    v += c[h] * std::cos(phase) + s[h] * std::sin(phase);
+  }
+  return v;
+}
+
+AirGapSeries AirGapRadialSeries(const AirGap &band, const std::vector<double> &br)
+{
+  // A periodic band of arc span S repeats every S: harmonics 0, 1, 2, ... in units of
+  // 360/S, up to Nyquist.  An anti-periodic one changes sign every S: odd multiples of
+  // 180/S only.  DC and the Nyquist term of an even periodic count have weight 1/arcs,
+  // the others 2/arcs (a real DFT at the arc centres).
+  const int32_t arcs = band.arcs();
+  const double dt = (kPi / 180.0) * band.arc_deg / static_cast<double>(arcs);
+  const size_t count = band.antiperiodic ? static_cast<size_t>((arcs + 1) / 2) : static_cast<size_t>(arcs / 2 + 1);
+  const int32_t base = static_cast<int32_t>(std::lround((band.antiperiodic ? 180.0 : 360.0) / band.arc_deg));
+  AirGapSeries f;
+  f.order.resize(count);
+  f.c.assign(count, 0.0);
+  f.s.assign(count, 0.0);
+  for (size_t h = 0; h < count; ++h) {
+    const int32_t n = band.antiperiodic ? base * static_cast<int32_t>(2 * h + 1) : base * static_cast<int32_t>(h);
+    f.order[h] = n;
+    for (int32_t k = 0; k < arcs; ++k) {
+      const double phase = (static_cast<double>(k) + 0.5) * dt * static_cast<double>(n);
+      f.c[h] += br[k] * std::cos(phase);
+      f.s[h] += br[k] * std::sin(phase);
+    }
+    const bool single = n == 0 || (!band.antiperiodic && h + 1 == count && arcs % 2 == 0);
+    const double norm = single ? static_cast<double>(arcs) : static_cast<double>(arcs) / 2.0;
+    f.c[h] /= norm;
+    f.s[h] /= norm;
+  }
+  return f;
+}
+
+namespace
+{
+
+bool BandGeometry(const AirGap &band, double *dt, double *radius)
+{
+  *dt = (kPi / 180.0) * band.arc_deg / static_cast<double>(band.arcs());
+  *radius = 0.5 * (band.ri + band.ro);
+  return *dt > 0.0 && *radius > 0.0 && band.ro - band.ri > 0.0;
+}
+
+} // namespace
+
+AirGapPostResult AirGapPostprocess(const std::vector<AirGap> &bands, double depth_m, const double *a,
+                                   const std::vector<double> &angles)
+{
+  AirGapPostResult r;
+  if (bands.empty() || !a) {
+    r.status = static_cast<int32_t>(Status::kInvalidArgument);
+    return r;
+  }
+  AirGapSeries first;
+  for (size_t b = 0; b < bands.size(); ++b) {
+    const AirGap &band = bands[b];
+    double dt, radius;
+    if (band.arcs() < 2 || !BandGeometry(band, &dt, &radius)) {
+      r.status = static_cast<int32_t>(Status::kMeshInvalid);
+      return r;
+    }
+    std::vector<double> br, bt;
+    if (!AirGapArcFields(band, a, &br, &bt)) {
+      r.status = static_cast<int32_t>(Status::kNumericalNonfinite);
+      return r;
+    }
+    // Maxwell stress on the band's mid circle: normal (Br^2 - Bt^2) / 2mu0 and shear
+    // Br Bt / mu0 per unit area, resolved at each arc centre.
+    const double scale = depth_m * radius * dt / (2.0 * kMu0);
+    for (int32_t k = 0; k < band.arcs(); ++k) {
+      const double theta = (static_cast<double>(k) + 0.5) * dt;
+      const double normal = br[k] * br[k] - bt[k] * bt[k], shear = 2.0 * br[k] * bt[k];
+      r.fx += scale * (normal * std::cos(theta) - shear * std::sin(theta));
+      r.fy += scale * (normal * std::sin(theta) + shear * std::cos(theta));
+      r.torque += depth_m * radius * radius * dt * br[k] * bt[k] / kMu0;
+    }
+    if (b == 0)
+      first = AirGapRadialSeries(band, br);
+  }
+  for (const double angle : angles) {
+    if (!std::isfinite(angle)) {
+      r.status = static_cast<int32_t>(Status::kInvalidArgument);
+      return r;
+    }
+    r.radial.push_back(first.At(angle));
+  }
+  if (!std::isfinite(r.fx) || !std::isfinite(r.fy) || !std::isfinite(r.torque))
+    r.status = static_cast<int32_t>(Status::kNumericalNonfinite);
+  return r;
+}
+
+AirGapPostResult AirGapTangentPostprocess(const std::vector<AirGap> &bands, double depth_m, const double *a,
+                                          const double *da, const std::vector<double> &angles)
+{
+  AirGapPostResult r;
+  if (bands.empty() || !a || !da) {
+    r.status = static_cast<int32_t>(Status::kInvalidArgument);
+    return r;
+  }
+  AirGapSeries first;
+  for (size_t b = 0; b < bands.size(); ++b) {
+    const AirGap &band = bands[b];
+    double dt, radius;
+    if (band.arcs() < 2 || !BandGeometry(band, &dt, &radius)) {
+      r.status = static_cast<int32_t>(Status::kMeshInvalid);
+      return r;
+    }
+    std::vector<double> br, bt, dbr, dbt;
+    AirGapArcFields(band, a, &br, &bt);
+    AirGapArcFields(band, da, &dbr, &dbt);
+    const double scale = depth_m * radius * dt / (2.0 * kMu0);
+    for (int32_t k = 0; k < band.arcs(); ++k) {
+      const double theta = (static_cast<double>(k) + 0.5) * dt;
+      const double dnormal = 2.0 * (br[k] * dbr[k] - bt[k] * dbt[k]);
+      const double dshear = 2.0 * (dbr[k] * bt[k] + br[k] * dbt[k]);
+      r.fx += scale * (dnormal * std::cos(theta) - dshear * std::sin(theta));
+      r.fy += scale * (dnormal * std::sin(theta) + dshear * std::cos(theta));
+      r.torque += depth_m * radius * radius * dt * (dbr[k] * bt[k] + br[k] * dbt[k]) / kMu0;
+    }
+    if (b == 0)
+      first = AirGapRadialSeries(band, dbr);
+  }
+  for (const double angle : angles)
+    r.radial.push_back(first.At(angle));
+  r.status = std::isfinite(r.fx) && std::isfinite(r.fy) && std::isfinite(r.torque)
+                 ? 0
+                 : static_cast<int32_t>(Status::kNumericalNonfinite);
+  return r;
+}
+
 } // namespace fg

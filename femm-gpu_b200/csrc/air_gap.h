@@ -52,4 +52,39 @@ bool AirGapElementMatrix(double K, double Ki, double ci, double co, double m[10]
 // closure's extra sign on the stencil ends that wrap around the band.
 void AirGapStencil(const AirGap &band, int32_t k, int32_t node[10], double weight[10]);
 
+// B at the centre of every arc of a band from nodal A [N]: br radial, bt circumferential.
+// The arc's corner potentials come from the same Catmull-Rom ring interpolation as the
+// stiffness, at t = 1 - (the side's own shift), so the arcs sit on the band's absolute
+// angular grid; then Br = (1/r) dA/dtheta and Bt = -dA/dr are the corner differences
+// averaged over the arc.  Returns false if a value is not finite.
+bool AirGapArcFields(const AirGap &band, const double *a, std::vector<double> *br, std::vector<double> *bt);
+
+// The radial-B Fourier series of a band's arc values, as FEMM's viewer builds it for
+// mo_getgapb: the harmonics a periodic (all) or anti-periodic (odd) band carries, in units
+// of the band's repeat; value at angle theta = sum_h c_h cos(n_h theta) + s_h sin(n_h theta).
+struct AirGapSeries {
+  std::vector<int32_t> order;
+  std::vector<double> c, s;
+  double At(double theta) const;
+};
+AirGapSeries AirGapRadialSeries(const AirGap &band, const std::vector<double> &br);
+
+// Maxwell-stress force / torque of the band and the series' radial B at the given angles
+// (ComputeAirGapElementPostprocess, postprocess/airgap_postprocess.cpp:44-161).  Status as
+// the reference: INVALID_ARGUMENT without a band or for a non-finite angle, MESH_INVALID for
+// a degenerate band, NUMERICAL_NONFINITE for non-finite fields or totals.
+struct AirGapPostResult {
+  int32_t status = 0;
+  double fx = 0.0, fy = 0.0, torque = 0.0;
+  std::vector<double> radial;
+};
+AirGapPostResult AirGapPostprocess(const std::vector<AirGap> &bands, double depth_m, const double *a,
+                                   const std::vector<double> &angles);
+
+// The first-order change of the same quantities along a tangent dA at the base A
+// (ComputeAirGapElementTangentPostprocess, airgap_postprocess.cpp:163-285): force and torque
+// bilinear in (B, dB), the radial series of dBr.
+AirGapPostResult AirGapTangentPostprocess(const std::vector<AirGap> &bands, double depth_m, const double *a,
+                                          const double *da, const std::vector<double> &angles);
+
 } // namespace fg

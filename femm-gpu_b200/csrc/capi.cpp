@@ -515,4 +515,44 @@ void fg_bh_eval(int32_t count, const double *b, const double *h, const double *s
   fg::EvaluateBh(c, field_b, out);
 }
 
+int fg_air_gap_postprocess(const fg_plan *plan, int32_t items, const double *a, int32_t angle_count,
+                           const double *angles_rad, fg_postprocess_result *results,
+                           double *airgap_radial_b_t)
+{
+  if (!plan || items < 0 || !results || (items > 0 && !a) || angle_count < 0 ||
+      (angle_count > 0 && (!angles_rad || !airgap_radial_b_t)))
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostModel &m = plan->plan.model();
+  const std::vector<double> angles(angles_rad, angles_rad + angle_count);
+  const size_t N = static_cast<size_t>(m.nodes());
+  for (int32_t i = 0; i < items; ++i) {
+    const fg::AirGapPostResult r = fg::AirGapPostprocess(m.ages, m.depth_m, a + i * N, angles);
+    results[i] = fg_postprocess_result{r.status, 0, r.fx, r.fy, r.torque};
+    for (int32_t j = 0; j < angle_count; ++j)
+      airgap_radial_b_t[static_cast<size_t>(i) * angle_count + j] =
+          j < static_cast<int32_t>(r.radial.size()) ? r.radial[j] : 0.0;
+  }
+  return 0;
+}
+
+int fg_air_gap_tangent(const fg_plan *plan, int32_t directions, const double *base_a, const double *da,
+                       int32_t angle_count, const double *angles_rad, fg_postprocess_result *results,
+                       double *airgap_radial_b_t)
+{
+  if (!plan || directions < 0 || !results || !base_a || (directions > 0 && !da) || angle_count < 0 ||
+      (angle_count > 0 && (!angles_rad || !airgap_radial_b_t)))
+    return ToInt(Status::kInvalidArgument);
+  const fg::HostModel &m = plan->plan.model();
+  const std::vector<double> angles(angles_rad, angles_rad + angle_count);
+  const size_t N = static_cast<size_t>(m.nodes());
+  for (int32_t i = 0; i < directions; ++i) {
+    const fg::AirGapPostResult r = fg::AirGapTangentPostprocess(m.ages, m.depth_m, base_a, da + i * N, angles);
+    results[i] = fg_postprocess_result{r.status, 0, r.fx, r.fy, r.torque};
+    for (int32_t j = 0; j < angle_count; ++j)
+      airgap_radial_b_t[static_cast<size_t>(i) * angle_count + j] =
+          j < static_cast<int32_t>(r.radial.size()) ? r.radial[j] : 0.0;
+  }
+  return 0;
+}
+
 } // extern "C"

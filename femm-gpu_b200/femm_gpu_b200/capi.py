@@ -37,7 +37,7 @@ EXPORTED = [
     "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
     "fg_plan_destroy", "fg_plan_sizes_get", "fg_plan_symbolic", "fg_assemble", "fg_pcg_solve",
     "fg_csr_pcg", "fg_solve_batch", "fg_solve_batch_device", "fg_plan_last_timing",
-    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_plan_air_gap", "fg_csr_pcg_noalloc",
+    "fg_bh_build", "fg_bh_eval", "fg_plan_contributors", "fg_plan_air_gap", "fg_air_gap_postprocess", "fg_air_gap_tangent", "fg_csr_pcg_noalloc",
     "fg_mlp_create", "fg_mlp_destroy", "fg_mlp_parameter_count", "fg_mlp_get_parameters",
     "fg_mlp_set_parameters", "fg_mlp_forward", "fg_mlp_loss_gradient", "fg_mlp_train",
     "fg_warm_create", "fg_warm_destroy", "fg_warm_project", "fg_warm_project_device",
@@ -285,6 +285,38 @@ class Plan:
         if st:
             raise FgError(st, "fg_plan_air_gap")
         return vals, rhs
+
+    def air_gap_postprocess(self, a, angles_rad=()):
+        """fg_air_gap_postprocess of host nodal solutions a [k, N]: (status [k], force [k, 2],
+        torque [k], radial B [k, angles])."""
+        a = np.ascontiguousarray(np.atleast_2d(a), np.float64)
+        k = a.shape[0]
+        ang = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+        res = (FgPostprocessResult * max(k, 1))()
+        radial = np.zeros((k, ang.size))
+        st = lib().fg_air_gap_postprocess(self._h, C.c_int32(k), _p(a), C.c_int32(ang.size),
+                                          _p(ang) if ang.size else None, res, _p(radial) if ang.size else None)
+        if st:
+            raise FgError(st, "fg_air_gap_postprocess")
+        return PostprocessResult(status=np.array([res[i].status for i in range(k)]),
+                                 force=np.array([[res[i].force_x_n, res[i].force_y_n] for i in range(k)]),
+                                 torque=np.array([res[i].torque_nm for i in range(k)]), radial_b=radial)
+
+    def air_gap_tangent(self, base_a, da, angles_rad=()):
+        """fg_air_gap_tangent: derivatives along tangent solutions da [m, N] about base_a [N]."""
+        base_a = np.ascontiguousarray(base_a, np.float64).ravel()
+        da = np.ascontiguousarray(np.atleast_2d(da), np.float64)
+        m = da.shape[0]
+        ang = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+        res = (FgPostprocessResult * max(m, 1))()
+        radial = np.zeros((m, ang.size))
+        st = lib().fg_air_gap_tangent(self._h, C.c_int32(m), _p(base_a), _p(da), C.c_int32(ang.size),
+                                      _p(ang) if ang.size else None, res, _p(radial) if ang.size else None)
+        if st:
+            raise FgError(st, "fg_air_gap_tangent")
+        return PostprocessResult(status=np.array([res[i].status for i in range(m)]),
+                                 force=np.array([[res[i].force_x_n, res[i].force_y_n] for i in range(m)]),
+                                 torque=np.array([res[i].torque_nm for i in range(m)]), radial_b=radial)
 
     def assemble(self, states, currents, use_newton):
         states = np.ascontiguousarray(np.atleast_2d(states), np.float64)

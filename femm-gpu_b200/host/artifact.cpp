@@ -48,7 +48,58 @@ fg_model Artifact::Model()
   m.constraint_signs = con_signs.data();
   m.circuit_count = static_cast<int32_t>(circuit_currents.size());
   m.depth_m = depth_m;
+  band_view.clear();
+  for (const AirGapBand &b : bands) {
+    fg_air_gap_element e{};
+    e.antiperiodic = b.antiperiodic ? 1 : 0;
+    e.point_count = static_cast<int32_t>(b.nodes.size() / 4);
+    e.center_x_m = b.center_m[0];
+    e.center_y_m = b.center_m[1];
+    e.inner_radius_m = b.ri_m;
+    e.outer_radius_m = b.ro_m;
+    e.arc_length_deg = b.arc_deg;
+    e.inner_shift = b.inner_shift;
+    e.outer_shift = b.outer_shift;
+    e.nodes = b.nodes.data();
+    e.weights = b.weights.data();
+    band_view.push_back(e);
+  }
+  m.air_gap_count = static_cast<int32_t>(band_view.size());
+  m.air_gap_elements = band_view.empty() ? nullptr : band_view.data();
   return m;
+}
+
+bool Artifact::SlideBands(double rotor_angle_deg)
+{
+  if (!sliding_band)
+    return true;
+  const double delta = rotor_angle_deg - this->rotor_angle_deg;
+  if (!std::isfinite(delta))
+    return false;
+  for (AirGapBand &b : bands) {
+    const int64_t arcs = static_cast<int64_t>(b.nodes.size() / 4) - 1;
+    if (arcs <= 0 || !(b.arc_deg > 0.0))
+      return false;
+    const double slid = b.inner_shift + delta * static_cast<double>(arcs) / b.arc_deg;
+    const int64_t whole = static_cast<int64_t>(std::floor(slid));
+    b.inner_shift = slid - static_cast<double>(whole);
+    const std::vector<int32_t> nodes = b.nodes;
+    const std::vector<double> weights = b.weights;
+    for (int64_t k = 0; k < arcs; ++k) {
+      int64_t from = (k - whole) % arcs;
+      if (from < 0)
+        from += arcs;
+      for (int l = 0; l < 2; ++l) {
+        b.nodes[4 * k + l] = nodes[4 * from + l];
+        b.weights[4 * k + l] = weights[4 * from + l];
+      }
+    }
+    for (int l = 0; l < 2; ++l) {
+      b.nodes[4 * arcs + l] = b.nodes[l];
+      b.weights[4 * arcs + l] = b.weights[l];
+    }
+  }
+  return true;
 }
 
 // The 180-degree sector metadata of gpu_femm_mesh_v3 (mesh_artifact.cpp:441-608): p pole
@@ -168,6 +219,95 @@ bool ParseSector(const Json &sec, Artifact *a, std::string *error)
   return true;
 }
 
+// The air_gap_elements of gpu_femm_mesh_v2 (mesh_artifact.cpp:609-697): a centred,
+// zero-degree reference pose; one element object or a nonempty array of them, each with
+// exactly its ten members, sector_count >= 2 arcs and sector_count + 1 points of integer
+// nodes and numeric weights; every node in range (ValidateNonlinearModel's check).
+bool ParseBands(const Json &res, Artifact *a, std::string *error)
+{
+  const auto it = res.members.find("air_gap_elements");
+  if (it == res.members.end() || (!it->second.is(K::Array) && !it->second.is(K::Object)) ||
+      a->displacement_mm[0] != 0.0 || a->displacement_mm[1] != 0.0 || a->rotor_angle_deg != 0.0) {
+    *error = "sliding-band artifacts require a centered zero-degree reference mesh";
+    return false;
+  }
+  std::vector<const Json *> entries;
+  if (it->second.is(K::Array)) {
+    if (it->second.items.empty()) {
+      *error = "sliding-band requires an air-gap element";
+      return false;
+    }
+    for (const Json &e : it->second.items)
+      entries.push_back(&e);
+  } else {
+    entries.push_back(&it->second);
+  }
+  const size_t N = a->xy.size() / 2;
+  for (const Json *e : entries) {
+    if (!HasExactly(*e, {"name", "periodicity", "center_mm", "ri_mm", "ro_mm", "arc_length_deg", "sector_count",
+                         "inner_shift", "outer_shift", "quad_points"},
+                    error))
+      return false;
+    const Json *name = e->get("name", K::String, error);
+    const Json *per = e->get("periodicity", K::String, error);
+    const Json *center = e->get("center_mm", K::Array, error);
+    const Json *ri = e->get("ri_mm", K::Number, error);
+    const Json *ro = e->get("ro_mm", K::Number, error);
+    const Json *arc = e->get("arc_length_deg", K::Number, error);
+    const Json *sectors = e->get("sector_count", K::Number, error);
+    const Json *ishift = e->get("inner_shift", K::Number, error);
+    const Json *oshift = e->get("outer_shift", K::Number, error);
+    const Json *points = e->get("quad_points", K::Array, error);
+    int32_t count = 0;
+    if (!name || name->text.empty() || !per || !center || !ri || !ro || !arc || !sectors || !ishift || !oshift ||
+        !points || center->items.size() != 2 || !center->items[0].is(K::Number) ||
+        !center->items[1].is(K::Number) || !AsInt32(*sectors, &count) || count < 2 ||
+        points->items.size() != static_cast<size_t>(count) + 1 ||
+        (per->text != "periodic" && per->text != "antiperiodic")) {
+      *error = "invalid sliding-band air-gap element";
+      return false;
+    }
+    AirGapBand b;
+    b.name = name->text;
+    b.antiperiodic = per->text == "antiperiodic";
+    b.center_m[0] = center->items[0].number * 1e-3;
+    b.center_m[1] = center->items[1].number * 1e-3;
+    b.ri_m = ri->number * 1e-3;
+    b.ro_m = ro->number * 1e-3;
+    b.arc_deg = arc->number;
+    b.sector_count = count;
+    b.inner_shift = ishift->number;
+    b.outer_shift = oshift->number;
+    for (const Json &pt : points->items) {
+      if (!HasExactly(pt, {"n0", "w0", "n1", "w1", "n2", "w2", "n3", "w3"}, error))
+        return false;
+      for (int l = 0; l < 4; ++l) {
+        const std::string nn = std::string("n") + char('0' + l), wn = std::string("w") + char('0' + l);
+        const Json *node = pt.get(nn.c_str(), K::Number, error);
+        const Json *weight = pt.get(wn.c_str(), K::Number, error);
+        int32_t id = -1;
+        if (!node || !weight || !AsInt32(*node, &id)) {
+          *error = "invalid sliding-band quadrature point";
+          return false;
+        }
+        b.nodes.push_back(id);
+        b.weights.push_back(weight->number);
+      }
+    }
+    a->bands.push_back(std::move(b));
+  }
+  for (const AirGapBand &b : a->bands)
+    for (size_t l = 0; l < b.nodes.size(); ++l)
+      if (b.nodes[l] < 0 || static_cast<size_t>(b.nodes[l]) >= N || !std::isfinite(b.weights[l]) ||
+          !(b.ri_m > 0.0) || !(b.ro_m > b.ri_m) || !(b.arc_deg > 0.0) || !std::isfinite(b.inner_shift) ||
+          !std::isfinite(b.outer_shift)) {
+        *error = "mapped mesh model validation failed";
+        return false;
+      }
+  a->sliding_band = true;
+  return true;
+}
+
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
 {
   Json root;
@@ -180,10 +320,11 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const bool generic = schema->text == "gpu_femm_magnetostatic_mesh_v1";
   const bool neutral = planar_dc || generic;
   const bool motor_v1 = schema->text == "gpu_femm_mesh_v1";
+  const bool sliding = schema->text == "gpu_femm_mesh_v2";
   const bool sector = schema->text == "gpu_femm_mesh_v3";
-  const bool motor = motor_v1 || sector;
-  if (schema->text == "gpu_femm_mesh_v2" || schema->text == "gpu_femm_mesh_v4") {
-    *error = "unsupported mesh artifact schema (native air-gap element artifacts are not served here)";
+  const bool motor = motor_v1 || sliding || sector;
+  if (schema->text == "gpu_femm_mesh_v4") {
+    *error = "unsupported mesh artifact schema (native air-gap element sectors are not served here)";
     return false;
   }
   if (!neutral && !motor) {
@@ -213,6 +354,9 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
                : motor_v1 ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
                                               "nodes_mm", "triangles", "regions", "materials", "circuits",
                                               "outer_dirichlet"}, error)
+               : sliding ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
+                                             "nodes_mm", "triangles", "regions", "materials", "circuits",
+                                             "outer_dirichlet", "air_gap_elements"}, error)
                           : HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
                                               "nodes_mm", "triangles", "regions", "materials", "circuits",
                                               "outer_dirichlet", "air_gap_elements", "node_constraints",
@@ -492,6 +636,8 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
     }
   }
   if (sector && !ParseSector(*sector_meta, &a, error))
+    return false;
+  if (sliding && !ParseBands(*res, &a, error))
     return false;
   *out = std::move(a);
   return true;

@@ -10,6 +10,20 @@
 namespace fgio
 {
 
+// One native air-gap element of a sliding-band artifact (AirGapElement as
+// ParseGpuFemmMeshArtifactJson maps it, io/mesh_artifact.cpp:633-696): millimetres to
+// metres, per band point the inner-ring pair n0 / n1 and the outer-ring pair n2 / n3 with
+// their copy signs.
+struct AirGapBand {
+  std::string name;
+  bool antiperiodic = false;
+  double center_m[2] = {0.0, 0.0}, ri_m = 0.0, ro_m = 0.0, arc_deg = 0.0;
+  double inner_shift = 0.0, outer_shift = 0.0;
+  int32_t sector_count = 0;
+  std::vector<int32_t> nodes;  // [4 * (sector_count + 1)]
+  std::vector<double> weights; // [4 * (sector_count + 1)]
+};
+
 // A parsed artifact owning every array an fg_model points at.
 struct Artifact {
   std::string schema_version, source_fem_sha256, canonical_identity_sha256;
@@ -39,9 +53,20 @@ struct Artifact {
   std::vector<int8_t> con_signs;
   std::vector<double> circuit_currents;
   std::vector<int32_t> group_numbers; // per expanded label material
+  // gpu_femm_mesh_v2: a zero-degree reference mesh whose air gap is native air-gap elements;
+  // each rotor angle is a pose of the bands (SlideBands), not a new mesh.
+  bool sliding_band = false;
+  std::vector<AirGapBand> bands;
+  std::vector<fg_air_gap_element> band_view; // filled by Model()
 
   // The fg_model view (valid while this object lives and is not modified).
   fg_model Model();
+  // ApplySlidingBandAngle (io/sample_request.cpp:448-491): poses the bands of this
+  // zero-degree artifact at rotor_angle_deg.  The inner ring slides by the angle over the
+  // band's arc: the whole arcs rotate the inner records cyclically (the last point repeats
+  // the first), the fraction becomes the new inner shift; the stator side stays.  False for
+  // a non-finite angle or a degenerate band.
+  bool SlideBands(double rotor_angle_deg);
 };
 
 // ParseGpuFemmMeshArtifactJson (gpu_solver/src/io/mesh_artifact.cpp:14-715) for the two
@@ -50,7 +75,9 @@ struct Artifact {
 // label material per region appended after the base materials (group, circuit, magnet
 // angle, J = turns / region area), zero outer Dirichlet values, signed node constraints.
 // and its conforming 180-degree sector gpu_femm_mesh_v3 (sector metadata, apex self-pairs,
-// circuit partners).  The native air-gap element schemas (gpu_femm_mesh_v2, v4) are refused.
+// circuit partners), and the sliding-band schema gpu_femm_mesh_v2 (a zero-degree reference
+// mesh with native air-gap elements).  The native air-gap sector schema gpu_femm_mesh_v4 is
+// refused.
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error);
 
 } // namespace fgio

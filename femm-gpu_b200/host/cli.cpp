@@ -7,7 +7,7 @@
 //   femm_gpu [options] --motor-single-sample REQUEST.json RESPONSE.json
 //   femm_gpu [options] --motor-batch[-profile] BATCH.json RESPONSE.json
 //   femm_gpu --capabilities
-//   femm_gpu --describe-artifact ARTIFACT.json   (parsed model and plan sizes, as JSON)
+//   femm_gpu --describe-artifact ARTIFACT.json [ROTOR_DEG]   (parsed model and plan sizes, as JSON)
 //   femm_gpu --sha256 FILE                        (the file-bytes SHA-256 a request names)
 //   femm_gpu --describe-femm-ans STEM CURVE_DIR   (the model --single-sample reads, as JSON)
 //   options: --preconditioner jacobi|block-jacobi  --block-size 8|32  --precision fp64|mixed
@@ -842,6 +842,18 @@ int DescribeModel(Artifact &a, const std::string &sha256)
     o << (i ? ", " : "") << static_cast<int>(a.con_signs[i]);
   o << "], \"circuit_currents_A\": [";
   List(o, a.circuit_currents);
+  o << "], \"air_gap_elements\": [";
+  for (size_t b = 0; b < a.bands.size(); ++b) {
+    const fgio::AirGapBand &g = a.bands[b];
+    o << (b ? ", " : "") << "{\"antiperiodic\": " << (g.antiperiodic ? 1 : 0) << ", \"center_m\": ["
+      << g.center_m[0] << ", " << g.center_m[1] << "], \"ri_m\": " << g.ri_m << ", \"ro_m\": " << g.ro_m
+      << ", \"arc_length_deg\": " << g.arc_deg << ", \"inner_shift\": " << g.inner_shift
+      << ", \"outer_shift\": " << g.outer_shift << ", \"nodes\": [";
+    List(o, g.nodes);
+    o << "], \"weights\": [";
+    List(o, g.weights);
+    o << "]}";
+  }
   o << "], \"rows\": " << sz.rows << ", \"nnz\": " << sz.nnz << "}\n";
   if (plan)
     fg_plan_destroy(plan);
@@ -849,8 +861,9 @@ int DescribeModel(Artifact &a, const std::string &sha256)
   return rc == 0 ? 0 : 1;
 }
 
-// --describe-artifact ARTIFACT.json
-int DescribeArtifact(const std::string &path)
+// --describe-artifact ARTIFACT.json [ROTOR_ANGLE_DEG]: a sliding-band artifact is described
+// posed at the angle (its bands slid as a motor request at that angle solves them).
+int DescribeArtifact(const std::string &path, const char *rotor_angle_deg = nullptr)
 {
   std::string bytes, error;
   Artifact a;
@@ -860,6 +873,10 @@ int DescribeArtifact(const std::string &path)
   }
   if (!fgio::ParseArtifact(bytes, &a, &error)) {
     std::cout << "{\"status\": \"FAIL\", \"error\": \"" << fgio::Escape(error) << "\"}\n";
+    return 1;
+  }
+  if (rotor_angle_deg && !a.SlideBands(std::strtod(rotor_angle_deg, nullptr))) {
+    std::cout << "{\"status\": \"FAIL\", \"error\": \"could not apply the requested sliding-band angle\"}\n";
     return 1;
   }
   return DescribeModel(a, fgio::Sha256Hex(bytes));
@@ -927,9 +944,12 @@ int main(int argc, char **argv)
   if (rest == 1 && std::strcmp(argv[next], "--capabilities") == 0) {
     std::cout << "{\n  \"protocols\": [\"gpu_femm_planar_dc_sample_v1\", \"gpu_femm_magnetostatic_sample_v1\", "
                  "\"gpu_femm_magnetostatic_batch_v1\", \"gpu_femm_single_sample_v1\", \"gpu_femm_motor_sample_v1\", "
-                 "\"gpu_femm_motor_sample_v2\", \"gpu_femm_motor_batch_v1\", \"gpu_femm_motor_batch_v2\"],\n"
+                 "\"gpu_femm_motor_sample_v2\", \"gpu_femm_motor_sample_v3\", \"gpu_femm_motor_batch_v1\", "
+                 "\"gpu_femm_motor_batch_v2\", \"gpu_femm_motor_batch_v3\"],\n"
               << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\", "
-                 "\"gpu_femm_mesh_v1\"],\n"
+                 "\"gpu_femm_mesh_v1\", \"gpu_femm_mesh_v2\", \"gpu_femm_mesh_v3\"],\n"
+              << "  \"native_sliding_band\": true,\n"
+              << "  \"motor_sector_native_age_cyclic_v1\": false,\n"
               << "  \"preconditioners\": [\"jacobi\", \"block-jacobi\"],\n"
               << "  \"precisions\": [\"fp64\", \"mixed\"],\n"
               << "  \"abi_version\": " << fg_abi_version() << "\n}\n";
@@ -946,6 +966,8 @@ int main(int argc, char **argv)
   }
   if (rest == 2 && std::strcmp(argv[next], "--describe-artifact") == 0)
     return DescribeArtifact(argv[next + 1]);
+  if (rest == 3 && std::strcmp(argv[next], "--describe-artifact") == 0)
+    return DescribeArtifact(argv[next + 1], argv[next + 2]);
   if (rest == 3 && std::strcmp(argv[next], "--describe-femm-ans") == 0)
     return DescribeFemmAns(argv[next + 1], argv[next + 2]);
   if (rest == 3 && std::strcmp(argv[next], "--solve") == 0)

@@ -94,6 +94,40 @@ int RunPost(fg_postprocess *pp, const Solved &s, Post *out)
   return r.status;
 }
 
+Prepared *PoseOf(Prepared &p, double rotor_angle_deg)
+{
+  if (p.status != 0 || !p.artifact.sliding_band)
+    return &p;
+  std::shared_ptr<Prepared> &slot = p.poses[rotor_angle_deg];
+  if (!slot) {
+    slot = std::make_shared<Prepared>();
+    slot->artifact = p.artifact;
+    if (!slot->artifact.SlideBands(rotor_angle_deg)) {
+      slot->status = FG_INVALID_ARGUMENT;
+      slot->error = "could not apply the requested sliding-band angle";
+    }
+  }
+  return slot.get();
+}
+
+int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out)
+{
+  std::vector<double> angles;
+  for (double deg : angles_deg)
+    angles.push_back(deg * kPi / 180.0);
+  out->radial.assign(angles.size(), 0.0);
+  fg_postprocess_result r{};
+  const int rc = fg_air_gap_postprocess(plan, 1, s.a.data(), static_cast<int32_t>(angles.size()),
+                                        angles.empty() ? nullptr : angles.data(), &r,
+                                        angles.empty() ? nullptr : out->radial.data());
+  if (rc != 0)
+    return rc;
+  out->fx = r.force_x_n;
+  out->fy = r.force_y_n;
+  out->torque = r.torque_nm;
+  return r.status;
+}
+
 void Prepare(const std::string &path, const std::string &sha, const Options &opt, Prepared *p)
 {
   std::string bytes;

@@ -113,6 +113,9 @@ struct Prepared {
   // relation (MakeMotorSectorTangentModel), built on first use.
   std::shared_ptr<Prepared> sector_tangent;
   bool sector_tangent_tried = false;
+  // A sliding-band artifact's poses: per requested rotor angle a copy of the artifact with
+  // its bands slid to that angle, and that copy's own plan (the operator differs per angle).
+  std::map<double, std::shared_ptr<Prepared>> poses;
   ~Prepared()
   {
     if (plan)
@@ -126,6 +129,14 @@ void Prepare(const std::string &path, const std::string &sha, const Options &opt
 void PreparePlanOnHost(Prepared *p, const Options &opt);
 // The plan (NonlinearP1Solver::Initialize), created once the requests have matched.
 int EnsurePlan(Prepared *p, const Options &opt);
+
+// The Prepared that solves rotor_angle_deg: `p` itself for a conforming artifact, else its
+// sliding-band pose at that angle, made on first use (ApplySlidingBandRotorAngle,
+// sample_request.cpp:493-497; status FG_INVALID_ARGUMENT when the angle cannot be applied).
+Prepared *PoseOf(Prepared &p, double rotor_angle_deg);
+// The sliding-band postprocess of one solved sample (ComputeAirGapElementPostprocess via
+// fg_air_gap_postprocess) at the request's probe angles in degrees.
+int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out);
 
 // Solves k samples (their circuit currents) on a prepared plan with the reference's
 // production options (ProductionSampleOptions); statuses[i] = the item's status.

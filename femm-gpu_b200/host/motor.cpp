@@ -286,11 +286,19 @@ void Tangent(fg_plan *plan, fg_postprocess *pp, const MotorSampleRequest &req, c
     d->tangent_status = rc;
     return;
   }
-  const size_t P = static_cast<size_t>(fg_postprocess_probe_count(pp));
+  // pp null: a sliding-band plan, whose derivatives come from its air-gap elements
+  // (ComputeAirGapElementTangentPostprocess) at the request's probe angles.
+  std::vector<double> angles;
+  for (double deg : req.airgap_angles_deg)
+    angles.push_back(deg * kPi / 180.0);
+  const size_t P = pp ? static_cast<size_t>(fg_postprocess_probe_count(pp)) : angles.size();
   std::vector<fg_postprocess_result> res(m);
   std::vector<double> radial(m * P);
-  rc = fg_postprocess_tangent(pp, static_cast<int32_t>(m), sol.b1.data(), sol.b2.data(), da.data(), db1.data(),
-                              db2.data(), res.data(), P ? radial.data() : nullptr);
+  rc = pp ? fg_postprocess_tangent(pp, static_cast<int32_t>(m), sol.b1.data(), sol.b2.data(), da.data(),
+                                   db1.data(), db2.data(), res.data(), P ? radial.data() : nullptr)
+          : fg_air_gap_tangent(plan, static_cast<int32_t>(m), sol.a.data(), da.data(),
+                               static_cast<int32_t>(P), P ? angles.data() : nullptr, res.data(),
+                               P ? radial.data() : nullptr);
   if (rc != 0) {
     d->tangent_status = rc;
     return;
@@ -342,22 +350,29 @@ int MotorSingleSample(const std::string &request_path, const std::string &respon
     status = FG_INVALID_ARGUMENT;
     error = "artifact identity, pose, or circuit-count mismatch";
   }
+  Prepared &q = status == 0 ? *PoseOf(p, req.rotor_angle_deg) : p;
+  if (status == 0 && q.status != 0) {
+    status = q.status;
+    error = q.error;
+  }
   const bool attempted = status == 0;
   std::vector<Solved> sols;
   Post post;
   if (attempted) {
-    status = EnsurePlan(&p, opt);
+    status = EnsurePlan(&q, opt);
     if (status == 0) {
       std::vector<int> st;
       int launches = 0;
-      status = SolveCurrents(p, {&req.circuit_currents_a}, &sols, &st, &launches);
+      status = SolveCurrents(q, {&req.circuit_currents_a}, &sols, &st, &launches);
       if (status == 0)
         status = st[0];
     }
-    if (status == 0) {
+    if (status == 0 && q.artifact.sliding_band) {
+      status = AirGapPost(q.plan, sols[0], req.airgap_angles_deg, &post);
+    } else if (status == 0) {
       fg_postprocess *pp = nullptr;
-      status = p.post.Get(p.plan, req.selected_group_number, req.air_group_number, req.airgap_radius_mm,
-                          req.airgap_angles_deg, &pp, nullptr, &p.artifact.apex_nodes);
+      status = q.post.Get(q.plan, req.selected_group_number, req.air_group_number, req.airgap_radius_mm,
+                          req.airgap_angles_deg, &pp, nullptr, &q.artifact.apex_nodes);
       if (status == 0)
         status = RunPost(pp, sols[0], &post);
     }
@@ -384,13 +399,16 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
   int cache_hits = 0, chunks = 0, launches = 0, width = 0, symbolic_hits = 0;
   double artifact_s = 0.0, solve_s = 0.0, post_s = 0.0, tangent_s = 0.0, tangent_post_s = 0.0;
   int64_t pcg_iterations = 0;
-  ArtifactKey cached_operator;
+  // An operator is an artifact, and for a sliding-band artifact also the rotor angle
+  // (MotorBatchOperatorKey, batch_prepare.cpp:220-233).
+  using OperatorKey = std::pair<ArtifactKey, double>;
+  OperatorKey cached_operator;
   bool have_cached = false;
   for (size_t first = 0; first < n; first += effective) {
     ++chunks;
     const size_t end = std::min(n, first + static_cast<size_t>(effective));
     // Artifact gate per item, then groups of items sharing one operator, first-seen order.
-    std::vector<std::pair<ArtifactKey, std::vector<size_t>>> groups;
+    std::vector<std::pair<OperatorKey, std::vector<size_t>>> groups;
     const auto a0 = Clock::now();
     for (size_t i = first; i < end; ++i) {
       const MotorSampleRequest &r = batch.items[i].request;
@@ -408,15 +426,21 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
         out[i].status = FG_INVALID_ARGUMENT;
         continue;
       }
-      auto g = std::find_if(groups.begin(), groups.end(), [&](const auto &x) { return x.first == key; });
+      const OperatorKey op{key, slot->artifact.sliding_band ? r.rotor_angle_deg : 0.0};
+      const Prepared *pose = PoseOf(*slot, r.rotor_angle_deg);
+      if (pose->status != 0) {
+        out[i].status = pose->status;
+        continue;
+      }
+      auto g = std::find_if(groups.begin(), groups.end(), [&](const auto &x) { return x.first == op; });
       if (g == groups.end())
-        groups.push_back({key, {i}});
+        groups.push_back({op, {i}});
       else
         g->second.push_back(i);
     }
     artifact_s += seconds(a0);
     for (auto &g : groups) {
-      Prepared &p = *(*artifacts)[g.first];
+      Prepared &p = *PoseOf(*(*artifacts)[g.first.first], g.first.second);
       const std::vector<size_t> &idx = g.second;
       const int plan_status = EnsurePlan(&p, opt);
       if (plan_status != 0) {
@@ -472,10 +496,14 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
           base_signs = FoldSectorAngles(start, d.base_sign, &folded);
           tangent_signs = FoldSectorAngles(start, d.tangent_sign, &tangent_folded);
         }
-        d.status = p.post.Get(p.plan, r.selected_group_number, r.air_group_number, r.airgap_radius_mm,
-                              r.airgap_angles_deg, &pp, sector ? &folded : nullptr, &p.artifact.apex_nodes);
-        if (d.status == 0)
-          d.status = RunPost(pp, sols[j], &post);
+        if (p.artifact.sliding_band) {
+          d.status = AirGapPost(p.plan, sols[j], r.airgap_angles_deg, &post);
+        } else {
+          d.status = p.post.Get(p.plan, r.selected_group_number, r.air_group_number, r.airgap_radius_mm,
+                                r.airgap_angles_deg, &pp, sector ? &folded : nullptr, &p.artifact.apex_nodes);
+          if (d.status == 0)
+            d.status = RunPost(pp, sols[j], &post);
+        }
         post_s += seconds(p0);
         if (d.status == 0 && sector)
           for (size_t k = 0; k < post.radial.size() && k < base_signs.size(); ++k)

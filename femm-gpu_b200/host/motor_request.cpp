@@ -183,9 +183,27 @@ bool MotorRequestMatchesArtifact(const MotorSampleRequest &r, const Artifact &a)
        a.sector_boundary_sign != (a.electrical_pole_pairs % 2 == 0 ? 1 : -1) || !r.sector_performance ||
        r.model_invariance_certificate_sha256 != a.model_invariance_certificate_sha256))
     return false;
+  // A sliding-band artifact serves any rotor angle at zero displacement; its postprocess
+  // groups must exist and the probe circle must lie in every band (sample_request.cpp:
+  // 413-438).  A conforming artifact is one pose.
+  bool pose = false, post = true;
+  if (a.sliding_band) {
+    pose = r.displacement_mm[0] == 0.0 && r.displacement_mm[1] == 0.0;
+    auto has_group = [&a](int32_t g) { return std::find(a.group_numbers.begin(), a.group_numbers.end(), g) != a.group_numbers.end(); };
+    post = has_group(r.selected_group_number) && has_group(r.air_group_number);
+    if (post && !r.airgap_angles_deg.empty()) {
+      post = !a.bands.empty();
+      for (const AirGapBand &b : a.bands) {
+        const double ri = 1000.0 * b.ri_m, ro = 1000.0 * b.ro_m, tol = 1e-9 * std::max(1.0, std::abs(ro));
+        post = post && r.airgap_radius_mm >= ri - tol && r.airgap_radius_mm <= ro + tol;
+      }
+    }
+  } else {
+    pose = r.rotor_angle_deg == a.rotor_angle_deg && r.displacement_mm[0] == a.displacement_mm[0] &&
+           r.displacement_mm[1] == a.displacement_mm[1];
+  }
   return r.base_motor_fem_sha256 == a.base_motor_fem_sha256 && r.source_fem_sha256 == a.source_fem_sha256 &&
-         r.rotor_angle_deg == a.rotor_angle_deg && r.displacement_mm[0] == a.displacement_mm[0] &&
-         r.displacement_mm[1] == a.displacement_mm[1] && r.circuit_currents_a.size() == a.circuit_currents.size();
+         pose && post && r.circuit_currents_a.size() == a.circuit_currents.size();
 }
 
 bool ParseMotorBatchRequestText(const std::string &text, MotorBatchRequest *b, std::string *error)

@@ -487,6 +487,26 @@ int fg_postprocess_frozen(const fg_plan *plan, const fg_postprocess_options *opt
                           const double *a, const double *b1, const double *b2,
                           fg_postprocess_result *result, double *airgap_radial_b_t);
 
+/* The sliding-band postprocess of a plan whose model carries native air-gap elements
+ * (ComputeAirGapElementPostprocess, gpu_solver/src/postprocess/airgap_postprocess.cpp:
+ * 44-161): B at the centre of every band arc from nodal A, the Maxwell-stress force and
+ * torque summed over the arcs of every band, and the radial B of the first band's Fourier
+ * series at angles_rad (FEMM's mo_getgapb).  a [items][node_count] (host); results [items];
+ * airgap_radial_b_t [items][angle_count].  Per-item statuses as the reference's
+ * (FG_INVALID_ARGUMENT without a band or for a non-finite angle, FG_MESH_INVALID for a
+ * degenerate band, FG_NUMERICAL_NONFINITE); the call returns FG_OK unless its arguments
+ * are unusable. */
+int fg_air_gap_postprocess(const fg_plan *plan, int32_t items, const double *a, int32_t angle_count,
+                           const double *angles_rad, fg_postprocess_result *results,
+                           double *airgap_radial_b_t);
+/* Derivatives of the same along tangent solutions da [directions][node_count] about base_a
+ * [node_count] (ComputeAirGapElementTangentPostprocess, airgap_postprocess.cpp:163-285):
+ * force / torque per amp from the cross terms of B and dB, radial dB from the series of the
+ * first band's dBr.  results [directions]; airgap_radial_b_t [directions][angle_count]. */
+int fg_air_gap_tangent(const fg_plan *plan, int32_t directions, const double *base_a, const double *da,
+                       int32_t angle_count, const double *angles_rad, fg_postprocess_result *results,
+                       double *airgap_radial_b_t);
+
 #ifdef __cplusplus
 }
 #endif

@@ -659,3 +659,62 @@ def ref_prepared_age(model):
     r.ref_prepared_age(h, _p(vals), _p(rhs))
     r.ref_prepared_free(h)
     return 0, vals, rhs
+
+
+def ref_sliding_band_pose(handle, angle_deg):
+    """ApplySlidingBandAngle (io/sample_request.cpp:448-491): a new handle posed at angle_deg."""
+    r = ref()
+    h = C.c_void_p()
+    rc = r.ref_sliding_band_pose(handle.h, C.c_double(angle_deg), C.byref(h))
+    out = RefHandle(h)
+    if rc:
+        raise RuntimeError("ApplySlidingBandAngle refused")
+    return out
+
+
+def ref_age_records(handle):
+    """The air-gap elements of a handle: [(meta [8], nodes [P, 4], weights [P, 4])], meta =
+    antiperiodic, cx, cy, ri, ro, arc degrees, inner shift, outer shift."""
+    r = ref()
+    out = []
+    for b in range(r.ref_age_count(handle.h)):
+        P = r.ref_age_points(handle.h, C.c_int32(b))
+        meta, nodes, weights = np.zeros(8), np.zeros((P, 4), np.int32), np.zeros((P, 4))
+        r.ref_age_copy(handle.h, C.c_int32(b), _p(meta), _p(nodes), _p(weights))
+        out.append((meta, nodes, weights))
+    return out
+
+
+def ref_age_postprocess(handle, a, angles_rad=()):
+    """ComputeAirGapElementPostprocess: (status, Fx, Fy, torque, radial [angles])."""
+    a = np.ascontiguousarray(a, np.float64)
+    ang = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+    out3, radial = np.zeros(3), np.zeros(max(ang.size, 1))
+    st = ref().ref_age_postprocess(handle.h, _p(a), C.c_int32(ang.size), _p(ang), _p(out3), _p(radial))
+    return int(st), out3[0], out3[1], out3[2], radial[:ang.size]
+
+
+def ref_age_tangent_postprocess(handle, a, da, angles_rad=()):
+    """ComputeAirGapElementTangentPostprocess with the base model as tangent model."""
+    a = np.ascontiguousarray(a, np.float64)
+    da = np.ascontiguousarray(da, np.float64)
+    ang = np.ascontiguousarray(np.asarray(angles_rad, np.float64).ravel())
+    out3, radial = np.zeros(3), np.zeros(max(ang.size, 1))
+    st = ref().ref_age_tangent_postprocess(handle.h, _p(a), _p(da), C.c_int32(ang.size), _p(ang), _p(out3),
+                                           _p(radial))
+    return int(st), out3[0], out3[1], out3[2], radial[:ang.size]
+
+
+def ref_artifact_cpu_solve(handle, currents, node_count, circuit_count, options=None, threads=1):
+    """The reference CPU Newton path on a handle's model: (a [k, N], flux [k, C], status [k],
+    Newton iterations [k])."""
+    currents = np.ascontiguousarray(np.atleast_2d(currents), np.float64)
+    k = currents.shape[0]
+    a, flux = np.zeros((k, node_count)), np.zeros((k, max(circuit_count, 1)))
+    status, newton = np.zeros(k, np.int32), np.zeros(k, np.int32)
+    opts = options if options is not None else production_options()
+    rc = ref().ref_artifact_cpu_solve(handle.h, C.c_int32(k), _p(currents), C.byref(opts), C.c_int32(threads),
+                                      _p(a), _p(flux), _p(status), _p(newton))
+    if rc:
+        raise RuntimeError(f"reference CPU solve status {rc}")
+    return a, flux[:, :circuit_count], status, newton

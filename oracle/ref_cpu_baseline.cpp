@@ -35,6 +35,9 @@ extern "C" {
 int ref_validate(const or_model *m);
 }
 bool RefModelFromOracle(const or_model *m, NonlinearModel *out); // ref_driver.cpp
+int RefCpuNewtonModel(const NonlinearModel &model, int32_t k, const double *currents, const or_options *o,
+                      int32_t threads, double *a_out, double *flux_out, int32_t *status,
+                      int32_t *newton_iterations, int32_t *pcg_calls, double *max_true_residual);
 
 namespace
 {
@@ -252,6 +255,15 @@ int ref_cpu_newton_batch(const or_model *m, int32_t k, const double *currents,
   NonlinearModel model;
   if (m->problem_type != 0 || !BuildModel(m, &model))
     return static_cast<int>(Status::kInvalidArgument);
+  return RefCpuNewtonModel(model, k, currents, o, threads, a_out, flux_out, status, newton_iterations,
+                           pcg_calls, max_true_residual);
+}
+}
+
+int RefCpuNewtonModel(const NonlinearModel &model, int32_t k, const double *currents, const or_options *o,
+                      int32_t threads, double *a_out, double *flux_out, int32_t *status,
+                      int32_t *newton_iterations, int32_t *pcg_calls, double *max_true_residual)
+{
   const NonlinearOptions options = ToOptions(o);
   const size_t N = model.nodes.size();
   const int C = model.circuit_count;
@@ -270,6 +282,8 @@ int ref_cpu_newton_batch(const or_model *m, int32_t k, const double *currents,
   });
   return 0;
 }
+
+extern "C" {
 
 // Session of k samples (currents [k*c]) for step-wise timing; *out receives the handle.
 int ref_session_create(const or_model *m, int32_t k, const double *currents,

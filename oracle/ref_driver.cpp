@@ -563,3 +563,98 @@ extern "C" int ref_age_matrix(double K, double Ki, double ci, double co, double 
   std::memcpy(out, m, sizeof(m));
   return 0;
 }
+
+int RefCpuNewtonModel(const NonlinearModel &model, int32_t k, const double *currents, const or_options *o,
+                      int32_t threads, double *a_out, double *flux_out, int32_t *status,
+                      int32_t *newton_iterations, int32_t *pcg_calls, double *max_true_residual);
+
+extern "C" {
+
+// ApplySlidingBandAngle (io/sample_request.cpp:448-491) on a handle: a new handle whose
+// model is posed at angle_deg.  A handle built from an oracle model with air-gap elements
+// counts as a zero-degree sliding-band artifact.
+int ref_sliding_band_pose(const ref_artifact *h, double angle_deg, ref_artifact **out)
+{
+  auto posed = std::make_unique<ref_artifact>();
+  posed->artifact = h->artifact;
+  GpuFemmMeshArtifact source = h->artifact;
+  if (!source.model.air_gap_elements.empty())
+    source.has_sliding_band = true;
+  const bool ok = ApplySlidingBandAngle(angle_deg, source, &posed->artifact.model);
+  *out = posed.release();
+  return ok ? 0 : 1;
+}
+
+int32_t ref_age_count(const ref_artifact *h) { return (int32_t)h->artifact.model.air_gap_elements.size(); }
+
+int32_t ref_age_points(const ref_artifact *h, int32_t b)
+{
+  return (int32_t)h->artifact.model.air_gap_elements[b].quad_points.size();
+}
+
+// meta: antiperiodic, center x, center y, ri, ro, arc degrees, inner shift, outer shift.
+void ref_age_copy(const ref_artifact *h, int32_t b, double *meta, int32_t *nodes, double *weights)
+{
+  const AirGapElement &g = h->artifact.model.air_gap_elements[b];
+  const double m[8] = {g.antiperiodic ? 1.0 : 0.0, g.center_x_m, g.center_y_m, g.inner_radius_m,
+                       g.outer_radius_m, g.arc_length_deg, g.inner_shift, g.outer_shift};
+  std::memcpy(meta, m, sizeof(m));
+  for (size_t p = 0; p < g.quad_points.size(); ++p)
+    for (int l = 0; l < 4; ++l) {
+      nodes[4 * p + l] = g.quad_points[p].node[l];
+      weights[4 * p + l] = g.quad_points[p].weight[l];
+    }
+}
+
+// ComputeAirGapElementPostprocess (postprocess/airgap_postprocess.cpp:44-161): out3 = Fx, Fy,
+// torque; radial [angle_count].
+int ref_age_postprocess(const ref_artifact *h, const double *a, int32_t angle_count, const double *angles_rad,
+                        double *out3, double *radial)
+{
+  NonlinearSolveResult solution;
+  solution.a_wb_per_m.assign(a, a + h->artifact.model.nodes.size());
+  FrozenPostprocessOptions o;
+  o.airgap_angles_rad.assign(angles_rad, angles_rad + angle_count);
+  const FrozenPostprocessResult r = ComputeAirGapElementPostprocess(h->artifact.model, solution, o);
+  out3[0] = r.force_x_n;
+  out3[1] = r.force_y_n;
+  out3[2] = r.torque_nm;
+  for (size_t i = 0; i < r.airgap_samples.size(); ++i)
+    radial[i] = r.airgap_samples[i].radial_b_t;
+  return static_cast<int>(r.status);
+}
+
+// ComputeAirGapElementTangentPostprocess (airgap_postprocess.cpp:163-285) with the base model
+// as the tangent model.
+int ref_age_tangent_postprocess(const ref_artifact *h, const double *a, const double *da, int32_t angle_count,
+                                const double *angles_rad, double *out3, double *radial)
+{
+  NonlinearSolveResult base, derivative;
+  const size_t N = h->artifact.model.nodes.size();
+  base.a_wb_per_m.assign(a, a + N);
+  derivative.a_wb_per_m.assign(da, da + N);
+  FrozenPostprocessOptions o;
+  o.airgap_angles_rad.assign(angles_rad, angles_rad + angle_count);
+  const TangentPostprocessResult r =
+      ComputeAirGapElementTangentPostprocess(h->artifact.model, h->artifact.model, base, derivative, o);
+  out3[0] = r.force_x_n_per_a;
+  out3[1] = r.force_y_n_per_a;
+  out3[2] = r.torque_nm_per_a;
+  for (size_t i = 0; i < r.airgap_radial_flux_density_t_per_a.size(); ++i)
+    radial[i] = r.airgap_radial_flux_density_t_per_a[i];
+  return static_cast<int>(r.status);
+}
+
+// The reference CPU Newton path (ref_cpu_baseline.cpp) on a handle's model.
+int ref_artifact_cpu_solve(const ref_artifact *h, int32_t k, const double *currents, const or_options *o,
+                           int32_t threads, double *a_out, double *flux_out, int32_t *status,
+                           int32_t *newton_iterations)
+{
+  std::vector<int32_t> calls(k);
+  std::vector<double> worst(k);
+  return RefCpuNewtonModel(h->artifact.model, k, currents, o, threads, a_out, flux_out, status,
+                           newton_iterations, calls.data(), worst.data());
+}
+
+} // extern "C"
+
