@@ -386,22 +386,28 @@ def two_pole_machine(nr: int = 160, nt: int = 120, full: bool = False, hc: float
 
 
 def sliding_band_machine(nr: int = 160, nt: int = 120, rotor_deg: float = 0.0, hc: float = 9.0e5,
-                         turns: float = 20.0) -> Model:
-    """The full two-pole machine of ``two_pole_machine(full=True)`` with its 1 mm air gap
-    [0.045, 0.046] m left untriangulated and spanned by one periodic native air-gap
-    element (FEMM's AGE).  The rotor (r <= 0.045, iron, magnets and the air between them)
-    and the stator (r >= 0.046) are meshed separately on polar grids of the same radial
-    step 0.04 / ``nr`` and 2 ``nt`` uniform columns; the rotor mesh, magnets included, is
-    turned by ``rotor_deg``.  The band's records follow FEMM's preprocessor: each ring
-    sorted by angle in [0, 360), point p bracketed by ring entries p - 1 and p (weights +1),
-    and each ring's shift = the angle of its first entry in units of one column.  Groups:
-    air 50, rotor 20, stator 30, slots 40-42.  A = 0 on the outer radius."""
+                         turns: float = 20.0, sector: bool = False) -> Model:
+    """The two-pole machine of ``two_pole_machine`` with its 1 mm air gap [0.045, 0.046] m
+    left untriangulated and spanned by one native air-gap element (FEMM's AGE).  The rotor
+    (r <= 0.045: iron, magnets and the air between them) and the stator (r >= 0.046) are
+    meshed separately on polar grids of the same radial step 0.04 / ``nr`` and ``nt``
+    uniform columns per half turn; the rotor mesh, magnets included, is turned by
+    ``rotor_deg``.  ``sector=False``: the full machine, a periodic band over 360 degrees.
+    ``sector=True``: the half [0, 180] degrees with anti-periodic edges (the 180-degree
+    nodes partner the 0-degree ones), the band over 180 degrees, anti-periodic, the three
+    slots of the upper half only (materials 0-6).  The band's records follow FEMM's
+    preprocessor: each ring's nodes and their copies around the full turn (copy signs -1
+    for odd copies of an anti-periodic sector) sorted by angle in [0, 360), point p
+    bracketed by ring entries p - 1 and p, each ring's shift = the angle of its first entry
+    in units of one column.  Groups: air 50, rotor 20, stator 30, slots 40-42.  A = 0 on
+    the outer radius."""
     h = 0.04 / nr
     rows_r, rows_s = int(round(0.025 / h)), int(round(0.014 / h))
     if abs(rows_r * h - 0.025) > 1e-12 or abs(rows_s * h - 0.014) > 1e-12:
         raise ValueError("nr must put the gap radii 0.045 and 0.046 m on grid rows")
-    cols = 2 * nt
-    dt = 360.0 / cols
+    ring = nt if sector else 2 * nt           # ring nodes of the model (one per column)
+    cols = nt + 1 if sector else 2 * nt       # mesh columns (the sector keeps its 180-degree edge)
+    dt = 180.0 / nt
     rot = np.radians(rotor_deg)
 
     def polar(r_in, r_out, rows, turn):
@@ -409,7 +415,10 @@ def sliding_band_machine(nr: int = 160, nt: int = 120, rotor_deg: float = 0.0, h
         ts = np.radians(np.arange(cols) * dt) + turn
         T, R = np.meshgrid(ts, rs)
         xy = np.stack([(R * np.cos(T)).ravel(), (R * np.sin(T)).ravel()], axis=1)
-        i, j = np.meshgrid(np.arange(rows), np.arange(cols), indexing="ij")
+        if sector:  # the 180-degree edge is the exact half-turn of the 0-degree edge
+            edge = np.arange(rows + 1) * cols
+            xy[edge + cols - 1] = -xy[edge]
+        i, j = np.meshgrid(np.arange(rows), np.arange(cols - 1 if sector else cols), indexing="ij")
         a = (i * cols + j).ravel()
         b = (i * cols + (j + 1) % cols).ravel()
         c = a + cols
@@ -440,36 +449,48 @@ def sliding_band_machine(nr: int = 160, nt: int = 120, rotor_deg: float = 0.0, h
         slot = stator & (rc < 0.050) & (np.abs(tl - centre) <= 10.0)
         mat[slot & upper] = 4 + k
         mat[slot & ~upper] = 7 + k
+    M = 7 if sector else 10
     area = 0.5 * _signed_area2(xy, tri)
     jpa = [turns / area[mat == 4 + k].sum() for k in range(3)]
     nu_air = 1.0 / MU0
     b_t, hh = bh_table_saturating(24)
     outer = (off + rows_s * cols + np.arange(cols)).astype(np.int32)
+    con_a, con_b = np.zeros(0, np.int32), np.zeros(0, np.int32)
+    if sector:  # 0-degree edge -> 180-degree edge, every row but the fixed outer one
+        left = np.concatenate([np.arange(rows_r + 1) * cols, off + np.arange(rows_s) * cols])
+        con_a, con_b = left.astype(np.int32), (left + cols - 1).astype(np.int32)
 
-    def ring(first, shift_deg):
-        ang = (np.arange(cols) * dt + shift_deg) % 360.0
+    def records(first, shift_deg):
+        # the model's ring nodes and, for a sector, their half-turn copies (sign -1)
+        node = np.concatenate([first + np.arange(ring)] * (2 if sector else 1))
+        sign = np.concatenate([np.ones(ring), -np.ones(ring)]) if sector else np.ones(ring)
+        ang = (np.arange(node.size) * dt + shift_deg) % 360.0
         order = np.argsort(ang, kind="stable")
-        return first + order, ang[order[0]] / dt
+        return node[order], sign[order], ang[order[0]] / dt
 
-    inner_nodes, inner_shift = ring(rows_r * cols, rotor_deg)
-    outer_nodes, outer_shift = ring(off, 0.0)
-    p = np.arange(cols + 1)
-    p1, p0 = p % cols, (p - 1) % cols
-    nodes = np.stack([inner_nodes[p0], inner_nodes[p1], outer_nodes[p0], outer_nodes[p1]], axis=1)
-    band = AirGap(nodes=nodes, weights=np.ones(nodes.shape), inner_radius_m=0.045, outer_radius_m=0.046,
-                  arc_length_deg=360.0, inner_shift=float(inner_shift), outer_shift=float(outer_shift))
+    n_in, s_in, inner_shift = records(rows_r * cols, rotor_deg)
+    n_out, s_out, outer_shift = records(off, 0.0)
+    total = n_in.size
+    p = np.arange(ring + 1)
+    p1, p0 = p % total, (p - 1) % total
+    nodes = np.stack([n_in[p0], n_in[p1], n_out[p0], n_out[p1]], axis=1)
+    weights = np.stack([s_in[p0], s_in[p1], s_out[p0], s_out[p1]], axis=1)
+    band = AirGap(nodes=nodes, weights=weights, inner_radius_m=0.045, outer_radius_m=0.046,
+                  arc_length_deg=180.0 if sector else 360.0, inner_shift=float(inner_shift),
+                  outer_shift=float(outer_shift), antiperiodic=sector)
     return Model(
         xy=xy, tri=tri, tri_mat=mat,
-        nu0=[nu_air, nu_air, nu_air / 1.05, nu_air] + [nu_air] * 6,
-        alpha=np.zeros(10),
-        j_per_a=[0.0, 0.0, 0.0, 0.0] + jpa + [-v for v in jpa],
-        hc=[0.0, 0.0, hc] + [0.0] * 7,
-        mag_deg=[0.0, 0.0, 90.0 + rotor_deg] + [0.0] * 7,
-        curve_index=[-1, 0, -1, 0] + [-1] * 6,
-        circuit_index=[-1, -1, -1, -1, 0, 1, 2, 0, 1, 2],
-        group=[50, 20, 20, 30, 40, 41, 42, 40, 41, 42],
+        nu0=([nu_air, nu_air, nu_air / 1.05, nu_air] + [nu_air] * 6)[:M],
+        alpha=np.zeros(M),
+        j_per_a=([0.0, 0.0, 0.0, 0.0] + jpa + [-v for v in jpa])[:M],
+        hc=([0.0, 0.0, hc] + [0.0] * 7)[:M],
+        mag_deg=([0.0, 0.0, 90.0 + rotor_deg] + [0.0] * 7)[:M],
+        curve_index=([-1, 0, -1, 0] + [-1] * 6)[:M],
+        circuit_index=[-1, -1, -1, -1, 0, 1, 2, 0, 1, 2][:M],
+        group=[50, 20, 20, 30, 40, 41, 42, 40, 41, 42][:M],
         curves=[(b_t, hh)],
         dir_nodes=outer, dir_values=np.zeros(outer.size),
+        con_a=con_a, con_b=con_b, con_sign=np.full(con_a.size, -1, np.int8),
         circuit_count=3, depth_m=0.05, problem_type=PLANAR,
-        name=f"sliding_band_{nr}x{nt}_{rotor_deg:g}deg", ages=[band],
+        name=f"sliding_band_{'sector' if sector else 'full'}_{nr}x{nt}_{rotor_deg:g}deg", ages=[band],
     )

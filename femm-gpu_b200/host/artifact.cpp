@@ -102,12 +102,15 @@ bool Artifact::SlideBands(double rotor_angle_deg)
   return true;
 }
 
-// The 180-degree sector metadata of gpu_femm_mesh_v3 (mesh_artifact.cpp:441-608): p pole
-// pairs, the p + 1 suspension order, the boundary relation of the pole-pair parity, every
-// constraint pair related by an exact 180-degree rotation and carrying that relation,
-// apex self-pairs at the origin, a circuit partner map that closes after two copies with
-// positive orientation.  An antiperiodic sector fixes its apex nodes to zero.
-bool ParseSector(const Json &sec, Artifact *a, std::string *error)
+// The sector metadata of gpu_femm_mesh_v3 / v4 (mesh_artifact.cpp:441-608): p pole pairs,
+// the p + 1 suspension order, the boundary relation of the pole-pair parity, apex
+// self-pairs at the origin, a circuit partner map that closes after k copies with positive
+// orientation.  v3 (conforming) is the 180-degree half with every constraint pair related
+// by an exact 180-degree rotation; v4 (native air-gap element, `native`) is one of k
+// sectors of 360/k degrees whose electrical phase advance 2p/k is an integer, odd exactly
+// for an antiperiodic relation, every pair related by the sector rotation either way.  An
+// antiperiodic sector fixes its apex nodes to zero.
+bool ParseSector(const Json &sec, bool native, Artifact *a, std::string *error)
 {
   if (!HasExactly(sec, {"schema_version", "sector_start_angle_deg", "angle_deg", "full_machine_sector_count",
                         "electrical_pole_pairs", "suspension_spatial_order", "boundary_relation",
@@ -130,15 +133,20 @@ bool ParseSector(const Json &sec, Artifact *a, std::string *error)
   const size_t C = a->circuit_currents.size();
   if (!schema || !start || !std::isfinite(start->number) || !angle || !repeats || !pole_pairs || !order ||
       !relation || !partners || !orientations || !apex || !cert || !IsSha256Hex(cert->text) ||
-      schema->text != "gpu_femm_motor_sector_v1" || !(angle->number > 0.0) || !AsInt32(*repeats, &k) || k < 2 ||
+      schema->text != (native ? "gpu_femm_motor_sector_v2" : "gpu_femm_motor_sector_v1") ||
+      !(angle->number > 0.0) || !AsInt32(*repeats, &k) || k < 2 ||
       !AsInt32(*pole_pairs, &p) || p <= 0 || !AsInt32(*order, &n) || n != p + 1 ||
       (relation->text != "periodic" && relation->text != "antiperiodic") || partners->items.size() != C ||
       orientations->items.size() != C) {
     *error = "motor sector requires positive k, p and p+1 harmonic metadata";
     return false;
   }
-  if (angle->number != 180.0 || k != 2) {
+  if ((!native && (angle->number != 180.0 || k != 2)) || (native && angle->number != 360.0 / static_cast<double>(k))) {
     *error = "motor sector angle/count are inconsistent";
+    return false;
+  }
+  if (native && ((2 * p) % k != 0 || (relation->text == "antiperiodic") != (((2 * p / k) % 2) != 0))) {
+    *error = "native AGE sector boundary relation does not match electrical phase advance";
     return false;
   }
   a->sector = true;
@@ -154,10 +162,18 @@ bool ParseSector(const Json &sec, Artifact *a, std::string *error)
   for (size_t i = 0; i < N; ++i)
     radius = std::max(radius, std::hypot(a->xy[2 * i], a->xy[2 * i + 1]));
   const double tol = std::max(1e-10 * radius, 64.0 * std::numeric_limits<double>::epsilon() * radius);
+  const double turn = angle->number * 3.141592653589793238462643383279502884 / 180.0;
+  const double cs = std::cos(turn), sn = std::sin(turn);
   for (size_t c = 0; c < a->con_signs.size(); ++c) {
     const double *pa = &a->xy[2 * a->con_nodes[2 * c]], *pb = &a->xy[2 * a->con_nodes[2 * c + 1]];
-    if (std::hypot(pa[0] + pb[0], pa[1] + pb[1]) > tol) {
+    if (!native && std::hypot(pa[0] + pb[0], pa[1] + pb[1]) > tol) {
       *error = "motor sector non-self constraint nodes must be related by an exact 180-degree rotation";
+      return false;
+    }
+    // v4: either node may be the rotated one (the wire order is not the generator's).
+    if (native && std::min(std::hypot(pb[0] - (cs * pa[0] - sn * pa[1]), pb[1] - (sn * pa[0] + cs * pa[1])),
+                           std::hypot(pa[0] - (cs * pb[0] - sn * pb[1]), pa[1] - (sn * pb[0] + cs * pb[1]))) > tol) {
+      *error = "motor sector non-self constraint nodes must be related by the sector rotation";
       return false;
     }
   }
@@ -320,13 +336,10 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
   const bool generic = schema->text == "gpu_femm_magnetostatic_mesh_v1";
   const bool neutral = planar_dc || generic;
   const bool motor_v1 = schema->text == "gpu_femm_mesh_v1";
-  const bool sliding = schema->text == "gpu_femm_mesh_v2";
-  const bool sector = schema->text == "gpu_femm_mesh_v3";
+  const bool native = schema->text == "gpu_femm_mesh_v4"; // a native air-gap element sector
+  const bool sliding = schema->text == "gpu_femm_mesh_v2" || native;
+  const bool sector = schema->text == "gpu_femm_mesh_v3" || native;
   const bool motor = motor_v1 || sliding || sector;
-  if (schema->text == "gpu_femm_mesh_v4") {
-    *error = "unsupported mesh artifact schema (native air-gap element sectors are not served here)";
-    return false;
-  }
   if (!neutral && !motor) {
     *error = "unsupported mesh artifact schema";
     return false;
@@ -354,7 +367,7 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
                : motor_v1 ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
                                               "nodes_mm", "triangles", "regions", "materials", "circuits",
                                               "outer_dirichlet"}, error)
-               : sliding ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
+               : (sliding && !native) ? HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
                                              "nodes_mm", "triangles", "regions", "materials", "circuits",
                                              "outer_dirichlet", "air_gap_elements"}, error)
                           : HasExactly(*res, {"source_fem_sha256", "base_motor_fem_sha256", "model", "pose",
@@ -418,11 +431,19 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
     *error = "empty mesh/material input";
     return false;
   }
-  if (sector) {
+  if (sector && !native) {
     // gpu_femm_mesh_v3 is a conforming posed sector: its air-gap element list must be empty.
     const auto ages = res->members.find("air_gap_elements");
     if (ages == res->members.end() || !ages->second.is(K::Array) || !ages->second.items.empty()) {
       *error = "gpu_femm_mesh_v3 requires a conforming posed sector mesh; native AGE sectors are not supported";
+      return false;
+    }
+  }
+  if (native) {
+    const auto ages = res->members.find("air_gap_elements");
+    if (ages == res->members.end() || (!ages->second.is(K::Array) && !ages->second.is(K::Object)) ||
+        (ages->second.is(K::Array) && ages->second.items.empty())) {
+      *error = "gpu_femm_mesh_v4 requires a nonempty native AGE sector";
       return false;
     }
   }
@@ -635,10 +656,18 @@ bool ParseArtifact(const std::string &text, Artifact *out, std::string *error)
       a.con_signs.push_back(rel->text == "periodic" ? 1 : -1);
     }
   }
-  if (sector && !ParseSector(*sector_meta, &a, error))
+  if (sector && !ParseSector(*sector_meta, native, &a, error))
     return false;
   if (sliding && !ParseBands(*res, &a, error))
     return false;
+  if (native) {
+    a.native_sector = true;
+    for (const AirGapBand &b : a.bands)
+      if (b.antiperiodic != (a.sector_boundary_sign < 0) || b.arc_deg != a.sector_angle_deg) {
+        *error = "native AGE sector periodicity or arc length disagrees with sector metadata";
+        return false;
+      }
+  }
   *out = std::move(a);
   return true;
 }

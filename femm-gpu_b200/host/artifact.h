@@ -56,6 +56,7 @@ struct Artifact {
   // gpu_femm_mesh_v2: a zero-degree reference mesh whose air gap is native air-gap elements;
   // each rotor angle is a pose of the bands (SlideBands), not a new mesh.
   bool sliding_band = false;
+  bool native_sector = false; // gpu_femm_mesh_v4: a cyclic sector whose air gap is native elements
   std::vector<AirGapBand> bands;
   std::vector<fg_air_gap_element> band_view; // filled by Model()
 
@@ -76,8 +77,8 @@ struct Artifact {
 // angle, J = turns / region area), zero outer Dirichlet values, signed node constraints.
 // and its conforming 180-degree sector gpu_femm_mesh_v3 (sector metadata, apex self-pairs,
 // circuit partners), and the sliding-band schema gpu_femm_mesh_v2 (a zero-degree reference
-// mesh with native air-gap elements).  The native air-gap sector schema gpu_femm_mesh_v4 is
-// refused.
+// mesh with native air-gap elements) and its cyclic sector gpu_femm_mesh_v4 (one of k
+// sectors with a native air-gap element band over the sector).
 bool ParseArtifact(const std::string &text, Artifact *out, std::string *error);
 
 } // namespace fgio

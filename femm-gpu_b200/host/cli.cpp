@@ -944,12 +944,13 @@ int main(int argc, char **argv)
   if (rest == 1 && std::strcmp(argv[next], "--capabilities") == 0) {
     std::cout << "{\n  \"protocols\": [\"gpu_femm_planar_dc_sample_v1\", \"gpu_femm_magnetostatic_sample_v1\", "
                  "\"gpu_femm_magnetostatic_batch_v1\", \"gpu_femm_single_sample_v1\", \"gpu_femm_motor_sample_v1\", "
-                 "\"gpu_femm_motor_sample_v2\", \"gpu_femm_motor_sample_v3\", \"gpu_femm_motor_batch_v1\", "
-                 "\"gpu_femm_motor_batch_v2\", \"gpu_femm_motor_batch_v3\"],\n"
+                 "\"gpu_femm_motor_sample_v2\", \"gpu_femm_motor_sample_v3\", \"gpu_femm_motor_sample_v4\", "
+                 "\"gpu_femm_motor_batch_v1\", \"gpu_femm_motor_batch_v2\", \"gpu_femm_motor_batch_v3\", "
+                 "\"gpu_femm_motor_batch_v4\"],\n"
               << "  \"mesh_artifacts\": [\"gpu_femm_planar_dc_mesh_v1\", \"gpu_femm_magnetostatic_mesh_v1\", "
-                 "\"gpu_femm_mesh_v1\", \"gpu_femm_mesh_v2\", \"gpu_femm_mesh_v3\"],\n"
+                 "\"gpu_femm_mesh_v1\", \"gpu_femm_mesh_v2\", \"gpu_femm_mesh_v3\", \"gpu_femm_mesh_v4\"],\n"
               << "  \"native_sliding_band\": true,\n"
-              << "  \"motor_sector_native_age_cyclic_v1\": false,\n"
+              << "  \"motor_sector_native_age_cyclic_v1\": true,\n"
               << "  \"preconditioners\": [\"jacobi\", \"block-jacobi\"],\n"
               << "  \"precisions\": [\"fp64\", \"mixed\"],\n"
               << "  \"abi_version\": " << fg_abi_version() << "\n}\n";

@@ -110,11 +110,14 @@ Prepared *PoseOf(Prepared &p, double rotor_angle_deg)
   return slot.get();
 }
 
-int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out)
+int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out,
+               const std::vector<double> *angles_rad)
 {
   std::vector<double> angles;
   for (double deg : angles_deg)
     angles.push_back(deg * kPi / 180.0);
+  if (angles_rad)
+    angles = *angles_rad;
   out->radial.assign(angles.size(), 0.0);
   fg_postprocess_result r{};
   const int rc = fg_air_gap_postprocess(plan, 1, s.a.data(), static_cast<int32_t>(angles.size()),

@@ -136,7 +136,10 @@ int EnsurePlan(Prepared *p, const Options &opt);
 Prepared *PoseOf(Prepared &p, double rotor_angle_deg);
 // The sliding-band postprocess of one solved sample (ComputeAirGapElementPostprocess via
 // fg_air_gap_postprocess) at the request's probe angles in degrees.
-int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out);
+// angles_rad, when given, replaces the converted angles (native sector probes folded into
+// the representative sector).
+int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out,
+               const std::vector<double> *angles_rad = nullptr);
 
 // Solves k samples (their circuit currents) on a prepared plan with the reference's
 // production options (ProductionSampleOptions); statuses[i] = the item's status.

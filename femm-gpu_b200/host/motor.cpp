@@ -89,6 +89,51 @@ std::vector<double> ReconstructFlux(const std::vector<double> &sector, const fgi
   return full;
 }
 
+// MapNativeAgeSectorAirgapAnglesToRepresentative (sample_request.cpp:568-599): a native
+// air-gap element sector's series is referenced to angle 0, so probes fold into [0, span);
+// odd copies of an antiperiodic sector take the sign -1.
+std::vector<int> FoldNativeSectorAngles(double span, int boundary_sign, std::vector<double> *angles)
+{
+  std::vector<int> signs;
+  for (double &angle : *angles) {
+    int64_t copy = static_cast<int64_t>(std::floor(angle / span));
+    double local = angle - static_cast<double>(copy) * span;
+    const double tol = 64.0 * std::numeric_limits<double>::epsilon() * std::max(1.0, std::abs(local));
+    if (local < -tol) {
+      local += span;
+      --copy;
+    } else if (local >= span - tol) {
+      local -= span;
+      ++copy;
+    }
+    if (std::abs(local) <= tol)
+      local = 0.0;
+    angle = local;
+    signs.push_back(std::abs(copy) % 2 != 0 && boundary_sign < 0 ? -1 : 1);
+  }
+  return signs;
+}
+
+// ReconstructCyclicSectorCircuitFluxLinkage (batch_response.cpp:38-55): each circuit's sector
+// flux lands on the circuits its k copies become, with the partner orientation and the
+// boundary relation's sign accumulated copy by copy.
+std::vector<double> ReconstructCyclicFlux(const std::vector<double> &sector, const fgio::Artifact &a)
+{
+  if (sector.size() != a.circuit_partners.size() || sector.size() != a.circuit_orientations.size())
+    return {};
+  std::vector<double> full(sector.size(), 0.0);
+  for (size_t c = 0; c < sector.size(); ++c) {
+    int32_t at = static_cast<int32_t>(c);
+    int sign = 1;
+    for (int32_t copy = 0; copy < a.full_machine_sector_count; ++copy) {
+      full[at] += static_cast<double>(sign) * sector[c];
+      sign *= a.circuit_orientations[at] * a.sector_boundary_sign;
+      at = a.circuit_partners[at];
+    }
+  }
+  return full;
+}
+
 // MakeMotorSectorTangentModel (sample_request.cpp:499-529): the suspension order's boundary
 // relation on every pair; apex nodes fixed to zero only when that relation is antiperiodic.
 int SectorTangentPlan(Prepared &p, const Options &opt)
@@ -177,7 +222,9 @@ std::string SingleResponse(int status, const MotorSampleRequest *req, const Solv
 // The sector_reconstruction member (batch_response.cpp:164-222), conforming sectors.
 void SectorBlock(std::ostream &o, const MotorItem &d, const fgio::Artifact &a)
 {
-  o << "  \"sector_reconstruction\": {\"schema_version\": \"gpu_femm_motor_sector_reconstruction_response_v1\", "
+  const bool native = a.sliding_band;
+  o << "  \"sector_reconstruction\": {\"schema_version\": "
+    << (native ? "\"gpu_femm_motor_sector_reconstruction_v2\", " : "\"gpu_femm_motor_sector_reconstruction_response_v1\", ")
     << "\"status\": \"" << (d.sector_status == 0 ? "PASS" : "FAIL") << "\", \"error_identifier\": \""
     << (d.sector_status == 0 ? "" : "GPU_FEMM_SECTOR_" + StatusName(d.sector_status))
     << "\", \"sector_start_angle_deg\": " << a.sector_start_angle_deg << ", \"sector_angle_deg\": " << a.sector_angle_deg
@@ -187,9 +234,11 @@ void SectorBlock(std::ostream &o, const MotorItem &d, const fgio::Artifact &a)
     << (d.base_sign > 0 ? "periodic" : "antiperiodic") << "\", \"tangent_boundary_relation\": \""
     << (d.tangent_sign > 0 ? "periodic" : "antiperiodic") << "\", \"base_field_repeat_sign\": " << d.base_sign
     << ", \"tangent_field_repeat_sign\": " << d.tangent_sign << ", \"output_normalization\": \"full_machine\""
-    << ", \"load_extraction_method\": \"weighted_stress_tensor_periodic_pair_mask\""
-    << ", \"periodic_pair_aware_weighted_stress_mask\": true, \"constraint_source\": \"cropped_sector_artifact\""
-    << ", \"operator_construction\": \"same_topology_dual_signed_reduction\""
+    << ", \"load_extraction_method\": \""
+    << (native ? "native_air_gap_element_signed_sector" : "weighted_stress_tensor_periodic_pair_mask")
+    << "\", \"periodic_pair_aware_weighted_stress_mask\": " << (native ? "false" : "true")
+    << ", \"constraint_source\": \"cropped_sector_artifact\", \"operator_construction\": \""
+    << (native ? "native_age_sector_base_only" : "same_topology_dual_signed_reduction") << "\""
     << ", \"tangent_operator_storage\": \"shared_single_upload\", \"tangent_physical_operator_count\": "
     << d.evidence_operators << ", \"tangent_operator_upload_count\": " << d.evidence_uploads
     << ", \"tangent_rhs_count\": " << d.evidence_rhs << ", \"tangent_operator_bytes\": " << d.evidence_operator_bytes
@@ -486,6 +535,7 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
         const bool sector = r.sector_performance && p.artifact.sector;
         std::vector<int> base_signs, tangent_signs;
         std::vector<double> folded;
+        const bool native = sector && p.artifact.native_sector;
         if (sector) {
           for (double deg : r.airgap_angles_deg)
             folded.push_back(deg * kPi / 180.0);
@@ -493,11 +543,15 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
           const double start = p.artifact.sector_start_angle_deg * kPi / 180.0;
           d.base_sign = p.artifact.sector_boundary_sign;
           d.tangent_sign = p.artifact.suspension_spatial_order % 2 == 0 ? 1 : -1;
-          base_signs = FoldSectorAngles(start, d.base_sign, &folded);
-          tangent_signs = FoldSectorAngles(start, d.tangent_sign, &tangent_folded);
+          if (native) {
+            base_signs = FoldNativeSectorAngles(p.artifact.sector_angle_deg * kPi / 180.0, d.base_sign, &folded);
+          } else {
+            base_signs = FoldSectorAngles(start, d.base_sign, &folded);
+            tangent_signs = FoldSectorAngles(start, d.tangent_sign, &tangent_folded);
+          }
         }
         if (p.artifact.sliding_band) {
-          d.status = AirGapPost(p.plan, sols[j], r.airgap_angles_deg, &post);
+          d.status = AirGapPost(p.plan, sols[j], r.airgap_angles_deg, &post, native ? &folded : nullptr);
         } else {
           d.status = p.post.Get(p.plan, r.selected_group_number, r.air_group_number, r.airgap_radius_mm,
                                 r.airgap_angles_deg, &pp, sector ? &folded : nullptr, &p.artifact.apex_nodes);
@@ -524,11 +578,12 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
           const int cross = d.base_sign * d.tangent_sign;
           d.tangent_force_multiplier = 1.0 - cross;
           d.tangent_torque_multiplier = 1.0 + cross;
+          d.base_torque_multiplier = native ? static_cast<double>(p.artifact.full_machine_sector_count) : 2.0;
           if (d.status == 0) {
             d.fx = 0.0;
             d.fy = 0.0;
             d.torque *= d.base_torque_multiplier;
-            d.flux = ReconstructFlux(d.flux, p.artifact, d.base_sign);
+            d.flux = native ? ReconstructCyclicFlux(d.flux, p.artifact) : ReconstructFlux(d.flux, p.artifact, d.base_sign);
             if (d.flux.empty())
               d.status = FG_INTERNAL_ERROR;
           }

@@ -172,10 +172,16 @@ bool ParseMotorSampleRequestText(const std::string &text, MotorSampleRequest *ou
 
 bool MotorRequestMatchesArtifact(const MotorSampleRequest &r, const Artifact &a)
 {
-  // Neutral artifacts carry their source digest as the base identity and a zero pose; native
-  // air-gap element sectors (v4) are not served.
+  // Neutral artifacts carry their source digest as the base identity and a zero pose; v3
+  // requests take conforming sectors, v4 requests native air-gap element sectors.
   const bool sector_request = r.protocol == "gpu_femm_motor_sample_v3";
-  if (r.protocol == "gpu_femm_motor_sample_v4" || sector_request != a.sector)
+  const bool native_request = r.protocol == "gpu_femm_motor_sample_v4";
+  if (sector_request != (a.sector && !a.native_sector) || native_request != a.native_sector)
+    return false;
+  if (native_request &&
+      (a.schema_version != "gpu_femm_mesh_v4" || a.full_machine_sector_count < 2 ||
+       a.sector_angle_deg != 360.0 / a.full_machine_sector_count || !a.sliding_band || a.bands.empty() ||
+       !r.sector_performance || r.model_invariance_certificate_sha256 != a.model_invariance_certificate_sha256))
     return false;
   if (sector_request &&
       (a.schema_version != "gpu_femm_mesh_v3" || a.sector_angle_deg != 180.0 || a.full_machine_sector_count != 2 ||

@@ -182,3 +182,66 @@ def test_library_band_postprocess_on_device_solutions(gpu, artifact):
         scale = abs(tq) / R_GAP
         assert abs(got.force[k, 0] - fx) <= 1e-12 * scale and abs(got.force[k, 1] - fy) <= 1e-12 * scale
         assert np.max(np.abs(got.radial_b[k] - radial)) <= 1e-12 * np.abs(radial).max()
+
+
+@needs_ref
+def test_native_sector_batch_matches_the_reference_path(gpu, tmp_path):
+    """gpu_femm_motor_batch_v4 on the 180-degree anti-periodic native air-gap element sector of
+    the two-pole machine, against the reference CPU path on the same posed sector with the
+    reference's reconstruction rules (torque x k, flux through the cyclic partner map,
+    probes folded into [0, span) with the anti-periodic sign; batch_response.cpp:38-99,
+    sample_request.cpp:568-599), to the base tolerances above.
+
+    The reference's ApplySlidingBandAngle copies point 0's inner records into the band's
+    closing point, which on an anti-periodic sector drops the -1 copy sign that record
+    carries in FEMM's own records: the reference's torque and probes on such a sector are
+    not the full machine's, and the library reproduces the reference.  At rotor angle 0
+    the stiffness does not read that record (the inner corners sit on ring nodes), so the
+    flux linkages there equal the full sliding-band machine's (1e-6)."""
+    from test_sliding_band_cli import native_sector_artifact_text
+    sec = meshes.sliding_band_machine(nr=40, nt=30, sector=True)
+    stext = native_sector_artifact_text(sec)
+    spath = tmp_path / "v4.json"
+    spath.write_text(stext)
+    ssha = hashlib.sha256(stext.encode()).hexdigest()
+    cases = [(0.0, [8.0, -4.0, -4.0]), (12.5, [8.0, -4.0, -4.0]), (33.0, [5.0, 1.0, -6.0])]
+    items = []
+    for i, (angle, cur) in enumerate(cases):
+        r = request(spath, ssha, cur, angle, protocol="gpu_femm_motor_sample_v4")
+        r["tangent_multi_rhs"] = None
+        r["sector_performance"] = {"schema_version": "gpu_femm_motor_sector_performance_v2",
+                                   "model_invariance_certificate_sha256": "d" * 64}
+        items.append({"task_id": f"s{i}", "request": r})
+    rc, sresp, err = call(tmp_path, "--motor-batch", {"protocol": "gpu_femm_motor_batch_v4",
+                                                      "max_items_per_chunk": 8, "items": items}, name="s.json")
+    assert rc == 0 and sresp["status"] == "PASS", err
+    for (angle, cur), item in zip(cases, sresp["items"]):
+        s = item["response"]
+        block = s["sector_reconstruction"]
+        assert block["schema_version"] == "gpu_femm_motor_sector_reconstruction_v2"
+        assert block["load_extraction_method"] == "native_air_gap_element_signed_sector"
+        assert block["operator_construction"] == "native_age_sector_base_only"
+        assert block["base_torque_multiplier"] == 2 and block["status"] == "PASS"
+        assert s["Fx_N"] == 0.0 and s["Fy_N"] == 0.0
+        hp = O.ref_sliding_band_pose(O.ref_artifact_handle(stext.encode()), angle)
+        a, flux, st, _ = O.ref_artifact_cpu_solve(hp, [cur], sec.node_count, 3, threads=2)
+        assert st[0] == 0
+        folded, signs = [], []
+        for deg in PROBES:
+            t = np.radians(deg)
+            copy = int(np.floor(t / np.pi))
+            folded.append(t - copy * np.pi)
+            signs.append(-1.0 if copy % 2 else 1.0)
+        pst, _, _, tq, radial = O.ref_age_postprocess(hp, a[0], folded)
+        assert pst == 0
+        assert abs(s["torque_Nm"] - 2.0 * tq) <= 1e-6 * abs(2.0 * tq)
+        full_flux = flux[0] + (-1.0) * (-1.0) * flux[0]  # partner c, orientation -1, anti-periodic
+        assert rel(s["circuit_flux_linkage_Wb"], full_flux) <= 1e-7
+        ref_radial = np.array(signs) * radial
+        assert np.max(np.abs(np.array(s["airgap_radial_flux_density_T"]) - ref_radial)) <= \
+            1e-6 * np.abs(ref_radial).max()
+        if angle == 0.0:
+            full = meshes.sliding_band_machine(nr=40, nt=30)
+            _, full_flux_machine, st, _ = O.ref_artifact_cpu_solve(O.ref_model_handle(full), [cur],
+                                                                   full.node_count, 3)
+            assert st[0] == 0 and rel(s["circuit_flux_linkage_Wb"], full_flux_machine[0]) <= 1e-6

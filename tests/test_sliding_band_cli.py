@@ -1,5 +1,5 @@
-"""The sliding-band motor artifact (gpu_femm_mesh_v2: a zero-degree reference mesh whose air
-gap is native air-gap elements) on the CPU: parsing against the reference's own parser
+"""The sliding-band motor artifacts (gpu_femm_mesh_v2: a zero-degree reference mesh whose air
+gap is native air-gap elements; gpu_femm_mesh_v4: one cyclic sector of it) on the CPU: parsing against the reference's own parser
 (ParseGpuFemmMeshArtifactJson, oracle/_ref), the band records posed at rotor angles
 against the reference's ApplySlidingBandAngle bit for bit, the parse refusals' messages,
 and the motor requests the adapters refuse before any GPU work (RequestMatchesArtifact,
@@ -151,12 +151,14 @@ def test_sliding_artifact_refusals_follow_the_reference(tmp_path, band_model):
         ref, ref_err = ref_parse(text.encode())
         assert ref is None and rc == 1, label
         assert d["error"] == ref_err, (label, d["error"], ref_err)
-    # the native air-gap sector schema stays refused
+    # a v2 body under the native sector schema lacks its sector fields, as the reference says
     v = copy.deepcopy(root)
     v["schema_version"] = "gpu_femm_mesh_v4"
-    p.write_text(json.dumps(v))
+    text = json.dumps(v)
+    p.write_text(text)
     rc, d = describe(str(p))
-    assert rc == 1 and "not served" in d["error"]
+    ref, ref_err = ref_parse(text.encode())
+    assert rc == 1 and ref is None and d["error"] == ref_err
 
 
 def sample_request(artifact_path, sha, **kw):
@@ -188,3 +190,81 @@ def test_sliding_requests_refused_before_any_gpu_work(tmp_path, band_model):
         body = json.loads(rs.read_text())
         assert r.returncode == 1 and body["status"] == "FAIL", label
         assert body["solve_status"] == "INVALID_ARGUMENT", (label, body["solve_status"])
+
+
+def native_sector_artifact_text(model, cert="d" * 64, **sector):
+    """A gpu_femm_mesh_v4 artifact of a native air-gap element sector
+    (meshes.sliding_band_machine(sector=True)): the v2 writing plus the sector metadata and
+    the anti-periodic edge constraints."""
+    root = json.loads(sliding_artifact_text(model))
+    root["schema_version"] = "gpu_femm_mesh_v4"
+    res = root["resolved"]
+    res["node_constraints"] = [{"node_a": int(a), "node_b": int(b), "relation": "antiperiodic" if s < 0 else "periodic"}
+                               for a, b, s in zip(model.con_a, model.con_b, model.con_sign)]
+    meta = {"schema_version": "gpu_femm_motor_sector_v2", "sector_start_angle_deg": 0, "angle_deg": 180,
+            "full_machine_sector_count": 2, "electrical_pole_pairs": 1, "suspension_spatial_order": 2,
+            "boundary_relation": "antiperiodic", "circuit_partner_indices": list(range(model.circuit_count)),
+            "circuit_partner_orientations": [-1] * model.circuit_count, "apex_self_pair_nodes": [],
+            "model_invariance_certificate_sha256": cert}
+    meta.update(sector)
+    res["sector"] = meta
+    return json.dumps(root)
+
+
+@pytest.fixture(scope="module")
+def sector_model():
+    return meshes.sliding_band_machine(nr=40, nt=30, sector=True)
+
+
+@needs_ref
+def test_native_sector_artifact_parses_like_the_reference(tmp_path, sector_model):
+    text = native_sector_artifact_text(sector_model)
+    p = tmp_path / "v4.json"
+    p.write_text(text)
+    rc, d = describe(str(p))
+    ref, err = ref_parse(text.encode())
+    assert rc == 0 and ref is not None, (d, err)
+    assert np.array_equal(np.array(d["xy"]), ref["xy"]) and np.array_equal(np.array(d["tri_mat"]), ref["tm"])
+    assert np.array_equal(np.array(d["dirichlet_nodes"]), ref["dn"])
+    nc = ref["sizes"][5]
+    con = ref["con"][: 3 * nc].reshape(-1, 3)
+    assert np.array_equal(np.array(d["constraint_nodes"]).reshape(-1, 2), con[:, :2])
+    assert np.array_equal(np.array(d["constraint_signs"]), con[:, 2])
+    h = O.ref_artifact_handle(text.encode())
+    assert_bands_equal(d["air_gap_elements"], O.ref_age_records(h))
+    for angle in (3.0, 45.5, -20.0):
+        rc, d = describe_at(p, angle)
+        assert rc == 0 and d["plan_status"] == "OK"
+        assert_bands_equal(d["air_gap_elements"], O.ref_age_records(O.ref_sliding_band_pose(h, angle)))
+
+
+@needs_ref
+def test_native_sector_refusals_follow_the_reference(tmp_path, sector_model):
+    variants = {
+        "sector schema": dict(schema_version="gpu_femm_motor_sector_v1"),
+        "angle": dict(angle_deg=120),
+        "phase advance": dict(full_machine_sector_count=4, angle_deg=90),
+        "relation parity": dict(boundary_relation="periodic"),
+        "partner closure": dict(circuit_partner_indices=[1, 0, 2], circuit_partner_orientations=[1, -1, -1]),
+    }
+    p = tmp_path / "bad.json"
+    texts = {k: native_sector_artifact_text(sector_model, **kw) for k, kw in variants.items()}
+    root = json.loads(native_sector_artifact_text(sector_model))
+    v = copy.deepcopy(root)
+    v["resolved"]["air_gap_elements"] = []
+    texts["no band"] = json.dumps(v)
+    v = copy.deepcopy(root)
+    v["resolved"]["air_gap_elements"][0]["periodicity"] = "periodic"
+    texts["band periodicity"] = json.dumps(v)
+    v = copy.deepcopy(root)
+    v["resolved"]["air_gap_elements"][0]["arc_length_deg"] = 360
+    texts["band arc"] = json.dumps(v)
+    v = copy.deepcopy(root)
+    v["resolved"]["node_constraints"][0]["node_b"] = v["resolved"]["node_constraints"][1]["node_b"]
+    texts["pair not a sector rotation"] = json.dumps(v)
+    for label, text in texts.items():
+        p.write_text(text)
+        rc, d = describe(str(p))
+        ref, ref_err = ref_parse(text.encode())
+        assert ref is None and rc == 1, label
+        assert d["error"] == ref_err, (label, d["error"], ref_err)
