@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
     p.add_argument("--sector-samples", type=int, default=64, help="samples of the shared-geometry sector form")
     p.add_argument("--hetero-meshes", type=int, default=64, help="meshes of the heterogeneous-batch form")
-    p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker"],
+    p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker", "sliding_band"],
                    help="run one form alone and print its JSON (profiling)")
     return p.parse_args()
 
@@ -405,6 +405,8 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
 
     out["streaming_worker"] = worker_form()
 
+    out["sliding_band"] = sliding_band_form()
+
     # Heterogeneous meshes: jittered squares with node counts log-uniform in [5k, 200k],
     # one sample each, in one multi-plan PCG launch per Newton step vs one plan at a time.
     rng = np.random.default_rng(11)
@@ -579,6 +581,58 @@ def postprocess_tangent_form(sector, cur, hcs, dev, stream, err):
     return out
 
 
+def sliding_band_form(angles=8, items=8):
+    """The native air-gap element row: the full two-pole sliding-band machine (38k nodes, the
+    1 mm gap a periodic band of 240 arcs) solved over a rotor-angle sweep.  Each angle is its
+    own operator (the band's pose), so each gets its own plan: the sweep is timed with host
+    buffers, plan set-up and the band postprocess (torque, 45 Fourier probes) included.
+    The reference CPU path (its host assembler with the band and FEMM's PCG, one sample per
+    host thread) solves one angle's samples as the CPU baseline, and their flux linkages
+    give the parity figure."""
+    import femm_gpu_b200 as fg
+    import oracle as O
+    from femm_gpu_b200 import meshes
+
+    degs = np.linspace(0.0, 30.0, angles, endpoint=False)
+    cur = meshes.seeded_currents(items, 3, 10.0, seed=6100)
+    probes = np.radians(np.linspace(0.0, 358.0, 45))
+    warm = fg.Plan(meshes.sliding_band_machine(rotor_deg=0.0))
+    warm.solve(cur[:2], outputs="a")
+    warm.close()
+    models = [meshes.sliding_band_machine(rotor_deg=float(d)) for d in degs]
+    t0 = time.perf_counter()
+    torques, statuses, first = [], [], None
+    for m in models:
+        p = fg.Plan(m)
+        r = p.solve(cur, outputs="a")
+        post = p.air_gap_postprocess(r.a, probes)
+        torques.append(post.torque.tolist())
+        statuses += [i.status for i in r.info] + list(post.status)
+        if first is None:
+            first = r
+        p.close()
+    sweep_s = time.perf_counter() - t0
+    out = {"workload": f"full two-pole sliding-band machine, {models[0].node_count} nodes, "
+                       f"{models[0].ages[0].nodes.shape[0] - 1}-arc periodic band; {angles} rotor angles x "
+                       f"{items} samples, a plan per angle, host buffers, band postprocess included",
+           "solves_per_s_e2e": angles * items / sweep_s, "sweep_seconds": sweep_s,
+           "all_ok": all(s_ == 0 for s_ in statuses),
+           "torque_nm_at_first_sample": [t[0] for t in torques]}
+    if O.ref() is not None:
+        threads = min(os.cpu_count() or 1, items)
+        t0 = time.perf_counter()
+        a, flux, st, *_ = O.ref_cpu_newton_batch(models[0], cur[:threads], threads=threads)
+        cpu_s = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": threads / cpu_s, "unit": "solves/s", "cores": threads,
+                               "kind": "reference",
+                               "sample": f"{threads} samples of the first angle, one per host thread"}
+        out["speedup_vs_cpu"] = out["solves_per_s_e2e"] / out["cpu_baseline"]["value"]
+        out["flux_rel_err_vs_reference"] = float(max(
+            np.linalg.norm(first.flux[i] - flux[i]) / np.linalg.norm(flux[i]) for i in range(threads)))
+        out["reference_all_converged"] = bool((st == 0).all())
+    return out
+
+
 def worker_form(jobs=8, items=8):
     """The JSON boundary as a service: `jobs` batch files of `items` samples on one 40,401-node
     artifact, streamed through one `femm_gpu --worker` (plans resident across jobs, the next
@@ -715,6 +769,8 @@ def only_form(args):
     stream = torch.cuda.current_stream(dev)
     if args.only_form == "streaming_worker":
         out = worker_form()
+    elif args.only_form == "sliding_band":
+        out = sliding_band_form()
     else:
         rng = np.random.default_rng(77)
         cur = rng.uniform(-15.0, 15.0, size=(args.sector_samples, 3))
