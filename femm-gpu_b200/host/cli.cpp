@@ -145,7 +145,9 @@ std::string SampleResponse(int status, int solve_status, bool post_requested, in
   return o.str();
 }
 
-// PlanarDcRequestMatchesArtifact (sample_adapter.cpp:181-234) for neutral artifacts.
+// PlanarDcRequestMatchesArtifact (sample_adapter.cpp:181-234): the generic protocol on
+// generic artifacts (field solve only), the planar-DC protocol on the others; a sliding-band
+// artifact takes any sliding_band_angle_deg and needs the probe circle inside every band.
 bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
 {
   const bool generic_artifact = a.schema_version == "gpu_femm_magnetostatic_mesh_v1";
@@ -164,7 +166,30 @@ bool RequestMatchesArtifact(const SampleRequest &r, const Artifact &a)
   if (r.generic())
     return !post && r.force_group_number == -1 && r.stress_air_group_number == -1 &&
            r.airgap_radius_mm == 0.0 && r.airgap_angles_deg.empty() && r.sliding_band_angle_deg == 0.0;
-  return r.sliding_band_angle_deg == 0.0 && (!post || groups);
+  if (!a.sliding_band)
+    return r.sliding_band_angle_deg == 0.0 && (!post || groups);
+  if (!r.airgap_angles_deg.empty()) {
+    if (a.bands.empty())
+      return false;
+    for (const fgio::AirGapBand &b : a.bands) {
+      const double ri = 1000.0 * b.ri_m, ro = 1000.0 * b.ro_m, tol = 1e-9 * std::max(1.0, std::abs(ro));
+      if (r.airgap_radius_mm < ri - tol || r.airgap_radius_mm > ro + tol)
+        return false;
+    }
+  }
+  return true;
+}
+
+// The postprocess of one planar-DC sample: the band's for a sliding-band artifact, else the
+// weighted-stress one (sample_adapter.cpp:426-439).
+int PostSample(Prepared &p, const SampleRequest &r, const Solved &sol, Post *out)
+{
+  if (p.artifact.sliding_band)
+    return AirGapPost(p.plan, sol, r.airgap_angles_deg, out);
+  fg_postprocess *pp = nullptr;
+  const int rc = p.post.Get(p.plan, r.force_group_number, r.stress_air_group_number, r.airgap_radius_mm,
+                            r.airgap_angles_deg, &pp);
+  return rc != 0 ? rc : RunPost(pp, sol, out);
 }
 
 // Solves k samples on a prepared plan; statuses[i] = per-item status.
@@ -203,13 +228,20 @@ int Solve(const std::string &request_path, const std::string &response_path, con
     std::cerr << "FAIL planar-DC request: " << error << '\n';
     return 1;
   }
-  Prepared p;
-  Prepare(req.mesh_artifact_path, req.mesh_artifact_sha256, opt, &p);
-  int status = p.status;
-  std::string diagnostic = p.error;
-  if (status == 0 && !RequestMatchesArtifact(req, p.artifact)) {
+  Prepared base;
+  Prepare(req.mesh_artifact_path, req.mesh_artifact_sha256, opt, &base);
+  int status = base.status;
+  std::string diagnostic = base.error;
+  if (status == 0 && !RequestMatchesArtifact(req, base.artifact)) {
     status = FG_INVALID_ARGUMENT;
     diagnostic = "artifact physics, circuit count, group, or sliding-band request mismatch";
+  }
+  // ApplySlidingBandAngle (sample_adapter.cpp:404-408): a sliding-band artifact is solved at
+  // the request's band angle.
+  Prepared &p = status == 0 ? *PoseOf(base, req.sliding_band_angle_deg) : base;
+  if (status == 0 && p.status != 0) {
+    status = p.status;
+    diagnostic = p.error;
   }
   std::vector<Solved> sols;
   std::vector<int> st;
@@ -227,11 +259,7 @@ int Solve(const std::string &request_path, const std::string &response_path, con
   int post_status = 0;
   Post result;
   if (solve_status == 0 && post) {
-    fg_postprocess *pp = nullptr;
-    post_status = p.post.Get(p.plan, req.force_group_number, req.stress_air_group_number, req.airgap_radius_mm,
-                             req.airgap_angles_deg, &pp);
-    if (post_status == 0)
-      post_status = RunPost(pp, sols[0], &result);
+    post_status = PostSample(p, req, sols[0], &result);
     status = post_status;
   }
   const std::string body = SampleResponse(status, solve_status, post, post_status, &req,
@@ -246,6 +274,52 @@ int Solve(const std::string &request_path, const std::string &response_path, con
     return 1;
   }
   return 0;
+}
+
+// Solves the ready items of one operator (an artifact, or one band angle of a sliding-band
+// artifact) in chunks of max_items_per_chunk and writes their response bodies.
+void SolvePose(const fgio::BatchRequest &batch, const Options &opt, Prepared &p, const std::vector<size_t> &ready,
+               std::vector<std::string> *bodies, std::vector<int> *final_status, int *chunks, int *launches,
+               double *solve_s)
+{
+  const int plan_status = p.status != 0 ? p.status : EnsurePlan(&p, opt);
+  if (plan_status != 0) {
+    for (size_t i : ready) {
+      const SampleRequest &r = batch.items[i].request;
+      (*bodies)[i] = SampleResponse(plan_status, plan_status, r.postprocess_requested(), 0, &r, nullptr, p.error,
+                                    nullptr, "    ");
+      (*final_status)[i] = plan_status;
+    }
+    return;
+  }
+  const auto s0 = std::chrono::steady_clock::now();
+  for (size_t first = 0; first < ready.size(); first += batch.max_items_per_chunk) {
+    const size_t n = std::min<size_t>(batch.max_items_per_chunk, ready.size() - first);
+    std::vector<const SampleRequest *> reqs;
+    for (size_t j = 0; j < n; ++j)
+      reqs.push_back(&batch.items[ready[first + j]].request);
+    std::vector<Solved> sols;
+    std::vector<int> st;
+    SolveItems(p, reqs, &sols, &st, launches);
+    ++*chunks;
+    for (size_t j = 0; j < n; ++j) {
+      const size_t i = ready[first + j];
+      const SampleRequest &r = *reqs[j];
+      int status = st[j];
+      const int solve_status = status;
+      int post_status = 0;
+      Post result;
+      if (solve_status == 0 && r.postprocess_requested()) {
+        post_status = PostSample(p, r, sols[j], &result);
+        status = post_status;
+      }
+      (*bodies)[i] = SampleResponse(status, solve_status, r.postprocess_requested(), post_status, &r,
+                                    sols.empty() ? nullptr : &sols[j], "", &p.artifact, "    ",
+                                    post_status == 0 ? &result : nullptr);
+      (*final_status)[i] = status;
+    }
+  }
+  *solve_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
 }
 
 // Solves a parsed batch and returns the response text.  Items naming the same artifact are
@@ -289,48 +363,13 @@ std::string RunBatch(const fgio::BatchRequest &batch, const Options &opt, Artifa
       bodies[i] = SampleResponse(status, status, r.postprocess_requested(), 0, &r, nullptr, diag, nullptr, "    ");
       final_status[i] = status;
     }
-    const int plan_status = ready.empty() ? 0 : EnsurePlan(&p, opt);
-    if (plan_status != 0) {
-      for (size_t i : ready) {
-        const SampleRequest &r = batch.items[i].request;
-        bodies[i] = SampleResponse(plan_status, plan_status, r.postprocess_requested(), 0, &r, nullptr, "",
-                                   nullptr, "    ");
-        final_status[i] = plan_status;
-      }
-      ready.clear();
-    }
-    const auto s0 = std::chrono::steady_clock::now();
-    for (size_t first = 0; first < ready.size(); first += batch.max_items_per_chunk) {
-      const size_t n = std::min<size_t>(batch.max_items_per_chunk, ready.size() - first);
-      std::vector<const SampleRequest *> reqs;
-      for (size_t j = 0; j < n; ++j)
-        reqs.push_back(&batch.items[ready[first + j]].request);
-      std::vector<Solved> sols;
-      std::vector<int> st;
-      SolveItems(p, reqs, &sols, &st, &launches);
-      ++chunks;
-      for (size_t j = 0; j < n; ++j) {
-        const size_t i = ready[first + j];
-        const SampleRequest &r = *reqs[j];
-        int status = st[j];
-        const int solve_status = status;
-        int post_status = 0;
-        Post result;
-        if (solve_status == 0 && r.postprocess_requested()) {
-          fg_postprocess *pp = nullptr;
-          post_status = p.post.Get(p.plan, r.force_group_number, r.stress_air_group_number, r.airgap_radius_mm,
-                                   r.airgap_angles_deg, &pp);
-          if (post_status == 0)
-            post_status = RunPost(pp, sols[j], &result);
-          status = post_status;
-        }
-        bodies[i] = SampleResponse(status, solve_status, r.postprocess_requested(), post_status, &r,
-                                   sols.empty() ? nullptr : &sols[j], "", &p.artifact, "    ",
-                                   post_status == 0 ? &result : nullptr);
-        final_status[i] = status;
-      }
-    }
-    solve_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - s0).count();
+    // A sliding-band artifact has one operator per band angle: its items are solved per pose.
+    std::map<double, std::vector<size_t>> poses;
+    for (size_t i : ready)
+      poses[p.artifact.sliding_band ? batch.items[i].request.sliding_band_angle_deg : 0.0].push_back(i);
+    for (auto &pose : poses)
+      SolvePose(batch, opt, *PoseOf(p, pose.first), pose.second, &bodies, &final_status, &chunks, &launches,
+                &solve_s);
   }
   bool &pass = *all_pass;
   pass = true;

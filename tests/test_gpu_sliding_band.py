@@ -245,3 +245,40 @@ def test_native_sector_batch_matches_the_reference_path(gpu, tmp_path):
             _, full_flux_machine, st, _ = O.ref_artifact_cpu_solve(O.ref_model_handle(full), [cur],
                                                                    full.node_count, 3)
             assert st[0] == 0 and rel(s["circuit_flux_linkage_Wb"], full_flux_machine[0]) <= 1e-6
+
+
+def planar_request(path, sha, currents, band_deg, **kw):
+    r = {"protocol": "gpu_femm_planar_dc_sample_v1", "mesh_artifact_path": str(path), "mesh_artifact_sha256": sha,
+         "circuit_currents_A": [float(c) for c in currents], "force_group_number": 20,
+         "stress_air_group_number": 50, "airgap_radius_mm": 1e3 * R_GAP, "airgap_angles_deg": PROBES,
+         "sliding_band_angle_deg": band_deg, "compute_force_torque": True, "include_field_solution": False}
+    r.update(kw)
+    return r
+
+
+@needs_ref
+def test_planar_dc_solve_and_batch_on_a_sliding_band_artifact(gpu, tmp_path, artifact):
+    """The planar-DC adapter serves sliding-band artifacts as the reference does
+    (sample_adapter.cpp:396-439): sliding_band_angle_deg poses the bands, the band
+    postprocess answers; --solve equals --motor-single-sample at the same rotor angle bit for
+    bit, and a batch over two band angles equals its single solves."""
+    path, text, sha = artifact
+    cur = [8.0, -4.0, -4.0]
+    rc, s, err = call(tmp_path, "--solve", planar_request(path, sha, cur, 12.5), name="p.json")
+    assert rc == 0 and s["status"] == "PASS", err
+    rc, m, err = call(tmp_path, "--motor-single-sample", request(path, sha, cur, 12.5), name="m.json")
+    assert rc == 0, err
+    for key in ("Fx_N", "Fy_N", "torque_Nm", "circuit_flux_linkage_Wb", "airgap_radial_flux_density_T"):
+        assert s[key] == m[key], key
+    items = [{"task_id": f"i{i}", "request": planar_request(path, sha, c, a)}
+             for i, (c, a) in enumerate([(cur, 12.5), ([-3.0, 6.0, -3.0], 0.0), (cur, 0.0)])]
+    rc, b, err = call(tmp_path, "--batch", {"protocol": "gpu_femm_magnetostatic_batch_v1",
+                                            "max_items_per_chunk": 8, "items": items}, name="b.json")
+    assert rc == 0 and b["status"] == "PASS", err
+    first = b["items"][0]["response"]
+    assert first["torque_Nm"] == s["torque_Nm"] and first["circuit_flux_linkage_Wb"] == s["circuit_flux_linkage_Wb"]
+    _, _, _, flux, post = reference(path, text, 0.0, cur)
+    check_base(b["items"][2]["response"], flux, post)
+    # the probe circle must lie in the band
+    rc, bad, _ = call(tmp_path, "--solve", planar_request(path, sha, cur, 0.0, airgap_radius_mm=47.0), name="x.json")
+    assert rc == 1 and bad["status"] == "FAIL"
