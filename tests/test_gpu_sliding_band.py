@@ -282,3 +282,30 @@ def test_planar_dc_solve_and_batch_on_a_sliding_band_artifact(gpu, tmp_path, art
     # the probe circle must lie in the band
     rc, bad, _ = call(tmp_path, "--solve", planar_request(path, sha, cur, 0.0, airgap_radius_mm=47.0), name="x.json")
     assert rc == 1 and bad["status"] == "FAIL"
+
+
+@needs_ref
+def test_sliding_band_transactions_in_the_worker(gpu, tmp_path, artifact):
+    """Two worker transactions on one sliding-band artifact at different rotor angles (the
+    artifact and its poses resident between jobs) answer as one-shot --motor-batch runs."""
+    from test_worker_cli import envelope, run_worker
+    path, _, sha = artifact
+    bodies = []
+    for j, angles in enumerate(((0.0, 12.5), (12.5, 40.0))):
+        bodies.append({"protocol": "gpu_femm_motor_batch_v1", "max_items_per_chunk": 4,
+                       "items": [{"task_id": f"j{j}i{i}", "request": request(path, sha, [8.0, -4.0, -4.0 + i], a)}
+                                 for i, a in enumerate(angles)]})
+    out = tmp_path / "out"
+    out.mkdir()
+    envs = []
+    for j, body in enumerate(bodies):
+        b = tmp_path / f"b{j}.json"
+        b.write_text(json.dumps(body))
+        envs.append(envelope(j + 1, b, out / f"w{j}.json"))
+    st = run_worker(envs)
+    assert all(s["exit_code"] == 0 and s["error"] == "" for s in st), st
+    for j, body in enumerate(bodies):
+        got = json.load(open(out / f"w{j}.json"))
+        rc, ref, _ = call(tmp_path, "--motor-batch-profile", body, name=f"p{j}.json")
+        assert rc == 0
+        assert [i["response"] for i in got["items"]] == [i["response"] for i in ref["items"]]
