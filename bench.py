@@ -618,6 +618,28 @@ def sliding_band_form(angles=8, items=8):
            "solves_per_s_e2e": angles * items / sweep_s, "sweep_seconds": sweep_s,
            "all_ok": all(s_ == 0 for s_ in statuses),
            "torque_nm_at_first_sample": [t[0] for t in torques]}
+    # The torque-vs-angle pattern: one sample per rotor angle.  Each angle's own launch is
+    # latency-bound at this size, so the angles share one multi-plan launch per Newton step
+    # (what --motor-batch does for the poses of a chunk).
+    sweep = [meshes.sliding_band_machine(rotor_deg=float(d)) for d in np.linspace(0.0, 30.0, 16, endpoint=False)]
+    plans = [fg.Plan(m) for m in sweep]
+    c1 = cur[0]
+    t0 = time.perf_counter()
+    one = [p.solve([c1], outputs="a") for p in plans]
+    per_plan_s = time.perf_counter() - t0
+    multi = fg.Multi(plans)
+    multi.solve([c1] * len(plans), outputs=False)
+    t0 = time.perf_counter()
+    _, _, _, mflux, minfo = multi.solve([c1] * len(plans), outputs="a")
+    multi_s = time.perf_counter() - t0
+    out["one_sample_per_angle"] = {
+        "angles": len(plans), "per_plan_solves_per_s": len(plans) / per_plan_s,
+        "multi_plan_solves_per_s": len(plans) / multi_s, "speedup": per_plan_s / multi_s,
+        "flux_rel_err_multi_vs_per_plan": float(max(np.linalg.norm(mflux[i] - one[i].flux[0]) /
+                                                    np.linalg.norm(one[i].flux[0]) for i in range(len(plans)))),
+        "all_ok": all(i.status == 0 for i in minfo) and all(r.info[0].status == 0 for r in one)}
+    for p in plans:
+        p.close()
     if O.ref() is not None:
         threads = min(os.cpu_count() or 1, items)
         t0 = time.perf_counter()

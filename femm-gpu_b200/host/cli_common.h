@@ -116,8 +116,13 @@ struct Prepared {
   // A sliding-band artifact's poses: per requested rotor angle a copy of the artifact with
   // its bands slid to that angle, and that copy's own plan (the operator differs per angle).
   std::map<double, std::shared_ptr<Prepared>> poses;
+  // Further plans of this pose's model: one per extra sample when several samples of one
+  // pose share a multi-plan launch with other poses (one sample per plan there).
+  std::vector<fg_plan *> replicas;
   ~Prepared()
   {
+    for (fg_plan *r : replicas)
+      fg_plan_destroy(r);
     if (plan)
       fg_plan_destroy(plan);
   }
