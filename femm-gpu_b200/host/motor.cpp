@@ -380,13 +380,16 @@ void Tangent(fg_plan *plan, fg_postprocess *pp, const MotorSampleRequest &req, c
     d->tangent_status = FG_INTERNAL_ERROR;
 }
 
-// The samples of a chunk's sliding-band poses in one multi-plan launch per Newton step
-// (fg_multi): poses differ in their operator, and at motor mesh sizes each pose's own PCG
-// launch is latency-bound, so solving them side by side amortises every CG iteration's
-// barriers over all poses.  A pose's first sample runs on its plan, further samples on
-// replica plans of the same pose (the multi-plan launch takes one sample per plan).  Only
-// the plain FP64 Jacobi form (the multi-plan kernel's) and at least two poses; otherwise
-// false, and the caller solves pose by pose.  pre[item] = (solution, status).
+// The samples of a chunk's operators -- motor artifacts, and the poses of sliding-band
+// artifacts -- in one multi-plan launch per Newton step (fg_multi).  At motor mesh sizes
+// each operator's own PCG launch is latency-bound, so solving them side by side amortises
+// every CG iteration's barriers over all of them.  An operator's first sample runs on its
+// plan, further samples on replica plans of the same model (the multi-plan launch takes
+// one sample per plan).  Only the plain FP64 Jacobi form (the multi-plan kernel's), at
+// least two operators and at most kMultiGroupItems samples per operator (a large group is
+// better served by its own batched launch); otherwise false, and the caller solves operator
+// by operator.  pre[item] = (solution, status).
+constexpr size_t kMultiGroupItems = 8;
 template <class Groups>
 bool MultiSolvePoses(const Groups &groups, const fgio::MotorBatchRequest &batch, const Options &opt,
                      ArtifactCache *artifacts, std::map<size_t, std::pair<Solved, int>> *pre, int *launches,
@@ -398,8 +401,9 @@ bool MultiSolvePoses(const Groups &groups, const fgio::MotorBatchRequest &batch,
   std::vector<std::pair<Prepared *, const std::vector<size_t> *>> poses;
   for (const auto &g : groups) {
     Prepared &base = *(*artifacts)[g.first.first];
-    if (base.status == 0 && base.artifact.sliding_band)
-      poses.push_back({PoseOf(base, g.first.second), &g.second});
+    if (base.status != 0 || g.second.size() > kMultiGroupItems)
+      return false;
+    poses.push_back({PoseOf(base, g.first.second), &g.second});
   }
   if (poses.size() < 2)
     return false;

@@ -217,3 +217,30 @@ def test_sector_batch_reconstructs_the_full_machine(gpu, tmp_path):
         np.testing.assert_allclose(rhs["circuit_flux_linkage_derivative_Wb_per_A"], part, atol=1e-12)
         np.testing.assert_allclose(rhs["airgap_radial_flux_density_derivative_T_per_A"], t.radial_b[0], rtol=0,
                                    atol=1e-6 * np.abs(t.radial_b[0]).max())
+
+
+def test_batch_over_several_artifacts_shares_one_launch_and_equals_separate_batches(gpu, tmp_path):
+    """Items on two posed artifacts in one chunk are solved in one multi-plan launch per
+    Newton step (a replica plan for the second sample of an artifact); each item agrees with
+    a batch of its artifact alone (per-artifact batched launch) to 1e-9."""
+    path, _, source = motor_artifact(tmp_path)
+    src = json.load(open(path))
+    src["resolved"]["pose"] = {"rotor_angle_deg": 5, "displacement_mm": [0, 0]}
+    other = tmp_path / "motor5.gpu.json"
+    other.write_text(json.dumps(src))
+    items = [{"task_id": "a0", "request": motor_request(path, source, [12.0])},
+             {"task_id": "b0", "request": motor_request(other, source, [12.0], rotor_angle_deg=5)},
+             {"task_id": "a1", "request": motor_request(path, source, [-4.0])}]
+    rc, both, err = call(tmp_path, "--motor-batch", {"protocol": "gpu_femm_motor_batch_v1",
+                                                     "max_items_per_chunk": 4, "items": items}, name="both.json")
+    assert rc == 0 and both["status"] == "PASS", err
+    for k, item in enumerate(items):
+        rc, alone, err = call(tmp_path, "--motor-batch", {"protocol": "gpu_femm_motor_batch_v1",
+                                                          "max_items_per_chunk": 4, "items": [item]},
+                              name=f"alone{k}.json")
+        assert rc == 0, err
+        got, want = both["items"][k]["response"], alone["items"][0]["response"]
+        for key in ("torque_Nm", "Fx_N", "Fy_N"):
+            assert abs(got[key] - want[key]) <= 1e-9 * max(abs(want["torque_Nm"]), abs(want["Fx_N"]), 1e-12), key
+        f, w = np.array(got["circuit_flux_linkage_Wb"]), np.array(want["circuit_flux_linkage_Wb"])
+        assert np.linalg.norm(f - w) <= 1e-9 * np.linalg.norm(w)
