@@ -364,6 +364,7 @@ std::string RunBatch(const fgio::BatchRequest &batch, const Options &opt, Artifa
       final_status[i] = status;
     }
     // A sliding-band artifact has one operator per band angle: its items are solved per pose.
+    TrimPoses(p, kResidentPoses);
     std::map<double, std::vector<size_t>> poses;
     for (size_t i : ready)
       poses[p.artifact.sliding_band ? batch.items[i].request.sliding_band_angle_deg : 0.0].push_back(i);

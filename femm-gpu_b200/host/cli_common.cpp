@@ -107,7 +107,19 @@ Prepared *PoseOf(Prepared &p, double rotor_angle_deg)
       slot->error = "could not apply the requested sliding-band angle";
     }
   }
+  slot->last_use = ++p.pose_clock;
   return slot.get();
+}
+
+void TrimPoses(Prepared &p, size_t keep)
+{
+  while (p.poses.size() > keep) {
+    auto oldest = p.poses.begin();
+    for (auto it = p.poses.begin(); it != p.poses.end(); ++it)
+      if (it->second->last_use < oldest->second->last_use)
+        oldest = it;
+    p.poses.erase(oldest);
+  }
 }
 
 int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out,

@@ -116,6 +116,7 @@ struct Prepared {
   // A sliding-band artifact's poses: per requested rotor angle a copy of the artifact with
   // its bands slid to that angle, and that copy's own plan (the operator differs per angle).
   std::map<double, std::shared_ptr<Prepared>> poses;
+  uint64_t pose_clock = 0, last_use = 0; // pose recency (PoseOf), for TrimPoses
   // Further plans of this pose's model: one per extra sample when several samples of one
   // pose share a multi-plan launch with other poses (one sample per plan there).
   std::vector<fg_plan *> replicas;
@@ -139,6 +140,11 @@ int EnsurePlan(Prepared *p, const Options &opt);
 // sliding-band pose at that angle, made on first use (ApplySlidingBandRotorAngle,
 // sample_request.cpp:493-497; status FG_INVALID_ARGUMENT when the angle cannot be applied).
 Prepared *PoseOf(Prepared &p, double rotor_angle_deg);
+// Keeps the `keep` most recently used poses of a sliding-band artifact and frees the
+// others' plans; call between chunks, when no pose is in use (a long-running worker meets
+// ever new rotor angles).
+void TrimPoses(Prepared &p, size_t keep);
+constexpr size_t kResidentPoses = 64;
 // The sliding-band postprocess of one solved sample (ComputeAirGapElementPostprocess via
 // fg_air_gap_postprocess) at the request's probe angles in degrees.
 // angles_rad, when given, replaces the converted angles (native sector probes folded into

@@ -541,6 +541,9 @@ std::string RunMotorBatch(const fgio::MotorBatchRequest &batch, const Options &o
   bool have_cached = false;
   for (size_t first = 0; first < n; first += effective) {
     ++chunks;
+    for (auto &kv : *artifacts)
+      if (kv.second)
+        TrimPoses(*kv.second, kResidentPoses);
     const size_t end = std::min(n, first + static_cast<size_t>(effective));
     // Artifact gate per item, then groups of items sharing one operator, first-seen order.
     std::vector<std::pair<OperatorKey, std::vector<size_t>>> groups;

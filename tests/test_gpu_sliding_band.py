@@ -309,3 +309,37 @@ def test_sliding_band_transactions_in_the_worker(gpu, tmp_path, artifact):
         rc, ref, _ = call(tmp_path, "--motor-batch-profile", body, name=f"p{j}.json")
         assert rc == 0
         assert [i["response"] for i in got["items"]] == [i["response"] for i in ref["items"]]
+
+
+@needs_ref
+def test_worker_bounds_resident_poses_and_recreates_evicted_ones(gpu, tmp_path):
+    """A worker meeting more rotor angles than it keeps resident (kResidentPoses = 64) trims
+    the least recently used poses between chunks and rebuilds an evicted pose on demand:
+    jobs over 70 angles, then a job revisiting evicted and resident angles, answer as
+    one-shot runs."""
+    from test_worker_cli import envelope, run_worker
+    text = sliding_artifact_text(meshes.sliding_band_machine(nr=40, nt=12))
+    path = tmp_path / "small_v2.json"
+    path.write_text(text)
+    sha = hashlib.sha256(text.encode()).hexdigest()
+    angles = [0.5 * i for i in range(70)]
+    # worker transactions carry at most 32 items: three jobs meet 70 angles, the fourth
+    # (after the trim to 64 evicted the six oldest) revisits evicted and resident ones
+    jobs = [angles[:32], angles[32:64], angles[64:], [0.0, 0.5, 1.5, 34.5]]
+    bodies = [{"protocol": "gpu_femm_motor_batch_v1", "max_items_per_chunk": 32,
+               "items": [{"task_id": f"j{j}i{i}", "request": request(path, sha, [8.0, -4.0, -4.0], a)}
+                         for i, a in enumerate(js)]} for j, js in enumerate(jobs)]
+    out = tmp_path / "out"
+    out.mkdir()
+    envs = []
+    for j, body in enumerate(bodies):
+        b = tmp_path / f"pose{j}.json"
+        b.write_text(json.dumps(body))
+        envs.append(envelope(j + 1, b, out / f"pose{j}.json"))
+    st = run_worker(envs)
+    assert all(s["exit_code"] == 0 for s in st), st
+    for j, body in enumerate(bodies):
+        got = json.load(open(out / f"pose{j}.json"))
+        rc, ref, _ = call(tmp_path, "--motor-batch", body, name=f"one{j}.json")
+        assert rc == 0 and got["status"] == "PASS"
+        assert [i["response"] for i in got["items"]] == [i["response"] for i in ref["items"]]
