@@ -268,3 +268,32 @@ def test_native_sector_refusals_follow_the_reference(tmp_path, sector_model):
         ref, ref_err = ref_parse(text.encode())
         assert ref is None and rc == 1, label
         assert d["error"] == ref_err, (label, d["error"], ref_err)
+
+
+@needs_ref
+def test_planar_dc_requests_on_sliding_artifacts_refused_before_any_gpu_work(tmp_path, band_model):
+    """PlanarDcRequestMatchesArtifact (sample_adapter.cpp:181-234) on a sliding-band
+    artifact: the probe circle must lie in the band, and the generic protocol does not take
+    motor artifacts."""
+    import hashlib
+    text = sliding_artifact_text(band_model)
+    art = tmp_path / "v2.json"
+    art.write_text(text)
+    sha = hashlib.sha256(text.encode()).hexdigest()
+    base = {"protocol": "gpu_femm_planar_dc_sample_v1", "mesh_artifact_path": str(art), "mesh_artifact_sha256": sha,
+            "circuit_currents_A": [8.0, -4.0, -4.0], "force_group_number": 20, "stress_air_group_number": 50,
+            "airgap_radius_mm": 45.5, "airgap_angles_deg": [0.0, 90.0], "sliding_band_angle_deg": 7.5,
+            "compute_force_torque": True, "include_field_solution": False}
+    cases = {"circle outside the band": dict(airgap_radius_mm=47.0),
+             "absent force group": dict(force_group_number=9),
+             "generic protocol": dict(protocol="gpu_femm_magnetostatic_sample_v1", force_group_number=-1,
+                                      stress_air_group_number=-1, airgap_radius_mm=0, airgap_angles_deg=[],
+                                      compute_force_torque=False, sliding_band_angle_deg=0)}
+    for label, kw in cases.items():
+        rq, rs = tmp_path / "rq.json", tmp_path / "rs.json"
+        rq.write_text(json.dumps(dict(base, **kw)))
+        r = subprocess.run([CLI, "--solve", str(rq), str(rs)], capture_output=True, text=True, timeout=120)
+        body = json.loads(rs.read_text())
+        assert r.returncode == 1 and body["status"] == "FAIL", label
+        assert body["error_message"] == "artifact physics, circuit count, group, or sliding-band request mismatch", \
+            (label, body["error_message"])
