@@ -278,9 +278,12 @@ int Solve(const std::string &request_path, const std::string &response_path, con
 
 // Solves the ready items of one operator (an artifact, or one band angle of a sliding-band
 // artifact) in chunks of max_items_per_chunk and writes their response bodies.
+// given / given_status: the pose's samples already solved (with other poses, in one
+// multi-plan launch); then only the postprocess and the responses remain.
 void SolvePose(const fgio::BatchRequest &batch, const Options &opt, Prepared &p, const std::vector<size_t> &ready,
                std::vector<std::string> *bodies, std::vector<int> *final_status, int *chunks, int *launches,
-               double *solve_s)
+               double *solve_s, const std::vector<Solved> *given = nullptr,
+               const std::vector<int> *given_status = nullptr)
 {
   const int plan_status = p.status != 0 ? p.status : EnsurePlan(&p, opt);
   if (plan_status != 0) {
@@ -300,7 +303,12 @@ void SolvePose(const fgio::BatchRequest &batch, const Options &opt, Prepared &p,
       reqs.push_back(&batch.items[ready[first + j]].request);
     std::vector<Solved> sols;
     std::vector<int> st;
-    SolveItems(p, reqs, &sols, &st, launches);
+    if (given) {
+      sols.assign(given->begin() + first, given->begin() + first + n);
+      st.assign(given_status->begin() + first, given_status->begin() + first + n);
+    } else {
+      SolveItems(p, reqs, &sols, &st, launches);
+    }
     ++*chunks;
     for (size_t j = 0; j < n; ++j) {
       const size_t i = ready[first + j];
@@ -368,9 +376,29 @@ std::string RunBatch(const fgio::BatchRequest &batch, const Options &opt, Artifa
     std::map<double, std::vector<size_t>> poses;
     for (size_t i : ready)
       poses[p.artifact.sliding_band ? batch.items[i].request.sliding_band_angle_deg : 0.0].push_back(i);
-    for (auto &pose : poses)
-      SolvePose(batch, opt, *PoseOf(p, pose.first), pose.second, &bodies, &final_status, &chunks, &launches,
-                &solve_s);
+    // Several poses of a sliding-band artifact: their samples in one multi-plan launch per
+    // Newton step when SolveOperatorsTogether applies, else pose by pose.
+    std::vector<Operator> ops;
+    for (auto &pose : poses) {
+      Operator op{PoseOf(p, pose.first), {}};
+      for (size_t i : pose.second)
+        op.currents.push_back(&batch.items[i].request.circuit_currents_a);
+      ops.push_back(std::move(op));
+    }
+    std::vector<std::vector<Solved>> together;
+    std::vector<std::vector<int>> together_status;
+    int64_t unused_pcg = 0;
+    const auto m0 = std::chrono::steady_clock::now();
+    const bool joint = batch.max_items_per_chunk >= static_cast<int32_t>(ready.size()) &&
+                       SolveOperatorsTogether(ops, opt, &together, &together_status, &launches, &unused_pcg);
+    if (joint)
+      solve_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - m0).count();
+    size_t o = 0;
+    for (auto &pose : poses) {
+      SolvePose(batch, opt, *ops[o].p, pose.second, &bodies, &final_status, &chunks, &launches, &solve_s,
+                joint ? &together[o] : nullptr, joint ? &together_status[o] : nullptr);
+      ++o;
+    }
   }
   bool &pass = *all_pass;
   pass = true;

@@ -190,6 +190,79 @@ int EnsurePlan(Prepared *p, const Options &opt)
   return rc;
 }
 
+bool SolveOperatorsTogether(const std::vector<Operator> &ops, const Options &opt,
+                            std::vector<std::vector<Solved>> *out, std::vector<std::vector<int>> *statuses,
+                            int *launches, int64_t *pcg_iterations)
+{
+  if (opt.plan.preconditioner != FG_PRECOND_JACOBI || opt.plan.precision != FG_PRECISION_FP64 ||
+      (opt.plan.flags & FG_PLAN_PCG_FROM_ITERATE) || ops.size() < 2)
+    return false;
+  for (const Operator &op : ops)
+    if (!op.p || op.p->status != 0 || op.currents.empty() || op.currents.size() > kMultiGroupItems)
+      return false;
+  std::vector<fg_plan *> plans;
+  std::vector<std::pair<size_t, size_t>> where; // (operator, sample) of each plan
+  for (size_t o = 0; o < ops.size(); ++o) {
+    Prepared &p = *ops[o].p;
+    if (EnsurePlan(&p, opt) != 0)
+      return false;
+    fg_model m = p.artifact.Model();
+    while (p.replicas.size() + 1 < ops[o].currents.size()) {
+      fg_plan *r = nullptr;
+      if (fg_plan_create(&m, &opt.plan, &r) != 0)
+        return false;
+      p.replicas.push_back(r);
+    }
+    for (size_t j = 0; j < ops[o].currents.size(); ++j) {
+      plans.push_back(j == 0 ? p.plan : p.replicas[j - 1]);
+      where.push_back({o, j});
+    }
+  }
+  fg_multi *multi = nullptr;
+  if (fg_multi_create(plans.data(), static_cast<int32_t>(plans.size()), &multi) != 0)
+    return false;
+  out->assign(ops.size(), {});
+  statuses->assign(ops.size(), {});
+  for (size_t o = 0; o < ops.size(); ++o) {
+    (*out)[o].resize(ops[o].currents.size());
+    (*statuses)[o].assign(ops[o].currents.size(), FG_INTERNAL_ERROR);
+  }
+  const size_t M = plans.size();
+  std::vector<const double *> cur(M);
+  std::vector<double *> a(M), b1(M), b2(M), flux(M);
+  for (size_t i = 0; i < M; ++i) {
+    const Operator &op = ops[where[i].first];
+    const fg_model m = op.p->artifact.Model();
+    Solved &s = (*out)[where[i].first][where[i].second];
+    s.currents = *op.currents[where[i].second];
+    s.a.assign(m.node_count, 0.0);
+    s.b1.assign(m.triangle_count, 0.0);
+    s.b2.assign(m.triangle_count, 0.0);
+    s.flux.assign(m.circuit_count, 0.0);
+    cur[i] = s.currents.data();
+    a[i] = s.a.data();
+    b1[i] = s.b1.data();
+    b2[i] = s.b2.data();
+    flux[i] = s.flux.data();
+  }
+  std::vector<fg_item_info> info(M);
+  fg_solve_options o;
+  fg_production_options(&o);
+  const int rc = fg_multi_solve(multi, cur.data(), &o, a.data(), b1.data(), b2.data(), flux.data(), info.data());
+  fg_multi_timing t{};
+  fg_multi_last_timing(multi, &t);
+  *launches += static_cast<int>(t.pcg_launches);
+  fg_multi_destroy(multi);
+  for (size_t i = 0; i < M; ++i) {
+    Solved &s = (*out)[where[i].first][where[i].second];
+    *pcg_iterations += info[i].linear_iterations;
+    s.iterations = info[i].iterations;
+    s.residual = info[i].residual_l2;
+    (*statuses)[where[i].first][where[i].second] = rc != 0 ? rc : info[i].status;
+  }
+  return true;
+}
+
 int SolveCurrents(Prepared &p, const std::vector<const std::vector<double> *> &currents, std::vector<Solved> *out,
                   std::vector<int> *statuses, int *launches)
 {

@@ -152,6 +152,25 @@ constexpr size_t kResidentPoses = 64;
 int AirGapPost(fg_plan *plan, const Solved &s, const std::vector<double> &angles_deg, Post *out,
                const std::vector<double> *angles_rad = nullptr);
 
+// One operator of a multi-operator solve: a prepared plan (an artifact, or a sliding-band
+// pose) and the circuit currents of its samples.
+struct Operator {
+  Prepared *p = nullptr;
+  std::vector<const std::vector<double> *> currents;
+};
+constexpr size_t kMultiGroupItems = 8;
+// The samples of several operators in one multi-plan launch per Newton step (fg_multi).
+// At motor mesh sizes each operator's own PCG launch is latency-bound, so solving them side
+// by side amortises every CG iteration's barriers over all of them.  An operator's first
+// sample runs on its plan, further samples on replica plans of the same model (the
+// multi-plan launch takes one sample per plan).  Only the plain FP64 Jacobi form (the
+// multi-plan kernel's), at least two operators and at most kMultiGroupItems samples per
+// operator (a large group is better served by its own batched launch); otherwise false and
+// nothing is solved.  out[o][j] / statuses[o][j]: sample j of operator o.
+bool SolveOperatorsTogether(const std::vector<Operator> &ops, const Options &opt,
+                            std::vector<std::vector<Solved>> *out, std::vector<std::vector<int>> *statuses,
+                            int *launches, int64_t *pcg_iterations);
+
 // Solves k samples (their circuit currents) on a prepared plan with the reference's
 // production options (ProductionSampleOptions); statuses[i] = the item's status.
 int SolveCurrents(Prepared &p, const std::vector<const std::vector<double> *> &currents, std::vector<Solved> *out,

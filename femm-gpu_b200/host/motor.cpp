@@ -381,87 +381,33 @@ void Tangent(fg_plan *plan, fg_postprocess *pp, const MotorSampleRequest &req, c
 }
 
 // The samples of a chunk's operators -- motor artifacts, and the poses of sliding-band
-// artifacts -- in one multi-plan launch per Newton step (fg_multi).  At motor mesh sizes
-// each operator's own PCG launch is latency-bound, so solving them side by side amortises
-// every CG iteration's barriers over all of them.  An operator's first sample runs on its
-// plan, further samples on replica plans of the same model (the multi-plan launch takes
-// one sample per plan).  Only the plain FP64 Jacobi form (the multi-plan kernel's), at
-// least two operators and at most kMultiGroupItems samples per operator (a large group is
-// better served by its own batched launch); otherwise false, and the caller solves operator
-// by operator.  pre[item] = (solution, status).
-constexpr size_t kMultiGroupItems = 8;
+// artifacts -- in one multi-plan launch per Newton step (SolveOperatorsTogether); false
+// when that does not apply (then the caller solves operator by operator).
+// pre[item] = (solution, status).
 template <class Groups>
 bool MultiSolvePoses(const Groups &groups, const fgio::MotorBatchRequest &batch, const Options &opt,
                      ArtifactCache *artifacts, std::map<size_t, std::pair<Solved, int>> *pre, int *launches,
                      int64_t *pcg_iterations)
 {
-  if (opt.plan.preconditioner != FG_PRECOND_JACOBI || opt.plan.precision != FG_PRECISION_FP64 ||
-      (opt.plan.flags & FG_PLAN_PCG_FROM_ITERATE))
-    return false;
-  std::vector<std::pair<Prepared *, const std::vector<size_t> *>> poses;
+  std::vector<Operator> ops;
   for (const auto &g : groups) {
     Prepared &base = *(*artifacts)[g.first.first];
-    if (base.status != 0 || g.second.size() > kMultiGroupItems)
+    if (base.status != 0)
       return false;
-    poses.push_back({PoseOf(base, g.first.second), &g.second});
+    Operator op{PoseOf(base, g.first.second), {}};
+    for (size_t i : g.second)
+      op.currents.push_back(&batch.items[i].request.circuit_currents_a);
+    ops.push_back(std::move(op));
   }
-  if (poses.size() < 2)
+  std::vector<std::vector<Solved>> sols;
+  std::vector<std::vector<int>> st;
+  if (!SolveOperatorsTogether(ops, opt, &sols, &st, launches, pcg_iterations))
     return false;
-  std::vector<fg_plan *> plans;
-  std::vector<size_t> items;
-  std::vector<Prepared *> owner;
-  for (auto &ps : poses) {
-    Prepared &p = *ps.first;
-    if (p.status != 0 || EnsurePlan(&p, opt) != 0)
-      return false;
-    const std::vector<size_t> &idx = *ps.second;
-    fg_model m = p.artifact.Model();
-    while (p.replicas.size() + 1 < idx.size()) {
-      fg_plan *r = nullptr;
-      if (fg_plan_create(&m, &opt.plan, &r) != 0)
-        return false;
-      p.replicas.push_back(r);
-    }
-    for (size_t j = 0; j < idx.size(); ++j) {
-      plans.push_back(j == 0 ? p.plan : p.replicas[j - 1]);
-      items.push_back(idx[j]);
-      owner.push_back(&p);
-    }
-  }
-  fg_multi *multi = nullptr;
-  if (fg_multi_create(plans.data(), static_cast<int32_t>(plans.size()), &multi) != 0)
-    return false;
-  const size_t M = plans.size();
-  std::vector<Solved> sols(M);
-  std::vector<const double *> cur(M);
-  std::vector<double *> a(M), b1(M), b2(M), flux(M);
-  for (size_t i = 0; i < M; ++i) {
-    const fg_model m = owner[i]->artifact.Model();
-    Solved &s = sols[i];
-    s.currents = batch.items[items[i]].request.circuit_currents_a;
-    s.a.assign(m.node_count, 0.0);
-    s.b1.assign(m.triangle_count, 0.0);
-    s.b2.assign(m.triangle_count, 0.0);
-    s.flux.assign(m.circuit_count, 0.0);
-    cur[i] = s.currents.data();
-    a[i] = s.a.data();
-    b1[i] = s.b1.data();
-    b2[i] = s.b2.data();
-    flux[i] = s.flux.data();
-  }
-  std::vector<fg_item_info> info(M);
-  fg_solve_options o;
-  fg_production_options(&o);
-  const int rc = fg_multi_solve(multi, cur.data(), &o, a.data(), b1.data(), b2.data(), flux.data(), info.data());
-  fg_multi_timing t{};
-  fg_multi_last_timing(multi, &t);
-  *launches += static_cast<int>(t.pcg_launches);
-  fg_multi_destroy(multi);
-  for (size_t i = 0; i < M; ++i) {
-    *pcg_iterations += info[i].linear_iterations;
-    sols[i].iterations = info[i].iterations;
-    sols[i].residual = info[i].residual_l2;
-    (*pre)[items[i]] = {std::move(sols[i]), rc != 0 ? rc : info[i].status};
+  size_t o = 0;
+  for (const auto &g : groups) {
+    for (size_t j = 0; j < g.second.size(); ++j)
+      (*pre)[g.second[j]] = {std::move(sols[o][j]), st[o][j]};
+    ++o;
   }
   return true;
 }

@@ -261,7 +261,8 @@ def test_planar_dc_solve_and_batch_on_a_sliding_band_artifact(gpu, tmp_path, art
     """The planar-DC adapter serves sliding-band artifacts as the reference does
     (sample_adapter.cpp:396-439): sliding_band_angle_deg poses the bands, the band
     postprocess answers; --solve equals --motor-single-sample at the same rotor angle bit for
-    bit, and a batch over two band angles equals its single solves."""
+    bit, and a batch over two band angles (solved side by side) equals its single solves to
+    1e-7 (both converge to the production Newton tolerance)."""
     path, text, sha = artifact
     cur = [8.0, -4.0, -4.0]
     rc, s, err = call(tmp_path, "--solve", planar_request(path, sha, cur, 12.5), name="p.json")
@@ -275,8 +276,11 @@ def test_planar_dc_solve_and_batch_on_a_sliding_band_artifact(gpu, tmp_path, art
     rc, b, err = call(tmp_path, "--batch", {"protocol": "gpu_femm_magnetostatic_batch_v1",
                                             "max_items_per_chunk": 8, "items": items}, name="b.json")
     assert rc == 0 and b["status"] == "PASS", err
+    # the batch solves its two poses side by side (one multi-plan launch), converging within
+    # the production Newton tolerance of --solve's own launch: 1e-7
     first = b["items"][0]["response"]
-    assert first["torque_Nm"] == s["torque_Nm"] and first["circuit_flux_linkage_Wb"] == s["circuit_flux_linkage_Wb"]
+    assert abs(first["torque_Nm"] - s["torque_Nm"]) <= 1e-7 * abs(s["torque_Nm"])
+    assert rel(first["circuit_flux_linkage_Wb"], s["circuit_flux_linkage_Wb"]) <= 1e-7
     _, _, _, flux, post = reference(path, text, 0.0, cur)
     check_base(b["items"][2]["response"], flux, post)
     # the probe circle must lie in the band
