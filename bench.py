@@ -61,7 +61,8 @@ def parse():
     p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
     p.add_argument("--sector-samples", type=int, default=64, help="samples of the shared-geometry sector form")
     p.add_argument("--hetero-meshes", type=int, default=64, help="meshes of the heterogeneous-batch form")
-    p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker", "sliding_band"],
+    p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker", "sliding_band",
+                                           "planar_2m"],
                    help="run one form alone and print its JSON (profiling)")
     return p.parse_args()
 
@@ -72,6 +73,50 @@ def peaks():
         d = json.load(open(path))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def mesh_counts(model):
+    """Free rows and CSR entries of a constraint-free planar mesh, counted with numpy from
+    the triangles (used by both arms so their config keys agree)."""
+    fixed = np.zeros(model.node_count, bool)
+    fixed[model.dir_nodes] = True
+    t = model.tri
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    e = e[~(fixed[e[:, 0]] | fixed[e[:, 1]])]
+    e.sort(axis=1)
+    edges = np.unique(e[:, 0].astype(np.int64) * model.node_count + e[:, 1]).size
+    rows = int((~fixed).sum())
+    return rows, rows + 2 * edges
+
+
+def headline_config(model, mesh, world):
+    """The config both arms print (the driver compares them key for key)."""
+    rows, nnz = mesh_counts(model)
+    return {"workload": f"nonlinear planar solve, jittered {mesh}x{mesh} quads ({model.node_count} nodes, "
+                        f"{model.tri_count} triangles), iron B-H + PM strip + 3 circuits",
+            "nodes": model.node_count, "triangles": model.tri_count, "rows": rows, "nnz": nnz,
+            "precision": "fp64", "gates": "Newton step 1e-6, inner true residual 1e-10 (production options)",
+            "l2": "flushed between timed GPU steps", "parallelism": f"replicas{world}"}
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def traffic_per_cg_iteration(workload):
+    """DRAM bytes per CG iteration of the PCG kernel from the committed ncu capture of that
+    workload (profiles/traffic.json; the capture's command is in the profile beside it)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None, None
+    d = json.load(open(path)).get(workload)
+    return (float(d["dram_bytes_per_cg_iteration"]), d["profile"]) if d else (None, None)
 
 
 class ClockSampler:
@@ -148,19 +193,30 @@ def dist_setup(args):
     return world, rank, local
 
 
-def cpu_baseline(model, items_seed, budget_threads=None):
-    """Reference CPU path (oracle/_ref) on one full-size sample per host thread."""
+def cpu_baseline(model, items_seed, budget_threads=None, single_core=True):
+    """Reference CPU path (oracle/_ref) on one full-size sample per host thread, plus one
+    sample alone on one thread (single-core latency).  Returns the report and the
+    reference's answers (currents, A, flux, status, Newton iterations) for the parity check."""
     import oracle as O
     from femm_gpu_b200 import meshes
 
     threads = budget_threads or os.cpu_count() or 1
     currents = meshes.seeded_currents(threads, model.circuit_count, 20.0, seed=items_seed)
+    answers = None
+    extra = {}
     if O.ref() is not None:
         t0 = time.perf_counter()
         a, flux, status, newton, calls, worst = O.ref_cpu_newton_batch(model, currents, threads=threads)
         dt = time.perf_counter() - t0
         kind = "reference"
         ok = int((status == 0).sum())
+        answers = (currents, a, flux, status, newton)
+        extra = {"max_true_residual": float(worst.max()), "newton_iterations_mean": float(newton.mean()),
+                 "femm_pcg_calls_mean": float(calls.mean())}
+        if single_core:
+            t0 = time.perf_counter()
+            O.ref_cpu_newton_batch(model, currents[:1], threads=1)
+            extra["single_core_latency_s"] = time.perf_counter() - t0
     else:  # the C restatement, one Python thread per sample (ctypes releases the GIL)
         out = [None] * threads
 
@@ -174,9 +230,33 @@ def cpu_baseline(model, items_seed, budget_threads=None):
         dt = time.perf_counter() - t0
         kind = "port"
         ok = sum(1 for o in out if o[4][0].status == 0)
-    return {"value": threads / dt, "unit": "solves/s", "cores": threads, "kind": kind,
-            "sample": f"{threads} full nonlinear solves of the {model.node_count}-node workload, "
-                      f"one per host thread, {ok} converged, {dt:.1f} s wall"}
+    report = {"value": threads / dt, "unit": "solves/s", "cores": threads, "kind": kind,
+              "cpu_model": cpu_model(), "nproc": os.cpu_count(),
+              "sample": f"{threads} full nonlinear solves of the {model.node_count}-node workload, "
+                        f"one per host thread, {ok} converged, {dt:.1f} s wall", **extra}
+    return report, answers
+
+
+def parity_vs_reference(model, plan, answers):
+    """The library's answers for the reference's own samples (same currents): relative
+    2-norm errors of A and flux linkage, max |B| error relative to max |B|, statuses and
+    Newton iteration counts."""
+    import oracle as O
+
+    currents, ra, rflux, rst, rnewton = answers
+    got = plan.solve(currents)
+    ea, ef, eb = [], [], []
+    for i in range(len(currents)):
+        ea.append(float(np.linalg.norm(got.a[i] - ra[i]) / np.linalg.norm(ra[i])))
+        ef.append(float(np.linalg.norm(got.flux[i] - rflux[i]) / np.linalg.norm(rflux[i])))
+        b1, b2, _ = O.finalize(model, ra[i])
+        bmax = max(np.abs(b1).max(), np.abs(b2).max())
+        eb.append(float(max(np.abs(got.b1[i] - b1).max(), np.abs(got.b2[i] - b2).max()) / bmax))
+    return {"samples": len(currents), "a_rel_err_max": max(ea), "flux_rel_err_max": max(ef),
+            "b_err_max_over_max_b": max(eb),
+            "statuses_equal": bool(all(g.status == r for g, r in zip(got.info, rst))),
+            "newton_iterations_equal": bool(all(g.iterations == r for g, r in zip(got.info, rnewton))),
+            "reference": "the reference's host assembler + FEMM SSOR PCG (oracle/_ref), same currents"}
 
 
 def run_ours(args, world, rank, local):
@@ -249,16 +329,13 @@ def run_ours(args, world, rank, local):
     alg_bytes = item_its * per_item + pcg_its * shared
     achieved = alg_bytes / (pcg_ms / 1e3) / 1e9 if pcg_ms > 0 else 0.0
     peak, peak_kind = peaks()
-    # DRAM traffic of the PCG kernel from the committed ncu capture of this workload
-    # (profiles/pcg_square500_items8.md: bytes per CG iteration), per launch of this run.
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "pcg_square500_items8.md")
-    if os.path.exists(prof) and args.mesh == MESH_M and k == 8:
-        import re
-        m_ = re.search(r"traffic_bytes_per_cg_iteration:\s*([0-9.eE+]+)", open(prof).read())
-        launches_timed = max(1, newton)
-        if m_:
-            traffic = float(m_.group(1)) * pcg_its / launches_timed
+    # DRAM traffic of the PCG kernel from the committed ncu capture of this workload,
+    # per launch of this run.
+    traffic, traffic_src = None, None
+    if args.mesh == MESH_M and k == 8:
+        per_it, traffic_src = traffic_per_cg_iteration("square500_items8")
+        if per_it is not None:
+            traffic = per_it * pcg_its / max(1, newton)
 
     # End to end through the host-buffer C ABI (H2D currents, D2H A / B / flux / info).
     host_in = [meshes.seeded_currents(k, Cc, 20.0, seed=777000 + 100000 * rank + s) for s in range(args.steps)]
@@ -276,16 +353,14 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"nonlinear planar solve, jittered {args.mesh}x{args.mesh} quads "
-                               f"({N} nodes, {E} triangles), iron B-H + PM strip + 3 circuits",
-                   "items_per_step": k, "rows": n, "nnz": nnz, "l2": "flushed between steps",
-                   "parallelism": f"replicas{world}", "precision": "fp64 Jacobi PCG"},
+        "config": headline_config(model, args.mesh, world),
+        "items_per_step": k, "solver": "fp64 Jacobi PCG (the drop-in form)",
         "e2e": e2e,
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "kernel": "PcgKernel",
-                     "traffic_source": "ncu capture of this workload, bytes per CG iteration x "
-                                       "iterations per launch (profiles/pcg_square500_items8.md)",
+                     "traffic_source": (f"ncu capture of this workload, DRAM bytes per CG iteration x "
+                                        f"iterations per launch ({traffic_src})") if traffic_src else None,
                      "algorithmic_bytes_per_launch": alg_bytes / max(1, newton),
                      "peak_source": peak_kind, "pcg_ms": pcg_ms, "pcg_iterations": pcg_its,
                      "item_pcg_iterations": item_its},
@@ -296,12 +371,48 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_forms:
         line["forms"] = run_forms(args, model, plan, dev, stream, flush, value)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(model, items_seed=4242)
+        line["cpu_baseline"], answers = cpu_baseline(model, items_seed=4242)
+        if answers is not None:
+            line["parity_vs_reference"] = parity_vs_reference(model, plan, answers)
+            line["e2e_vs_cpu_baseline"] = e2e["value"] / line["cpu_baseline"]["value"]
+    if "forms" in line:
+        line["forms_summary"] = forms_summary(line["forms"])
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def forms_summary(forms):
+    """The forms' key figures, printed last on the line so a truncated log keeps them."""
+    out = {}
+
+    def pick(name, d, *keys):
+        if isinstance(d, dict):
+            out[name] = {k: (round(d[k], 4) if isinstance(d[k], float) else d[k]) for k in keys if k in d}
+
+    for name in ("fp64_jacobi", "fp64_block8", "mixed_jacobi", "mixed_block8", "mixed_block8_from_iterate"):
+        pick("planar_" + name, forms.get(name), "solves_per_s", "vs_fp64_jacobi", "pcg_iterations_per_item",
+             "a_rel_err", "flux_rel_err")
+    c4 = forms.get("planar_2m", {})
+    for name, d in c4.items():
+        pick("planar_2m_" + name, d, "solves_per_s", "vs_fp64_jacobi_k4", "pcg_gbs", "pcg_frac",
+             "newton_iterations_per_item", "pcg_iterations_per_item", "a_rel_err", "b_rel_err", "flux_rel_err")
+    sec = forms.get("shared_geometry_sector", {})
+    for name, d in sec.items():
+        pick("sector_" + name, d, "solves_per_s_e2e", "vs_fp64_jacobi", "a_rel_err", "flux_rel_err",
+             "a_rel_err_vs_oracle", "flux_rel_err_vs_oracle")
+    pick("heterogeneous", forms.get("heterogeneous_meshes"), "meshes", "multi_solves_per_s",
+         "one_plan_at_a_time_solves_per_s", "speedup", "a_rel_err_vs_single")
+    lw = forms.get("learned_warm_start", {})
+    for name, d in lw.items():
+        pick("learned_" + name, d, "solves_per_s_e2e", "vs_fp64_zero_start", "vs_same_form_zero_start",
+             "newton_iterations_per_item", "pcg_iterations_per_item", "a_rel_err", "flux_rel_err")
+    pick("sliding_band", forms.get("sliding_band"), "solves_per_s_e2e", "speedup_vs_cpu",
+         "flux_rel_err_vs_reference")
+    pick("worker", forms.get("streaming_worker"), "worker_solves_per_s", "speedup")
+    return out
 
 
 def time_device(plan, k, inputs, steps, warmup, dev, stream, flush):
@@ -369,6 +480,8 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
                      "a_rel_err": err(a, ref_a), "flux_rel_err": err(f, ref_f),
                      "all_converged": all(i.status == 0 for i in info)}
         p.close()
+    out["planar_2m"] = planar_2m_form(dev, stream, flush)
+
     # Shared geometry with per-sample magnets: the rotor-stator sector (40k nodes,
     # anti-periodic edges), currents U[-15, 15] A and Hc U[8.5e5, 9.5e5] A/m per sample.
     sector = meshes.annular_sector()
@@ -480,6 +593,89 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
             final_loss=float(ws.stats["final_loss"]), **res)
         fast.close()
         base.close()
+    return out
+
+
+def pcg_bytes_per_item_iteration(n, nnz, precision, block):
+    """Algorithmic bytes of one item's CG iteration (values + the 13 vector passes), FP64
+    or the FP32 inner form; block-Jacobi adds the block inverses' read."""
+    w = 8 if precision == 0 else 4
+    return w * nnz + 13 * w * n + (w * block * n if block else 0)
+
+
+def planar_2m_form(dev, stream, flush, samples=4):
+    """The mixed-precision-at-scale workload: the jittered planar square at m = 1414
+    (2,002,225 nodes, 3,998,792 triangles, 1,996,569 rows) with the config-2 physics.
+    Runs: plain FP64 Jacobi for 1 and 4 samples; the FP32-inner PCG (SpMV + 32-row
+    block-Jacobi, FP64 defect correction by reliable updates) for 4 samples, from zero and
+    from the Newton iterate.  Each: solves/s (CUDA events, device buffers), Newton (outer)
+    and PCG (inner) iterations per sample, PCG algorithmic GB/s and fraction of the HBM
+    peak, errors of A, B and flux linkage against the FP64 solutions of the same samples."""
+    import torch
+
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import meshes
+
+    model = meshes.square_nonlinear(m=1414, seed=2)
+    peak, _ = peaks()
+    cur = meshes.seeded_currents(samples, 3, 20.0, seed=1414)
+    runs = (("fp64_jacobi_k1", dict(), 1), ("fp64_jacobi_k4", dict(), samples),
+            ("mixed_block32_k4", dict(precision=1, preconditioner=1, block_size=32), samples),
+            ("mixed_block32_from_iterate_k4", dict(precision=1, preconditioner=1, block_size=32,
+                                                   from_iterate=True), samples))
+    out = {"workload": f"nonlinear planar solve, jittered 1414x1414 quads ({model.node_count} nodes, "
+                       f"{model.tri_count} triangles)"}
+    ref = None
+    for name, kw, k in runs:
+        p = fg.Plan(model, **kw)
+        N, E = p.N, p.E
+        x = torch.tensor(cur[:k], device=dev)
+        out_a = torch.empty((k, N), dtype=torch.float64, device=dev)
+        out_b1 = torch.empty((k, E), dtype=torch.float64, device=dev)
+        out_b2 = torch.empty((k, E), dtype=torch.float64, device=dev)
+        out_f = torch.empty((k, 3), dtype=torch.float64, device=dev)
+        ptrs = dict(a_ptr=out_a.data_ptr(), b1_ptr=out_b1.data_ptr(), b2_ptr=out_b2.data_ptr(),
+                    flux_ptr=out_f.data_ptr(), stream=stream.cuda_stream)
+        # warm-up: one Newton iteration sizes every workspace of this batch width
+        p.solve_device(k, x.data_ptr(), options=fg.production_options(max_newton_iterations=1), **ptrs)
+        torch.cuda.synchronize()
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        info = p.solve_device(k, x.data_ptr(), **ptrs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        t = p.last_timing()
+        item_its = sum(i.linear_iterations for i in info)
+        per_item = pcg_bytes_per_item_iteration(p.rows, p.nnz, kw.get("precision", 0),
+                                                kw.get("block_size", 0) if kw.get("preconditioner") else 0)
+        shared = 4.0 * p.nnz + 4.0 * (p.rows + 1)
+        gbs = (item_its * per_item + t.pcg_iterations * shared) / (t.pcg_ms / 1e3) / 1e9
+        a, b1, b2, f = (out_a.cpu().numpy(), out_b1.cpu().numpy(), out_b2.cpu().numpy(), out_f.cpu().numpy())
+        r = {"samples": k, "solves_per_s": k / (ms / 1e3), "seconds": ms / 1e3,
+             "newton_iterations_per_item": float(np.mean([i.iterations for i in info])),
+             "pcg_iterations_per_item": item_its / k, "pcg_ms": t.pcg_ms,
+             "pcg_ms_per_cg_iteration": t.pcg_ms / max(1, t.pcg_iterations),
+             "pcg_gbs": gbs, "pcg_frac": gbs / peak,
+             "mixed_fallbacks": int(t.mixed_fallbacks), "all_converged": all(i.status == 0 for i in info)}
+        if name == "fp64_jacobi_k4":
+            ref = (a, b1, b2, f)
+        elif ref is not None:
+            bmax = np.maximum(np.abs(ref[1]).max(axis=1), np.abs(ref[2]).max(axis=1))
+            r["a_rel_err"] = float(max(np.linalg.norm(a[i] - ref[0][i]) / np.linalg.norm(ref[0][i])
+                                       for i in range(k)))
+            r["b_rel_err"] = float(max(max(np.abs(b1[i] - ref[1][i]).max(), np.abs(b2[i] - ref[2][i]).max())
+                                       / bmax[i] for i in range(k)))
+            r["flux_rel_err"] = float(max(np.linalg.norm(f[i] - ref[3][i]) / np.linalg.norm(ref[3][i])
+                                          for i in range(k)))
+        out[name] = r
+        del out_a, out_b1, out_b2, out_f
+        p.close()
+    base = out["fp64_jacobi_k4"]["solves_per_s"]
+    for name in ("mixed_block32_k4", "mixed_block32_from_iterate_k4"):
+        out[name]["vs_fp64_jacobi_k4"] = out[name]["solves_per_s"] / base
+    out["errors_against"] = "the plain FP64 Jacobi solutions of the same samples (the drop-in form)"
     return out
 
 
@@ -726,7 +922,7 @@ def run_reference(args, world, rank, local):
     model = meshes.square_nonlinear(m=args.mesh, seed=SEED_MESH)
     threads = os.cpu_count() or 1
     if O.ref() is None:  # the C restatement: whole solves, one per thread
-        base = cpu_baseline(model, items_seed=4242, budget_threads=threads)
+        base, _ = cpu_baseline(model, items_seed=4242, budget_threads=threads)
         value, ms, sample = base["value"], 1e3 * threads / base["value"], base["sample"]
         kind = "port"
     else:
@@ -773,10 +969,10 @@ def run_reference(args, world, rank, local):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"nonlinear planar solve, jittered {args.mesh}x{args.mesh} quads",
-                       "samples": threads},
+            "config": headline_config(model, args.mesh, world), "items_per_step": threads,
+            "solver": "reference host assembler + FEMM 4.2 SSOR PCG, one sample per host thread",
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": threads, "kind": kind,
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "nproc": os.cpu_count(), "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
@@ -791,6 +987,9 @@ def only_form(args):
     stream = torch.cuda.current_stream(dev)
     if args.only_form == "streaming_worker":
         out = worker_form()
+    elif args.only_form == "planar_2m":
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+        out = planar_2m_form(dev, stream, flush)
     elif args.only_form == "sliding_band":
         out = sliding_band_form()
     else:

@@ -22,6 +22,10 @@
 // first call on each device -- with that device current -- resolves the device address
 // with cudaGetSymbolAddress and caches it; make that first call before any stream
 // capture begins.
+//
+// Host waits: every call synchronises `stream` -- once after the set-up kernel, to read
+// its verdict on the system, and again after the solve, to read the solve's status before
+// x is written -- so it returns only when x and info are final.
 #include "femm_gpu.h"
 #include "common.h"
 #include "kernels.cuh"
@@ -276,14 +280,24 @@ Status NoallocPcg(int32_t n, const int32_t *ro, const int32_t *col, const double
     cudaGetLastError();
     return Status::kInternalError;
   }
+  // The solve's status first: x is written only when the kernel finished without an error
+  // (a grid-barrier wait that ran out leaves x untouched and reports INTERNAL_ERROR).
+  if (cudaMemcpyAsync(&control, scratch + kOffControl, sizeof(Control), cudaMemcpyDeviceToHost,
+                      stream) != cudaSuccess ||
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    info->status = ToInt(Status::kInternalError);
+    return Status::kInternalError;
+  }
+  if (control.pcg_error != 0) {
+    info->status = ToInt(Status::kInternalError);
+    return Status::kInternalError;
+  }
   if (cudaMemcpyAsync(x, scratch + kOffX, sizeof(double) * n, cudaMemcpyDeviceToDevice, stream) !=
           cudaSuccess ||
-      cudaMemcpyAsync(&control, scratch + kOffControl, sizeof(Control), cudaMemcpyDeviceToHost,
-                      stream) != cudaSuccess ||
-      cudaStreamSynchronize(stream) != cudaSuccess)
+      cudaStreamSynchronize(stream) != cudaSuccess) {
+    info->status = ToInt(Status::kInternalError);
     return Status::kInternalError;
-  if (control.pcg_error != 0)
-    return Status::kInternalError;
+  }
   info->status = static_cast<int32_t>(control.info[0]);
   info->iterations = static_cast<int32_t>(control.info[1]);
   info->residual_l2 = control.info[2];

@@ -42,6 +42,7 @@
 #include "femm_gpu.h"
 #include "json.h"
 #include "request.h"
+#include "worker.h"
 
 #include <sys/stat.h>
 #include <unistd.h>
@@ -57,12 +58,7 @@
 #include <iostream>
 #include <map>
 #include <memory>
-#include <mutex>
-#include <condition_variable>
-#include <thread>
-#include <atomic>
 #include <set>
-#include <list>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -457,284 +453,16 @@ int Batch(const std::string &request_path, const std::string &response_path, con
   return pass ? 0 : 1;
 }
 
-// ---- --worker: the streaming batch worker (MotorBatchWorker, gpu_solver/src/app/
-// motor_worker.cpp:24-191) over the neutral batch protocol.
-//
-// Standard input carries one job envelope per line, {"session", "sequence", "request_path",
-// "response_path", "request_sha256"}; one thread prepares the next job (envelope, request
-// bytes and SHA-256, batch parse, the artifacts it names read, verified, parsed and their
-// plans built on the host by up to 4 threads) while the GPU solves the current one, with at
-// most one prepared job waiting.  Jobs of one session must come in sequence (1, 2, ...); a
-// refused job still consumes its number.  After each job one status line goes to standard
-// output.  Unlike the one-shot --batch, prepared artifacts -- device plans and postprocess
-// masks -- stay resident across jobs (at most kWorkerArtifacts, least recently used out);
-// an artifact file is still read and hashed for every job that names it, so a changed file
-// fails exactly as it would for --batch.
-constexpr size_t kWorkerArtifacts = 32;
-
-struct WorkerJob {
-  std::string session, request_path, response_path, request_sha256, error;
-  int32_t sequence = 0;
-  fgio::BatchRequest batch;
-  bool motor = false; // a gpu_femm_motor_batch_v* transaction
-  fgio::MotorBatchRequest motor_batch;
-  ArtifactCache staged; // artifacts read for this job that the resident set lacks or must replace
-  double prepare_seconds = 0.0;
-  std::chrono::steady_clock::time_point prepare_begin, prepare_end;
-};
-
-// The resident artifacts: the consumer owns the map, the producer asks which keys exist.
-struct WorkerArtifacts {
-  std::mutex mutex;
-  std::set<ArtifactKey> keys;
-  ArtifactCache map;
-  std::list<ArtifactKey> order; // most recently used first
-};
-
-std::unique_ptr<WorkerJob> PrepareWorkerJob(const std::string &line, const std::string &executable,
-                                            const Options &opt, WorkerArtifacts *resident)
-{
-  auto job = std::make_unique<WorkerJob>();
-  const auto started = std::chrono::steady_clock::now();
-  job->prepare_begin = started;
-  try {
-    fgio::Json root;
-    std::string error;
-    if (!fgio::ParseJson(line, &root, &error) ||
-        !fgio::HasExactly(root, {"session", "sequence", "request_path", "response_path", "request_sha256"},
-                          &error))
-      throw std::runtime_error("invalid stream job envelope");
-    using K = fgio::Json::Kind;
-    const fgio::Json *session = root.get("session", K::String, &error);
-    const fgio::Json *sequence = root.get("sequence", K::Number, &error);
-    const fgio::Json *request = root.get("request_path", K::String, &error);
-    const fgio::Json *response = root.get("response_path", K::String, &error);
-    const fgio::Json *hash = root.get("request_sha256", K::String, &error);
-    if (!session || !sequence || !request || !response || !hash || !fgio::IsSha256Hex(session->text) ||
-        !fgio::IsSha256Hex(hash->text) || !fgio::AsInt32(*sequence, &job->sequence) || job->sequence < 1)
-      throw std::runtime_error("invalid stream job identity");
-    job->session = session->text;
-    job->request_path = request->text;
-    job->response_path = response->text;
-    job->request_sha256 = hash->text;
-    if (job->request_path.empty() || job->response_path.empty() ||
-        SameFile(job->response_path, job->request_path) || SameFile(job->response_path, executable))
-      throw std::runtime_error("unsafe stream output path");
-    std::string bytes;
-    if (!ReadFile(job->request_path, &bytes) || fgio::Sha256Hex(bytes) != job->request_sha256)
-      throw std::runtime_error("stream request SHA-256 mismatch");
-    {
-      // Motor transactions name a gpu_femm_motor_batch_v* protocol; the rest take the neutral reader.
-      fgio::Json probe;
-      std::string ignored;
-      if (fgio::ParseJson(bytes, &probe, &ignored) && probe.is(fgio::Json::Kind::Object)) {
-        auto it = probe.members.find("protocol");
-        job->motor = it != probe.members.end() && it->second.is(fgio::Json::Kind::String) &&
-                     it->second.text.rfind("gpu_femm_motor_batch_v", 0) == 0;
-      }
-    }
-    if (job->motor ? !fgio::ParseMotorBatchRequestText(bytes, &job->motor_batch, &error)
-                   : !fgio::ParseBatchRequestText(bytes, &job->batch, &error))
-      throw std::runtime_error(error);
-    // A transaction is bounded independently of the number of submissions.
-    if ((job->motor ? job->motor_batch.items.size() : job->batch.items.size()) > 32)
-      throw std::runtime_error("stream transaction exceeds 32 items");
-    std::vector<ArtifactKey> keys;
-    auto add_key = [&](const std::string &path, const std::string &sha) {
-      const ArtifactKey key{path, sha};
-      if (std::find(keys.begin(), keys.end(), key) == keys.end())
-        keys.push_back(key);
-    };
-    if (job->motor)
-      for (const fgio::MotorBatchItem &item : job->motor_batch.items)
-        add_key(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
-    else
-      for (const fgio::BatchItem &item : job->batch.items)
-        add_key(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
-    for (const ArtifactKey &key : keys)
-      if (SameFile(job->response_path, key.first))
-        throw std::runtime_error("stream response would overwrite an artifact");
-    std::set<ArtifactKey> have;
-    {
-      std::lock_guard<std::mutex> lock(resident->mutex);
-      have = resident->keys;
-    }
-    std::vector<std::shared_ptr<Prepared>> loads(keys.size());
-    std::atomic<size_t> next{0};
-    auto load = [&] {
-      for (;;) {
-        const size_t slot = next.fetch_add(1, std::memory_order_relaxed);
-        if (slot >= keys.size())
-          return;
-        const ArtifactKey &key = keys[slot];
-        if (have.count(key)) {
-          // Resident: the file must still hold the bytes that were verified.
-          std::string art;
-          auto check = std::make_shared<Prepared>();
-          if (!ReadFile(key.first, &art)) {
-            check->status = FG_INPUT_IO;
-            check->error = "cannot open mesh artifact";
-          } else if (fgio::Sha256Hex(art) != key.second) {
-            check->status = FG_INVALID_ARGUMENT;
-            check->error = "mesh artifact SHA mismatch";
-          } else {
-            continue;
-          }
-          loads[slot] = check;
-          continue;
-        }
-        auto p = std::make_shared<Prepared>();
-        Prepare(key.first, key.second, opt, p.get());
-        PreparePlanOnHost(p.get(), opt);
-        loads[slot] = p;
-      }
-    };
-    std::vector<std::thread> loaders;
-    const size_t width = std::min<size_t>(4, keys.size());
-    for (size_t i = 1; i < width; ++i) {
-      try {
-        loaders.emplace_back(load);
-      } catch (const std::system_error &) {
-        break;
-      }
-    }
-    load();
-    for (std::thread &t : loaders)
-      t.join();
-    for (size_t i = 0; i < keys.size(); ++i)
-      if (loads[i])
-        job->staged[keys[i]] = loads[i];
-  } catch (const std::exception &e) {
-    job->error = e.what();
-  }
-  job->prepare_end = std::chrono::steady_clock::now();
-  job->prepare_seconds = std::chrono::duration<double>(job->prepare_end - started).count();
-  return job;
-}
-
-// Runs a prepared job against the resident artifacts; the exit code of --batch.
-int RunWorkerJob(WorkerJob *job, const Options &opt, WorkerArtifacts *resident)
-{
-  ArtifactCache view;
-  {
-    std::lock_guard<std::mutex> lock(resident->mutex);
-    for (auto &kv : job->staged) {
-      const bool failed = kv.second->status != 0;
-      if (failed) {
-        view[kv.first] = kv.second; // a stale or unreadable file: fail this job only
-        continue;
-      }
-      resident->map[kv.first] = kv.second;
-      resident->keys.insert(kv.first);
-    }
-    std::vector<ArtifactKey> keys;
-    if (job->motor)
-      for (const fgio::MotorBatchItem &item : job->motor_batch.items)
-        keys.emplace_back(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
-    else
-      for (const fgio::BatchItem &item : job->batch.items)
-        keys.emplace_back(item.request.mesh_artifact_path, item.request.mesh_artifact_sha256);
-    for (const ArtifactKey &key : keys) {
-      if (view.count(key))
-        continue;
-      auto it = resident->map.find(key);
-      if (it != resident->map.end()) {
-        view[key] = it->second;
-        resident->order.remove(key);
-        resident->order.push_front(key);
-      }
-    }
-    while (resident->order.size() > kWorkerArtifacts) {
-      const ArtifactKey old = resident->order.back();
-      resident->order.pop_back();
-      if (!view.count(old)) {
-        resident->map.erase(old);
-        resident->keys.erase(old);
-      }
-    }
-  }
-  bool pass = false;
-  // Motor transactions carry the reference worker's timing block.
-  const std::string text = job->motor ? RunMotorBatch(job->motor_batch, opt, &view, true, job->prepare_begin, &pass)
-                                      : RunBatch(job->batch, opt, &view, job->prepare_begin, &pass);
-  if (!PublishAtomically(job->response_path, text)) {
-    job->error = "could not atomically publish response";
-    return 1;
-  }
-  return pass ? 0 : 1;
-}
-
+// ---- --worker: the streaming batch worker (host/worker.cpp).  Each admitted transaction
+// is solved by the one-shot adapters' code against the worker's resident artifacts; motor
+// transactions carry the reference worker's timing block.
 int Worker(const Options &opt, const std::string &executable)
 {
-  const auto worker_start = std::chrono::steady_clock::now();
-  WorkerArtifacts resident;
-  std::mutex mutex;
-  std::condition_variable changed;
-  std::unique_ptr<WorkerJob> ready;
-  bool eof = false;
-  std::thread producer([&] {
-    for (;;) {
-      // Wait before reading: at most one prepared job besides the one on the GPU.
-      std::unique_lock<std::mutex> lock(mutex);
-      changed.wait(lock, [&] { return !ready; });
-      lock.unlock();
-      std::string line;
-      if (!std::getline(std::cin, line))
-        break;
-      auto job = PrepareWorkerJob(line, executable, opt, &resident);
-      lock.lock();
-      ready = std::move(job);
-      changed.notify_all();
-    }
-    std::lock_guard<std::mutex> lock(mutex);
-    eof = true;
-    changed.notify_all();
-  });
-  std::string session;
-  int32_t previous = 0;
-  for (;;) {
-    std::unique_lock<std::mutex> lock(mutex);
-    changed.wait(lock, [&] { return ready || eof; });
-    if (!ready)
-      break;
-    std::unique_ptr<WorkerJob> job = std::move(ready);
-    changed.notify_all();
-    lock.unlock();
-    int result = 1;
-    const auto solve_begin = std::chrono::steady_clock::now();
-    const bool in_sequence = (session.empty() || session == job->session) && job->sequence == previous + 1;
-    if (job->error.empty()) {
-      if (in_sequence) {
-        session = job->session;
-        previous = job->sequence;
-        try {
-          result = RunWorkerJob(job.get(), opt, &resident);
-        } catch (const std::exception &e) {
-          job->error = e.what();
-        }
-      } else {
-        job->error = "stream session or submission sequence mismatch";
-      }
-    } else if (in_sequence) {
-      // A refused request still consumes its envelope number, not GPU work.
-      session = job->session;
-      previous = job->sequence;
-    }
-    const auto solve_end = std::chrono::steady_clock::now();
-    auto since = [&](std::chrono::steady_clock::time_point t) {
-      return std::chrono::duration<double>(t - worker_start).count();
-    };
-    std::cout << std::setprecision(17) << "{\"session\":\"" << fgio::Escape(job->session)
-              << "\",\"sequence\":" << job->sequence << ",\"request_sha256\":\"" << job->request_sha256
-              << "\",\"exit_code\":" << result << ",\"prepare_seconds\":" << job->prepare_seconds
-              << ",\"prepare_begin_seconds\":" << since(job->prepare_begin)
-              << ",\"prepare_end_seconds\":" << since(job->prepare_end)
-              << ",\"solve_begin_seconds\":" << since(solve_begin)
-              << ",\"solve_end_seconds\":" << since(solve_end) << ",\"error\":\"" << fgio::Escape(job->error)
-              << "\"}" << std::endl;
-  }
-  producer.join();
-  return 0;
+  return ServeStream(std::cin, std::cout, opt, executable,
+                     [&opt](const StreamTransaction &txn, ArtifactCache *artifacts, bool *pass) {
+                       return txn.motor ? RunMotorBatch(txn.motor_batch, opt, artifacts, true, txn.prepare_begin, pass)
+                                        : RunBatch(txn.neutral, opt, artifacts, txn.prepare_begin, pass);
+                     });
 }
 
 // WriteSingleSampleResponse (gpu_solver/tests/native/reference_adapter.cu:16-61).

@@ -200,6 +200,16 @@ bool SolveOperatorsTogether(const std::vector<Operator> &ops, const Options &opt
   for (const Operator &op : ops)
     if (!op.p || op.p->status != 0 || op.currents.empty() || op.currents.size() > kMultiGroupItems)
       return false;
+  // Replica plans live only for this solve: a resident artifact keeps just its own plan,
+  // so a long-running worker's device memory does not grow with the batches it has served.
+  struct ReplicaPlans {
+    std::vector<fg_plan *> plans;
+    ~ReplicaPlans()
+    {
+      for (fg_plan *r : plans)
+        fg_plan_destroy(r);
+    }
+  } replicas;
   std::vector<fg_plan *> plans;
   std::vector<std::pair<size_t, size_t>> where; // (operator, sample) of each plan
   for (size_t o = 0; o < ops.size(); ++o) {
@@ -207,14 +217,15 @@ bool SolveOperatorsTogether(const std::vector<Operator> &ops, const Options &opt
     if (EnsurePlan(&p, opt) != 0)
       return false;
     fg_model m = p.artifact.Model();
-    while (p.replicas.size() + 1 < ops[o].currents.size()) {
-      fg_plan *r = nullptr;
-      if (fg_plan_create(&m, &opt.plan, &r) != 0)
-        return false;
-      p.replicas.push_back(r);
-    }
     for (size_t j = 0; j < ops[o].currents.size(); ++j) {
-      plans.push_back(j == 0 ? p.plan : p.replicas[j - 1]);
+      fg_plan *plan = p.plan;
+      if (j > 0) {
+        plan = nullptr;
+        if (fg_plan_create(&m, &opt.plan, &plan) != 0)
+          return false;
+        replicas.plans.push_back(plan);
+      }
+      plans.push_back(plan);
       where.push_back({o, j});
     }
   }

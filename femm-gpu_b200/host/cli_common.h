@@ -117,13 +117,8 @@ struct Prepared {
   // its bands slid to that angle, and that copy's own plan (the operator differs per angle).
   std::map<double, std::shared_ptr<Prepared>> poses;
   uint64_t pose_clock = 0, last_use = 0; // pose recency (PoseOf), for TrimPoses
-  // Further plans of this pose's model: one per extra sample when several samples of one
-  // pose share a multi-plan launch with other poses (one sample per plan there).
-  std::vector<fg_plan *> replicas;
   ~Prepared()
   {
-    for (fg_plan *r : replicas)
-      fg_plan_destroy(r);
     if (plan)
       fg_plan_destroy(plan);
   }
@@ -163,7 +158,8 @@ constexpr size_t kMultiGroupItems = 8;
 // At motor mesh sizes each operator's own PCG launch is latency-bound, so solving them side
 // by side amortises every CG iteration's barriers over all of them.  An operator's first
 // sample runs on its plan, further samples on replica plans of the same model (the
-// multi-plan launch takes one sample per plan).  Only the plain FP64 Jacobi form (the
+// multi-plan launch takes one sample per plan; the replicas are freed when the solve
+// ends).  Only the plain FP64 Jacobi form (the
 // multi-plan kernel's), at least two operators and at most kMultiGroupItems samples per
 // operator (a large group is better served by its own batched launch); otherwise false and
 // nothing is solved.  out[o][j] / statuses[o][j]: sample j of operator o.

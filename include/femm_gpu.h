@@ -260,7 +260,9 @@ int fg_csr_pcg(int32_t n, const int32_t *row_offsets, const int32_t *columns,
  * own buffers.  Every array argument is DEVICE memory owned by the caller (row_offsets
  * [n + 1], columns / values [row_offsets[n]], diagonal / rhs / x [n]); info is host
  * memory; work is ordered on `stream` (a cudaStream_t, NULL = legacy default stream) and
- * the call returns when x and info are final.  All other memory is one fixed file-scope
+ * the call returns when x and info are final: it synchronises `stream`, reading a small
+ * status block back to the host.  x is written only by a solve that ran to its end; when
+ * the call returns FG_INTERNAL_ERROR, info->status says so and x is left as it was.  All other memory is one fixed file-scope
  * device array (about 5.5 MB per device that loads the library, held until exit), so no
  * cudaMalloc, cudaFree or allocating library routine is called.
  * Limits: n <= FG_NOALLOC_MAX_ROWS and at most FG_NOALLOC_MAX_POSITIONS SELL-32 slots

@@ -289,6 +289,31 @@ def test_planar_dc_solve_and_batch_on_a_sliding_band_artifact(gpu, tmp_path, art
 
 
 @needs_ref
+def test_planar_dc_batch_joint_and_per_pose_paths_agree(gpu, tmp_path, artifact):
+    """One planar-DC batch over two band angles, run down both paths: poses solved side by
+    side in one multi-plan launch (max_items_per_chunk 8) and pose by pose
+    (max_items_per_chunk 1).  Both meet the production Newton tolerance, so an item's
+    answer depends on the path only below it: torque and flux linkage agree within 1e-7,
+    and the 0-degree item matches the reference CPU path on both."""
+    path, text, sha = artifact
+    cases = [([8.0, -4.0, -4.0], 12.5), ([-3.0, 6.0, -3.0], 0.0), ([8.0, -4.0, -4.0], 0.0)]
+    items = [{"task_id": f"i{i}", "request": planar_request(path, sha, c, a)} for i, (c, a) in enumerate(cases)]
+    runs = []
+    for chunk in (8, 1):
+        rc, b, err = call(tmp_path, "--batch", {"protocol": "gpu_femm_magnetostatic_batch_v1",
+                                                "max_items_per_chunk": chunk, "items": items},
+                          name=f"chunk{chunk}.json")
+        assert rc == 0 and b["status"] == "PASS", err
+        runs.append([i["response"] for i in b["items"]])
+    for joint, single in zip(*runs):
+        assert abs(joint["torque_Nm"] - single["torque_Nm"]) <= 1e-7 * abs(single["torque_Nm"])
+        assert rel(joint["circuit_flux_linkage_Wb"], single["circuit_flux_linkage_Wb"]) <= 1e-7
+    _, _, _, flux, post = reference(path, text, 0.0, cases[2][0])
+    for r in runs:
+        check_base(r[2], flux, post)
+
+
+@needs_ref
 def test_sliding_band_transactions_in_the_worker(gpu, tmp_path, artifact):
     """Two worker transactions on one sliding-band artifact at different rotor angles (the
     artifact and its poses resident between jobs) answer as one-shot --motor-batch runs."""
