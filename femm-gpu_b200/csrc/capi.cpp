@@ -114,6 +114,8 @@ const char *fg_status_name(int status)
 
 int fg_abi_version(void) { return FG_ABI_VERSION; }
 
+int64_t fg_set_wait_limit_ns(int64_t ns) { return fg::SetPcgWaitLimitNs(ns); }
+
 int fg_plan_create(const fg_model *model, const fg_plan_options *options, fg_plan **plan)
 {
   if (!plan)

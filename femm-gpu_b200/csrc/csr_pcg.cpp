@@ -155,7 +155,7 @@ Status CsrPcg(int32_t n, const int32_t *ro, const int32_t *col, const double *va
   a.tolerance = tol;
   a.max_iterations = maxit;
   a.active_mask = items >= 32 ? 0xffffffffu : ((1u << items) - 1u);
-  a.timeout_ns = 5000000000LL;
+  a.timeout_ns = fg::PcgWaitLimitNs();
   if (fg::LaunchPcg(a, nullptr, nullptr, nullptr) != cudaSuccess) {
     cudaGetLastError();
     return Status::kInternalError;

@@ -122,11 +122,22 @@ cudaError_t LaunchBlockInverse(const DevicePlan &p, int kp, int items, int bs, c
 // Cooperative persistent PCG; *grid_out receives the number of CTAs used.
 cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream);
 int PcgMaxGrid(int kp);
-// One cooperative launch of `ctas` CTAs solving every group of t (FP64 Jacobi, one item per
-// group).  The caller zeroes the groups' barrier counters and error flags.
-cudaError_t LaunchMultiPcg(PcgGroups t, int ctas, cudaStream_t stream);
-// Co-resident CTAs of the multi-plan kernel (its grid limit), 0 without a device.
-int MultiPcgMaxGrid();
+// Bound of every grid-wide wait of the PCG launches of plans, fg_csr_pcg and multi-plan
+// solves, in nanoseconds (fg_set_wait_limit_ns; default kDefaultWaitLimitNs).
+constexpr long long kDefaultWaitLimitNs = 5000000000LL;
+long long PcgWaitLimitNs();
+long long SetPcgWaitLimitNs(long long ns);
+// One cooperative launch of `ctas` CTAs solving every group of t (FP64 Jacobi; every group
+// holds kp items: 1, or 32 for the chunks of a wide shared-geometry batch).  The caller
+// zeroes the groups' barrier counters and error flags and, when MultiPcgRingBytes(kp) is not
+// zero, sets each group's value_ring (offset 0).
+cudaError_t LaunchMultiPcg(PcgGroups t, int kp, int ctas, cudaStream_t stream);
+// Co-resident CTAs of the multi-plan kernel for kp items per group (its grid limit), 0
+// without a device or for an unsupported kp.
+int MultiPcgMaxGrid(int kp = 1);
+// Dynamic shared memory of the multi-plan kernel's value ring for kp items per group (0:
+// no ring for this width).
+size_t MultiPcgRingBytes(int kp);
 // Whether a PCG kernel exists for this shape (block size 32 in FP64 stops at 16 items).
 bool PcgSupported(int kp, int precision, int block_size);
 

@@ -15,8 +15,9 @@ constexpr int kMinRowsPerCta = 1024; // below this a CTA's rows no longer pay fo
 
 } // namespace
 
-Status MultiSolver::Create(std::vector<Plan *> plans)
+Status MultiSolver::Create(std::vector<Plan *> plans, int kp)
 {
+  kp_ = kp;
   if (plans.empty())
     return Status::kInvalidArgument;
   for (Plan *p : plans)
@@ -28,9 +29,10 @@ Status MultiSolver::Create(std::vector<Plan *> plans)
       if (plans[i] == plans[j])
         return Status::kInvalidArgument; // a plan's workspace serves one sample at a time
   plans_ = std::move(plans);
-  max_grid_ = MultiPcgMaxGrid();
+  max_grid_ = MultiPcgMaxGrid(kp_);
   if (max_grid_ <= 0)
-    return Status::kGpuUnavailable;
+    return kp_ == 1 || kp_ == kMaxItems ? Status::kGpuUnavailable : Status::kUnsupportedFeature;
+  ring_ = MultiPcgRingBytes(kp_) > 0;
   const size_t m = plans_.size();
   Status s;
   if ((s = args_.ensure(m)) != Status::kOk || (s = cta_group_.ensure(max_grid_)) != Status::kOk ||
@@ -116,7 +118,7 @@ Status MultiSolver::Iteration(const std::vector<int> &active, cudaStream_t st)
                       cudaMemcpyHostToDevice, st) != cudaSuccess)
     return Status::kInternalError;
   PcgGroups g{args_.get(), cta_group_.get(), group_first_.get(), group_size_.get()};
-  if (LaunchMultiPcg(g, graph_ctas_, st) != cudaSuccess)
+  if (LaunchMultiPcg(g, kp_, graph_ctas_, st) != cudaSuccess)
     return Status::kInternalError;
   for (int m : active) {
     Status s = plans_[m]->ChunkNorms(&chunks_[m], true);
@@ -126,51 +128,10 @@ Status MultiSolver::Iteration(const std::vector<int> &active, cudaStream_t st)
   return Status::kOk;
 }
 
-Status MultiSolver::Solve(const double *const *currents, const fg_solve_options &options,
-                          double *const *a_out, double *const *b1_out, double *const *b2_out,
-                          double *const *flux_out, fg_item_info *info)
+// The lock-step Newton loop over the begun chunks_, then recovery and finish.
+Status MultiSolver::Run(const fg_solve_options &options, std::vector<double> *first_its)
 {
-  const auto t0 = std::chrono::steady_clock::now();
-  timing_ = fg_multi_timing{};
   const size_t M = plans_.size();
-  if (!info)
-    return Status::kInvalidArgument;
-  reqs_.assign(M, SolveRequest{});
-  chunks_.assign(M, Plan::Chunk{});
-  std::vector<double> first_its(M, -1.0);
-  for (size_t m = 0; m < M; ++m) {
-    Plan &p = *plans_[m];
-    const size_t N = p.host_.N, E = p.host_.E, C = p.host_.C;
-    if ((C > 0 && (!currents || !currents[m])))
-      return Status::kInvalidArgument;
-    Status s;
-    if ((C > 0 && (s = p.in_currents_.upload(currents[m], C)) != Status::kOk) ||
-        (s = p.out_a_.ensure(N)) != Status::kOk || (s = p.out_b1_.ensure(E)) != Status::kOk ||
-        (s = p.out_b2_.ensure(E)) != Status::kOk || (s = p.out_flux_.ensure(C > 0 ? C : 1)) != Status::kOk)
-      return s;
-    p.timing_ = fg_timing{};
-  }
-  // The uploads above ran on the legacy stream; the solve runs on stream_.
-  if (cudaDeviceSynchronize() != cudaSuccess)
-    return Status::kInternalError;
-  for (size_t m = 0; m < M; ++m) {
-    Plan &p = *plans_[m];
-    Status s;
-    SolveRequest &r = reqs_[m];
-    r.items = 1;
-    r.currents = p.in_currents_.get();
-    r.options = options;
-    r.a_out = p.out_a_.get();
-    r.b1_out = p.out_b1_.get();
-    r.b2_out = p.out_b2_.get();
-    r.flux_out = p.out_flux_.get();
-    r.info = info + m;
-    r.stream = stream_;
-    chunks_[m].timed = false;
-    if ((s = p.ChunkBegin(r, 0, 1, &chunks_[m])) != Status::kOk)
-      return s;
-    chunks_[m].timed = false;
-  }
   for (;;) {
     std::vector<int> active;
     for (size_t m = 0; m < M; ++m)
@@ -189,8 +150,12 @@ Status MultiSolver::Solve(const double *const *currents, const fg_solve_options 
       Plan &p = *plans_[active[i]];
       Plan::Chunk &c = chunks_[active[i]];
       p.ChunkTolerance(&c);
-      if (!p.ChunkPcgArgs(c, p.barrier_.get(), p.error_.get(), host_args_.get() + i))
+      if (c.kp != kp_ || !p.ChunkPcgArgs(c, p.barrier_.get(), p.error_.get(), host_args_.get() + i))
         return Status::kUnsupportedFeature;
+      if (ring_) {
+        host_args_.get()[i].value_ring = 1;
+        host_args_.get()[i].value_ring_offset = 0;
+      }
       maps[max_grid_ + i] = next;
       maps[max_grid_ + M + i] = ctas[i];
       for (int j = 0; j < ctas[i]; ++j)
@@ -254,8 +219,8 @@ Status MultiSolver::Solve(const double *const *currents, const fg_solve_options 
       if ((s = p.ChunkDecide(&chunks_[m])) != Status::kOk || (s = p.ChunkUpdate(&chunks_[m])) != Status::kOk)
         return s;
       last_its_[m] = std::max(1.0, its);
-      if (first_its[m] < 0)
-        first_its[m] = its;
+      if ((*first_its)[m] < 0)
+        (*first_its)[m] = its;
     }
   }
   for (size_t m = 0; m < M; ++m) {
@@ -269,6 +234,90 @@ Status MultiSolver::Solve(const double *const *currents, const fg_solve_options 
   }
   if (cudaStreamSynchronize(stream_) != cudaSuccess)
     return Status::kInternalError;
+  return Status::kOk;
+}
+
+Status MultiSolver::SolveChunks(const SolveRequest &req, const std::vector<int> &firsts,
+                                const std::vector<int> &counts)
+{
+  const auto t0 = std::chrono::steady_clock::now();
+  timing_ = fg_multi_timing{};
+  const size_t M = plans_.size();
+  if (firsts.size() != M || counts.size() != M || !req.info)
+    return Status::kInvalidArgument;
+  // The request's inputs were queued on its stream; the chunks run on stream_.
+  if (cudaStreamSynchronize(req.stream) != cudaSuccess)
+    return Status::kInternalError;
+  reqs_.assign(M, req);
+  chunks_.assign(M, Plan::Chunk{});
+  std::vector<double> first_its(M, -1.0);
+  for (size_t m = 0; m < M; ++m) {
+    Plan &p = *plans_[m];
+    reqs_[m].stream = stream_;
+    p.timing_ = fg_timing{};
+    chunks_[m].timed = false;
+    const Status s = p.ChunkBegin(reqs_[m], firsts[m], counts[m], &chunks_[m], kp_);
+    if (s != Status::kOk)
+      return s;
+    chunks_[m].timed = false;
+  }
+  const Status s = Run(req.options, &first_its);
+  if (s != Status::kOk)
+    return s;
+  for (size_t m = 0; m < M; ++m)
+    timing_.kernel_launches += plans_[m]->timing_.kernel_launches;
+  timing_.total_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  return Status::kOk;
+}
+
+Status MultiSolver::Solve(const double *const *currents, const fg_solve_options &options,
+                          double *const *a_out, double *const *b1_out, double *const *b2_out,
+                          double *const *flux_out, fg_item_info *info)
+{
+  const auto t0 = std::chrono::steady_clock::now();
+  timing_ = fg_multi_timing{};
+  const size_t M = plans_.size();
+  if (!info)
+    return Status::kInvalidArgument;
+  reqs_.assign(M, SolveRequest{});
+  chunks_.assign(M, Plan::Chunk{});
+  std::vector<double> first_its(M, -1.0);
+  for (size_t m = 0; m < M; ++m) {
+    Plan &p = *plans_[m];
+    const size_t N = p.host_.N, E = p.host_.E, C = p.host_.C;
+    if ((C > 0 && (!currents || !currents[m])))
+      return Status::kInvalidArgument;
+    Status s;
+    if ((C > 0 && (s = p.in_currents_.upload(currents[m], C)) != Status::kOk) ||
+        (s = p.out_a_.ensure(N)) != Status::kOk || (s = p.out_b1_.ensure(E)) != Status::kOk ||
+        (s = p.out_b2_.ensure(E)) != Status::kOk || (s = p.out_flux_.ensure(C > 0 ? C : 1)) != Status::kOk)
+      return s;
+    p.timing_ = fg_timing{};
+  }
+  // The uploads above ran on the legacy stream; the solve runs on stream_.
+  if (cudaDeviceSynchronize() != cudaSuccess)
+    return Status::kInternalError;
+  for (size_t m = 0; m < M; ++m) {
+    Plan &p = *plans_[m];
+    Status s;
+    SolveRequest &r = reqs_[m];
+    r.items = 1;
+    r.currents = p.in_currents_.get();
+    r.options = options;
+    r.a_out = p.out_a_.get();
+    r.b1_out = p.out_b1_.get();
+    r.b2_out = p.out_b2_.get();
+    r.flux_out = p.out_flux_.get();
+    r.info = info + m;
+    r.stream = stream_;
+    chunks_[m].timed = false;
+    if ((s = p.ChunkBegin(r, 0, 1, &chunks_[m])) != Status::kOk)
+      return s;
+    chunks_[m].timed = false;
+  }
+  Status s0 = Run(options, &first_its);
+  if (s0 != Status::kOk)
+    return s0;
   for (size_t m = 0; m < M; ++m) {
     Plan &p = *plans_[m];
     const size_t N = p.host_.N, E = p.host_.E, C = p.host_.C;

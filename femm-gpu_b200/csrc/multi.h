@@ -24,15 +24,23 @@ public:
   MultiSolver(const MultiSolver &) = delete;
   MultiSolver &operator=(const MultiSolver &) = delete;
   ~MultiSolver();
-  Status Create(std::vector<Plan *> plans);
+  // kp: items per group of the launch (1: one sample per plan; 32: chunks of a wide batch).
+  Status Create(std::vector<Plan *> plans, int kp = 1);
   Status Solve(const double *const *currents, const fg_solve_options &options, double *const *a_out,
                double *const *b1_out, double *const *b2_out, double *const *flux_out, fg_item_info *info);
+  // Chunks of one shared-geometry request: plan m (a lane workspace of the request's model,
+  // created with kp = 32) solves items [firsts[m], firsts[m] + counts[m]) of req, writing
+  // req's device outputs and host item infos.  The request's stream is not used: the solve
+  // runs on this object's stream, ordered after everything queued before the call.
+  Status SolveChunks(const SolveRequest &req, const std::vector<int> &firsts, const std::vector<int> &counts);
   const fg_multi_timing &timing() const { return timing_; }
 
 private:
   // CTA counts for the active plans; returns the launch's CTA total.
   int Partition(const std::vector<int> &active, std::vector<int> *ctas);
   Status Iteration(const std::vector<int> &active, cudaStream_t st);
+  // The lock-step Newton loop over chunks_ (begun) and its recovery and finish.
+  Status Run(const fg_solve_options &options, std::vector<double> *first_its);
 
   std::vector<Plan *> plans_;
   std::vector<SolveRequest> reqs_;
@@ -40,6 +48,8 @@ private:
   std::vector<double> last_its_;   // PCG iterations of each plan's previous Newton step
   double sqrt_coeff_ = 4.0;        // fitted: iterations ~ coeff * sqrt(rows)
   int max_grid_ = 0;
+  int kp_ = 1;
+  bool ring_ = false; // the launch carries the value ring (dynamic shared memory)
   DeviceArray<PcgArgs> args_;
   DeviceArray<int32_t> cta_group_, group_first_, group_size_;
   DeviceArray<unsigned> barriers_;

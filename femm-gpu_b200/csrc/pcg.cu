@@ -2,6 +2,7 @@
 // (kernel template in pcg_kernel.cuh; instantiations in pcg_f64*.cu / pcg_f32*.cu).
 #include "kernels.cuh"
 
+#include <atomic>
 #include <cstdlib>
 
 namespace fg
@@ -11,7 +12,7 @@ const void *PcgKernelF64(int kp);
 const void *PcgKernelF32(int kp);
 const void *PcgKernelF64Block(int kp, int bs);
 const void *PcgKernelF32Block(int kp, int bs);
-const void *MultiPcgKernelF64();
+const void *MultiPcgKernelF64(int kp);
 
 namespace
 {
@@ -86,6 +87,18 @@ bool ColumnCacheEnabled()
 }
 
 } // namespace
+
+namespace
+{
+std::atomic<long long> g_wait_limit_ns{kDefaultWaitLimitNs};
+} // namespace
+
+long long PcgWaitLimitNs() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
+
+long long SetPcgWaitLimitNs(long long ns)
+{
+  return g_wait_limit_ns.exchange(ns > 0 ? ns : kDefaultWaitLimitNs, std::memory_order_relaxed);
+}
 
 bool PcgSupported(int kp, int precision, int block_size)
 {
@@ -180,15 +193,30 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   return e;
 }
 
-int MultiPcgMaxGrid() { return KernelGrid(MultiPcgKernelF64(), 0); }
-
-cudaError_t LaunchMultiPcg(PcgGroups t, int ctas, cudaStream_t stream)
+size_t MultiPcgRingBytes(int kp)
 {
-  const int max_grid = MultiPcgMaxGrid();
-  if (ctas < 1 || ctas > max_grid)
+  // The value ring carries 16-byte item vectors: FP64 with two items per thread.
+  const int iv = ItemsPerThread(kp, 0);
+  if (8 * iv != 16 || !ValueRingEnabled())
+    return 0;
+  return static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 16;
+}
+
+int MultiPcgMaxGrid(int kp)
+{
+  const void *kernel = MultiPcgKernelF64(kp);
+  return kernel ? KernelGrid(kernel, MultiPcgRingBytes(kp)) : 0;
+}
+
+cudaError_t LaunchMultiPcg(PcgGroups t, int kp, int ctas, cudaStream_t stream)
+{
+  const void *kernel = MultiPcgKernelF64(kp);
+  const int max_grid = MultiPcgMaxGrid(kp);
+  if (!kernel || ctas < 1 || ctas > max_grid)
     return cudaErrorInvalidConfiguration;
   void *params[] = {&t};
-  return cudaLaunchCooperativeKernel(MultiPcgKernelF64(), dim3(ctas), dim3(kPcgThreads), params, 0, stream);
+  return cudaLaunchCooperativeKernel(kernel, dim3(ctas), dim3(kPcgThreads), params, MultiPcgRingBytes(kp),
+                                     stream);
 }
 
 } // namespace fg

@@ -17,10 +17,15 @@ const void *PcgKernelF64(int kp)
   }
 }
 
-// The multi-plan kernel: one FP64 Jacobi solve of one item per group.
-const void *MultiPcgKernelF64()
+// The multi-plan kernel: FP64 Jacobi solves of one item per group (independent meshes), or
+// of 32 items per group (the chunks of a wide shared-geometry batch).
+const void *MultiPcgKernelF64(int kp)
 {
-  return reinterpret_cast<const void *>(&MultiPcgKernel<double, 1, 1, 0>);
+  switch (kp) {
+  case 1: return reinterpret_cast<const void *>(&MultiPcgKernel<double, 1, 1, 0>);
+  case 32: return reinterpret_cast<const void *>(&MultiPcgKernel<double, 32, 2, 0>);
+  default: return nullptr;
+  }
 }
 
 } // namespace fg

@@ -882,9 +882,18 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             ll = __ldg(a.row_len + rr);
             bb = static_cast<size_t>(__ldg(a.slice_off + (rr >> 5))) + (rr & 31);
           };
+          // Column indices travel one chunk ahead too (registers): a chunk's gathers then
+          // wait for one L2 round trip, not for the index load and then the gather.
+          int c[U];
+          auto columns = [&](size_t bb, int w, int ll, int (&cc)[U]) {
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              cc[u] = w + u < ll ? Column(a, colc, cbase, bb + 32 * static_cast<size_t>(w + u)) : 0;
+          };
           if (ws < ws1) {
             row_at(ws, r, len, base);
             issue(0, base, 0, len);
+            columns(base, 0, len, c);
           }
           T acc[IV];
 #pragma unroll
@@ -899,15 +908,17 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
               if (nws < ws1)
                 row_at(nws, nr, nlen, nbase);
             }
-            if (nws < ws1)
+            int cn[U];
+            if (nws < ws1) {
               issue(stage ^ 1, nbase, nw0, nlen);
-            else
+              columns(nbase, nw0, nlen, cn);
+            } else {
               CpAsyncCommit();
-            CpAsyncWait<1>(); // the current chunk's values have landed
-            int c[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u)
-              c[u] = w0 + u < len ? Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u)) : 0;
+              for (int u = 0; u < U; ++u)
+                cn[u] = 0;
+            }
+            CpAsyncWait<1>(); // the current chunk's values have landed
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
@@ -936,6 +947,9 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             w0 = nw0;
             base = nbase;
             stage ^= 1;
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              c[u] = cn[u];
           }
           CpAsyncWait<0>();
           any_mine = false; // done

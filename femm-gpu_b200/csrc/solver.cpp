@@ -11,6 +11,8 @@
 // summaries that cross back once per Newton iteration.
 #include "solver.h"
 
+#include "multi.h"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -49,7 +51,29 @@ float Elapsed(cudaEvent_t a, cudaEvent_t b)
   return ms;
 }
 
+// Chunks of a wide shared-geometry batch solved together in one multi-group launch.
+constexpr int kMaxLanes = 32;
+
+// FG_CHUNKS_TOGETHER=0 in the environment solves wide batches chunk after chunk (A/B timing).
+bool ChunksTogetherEnabled()
+{
+  static const bool enabled = [] {
+    const char *v = std::getenv("FG_CHUNKS_TOGETHER");
+    return !(v && v[0] == '0');
+  }();
+  return enabled;
+}
+
 } // namespace
+
+Plan::~Plan()
+{
+  lane_solver_.reset();
+  lanes_.clear();
+  for (cudaEvent_t e : {ev_start_, ev_mid_, ev_pcg_, ev_end_})
+    if (e)
+      cudaEventDestroy(e);
+}
 
 size_t Plan::DeviceBytes() const
 {
@@ -326,7 +350,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.tolerance = tolerance;
   a.max_iterations = max_iterations;
   a.active_mask = mask;
-  a.timeout_ns = 5000000000LL;
+  a.timeout_ns = PcgWaitLimitNs();
   a.trace = trace_enabled_ ? trace_.get() : nullptr;
   int grid = 0, block = 0;
   const cudaError_t e = LaunchPcg(a, &grid, &block, stream);
@@ -493,7 +517,7 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   a.item_tolerance = item_tol;
   a.max_iterations = max_iterations;
   a.active_mask = mask;
-  a.timeout_ns = 5000000000LL;
+  a.timeout_ns = PcgWaitLimitNs();
   a.trace = trace_enabled_ ? trace_.get() : nullptr;
   int grid = 0, block = 0;
   if (LaunchPcg(a, &grid, &block, st) != cudaSuccess) {
@@ -558,10 +582,36 @@ Status Plan::SolveDevice(const SolveRequest &req)
   if (block_fallbacks_.get() &&
       cudaMemsetAsync(block_fallbacks_.get(), 0, sizeof(int32_t), req.stream) != cudaSuccess)
     return Status::kInternalError;
-  for (int first = 0; first < req.items; first += chunk_cap_) {
-    const Status s = SolveChunk(req, first, std::min(chunk_cap_, req.items - first));
+  if (ChunksTogether(req)) {
+    // Waves of at most kMaxLanes chunks (fewer when device memory is short), balanced.
+    const int total = (req.items + chunk_cap_ - 1) / chunk_cap_;
+    Status s = EnsureWorkspace(kMaxItems);
     if (s != Status::kOk)
       return s;
+    size_t free_bytes = 0, total_bytes = 0;
+    int cap = kMaxLanes;
+    if (cudaMemGetInfo(&free_bytes, &total_bytes) == cudaSuccess) {
+      const size_t lane = std::max<size_t>(DeviceBytes(), 1);
+      const size_t fit = static_cast<size_t>(lanes_.size()) + 1 + free_bytes / 2 / lane;
+      cap = static_cast<int>(std::max<size_t>(1, std::min<size_t>(kMaxLanes, fit)));
+    } else {
+      cudaGetLastError();
+    }
+    const int waves = (total + cap - 1) / cap;
+    const int per_wave = (total + waves - 1) / waves;
+    for (int c0 = 0; c0 < total; c0 += per_wave) {
+      const int n = std::min(per_wave, total - c0);
+      const int first = c0 * chunk_cap_;
+      s = n > 1 ? SolveChunksTogether(req, first, n) : SolveChunk(req, first, std::min(chunk_cap_, req.items - first));
+      if (s != Status::kOk)
+        return s;
+    }
+  } else {
+    for (int first = 0; first < req.items; first += chunk_cap_) {
+      const Status s = SolveChunk(req, first, std::min(chunk_cap_, req.items - first));
+      if (s != Status::kOk)
+        return s;
+    }
   }
   if (block_size()) {
     int32_t fallbacks = 0;
@@ -580,6 +630,73 @@ Status Plan::SolveDevice(const SolveRequest &req)
     timing_.pcg_phase_ms[9] = static_cast<double>(t[9]);
   }
   return Status::kOk;
+}
+
+bool Plan::ChunksTogether(const SolveRequest &req) const
+{
+  return ChunksTogetherEnabled() && req.items > chunk_cap_ && chunk_cap_ == kMaxItems &&
+         options_.precision == FG_PRECISION_FP64 && block_size() == 0 && !from_iterate_ && !req.guard_warm &&
+         !trace_enabled_ && MultiPcgMaxGrid(kMaxItems) > 0;
+}
+
+Status Plan::EnsureLanes(int lanes)
+{
+  while (static_cast<int>(lanes_.size()) + 1 < lanes) {
+    // A lane: this plan's host model and plan, its own device constants and workspace.
+    auto lane = std::make_unique<Plan>();
+    lane->model_ = model_;
+    lane->host_ = host_;
+    lane->options_ = options_;
+    lane->options_.flags |= FG_PLAN_HOST_ONLY;
+    lane->chunk_cap_ = chunk_cap_;
+    lane->from_iterate_ = from_iterate_;
+    lane->host_only_ = true;
+    Status s = lane->AttachDevice();
+    if (s != Status::kOk)
+      return s;
+    lanes_.push_back(std::move(lane));
+  }
+  if (!lane_solver_ || lane_solver_lanes_ != lanes) {
+    std::vector<Plan *> plans{this};
+    for (int i = 0; i + 1 < lanes; ++i)
+      plans.push_back(lanes_[i].get());
+    auto solver = std::make_unique<MultiSolver>();
+    const Status s = solver->Create(plans, kMaxItems);
+    if (s != Status::kOk)
+      return s;
+    lane_solver_ = std::move(solver);
+    lane_solver_lanes_ = lanes;
+  }
+  return Status::kOk;
+}
+
+Status Plan::SolveChunksTogether(const SolveRequest &req, int first, int chunks)
+{
+  std::vector<int> firsts, counts;
+  for (int c = 0; c < chunks; ++c) {
+    const int f = first + c * chunk_cap_;
+    firsts.push_back(f);
+    counts.push_back(std::min(chunk_cap_, req.items - f));
+  }
+  Status s = EnsureLanes(chunks);
+  if (s != Status::kOk)
+    return s;
+  const fg_timing before = timing_;
+  s = lane_solver_->SolveChunks(req, firsts, counts);
+  // Every lane's own counters (this plan's included) were reset by the lock-step solve.
+  fg_timing lanes_sum{};
+  for (int i = 0; i < chunks; ++i) {
+    const fg_timing &t = i == 0 ? timing_ : lanes_[i - 1]->timing_;
+    lanes_sum.pcg_iterations += t.pcg_iterations;
+    lanes_sum.kernel_launches += t.kernel_launches;
+  }
+  const fg_multi_timing &mt = lane_solver_->timing();
+  timing_ = before;
+  timing_.pcg_iterations += lanes_sum.pcg_iterations;
+  timing_.kernel_launches += lanes_sum.kernel_launches + mt.pcg_launches;
+  timing_.pcg_launches += mt.pcg_launches;
+  timing_.newton_iterations += mt.newton_steps;
+  return s;
 }
 
 Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
@@ -602,7 +719,7 @@ Status Plan::SolveChunk(const SolveRequest &req, int first, int k)
   return ChunkFinish(&c);
 }
 
-Status Plan::ChunkBegin(const SolveRequest &req, int first, int k, Chunk *c)
+Status Plan::ChunkBegin(const SolveRequest &req, int first, int k, Chunk *c, int min_kp)
 {
   const fg_solve_options &o = req.options;
   const int N = host_.N, C = host_.C;
@@ -622,7 +739,7 @@ Status Plan::ChunkBegin(const SolveRequest &req, int first, int k, Chunk *c)
   if (!(o.relative_tolerance > 0.0) || !std::isfinite(o.relative_tolerance) ||
       o.max_newton_iterations < 0 || o.max_linear_iterations < 0)
     return Status::kOk; // per-item INVALID_ARGUMENT, as SolveBatch returns
-  const int kp = PadItems(k);
+  const int kp = std::max(PadItems(k), PadItems(min_kp));
   c->kp = kp;
   Status s = EnsureWorkspace(kp);
   if (s != Status::kOk)
@@ -761,7 +878,7 @@ bool Plan::ChunkPcgArgs(const Chunk &c, unsigned *barrier, int32_t *error, PcgAr
   a.tolerance = c.tol;
   a.max_iterations = c.req->options.max_linear_iterations;
   a.active_mask = c.active;
-  a.timeout_ns = 5000000000LL;
+  a.timeout_ns = PcgWaitLimitNs();
   *out = a;
   return true;
 }

@@ -8,10 +8,13 @@
 #include "kernels.cuh"
 #include "model.h"
 
+#include <memory>
 #include <vector>
 
 namespace fg
 {
+
+class MultiSolver;
 
 struct SolveRequest {
   int items = 0;
@@ -30,6 +33,10 @@ struct SolveRequest {
 class Plan
 {
 public:
+  Plan() = default;
+  Plan(const Plan &) = delete;
+  Plan &operator=(const Plan &) = delete;
+  ~Plan();
   Status Create(HostModel model, const fg_plan_options &options);
   // Gives a host-only plan its device side (upload, events); no-op on a device plan.
   Status AttachDevice();
@@ -61,6 +68,16 @@ private:
   Status Upload();
   Status EnsureWorkspace(int kp);
   Status SolveChunk(const SolveRequest &request, int first, int count);
+  // Shared-geometry batches wider than one launch: up to kMaxLanes chunks of 32 items, each
+  // on its own lane workspace of this model (this plan is lane 0), advance together through
+  // one multi-group PCG launch per Newton step (MultiSolver::SolveChunks).  FP64 Jacobi
+  // from the zero or a plain warm start only; lanes are created on first use and kept.
+  bool ChunksTogether(const SolveRequest &request) const;
+  Status EnsureLanes(int lanes);
+  Status SolveChunksTogether(const SolveRequest &request, int first, int chunks);
+  std::vector<std::unique_ptr<Plan>> lanes_; // lanes 1 .. n (lane 0 is this plan)
+  std::unique_ptr<MultiSolver> lane_solver_;
+  int lane_solver_lanes_ = 0;
 
 public:
   // One chunk's Newton solve as steps, so that several plans can advance together
@@ -77,7 +94,9 @@ public:
     double linfo[3 * kMaxItems];
     ItemScalars rel{};
   };
-  Status ChunkBegin(const SolveRequest &request, int first, int count, Chunk *c);
+  // min_kp: the chunk's item slots are at least this many (a multi-group launch needs every
+  // group at the same width).
+  Status ChunkBegin(const SolveRequest &request, int first, int count, Chunk *c, int min_kp = 1);
   void ChunkTolerance(Chunk *c);
   Status ChunkAssemble(Chunk *c);
   Status ChunkLinear(Chunk *c);

@@ -46,7 +46,7 @@ EXPORTED = [
     "fg_postprocess_default_options", "fg_postprocess_create", "fg_postprocess_destroy",
     "fg_postprocess_probe_count", "fg_postprocess_mask", "fg_postprocess_compute",
     "fg_postprocess_compute_device", "fg_postprocess_frozen", "fg_postprocess_tangent",
-    "fg_solve_tangent", "fg_plan_attach_device",
+    "fg_solve_tangent", "fg_plan_attach_device", "fg_set_wait_limit_ns",
 ]
 
 
@@ -158,7 +158,15 @@ def lib():
         _LIB.fg_multi_destroy.restype = None
         _LIB.fg_postprocess_destroy.restype = None
         _LIB.fg_postprocess_default_options.restype = None
+        _LIB.fg_set_wait_limit_ns.restype = C.c_int64
+        _LIB.fg_set_wait_limit_ns.argtypes = [C.c_int64]
     return _LIB
+
+
+def set_wait_limit_ns(ns: int) -> int:
+    """fg_set_wait_limit_ns: bound of the PCG launches' grid-wide waits (ns <= 0: the
+    default 5 s); returns the previous bound."""
+    return int(lib().fg_set_wait_limit_ns(int(ns)))
 
 
 def status_name(status: int) -> str:

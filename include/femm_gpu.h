@@ -205,6 +205,14 @@ void fg_production_options(fg_solve_options *options);
 const char *fg_status_name(int status);
 int fg_abi_version(void);
 
+/* Bound, in nanoseconds, of every grid-wide wait inside the PCG launches of plans,
+ * fg_csr_pcg and multi-plan solves (default 5 s; ns <= 0 restores the default); returns
+ * the previous bound.  When a wait runs out, every CTA of the launch returns and the call
+ * reports FG_INTERNAL_ERROR; the CUDA context stays usable.  The reference bounds its
+ * device loops the same way (gpu_solver/src/solvers/pcg_kernels.cu:555-566); this setter
+ * is the test hook that makes such a wait run out. */
+int64_t fg_set_wait_limit_ns(int64_t ns);
+
 /* NonlinearP1Solver::Initialize + device plan set-up (nonlinear_solver.cu:784-800,
  * nonlinear_assembly.cu:362-441, nonlinear_topology.cpp:12-248). */
 int fg_plan_create(const fg_model *model, const fg_plan_options *options, fg_plan **plan);

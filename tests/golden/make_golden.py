@@ -1,7 +1,6 @@
 """Regenerates tests/golden/ from the reference checkout's own test fixtures.
 
-Run once in a checkout that has the reference (default path /root/reference, or the
-FEMM_GPU_REFERENCE environment variable).  The files are the reference's frozen
+Run once with the FEMM_GPU_REFERENCE environment variable naming a reference checkout.  The files are the reference's frozen
 golden vectors for this path, copied byte for byte (gpu_solver/tests/fixtures/...):
 
 * 35PN230.tab, reference_samples.txt, smoothing_reference.txt  (B-H spline / eval)
@@ -19,7 +18,7 @@ import json
 import os
 import shutil
 
-REF = os.environ.get("FEMM_GPU_REFERENCE", "/root/reference")
+REF = os.environ.get("FEMM_GPU_REFERENCE", "")
 FIX = os.path.join(REF, "gpu_solver", "tests", "fixtures")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
@@ -43,6 +42,8 @@ FILES = {
 
 
 def main():
+    if not REF or not os.path.isdir(FIX):
+        raise SystemExit("set FEMM_GPU_REFERENCE to a reference checkout (gpu_solver/tests/fixtures)")
     expected = {}
     for src, dst in FILES.items():
         shutil.copyfile(os.path.join(FIX, src), os.path.join(HERE, dst))

@@ -93,3 +93,32 @@ def test_recovery_of_exhausted_items_matches_oracle(gpu, max_newton):
         assert got.info[i].verified_equation_residual_relative <= 1e-8
         assert rel(got.a[i], a[i]) <= 5e-9
         assert rel(got.flux[i], flux[i]) <= 1e-8
+
+
+def test_wide_batch_chunks_solved_together(gpu):
+    """A shared-geometry batch wider than one launch (80 samples: chunks of 32, 32 and 16)
+    advances all its chunks together, one multi-group PCG launch per Newton step.  Each item
+    equals the same sample solved in a batch of at most 32 (same status and Newton
+    iterations; A within 5e-9 and flux within 1e-8: the multi-group launch gives a chunk
+    fewer CTAs, so its reductions round differently) and the oracle's solve (A 5e-9)."""
+    model = meshes.square_nonlinear(m=40, seed=21)
+    currents = meshes.seeded_currents(80, 3, 20.0, seed=22)
+    hc = np.random.default_rng(23).uniform(0.9, 1.1, size=80)
+    plan = fg.Plan(model)
+    wide = plan.solve(currents, hc_scale=hc)
+    t = plan.last_timing()
+    assert t.pcg_launches == t.newton_iterations  # one launch per lock-step Newton step
+    for first in (0, 32, 64):
+        part = plan.solve(currents[first:first + 32], hc_scale=hc[first:first + 32])
+        for i in range(len(part.info)):
+            w = first + i
+            assert wide.info[w].status == part.info[i].status == 0
+            assert wide.info[w].iterations == part.info[i].iterations
+            assert rel(wide.a[w], part.a[i]) <= 5e-9
+            assert rel(wide.flux[w], part.flux[i]) <= 1e-8
+    for w in (0, 45, 79):
+        mi = meshes.square_nonlinear(m=40, seed=21)
+        mi.hc = np.asarray(mi.hc) * hc[w]
+        a, _, _, flux, info = O.solve_batch(mi, currents[w:w + 1])
+        assert info[0].status == 0 and info[0].iterations == wide.info[w].iterations
+        assert rel(wide.a[w], a[0]) <= 5e-9 and rel(wide.flux[w], flux[0]) <= 1e-8
