@@ -59,10 +59,13 @@ def parse():
     p.add_argument("--no-forms", action="store_true", help="skip the mixed / block / learned forms")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm start form")
     p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
-    p.add_argument("--sector-samples", type=int, default=64, help="samples of the shared-geometry sector form")
-    p.add_argument("--hetero-meshes", type=int, default=64, help="meshes of the heterogeneous-batch form")
+    p.add_argument("--learned-held", type=int, default=256, help="held-out samples of the learned form")
+    p.add_argument("--sector-samples", type=int, default=1024, help="samples of the shared-geometry sector form")
+    p.add_argument("--hetero-meshes", type=int, default=256, help="meshes of the heterogeneous-batch form")
+    p.add_argument("--all-forms", action="store_true",
+                   help="also the postprocess / tangent, streaming-worker and sliding-band forms")
     p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker", "sliding_band",
-                                           "planar_2m"],
+                                           "planar_2m", "reference_gpu", "learned", "sector", "hetero"],
                    help="run one form alone and print its JSON (profiling)")
     return p.parse_args()
 
@@ -339,11 +342,11 @@ def run_ours(args, world, rank, local):
 
     # End to end through the host-buffer C ABI (H2D currents, D2H A / B / flux / info).
     host_in = [meshes.seeded_currents(k, Cc, 20.0, seed=777000 + 100000 * rank + s) for s in range(args.steps)]
-    plan.solve(host_in[0])  # warm the host-path staging buffers
+    host_out = plan.solve(host_in[0])  # warm the staging buffers; its host arrays are reused
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for s in range(args.steps):
-        plan.solve(host_in[s])
+        plan.solve(host_in[s], out=host_out)
     e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
     e2e = {"value": weak_value(world, k, args.steps, e2e_s), "unit": "solves/s",
            "h2d_bytes_per_step": k * Cc * 8,
@@ -401,13 +404,17 @@ def forms_summary(forms):
              "newton_iterations_per_item", "pcg_iterations_per_item", "a_rel_err", "b_rel_err", "flux_rel_err")
     sec = forms.get("shared_geometry_sector", {})
     for name, d in sec.items():
-        pick("sector_" + name, d, "solves_per_s_e2e", "vs_fp64_jacobi", "a_rel_err", "flux_rel_err",
-             "a_rel_err_vs_oracle", "flux_rel_err_vs_oracle")
+        pick("sector_" + name, d, "solves_per_s_e2e", "vs_chunk_by_chunk", "a_rel_err_vs_oracle",
+             "flux_rel_err_vs_oracle", "newton_iterations_equal_oracle")
+    pick("reference_gpu_executable", forms.get("reference_gpu"), "reference_gpu_solve_seconds",
+         "ours_solve_seconds", "solve_speedup", "solve_flux_rel_err", "reference_gpu_batch_solves_per_s",
+         "ours_batch_solves_per_s", "batch_speedup", "batch_flux_rel_err", "batch_torque_rel_err")
     pick("heterogeneous", forms.get("heterogeneous_meshes"), "meshes", "multi_solves_per_s",
          "one_plan_at_a_time_solves_per_s", "speedup", "a_rel_err_vs_single")
     lw = forms.get("learned_warm_start", {})
     for name, d in lw.items():
         pick("learned_" + name, d, "solves_per_s_e2e", "vs_fp64_zero_start", "vs_same_form_zero_start",
+             "warm_starts_used",
              "newton_iterations_per_item", "pcg_iterations_per_item", "a_rel_err", "flux_rel_err")
     pick("sliding_band", forms.get("sliding_band"), "solves_per_s_e2e", "speedup_vs_cpu",
          "flux_rel_err_vs_reference")
@@ -453,7 +460,7 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
     import torch
 
     import femm_gpu_b200 as fg
-    from femm_gpu_b200 import learned, meshes
+    from femm_gpu_b200 import meshes
 
     k, Cc = args.items, plan.C
     steps, warmup = 3, 1
@@ -482,52 +489,114 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
         p.close()
     out["planar_2m"] = planar_2m_form(dev, stream, flush)
 
-    # Shared geometry with per-sample magnets: the rotor-stator sector (40k nodes,
-    # anti-periodic edges), currents U[-15, 15] A and Hc U[8.5e5, 9.5e5] A/m per sample.
+    out["shared_geometry_sector"] = sector_form(args.sector_samples)
+    out["heterogeneous_meshes"] = hetero_form(args.hetero_meshes)
+    out["reference_gpu"] = reference_gpu_form(args.mesh)
+    if not args.no_learned:
+        out["learned_warm_start"] = learned_form(args.learned_train, args.learned_held)
+    if args.all_forms:
+        rng = np.random.default_rng(77)
+        cur = rng.uniform(-15.0, 15.0, size=(64, 3))
+        hcs = rng.uniform(8.5e5, 9.5e5, size=64) / 9.0e5
+        out["postprocess_tangent_sector"] = postprocess_tangent_form(meshes.annular_sector(), cur, hcs, dev,
+                                                                     stream, err)
+        out["streaming_worker"] = worker_form()
+        out["sliding_band"] = sliding_band_form()
+    return out
+
+
+def oracle_solves(models, currents):
+    """The FP64 oracle (the C restatement) on one sample per model, one host thread each
+    (ctypes releases the GIL): (A, flux, status, Newton iterations) per sample."""
+    import oracle as O
+
+    out = [None] * len(models)
+
+    def run(i):
+        a, _, _, f, info = O.solve_batch(models[i], currents[i:i + 1])
+        out[i] = (a[0], f[0], info[0].status, info[0].iterations)
+
+    ths = [threading.Thread(target=run, args=(i,)) for i in range(len(models))]
+    [t.start() for t in ths]
+    [t.join() for t in ths]
+    return out
+
+
+def max_rel(a, b):
+    return float(max(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i]) for i in range(len(b))))
+
+
+def sector_form(samples, check=8):
+    """Shared geometry at scale: the rotor-stator sector (about 40k nodes, anti-periodic
+    90-degree edges), `samples` samples with per-sample currents U[-15, 15] A and magnet
+    Hc U[8.5e5, 9.5e5] A/m.  The plain FP64 Jacobi method solved chunk after chunk (32
+    items per launch, as the reference batches) and with all chunks advancing together (one
+    multi-group PCG launch per Newton step, CUDA-graph replays); then the fast form (mixed
+    precision, block-Jacobi 8, PCG from the iterate).  Host-buffer API timing.  The first
+    `check` samples are compared with the FP64 oracle solving each sample's own model."""
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import meshes
+
     sector = meshes.annular_sector()
     rng = np.random.default_rng(77)
-    ks = args.sector_samples
-    cur = rng.uniform(-15.0, 15.0, size=(ks, 3))
-    hcs = rng.uniform(8.5e5, 9.5e5, size=ks) / 9.0e5
-    res = {}
-    for name, kw in (("fp64_jacobi", {}),
-                     ("mixed_block8_from_iterate", dict(precision=1, preconditioner=1, block_size=8,
-                                                        from_iterate=True))):
-        p = fg.Plan(sector, **kw)
-        p.solve(cur[:8], hc_scale=hcs[:8], outputs="a")
-        t0 = time.perf_counter()
-        r = p.solve(cur, hc_scale=hcs, outputs="a")
-        dt = time.perf_counter() - t0
-        res[name] = {"solves_per_s_e2e": ks / dt,
-                     "newton_iterations_per_item": float(np.mean([i.iterations for i in r.info])),
-                     "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in r.info])),
-                     "all_converged": all(i.status == 0 for i in r.info), "a": r.a, "flux": r.flux}
-        p.close()
-    f = res["mixed_block8_from_iterate"]
-    f["a_rel_err"] = err(f["a"], res["fp64_jacobi"]["a"])
-    f["flux_rel_err"] = err(f["flux"], res["fp64_jacobi"]["flux"])
-    f["vs_fp64_jacobi"] = f["solves_per_s_e2e"] / res["fp64_jacobi"]["solves_per_s_e2e"]
-    for r_ in res.values():
-        r_.pop("a")
-        r_.pop("flux")
-    out["shared_geometry_sector"] = dict(
-        workload=f"rotor-stator sector, {sector.node_count} nodes, anti-periodic 90-degree edges, "
-                 f"{ks} samples with per-sample currents and magnet Hc; host-buffer API timing", **res)
+    cur = rng.uniform(-15.0, 15.0, size=(samples, 3))
+    hc = rng.uniform(8.5e5, 9.5e5, size=samples)
+    hcs = hc / 9.0e5
+    t0 = time.perf_counter()
+    ref = oracle_solves([meshes.annular_sector(hc=h) for h in hc[:check]], cur[:check])
+    oracle_s = time.perf_counter() - t0
+    ra = np.array([r[0] for r in ref])
+    rf = np.array([r[1] for r in ref])
+    out = {"workload": f"rotor-stator sector, {sector.node_count} nodes, anti-periodic 90-degree edges, "
+                       f"{samples} samples with per-sample currents and magnet Hc; host-buffer API timing",
+           "oracle_check_samples": check, "oracle_seconds": oracle_s,
+           "oracle_all_converged": all(r[2] == 0 for r in ref)}
+    saved = os.environ.get("FG_CHUNKS_TOGETHER")
+    try:
+        for name, kw, together in (("fp64_jacobi_chunk_by_chunk", {}, "0"),
+                                   ("fp64_jacobi_chunks_together", {}, "1"),
+                                   ("mixed_block8_from_iterate", dict(precision=1, preconditioner=1, block_size=8,
+                                                                      from_iterate=True), "1")):
+            os.environ["FG_CHUNKS_TOGETHER"] = together
+            p = fg.Plan(sector, **kw)
+            p.solve(cur[:64], hc_scale=hcs[:64], outputs=False)  # warm: workspaces and lanes
+            t0 = time.perf_counter()
+            r = p.solve(cur, hc_scale=hcs, outputs="a")
+            dt = time.perf_counter() - t0
+            t = p.last_timing()
+            out[name] = {"solves_per_s_e2e": samples / dt, "seconds": dt,
+                         "newton_iterations_per_item": float(np.mean([i.iterations for i in r.info])),
+                         "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in r.info])),
+                         "pcg_launches": int(t.pcg_launches), "all_converged": all(i.status == 0 for i in r.info),
+                         "a_rel_err_vs_oracle": max_rel(r.a[:check], ra),
+                         "flux_rel_err_vs_oracle": max_rel(r.flux[:check], rf),
+                         "newton_iterations_equal_oracle": all(r.info[i].iterations == ref[i][3] for i in range(check))}
+            p.close()
+    finally:
+        if saved is None:
+            os.environ.pop("FG_CHUNKS_TOGETHER", None)
+        else:
+            os.environ["FG_CHUNKS_TOGETHER"] = saved
+    base = out["fp64_jacobi_chunk_by_chunk"]["solves_per_s_e2e"]
+    for name in ("fp64_jacobi_chunks_together", "mixed_block8_from_iterate"):
+        out[name]["vs_chunk_by_chunk"] = out[name]["solves_per_s_e2e"] / base
+    return out
 
-    out["postprocess_tangent_sector"] = postprocess_tangent_form(sector, cur, hcs, dev, stream, err)
 
-    out["streaming_worker"] = worker_form()
+def hetero_form(count):
+    """Heterogeneous meshes: `count` jittered squares with node counts log-uniform in
+    [5k, 200k], one sample each, in one multi-plan PCG launch per Newton step against the
+    same solves one plan at a time.  Host-buffer API timing (plans built beforehand)."""
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import meshes
 
-    out["sliding_band"] = sliding_band_form()
-
-    # Heterogeneous meshes: jittered squares with node counts log-uniform in [5k, 200k],
-    # one sample each, in one multi-plan PCG launch per Newton step vs one plan at a time.
     rng = np.random.default_rng(11)
-    count = args.hetero_meshes
     ns = np.exp(rng.uniform(np.log(5e3), np.log(2e5), size=count))
     models = [meshes.square_nonlinear(m=int(round(np.sqrt(n))) - 1, seed=1000 + i) for i, n in enumerate(ns)]
     curs = [meshes.seeded_currents(1, 3, 20.0, seed=3000 + i)[0] for i in range(count)]
+    t0 = time.perf_counter()
     plans = [fg.Plan(mo) for mo in models]
+    plan_s = time.perf_counter() - t0
     multi = fg.Multi(plans)
     multi.solve(curs, outputs=False)
     t0 = time.perf_counter()
@@ -537,62 +606,166 @@ def run_forms(args, model, plan, dev, stream, flush, plain_value):
     t0 = time.perf_counter()
     single = [p.solve([c], outputs="a") for p, c in zip(plans, curs)]
     dt_single = time.perf_counter() - t0
-    out["heterogeneous_meshes"] = {
-        "workload": f"{count} jittered squares, {sum(mo.node_count for mo in models)} nodes in all "
-                    "(5k-200k each, log-uniform), one sample each; host-buffer API timing",
-        "multi_solves_per_s": count / dt_multi, "one_plan_at_a_time_solves_per_s": count / dt_single,
-        "speedup": dt_single / dt_multi, "newton_steps": int(mt.newton_steps),
-        "pcg_launches": int(mt.pcg_launches), "graph_launches": int(mt.graph_launches),
-        "graph_captures": int(mt.graph_captures), "max_ctas": int(mt.max_ctas),
-        "all_converged": all(i.status == 0 for i in minfo),
-        "a_rel_err_vs_single": err(ma, [s_.a[0] for s_ in single])}
+    out = {"workload": f"{count} jittered squares, {sum(mo.node_count for mo in models)} nodes in all "
+                       "(5k-200k each, log-uniform), one sample each; host-buffer API timing",
+           "meshes": count, "plan_build_seconds": plan_s,
+           "multi_solves_per_s": count / dt_multi, "one_plan_at_a_time_solves_per_s": count / dt_single,
+           "speedup": dt_single / dt_multi, "newton_steps": int(mt.newton_steps),
+           "pcg_launches": int(mt.pcg_launches), "graph_launches": int(mt.graph_launches),
+           "graph_captures": int(mt.graph_captures), "max_ctas": int(mt.max_ctas),
+           "all_converged": all(i.status == 0 for i in minfo),
+           "a_rel_err_vs_single": max_rel(ma, [s_.a[0] for s_ in single])}
     multi.close()
     for p in plans:
         p.close()
+    return out
 
-    if not args.no_learned:
-        ax = meshes.axisymmetric_plunger()
-        base = fg.Plan(ax)
-        ntrain, nheld = args.learned_train, 256
-        train = np.random.default_rng(2024).uniform(-30, 30, size=(ntrain, 2))
-        held = np.random.default_rng(2025).uniform(-30, 30, size=(nheld, 2))
+
+def learned_form(ntrain, nheld, block=1024):
+    """The learned warm start on the axisymmetric plunger (about 100k nodes, 2 coils
+    U[-30, 30] A): POD basis + MLP trained on `ntrain` FP64 solves of the plain method, then
+    `nheld` held-out samples solved three ways at the same gates -- the plain FP64 Jacobi
+    method from zero; the fast form (mixed precision, block-Jacobi 8, PCG from the iterate)
+    from zero; the same fast form from the network's guarded prediction.  The last two
+    isolate the network's own gain.  Errors: against the plain FP64 solutions."""
+    import torch
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import learned, meshes
+
+    ax = meshes.axisymmetric_plunger()
+    base = fg.Plan(ax)
+    train = np.random.default_rng(2024).uniform(-30, 30, size=(ntrain, 2))
+    held = np.random.default_rng(2025).uniform(-30, 30, size=(nheld, 2))
+    t0 = time.perf_counter()
+    ws = learned.LearnedWarmStart(base, current_scale=30.0, rank=64, hidden=256, seed=1)
+    ws.fit(train, pod_samples=min(512, ntrain), epochs=200, batch=256, lr=2e-3, block=block)
+    fit_s = time.perf_counter() - t0
+    fast = fg.Plan(ax, precision=1, preconditioner=1, block_size=8, from_iterate=True)
+    w = ws.warm
+    lw = learned.LearnedWarmStart(fast, 30.0)
+    lw.warm = learned.WarmModel(fast, w.mean, w.basis, ws.mlp, *w._keep)
+    res = {}
+    for name, fn in (("fp64_jacobi_zero_start", lambda c: base.solve(c, outputs="a")),
+                     ("fast_form_zero_start", lambda c: fast.solve(c, outputs="a")),
+                     ("learned_fast_form", lambda c: lw.solve(c, outputs="a"))):
+        fn(held[:32])
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
-        ws = learned.LearnedWarmStart(base, current_scale=30.0, rank=64, hidden=256, seed=1)
-        ws.fit(train, pod_samples=min(512, ntrain), epochs=200, batch=256, lr=2e-3)
-        fit_s = time.perf_counter() - t0
-        fast = fg.Plan(ax, precision=1, preconditioner=1, block_size=8, from_iterate=True)
-        w = ws.warm
-        lw = learned.LearnedWarmStart(fast, 30.0)
-        lw.warm = learned.WarmModel(fast, w.mean, w.basis, ws.mlp, *w._keep)
-        res = {}
-        for name, fn in (("fp64_jacobi_zero_start", lambda c: base.solve(c, outputs="a")),
-                         ("learned_mixed_block8_from_iterate", lambda c: lw.solve(c, outputs="a"))):
-            fn(held[:32])
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            rs = [fn(held[i:i + 32]) for i in range(0, nheld, 32)]
-            dt = time.perf_counter() - t0
-            info = [i for r in rs for i in r.info]
-            res[name] = {"solves_per_s_e2e": nheld / dt,
-                         "newton_iterations_per_item": float(np.mean([i.iterations for i in info])),
-                         "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in info])),
-                         "warm_starts_used": int(sum(i.warm_start == 1 for i in info)),
-                         "all_converged": all(i.status == 0 for i in info),
-                         "a": np.concatenate([r.a for r in rs]), "flux": np.concatenate([r.flux for r in rs])}
-        z, l = res["fp64_jacobi_zero_start"], res["learned_mixed_block8_from_iterate"]
-        l["a_rel_err"] = err(l["a"], z["a"])
-        l["flux_rel_err"] = err(l["flux"], z["flux"])
-        l["vs_fp64_zero_start"] = l["solves_per_s_e2e"] / z["solves_per_s_e2e"]
-        for r in res.values():
-            r.pop("a")
-            r.pop("flux")
-        out["learned_warm_start"] = dict(
-            workload=f"axisymmetric plunger r-z, {ax.node_count} nodes, 2 coils U[-30,30] A; "
-                     f"{ntrain} training solves, {nheld} held-out samples; host-buffer API timing",
-            fit_seconds=fit_s, pod_energy=float(ws.stats["pod_energy"]),
-            final_loss=float(ws.stats["final_loss"]), **res)
-        fast.close()
-        base.close()
+        rs = [fn(held[i:i + block]) for i in range(0, nheld, block)]
+        dt = time.perf_counter() - t0
+        info = [i for r in rs for i in r.info]
+        res[name] = {"solves_per_s_e2e": nheld / dt,
+                     "newton_iterations_per_item": float(np.mean([i.iterations for i in info])),
+                     "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in info])),
+                     "warm_starts_used": int(sum(i.warm_start == 1 for i in info)),
+                     "all_converged": all(i.status == 0 for i in info),
+                     "a": np.concatenate([r.a for r in rs]), "flux": np.concatenate([r.flux for r in rs])}
+    z = res["fp64_jacobi_zero_start"]
+    for name in ("fast_form_zero_start", "learned_fast_form"):
+        r = res[name]
+        r["a_rel_err"] = max_rel(r["a"], z["a"])
+        r["flux_rel_err"] = max_rel(r["flux"], z["flux"])
+        r["vs_fp64_zero_start"] = r["solves_per_s_e2e"] / z["solves_per_s_e2e"]
+    res["learned_fast_form"]["vs_same_form_zero_start"] = (res["learned_fast_form"]["solves_per_s_e2e"] /
+                                                          res["fast_form_zero_start"]["solves_per_s_e2e"])
+    for r in res.values():
+        r.pop("a")
+        r.pop("flux")
+    out = dict(workload=f"axisymmetric plunger r-z, {ax.node_count} nodes, 2 coils U[-30,30] A; "
+                        f"{ntrain} training solves, {nheld} held-out samples; host-buffer API timing",
+               fit_seconds=fit_s, pod_energy=float(ws.stats["pod_energy"]),
+               final_loss=float(ws.stats["final_loss"]), **res)
+    fast.close()
+    base.close()
+    return out
+
+
+def reference_gpu_form(mesh=MESH_M, items=8):
+    """GPU against GPU on the headline workload: the reference's own executable built for
+    sm_100a (oracle/_ref/bin/femm_gpu_ref, built by oracle/Makefile's refgpu target) and this
+    library's femm_gpu answer the same request files.  --solve: one sample per process
+    (wall clock, process start, artifact read and hash included), flux linkage and Newton
+    iterations compared.  --motor-batch-profile: `items` samples of the posed motor form of
+    the same artifact in one process (the reference's SolveBatch path, 32 items per chunk),
+    its own timing block and the wall clock, every item's flux linkage and torque compared."""
+    import hashlib
+    import tempfile
+    from femm_gpu_b200 import artifact, meshes
+
+    theirs = os.path.join(ROOT, "oracle", "_ref", "bin", "femm_gpu_ref")
+    ours = os.path.join(ROOT, "femm-gpu_b200", "bin", "femm_gpu")
+    if not os.path.exists(theirs):
+        return {"unavailable": "the reference executable was not built (no reference checkout)"}
+    tmp = tempfile.mkdtemp(prefix="fg_refgpu_")
+    model = meshes.square_nonlinear(m=mesh, seed=SEED_MESH)
+    text, _ = artifact.write_artifact(model, [0.0, 0.0, 0.0])
+    neutral = os.path.join(tmp, "square.gpu.json")
+    open(neutral, "w").write(text)
+    src = json.loads(text)
+    src["schema_version"] = "gpu_femm_mesh_v1"
+    base = "e" * 64
+    src["base_motor_fem_sha256"] = base
+    src["resolved"]["base_motor_fem_sha256"] = base
+    src["resolved"]["pose"] = {"rotor_angle_deg": 0, "displacement_mm": [0, 0]}
+    del src["resolved"]["node_constraints"]  # a posed motor artifact carries none
+    motor = os.path.join(tmp, "square_motor.gpu.json")
+    open(motor, "w").write(json.dumps(src))
+    sha = lambda p: hashlib.sha256(open(p, "rb").read()).hexdigest()  # noqa: E731
+    cur = meshes.seeded_currents(items, 3, 20.0, seed=5150)
+
+    def run(exe, command, body, name):
+        rq, rs = os.path.join(tmp, name + ".json"), os.path.join(tmp, name + "." + os.path.basename(exe) + ".out")
+        open(rq, "w").write(json.dumps(body))
+        t0 = time.perf_counter()
+        r = subprocess.run([exe, command, rq, rs], capture_output=True, text=True, timeout=1800)
+        return r.returncode, time.perf_counter() - t0, (json.load(open(rs)) if os.path.exists(rs) else {})
+
+    solve = {"protocol": "gpu_femm_magnetostatic_sample_v1", "mesh_artifact_path": neutral,
+             "mesh_artifact_sha256": sha(neutral), "circuit_currents_A": [float(c) for c in cur[0]],
+             "force_group_number": -1, "stress_air_group_number": -1, "airgap_radius_mm": 0,
+             "airgap_angles_deg": [], "sliding_band_angle_deg": 0, "compute_force_torque": False,
+             "include_field_solution": False}
+    out = {"workload": f"nonlinear planar solve, {model.node_count} nodes; the same request files to both "
+                       "executables; wall clock per process"}
+    res = {}
+    for name, exe in (("reference_gpu", theirs), ("ours", ours)):
+        run(exe, "--solve", solve, "warm")  # page in the executable and the driver
+        rc, dt, body = run(exe, "--solve", solve, "solve")
+        res[name] = (rc, dt, body)
+        out[f"{name}_solve_seconds"] = dt
+        out[f"{name}_solve_ok"] = rc == 0 and body.get("status") == "PASS"
+    fr, fo = res["reference_gpu"][2], res["ours"][2]
+    if out["reference_gpu_solve_ok"] and out["ours_solve_ok"]:
+        a, b = np.array(fo["circuit_flux_linkage_Wb"]), np.array(fr["circuit_flux_linkage_Wb"])
+        out["solve_flux_rel_err"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        out["solve_newton_iterations"] = [fr["convergence"]["iterations"], fo["convergence"]["iterations"]]
+        out["solve_speedup"] = out["reference_gpu_solve_seconds"] / out["ours_solve_seconds"]
+    batch = {"protocol": "gpu_femm_motor_batch_v1", "max_items_per_chunk": 32,
+             "items": [{"task_id": f"t{i}", "request": {
+                 "protocol": "gpu_femm_motor_sample_v1", "mesh_artifact_path": motor,
+                 "mesh_artifact_sha256": sha(motor), "base_motor_fem_sha256": base,
+                 "source_fem_sha256": src["source_fem_sha256"], "circuit_currents_A": [float(c) for c in cur[i]],
+                 "selected_group_number": 1, "air_group_number": 0, "airgap_radius_mm": 0,
+                 "airgap_angles_deg": [], "rotor_angle_deg": 0, "displacement_mm": [0, 0]}}
+                       for i in range(items)]}
+    for name, exe in (("reference_gpu", theirs), ("ours", ours)):
+        rc, dt, body = run(exe, "--motor-batch-profile", batch, "batch")
+        res[name] = (rc, dt, body)
+        out[f"{name}_batch_seconds"] = dt
+        out[f"{name}_batch_solves_per_s"] = items / dt
+        tm = body.get("timing", {})
+        out[f"{name}_batch_timing"] = {k: tm.get(k) for k in ("gpu_kernel_sync_seconds", "host_assembly_seconds",
+                                                               "device_assembly_seconds", "postprocess_seconds",
+                                                               "measured_before_response_write_seconds")}
+        out[f"{name}_batch_ok"] = rc == 0 and body.get("status") == "PASS"
+    if out["reference_gpu_batch_ok"] and out["ours_batch_ok"]:
+        ir, io = res["reference_gpu"][2]["items"], res["ours"][2]["items"]
+        out["batch_flux_rel_err"] = float(max(
+            np.linalg.norm(np.subtract(a["response"]["circuit_flux_linkage_Wb"], b["response"]["circuit_flux_linkage_Wb"]))
+            / np.linalg.norm(b["response"]["circuit_flux_linkage_Wb"]) for a, b in zip(io, ir)))
+        out["batch_torque_rel_err"] = float(max(abs(a["response"]["torque_Nm"] - b["response"]["torque_Nm"])
+                                                / max(abs(b["response"]["torque_Nm"]), 1e-300) for a, b in zip(io, ir)))
+        out["batch_speedup"] = out["reference_gpu_batch_seconds"] / out["ours_batch_seconds"]
     return out
 
 
@@ -987,6 +1160,14 @@ def only_form(args):
     stream = torch.cuda.current_stream(dev)
     if args.only_form == "streaming_worker":
         out = worker_form()
+    elif args.only_form == "learned":
+        out = learned_form(args.learned_train, args.learned_held)
+    elif args.only_form == "reference_gpu":
+        out = reference_gpu_form(args.mesh)
+    elif args.only_form == "sector":
+        out = sector_form(args.sector_samples)
+    elif args.only_form == "hetero":
+        out = hetero_form(args.hetero_meshes)
     elif args.only_form == "planar_2m":
         flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
         out = planar_2m_form(dev, stream, flush)

@@ -54,14 +54,12 @@ float Elapsed(cudaEvent_t a, cudaEvent_t b)
 // Chunks of a wide shared-geometry batch solved together in one multi-group launch.
 constexpr int kMaxLanes = 32;
 
-// FG_CHUNKS_TOGETHER=0 in the environment solves wide batches chunk after chunk (A/B timing).
+// FG_CHUNKS_TOGETHER=0 in the environment solves wide batches chunk after chunk (A/B timing;
+// read at every solve).
 bool ChunksTogetherEnabled()
 {
-  static const bool enabled = [] {
-    const char *v = std::getenv("FG_CHUNKS_TOGETHER");
-    return !(v && v[0] == '0');
-  }();
-  return enabled;
+  const char *v = std::getenv("FG_CHUNKS_TOGETHER");
+  return !(v && v[0] == '0');
 }
 
 } // namespace

@@ -354,25 +354,38 @@ class Plan:
         return x, [info[i] for i in range(k)]
 
     def solve(self, currents, hc_scale=None, warm=None, options: Optional[FgSolveOptions] = None,
-              outputs=True) -> SolveResult:
+              outputs=True, out: Optional[SolveResult] = None) -> SolveResult:
+        """fg_solve_batch.  outputs: True (A, B, flux), "a" (A and flux only) or False (item
+        info only).  out: a previous result of the same shape whose host arrays are reused
+        (a serving loop's preallocated buffers)."""
         currents = np.ascontiguousarray(np.atleast_2d(np.asarray(currents, np.float64)))
         k = currents.shape[0]
         currents = currents.reshape(k, self.C) if self.C else currents
         hc = None if hc_scale is None else np.ascontiguousarray(hc_scale, np.float64)
         wm = None if warm is None else np.ascontiguousarray(warm, np.float64).reshape(k, self.N)
         opts = options if options is not None else production_options()
-        # outputs: True (A, B, flux), "a" (A and flux only) or False (item info only)
-        a = np.zeros((k, self.N)) if outputs else None
-        b1 = np.zeros((k, self.E)) if outputs is True else None
-        b2 = np.zeros((k, self.E)) if outputs is True else None
-        flux = np.zeros((k, max(self.C, 1))) if outputs else None
+
+        def buf(name, shape, wanted):
+            if not wanted:
+                return None
+            old = getattr(out, name, None) if out is not None else None
+            if old is not None and old.shape == shape and old.dtype == np.float64 and old.flags.c_contiguous:
+                return old
+            return np.zeros(shape)
+
+        a = buf("a", (k, self.N), outputs)
+        b1 = buf("b1", (k, self.E), outputs is True)
+        b2 = buf("b2", (k, self.E), outputs is True)
+        flux = buf("_flux_full", (k, max(self.C, 1)), outputs)
         info = (FgItemInfo * k)()
         status = lib().fg_solve_batch(self._h, C.c_int32(k), _p(currents), _p(hc), _p(wm),
                                       C.byref(opts), _p(a), _p(b1), _p(b2), _p(flux), info)
         if status != 0:
             raise FgError(status, "fg_solve_batch")
-        return SolveResult(a, b1, b2, None if flux is None else flux[:, : self.C],
-                           [info[i] for i in range(k)])
+        res = SolveResult(a, b1, b2, None if flux is None else flux[:, : self.C],
+                          [info[i] for i in range(k)])
+        res._flux_full = flux
+        return res
 
     def solve_device(self, items, currents_ptr, options=None, hc_ptr=None, warm_ptr=None,
                      a_ptr=None, b1_ptr=None, b2_ptr=None, flux_ptr=None, stream=None):

@@ -177,9 +177,10 @@ class LearnedWarmStart:
         self.stats = {}
 
     def fit(self, currents, angles=0.0, pod_samples=256, epochs=200, batch=256, lr=2e-3,
-            options=None):
+            options=None, block=1024):
         """Solve every training sample (FP64, zero start), build the basis from the first
-        `pod_samples` solutions, project all of them and train the network."""
+        `pod_samples` solutions, project all of them and train the network.  The samples
+        are solved `block` at a time (a wide batch advances its chunks of 32 together)."""
         currents = np.atleast_2d(np.asarray(currents, np.float64))
         n = currents.shape[0]
         opts = options if options is not None else production_options()
@@ -191,8 +192,8 @@ class LearnedWarmStart:
         self.rank = basis.shape[0]
         proj = WarmModel(self.plan, mean, basis)
         coeffs = [proj.project(first.a)]
-        for s0 in range(m, n, 32):
-            r = self.plan.solve(currents[s0:s0 + 32], options=opts, outputs="a")
+        for s0 in range(m, n, block):
+            r = self.plan.solve(currents[s0:s0 + block], options=opts, outputs="a")
             if any(s != 0 for s in r.status):
                 raise RuntimeError("training solve did not converge")
             coeffs.append(proj.project(r.a))
