@@ -841,16 +841,45 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         be[j] = static_cast<T>(ctl.beta[item0 + j]);
         any_mine = any_mine || on(j);
       }
+      // Explicit search direction: p_new for this CTA's rows first (the same partition as
+      // the rows' epilogues below), then one plain grid barrier, and the SpMV gathers p_new
+      // alone.  The decision is uniform over the grid.
+      const bool xdir = a.explicit_direction != 0;
+      const T *G = Z;
+      if (xdir) {
+        if (any_mine) {
+          FG_ROWS_BEGIN
+          T zr[IV], pr[IV], pnew[IV];
+          Load<T, IV>(Z + ri, zr);
+          Load<T, IV>(pc + ri, pr);
+#pragma unroll
+          for (int j = 0; j < IV; ++j)
+            pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
+          Store<T, IV>(pn + ri, pnew);
+          FG_ROWS_END
+        }
+        if (!GridBarrier(a, gs, epoch, sm))
+          return;
+        G = pn;
+#pragma unroll
+        for (int j = 0; j < IV; ++j)
+          fold[j] = false;
+      }
       // Row epilogue: p_new of the row, q = acc, and p_new . q.
       auto finish_row = [&](int r, const T (&acc)[IV]) {
         const size_t ri = static_cast<size_t>(r) * KP + item0;
-        T zr[IV], pr[IV], pnew[IV];
-        Load<T, IV>(Z + ri, zr);
-        Load<T, IV>(pc + ri, pr);
+        T pnew[IV];
+        if (xdir) {
+          Load<T, IV>(pn + ri, pnew);
+        } else {
+          T zr[IV], pr[IV];
+          Load<T, IV>(Z + ri, zr);
+          Load<T, IV>(pc + ri, pr);
 #pragma unroll
-        for (int j = 0; j < IV; ++j)
-          pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
-        Store<T, IV>(pn + ri, pnew);
+          for (int j = 0; j < IV; ++j)
+            pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
+          Store<T, IV>(pn + ri, pnew);
+        }
         Store<T, IV>(Qv + ri, acc);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
@@ -882,18 +911,9 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             ll = __ldg(a.row_len + rr);
             bb = static_cast<size_t>(__ldg(a.slice_off + (rr >> 5))) + (rr & 31);
           };
-          // Column indices travel one chunk ahead too (registers): a chunk's gathers then
-          // wait for one L2 round trip, not for the index load and then the gather.
-          int c[U];
-          auto columns = [&](size_t bb, int w, int ll, int (&cc)[U]) {
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-              cc[u] = w + u < ll ? Column(a, colc, cbase, bb + 32 * static_cast<size_t>(w + u)) : 0;
-          };
           if (ws < ws1) {
             row_at(ws, r, len, base);
             issue(0, base, 0, len);
-            columns(base, 0, len, c);
           }
           T acc[IV];
 #pragma unroll
@@ -908,31 +928,33 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
               if (nws < ws1)
                 row_at(nws, nr, nlen, nbase);
             }
-            int cn[U];
-            if (nws < ws1) {
+            if (nws < ws1)
               issue(stage ^ 1, nbase, nw0, nlen);
-              columns(nbase, nw0, nlen, cn);
-            } else {
+            else
               CpAsyncCommit();
-#pragma unroll
-              for (int u = 0; u < U; ++u)
-                cn[u] = 0;
-            }
             CpAsyncWait<1>(); // the current chunk's values have landed
+            int c[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+              c[u] = w0 + u < len ? Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u)) : 0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
                 const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
-                T g[IV], pv[IV], vv[IV];
-                Load<T, IV>(Z + ci, g);
-                Load<T, IV>(pc + ci, pv);
+                T g[IV], vv[IV];
+                Load<T, IV>(G + ci, g);
+                if (!xdir) {
+                  T pv[IV];
+                  Load<T, IV>(pc + ci, pv);
+#pragma unroll
+                  for (int j = 0; j < IV; ++j)
+                    if (fold[j])
+                      g[j] = Fma(be[j], pv[j], g[j]);
+                }
                 Load<T, IV>(ring + ((stage * U + u) * 32 + lane) * IV, vv);
 #pragma unroll
-                for (int j = 0; j < IV; ++j) {
-                  if (fold[j])
-                    g[j] = Fma(be[j], pv[j], g[j]);
+                for (int j = 0; j < IV; ++j)
                   acc[j] = Fma(vv[j], g[j], acc[j]);
-                }
               }
             }
             if (w0 + U >= len) {
@@ -947,9 +969,6 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             w0 = nw0;
             base = nbase;
             stage ^= 1;
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-              c[u] = cn[u];
           }
           CpAsyncWait<0>();
           any_mine = false; // done
@@ -960,7 +979,10 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         const int len = __ldg(a.row_len + r);
         const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
         T acc[IV];
-        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
+        if (xdir)
+          RowProduct<T, KP, IV, false>(a, colc, cbase, base, len, item0, G, nullptr, fold, be, acc);
+        else
+          RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
         (void)ri;
         finish_row(r, acc);
         FG_ROWS_END
