@@ -526,14 +526,16 @@ def max_rel(a, b):
     return float(max(np.linalg.norm(a[i] - b[i]) / np.linalg.norm(b[i]) for i in range(len(b))))
 
 
-def sector_form(samples, check=8):
+def sector_form(samples, check=8, fast_samples=256):
     """Shared geometry at scale: the rotor-stator sector (about 40k nodes, anti-periodic
     90-degree edges), `samples` samples with per-sample currents U[-15, 15] A and magnet
     Hc U[8.5e5, 9.5e5] A/m.  The plain FP64 Jacobi method solved chunk after chunk (32
     items per launch, as the reference batches) and with all chunks advancing together (one
-    multi-group PCG launch per Newton step, CUDA-graph replays); then the fast form (mixed
-    precision, block-Jacobi 8, PCG from the iterate).  Host-buffer API timing.  The first
-    `check` samples are compared with the FP64 oracle solving each sample's own model."""
+    multi-group PCG launch per Newton step, CUDA-graph replays); then, on the first
+    `fast_samples` samples, the fast forms (block-Jacobi 8 and the PCG from the Newton
+    iterate, in FP64 and with the FP32 inner solve), compared with the plain method chunk by
+    chunk on the same samples.  Host-buffer API timing.  The first `check` samples are
+    compared with the FP64 oracle solving each sample's own model."""
     import femm_gpu_b200 as fg
     from femm_gpu_b200 import meshes
 
@@ -553,18 +555,23 @@ def sector_form(samples, check=8):
            "oracle_all_converged": all(r[2] == 0 for r in ref)}
     saved = os.environ.get("FG_CHUNKS_TOGETHER")
     try:
-        for name, kw, together in (("fp64_jacobi_chunk_by_chunk", {}, "0"),
-                                   ("fp64_jacobi_chunks_together", {}, "1"),
-                                   ("mixed_block8_from_iterate", dict(precision=1, preconditioner=1, block_size=8,
-                                                                      from_iterate=True), "1")):
+        fast = dict(preconditioner=1, block_size=8, from_iterate=True)
+        for name, kw, together, ks in (("fp64_jacobi_chunk_by_chunk", {}, "0", samples),
+                                       ("fp64_jacobi_chunks_together", {}, "1", samples),
+                                       ("fp64_jacobi_chunk_by_chunk_subset", {}, "0", fast_samples),
+                                       ("fp64_block8_from_iterate_subset", fast, "0", fast_samples),
+                                       ("mixed_block8_from_iterate_subset", dict(precision=1, **fast), "0",
+                                        fast_samples)):
+            if name == "fp64_jacobi_chunk_by_chunk_subset" and ks == samples:
+                continue
             os.environ["FG_CHUNKS_TOGETHER"] = together
             p = fg.Plan(sector, **kw)
             p.solve(cur[:64], hc_scale=hcs[:64], outputs=False)  # warm: workspaces and lanes
             t0 = time.perf_counter()
-            r = p.solve(cur, hc_scale=hcs, outputs="a")
+            r = p.solve(cur[:ks], hc_scale=hcs[:ks], outputs="a")
             dt = time.perf_counter() - t0
             t = p.last_timing()
-            out[name] = {"solves_per_s_e2e": samples / dt, "seconds": dt,
+            out[name] = {"samples": ks, "solves_per_s_e2e": ks / dt, "seconds": dt,
                          "newton_iterations_per_item": float(np.mean([i.iterations for i in r.info])),
                          "pcg_iterations_per_item": float(np.mean([i.linear_iterations for i in r.info])),
                          "pcg_launches": int(t.pcg_launches), "all_converged": all(i.status == 0 for i in r.info),
@@ -578,8 +585,10 @@ def sector_form(samples, check=8):
         else:
             os.environ["FG_CHUNKS_TOGETHER"] = saved
     base = out["fp64_jacobi_chunk_by_chunk"]["solves_per_s_e2e"]
-    for name in ("fp64_jacobi_chunks_together", "mixed_block8_from_iterate"):
-        out[name]["vs_chunk_by_chunk"] = out[name]["solves_per_s_e2e"] / base
+    out["fp64_jacobi_chunks_together"]["vs_chunk_by_chunk"] = out["fp64_jacobi_chunks_together"]["solves_per_s_e2e"] / base
+    sub = out.get("fp64_jacobi_chunk_by_chunk_subset", out["fp64_jacobi_chunk_by_chunk"])["solves_per_s_e2e"]
+    for name in ("fp64_block8_from_iterate_subset", "mixed_block8_from_iterate_subset"):
+        out[name]["vs_chunk_by_chunk"] = out[name]["solves_per_s_e2e"] / sub
     return out
 
 

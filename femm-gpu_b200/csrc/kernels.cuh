@@ -89,10 +89,6 @@ struct PcgArgs {
   // Value ring: the SpMV's operator values staged into shared memory by cp.async one chunk
   // ahead of their use (set by LaunchPcg for 16-byte item vectors).
   int32_t value_ring, value_ring_offset;
-  // Explicit search direction: Phase A first writes p_new = z + beta p for its own rows,
-  // passes one plain grid barrier and then gathers p_new alone in the SpMV (half the
-  // gathered bytes of the folded form, which gathers z and p); set by the launchers.
-  int32_t explicit_direction;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
   // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
   // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.
@@ -130,9 +126,6 @@ int PcgMaxGrid(int kp);
 // solves, in nanoseconds (fg_set_wait_limit_ns; default kDefaultWaitLimitNs).
 constexpr long long kDefaultWaitLimitNs = 5000000000LL;
 long long PcgWaitLimitNs();
-// Whether PCG launches use the explicit search direction (PcgArgs::explicit_direction):
-// FG_PCG_EXPLICIT_DIRECTION=1 / 0 in the environment, read once.
-bool PcgExplicitDirection();
 long long SetPcgWaitLimitNs(long long ns);
 // One cooperative launch of `ctas` CTAs solving every group of t (FP64 Jacobi; every group
 // holds kp items: 1, or 32 for the chunks of a wide shared-geometry batch).  The caller

@@ -156,7 +156,6 @@ Status MultiSolver::Run(const fg_solve_options &options, std::vector<double> *fi
         host_args_.get()[i].value_ring = 1;
         host_args_.get()[i].value_ring_offset = 0;
       }
-      host_args_.get()[i].explicit_direction = PcgExplicitDirection() ? 1 : 0;
       maps[max_grid_ + i] = next;
       maps[max_grid_ + M + i] = ctas[i];
       for (int j = 0; j < ctas[i]; ++j)

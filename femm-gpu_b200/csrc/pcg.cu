@@ -95,15 +95,6 @@ std::atomic<long long> g_wait_limit_ns{kDefaultWaitLimitNs};
 
 long long PcgWaitLimitNs() { return g_wait_limit_ns.load(std::memory_order_relaxed); }
 
-bool PcgExplicitDirection()
-{
-  static const bool enabled = [] {
-    const char *v = std::getenv("FG_PCG_EXPLICIT_DIRECTION");
-    return v && v[0] == '1';
-  }();
-  return enabled;
-}
-
 long long SetPcgWaitLimitNs(long long ns)
 {
   return g_wait_limit_ns.exchange(ns > 0 ? ns : kDefaultWaitLimitNs, std::memory_order_relaxed);
@@ -188,7 +179,6 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
       smem = total;
     }
   }
-  args.explicit_direction = PcgExplicitDirection() ? 1 : 0;
   cudaError_t e = cudaMemsetAsync(args.barrier, 0, sizeof(unsigned), stream);
   if (e == cudaSuccess)
     e = cudaMemsetAsync(args.error, 0, sizeof(int32_t), stream);

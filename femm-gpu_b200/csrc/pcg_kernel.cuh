@@ -841,45 +841,16 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         be[j] = static_cast<T>(ctl.beta[item0 + j]);
         any_mine = any_mine || on(j);
       }
-      // Explicit search direction: p_new for this CTA's rows first (the same partition as
-      // the rows' epilogues below), then one plain grid barrier, and the SpMV gathers p_new
-      // alone.  The decision is uniform over the grid.
-      const bool xdir = a.explicit_direction != 0;
-      const T *G = Z;
-      if (xdir) {
-        if (any_mine) {
-          FG_ROWS_BEGIN
-          T zr[IV], pr[IV], pnew[IV];
-          Load<T, IV>(Z + ri, zr);
-          Load<T, IV>(pc + ri, pr);
-#pragma unroll
-          for (int j = 0; j < IV; ++j)
-            pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
-          Store<T, IV>(pn + ri, pnew);
-          FG_ROWS_END
-        }
-        if (!GridBarrier(a, gs, epoch, sm))
-          return;
-        G = pn;
-#pragma unroll
-        for (int j = 0; j < IV; ++j)
-          fold[j] = false;
-      }
       // Row epilogue: p_new of the row, q = acc, and p_new . q.
       auto finish_row = [&](int r, const T (&acc)[IV]) {
         const size_t ri = static_cast<size_t>(r) * KP + item0;
-        T pnew[IV];
-        if (xdir) {
-          Load<T, IV>(pn + ri, pnew);
-        } else {
-          T zr[IV], pr[IV];
-          Load<T, IV>(Z + ri, zr);
-          Load<T, IV>(pc + ri, pr);
+        T zr[IV], pr[IV], pnew[IV];
+        Load<T, IV>(Z + ri, zr);
+        Load<T, IV>(pc + ri, pr);
 #pragma unroll
-          for (int j = 0; j < IV; ++j)
-            pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
-          Store<T, IV>(pn + ri, pnew);
-        }
+        for (int j = 0; j < IV; ++j)
+          pnew[j] = fold[j] ? Fma(be[j], pr[j], zr[j]) : zr[j];
+        Store<T, IV>(pn + ri, pnew);
         Store<T, IV>(Qv + ri, acc);
 #pragma unroll
         for (int j = 0; j < IV; ++j)
@@ -941,20 +912,16 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
                 const size_t ci = static_cast<size_t>(c[u]) * KP + item0;
-                T g[IV], vv[IV];
-                Load<T, IV>(G + ci, g);
-                if (!xdir) {
-                  T pv[IV];
-                  Load<T, IV>(pc + ci, pv);
-#pragma unroll
-                  for (int j = 0; j < IV; ++j)
-                    if (fold[j])
-                      g[j] = Fma(be[j], pv[j], g[j]);
-                }
+                T g[IV], pv[IV], vv[IV];
+                Load<T, IV>(Z + ci, g);
+                Load<T, IV>(pc + ci, pv);
                 Load<T, IV>(ring + ((stage * U + u) * 32 + lane) * IV, vv);
 #pragma unroll
-                for (int j = 0; j < IV; ++j)
+                for (int j = 0; j < IV; ++j) {
+                  if (fold[j])
+                    g[j] = Fma(be[j], pv[j], g[j]);
                   acc[j] = Fma(vv[j], g[j], acc[j]);
+                }
               }
             }
             if (w0 + U >= len) {
@@ -979,10 +946,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         const int len = __ldg(a.row_len + r);
         const size_t base = static_cast<size_t>(__ldg(a.slice_off + (r >> 5))) + (r & 31);
         T acc[IV];
-        if (xdir)
-          RowProduct<T, KP, IV, false>(a, colc, cbase, base, len, item0, G, nullptr, fold, be, acc);
-        else
-          RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
+        RowProduct<T, KP, IV, true>(a, colc, cbase, base, len, item0, Z, pc, fold, be, acc);
         (void)ri;
         finish_row(r, acc);
         FG_ROWS_END

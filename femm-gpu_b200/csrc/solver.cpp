@@ -54,8 +54,11 @@ float Elapsed(cudaEvent_t a, cudaEvent_t b)
 // Chunks of a wide shared-geometry batch solved together in one multi-group launch.
 constexpr int kMaxLanes = 32;
 
-// The PCG from the iterate at the exact inner tolerance solves to this fraction of it.
+// The PCG from the iterate at the exact inner tolerance solves to this fraction of it, but
+// not below kIterateFinalFloor (nor below a tolerance the caller set tighter still): the
+// FP64 true residual of a 1e-14 target is not reliably reachable.
 constexpr double kIterateFinalTightening = 0.01;
+constexpr double kIterateFinalFloor = 1e-12;
 
 // FG_CHUNKS_TOGETHER=0 in the environment solves wide batches chunk after chunk (A/B timing;
 // read at every solve).
@@ -413,7 +416,9 @@ Status Plan::LinearSolve(int kp, int items, uint32_t mask, double tolerance, int
       if (!((mask >> i) & 1u))
         continue;
       const double dn = std::sqrt(h[i]), bn = std::sqrt(h[kp + i]);
-      const double target = final_tolerance ? kIterateFinalTightening * tolerance : tolerance;
+      const double target =
+          final_tolerance ? std::max(kIterateFinalTightening * tolerance, std::min(tolerance, kIterateFinalFloor))
+                          : tolerance;
       if (std::isfinite(dn) && std::isfinite(bn) && dn <= target * bn) {
         solve &= ~(1u << i); // the iterate already meets the linear tolerance
         done[3 * i] = ToInt(Status::kOk);

@@ -219,14 +219,25 @@ def test_batch_widths_match_oracle(gpu, k):
     check_solve(model, meshes.seeded_currents(k, 3, 20.0, seed=k))
 
 
-def test_batches_beyond_32_are_chunked(gpu):
+def test_batches_beyond_32_are_chunked(gpu, monkeypatch):
+    """A batch of 40: chunks of 32 and 8.  Solved chunk after chunk, its first 32 items
+    equal a batch of those 32 bit for bit; with the chunks advancing together (the
+    default), within 5e-9 (a chunk then runs on fewer CTAs and its reductions round
+    differently) with the same Newton iteration counts."""
     model = meshes.square_nonlinear(m=10, seed=6)
     currents = meshes.seeded_currents(40, 3, 20.0, seed=2)
     plan = fg.Plan(model)
+    first = plan.solve(currents[:32])
+    monkeypatch.setenv("FG_CHUNKS_TOGETHER", "0")
     r = plan.solve(currents)
     assert all(s == 0 for s in r.status)
-    first = plan.solve(currents[:32])
     assert np.array_equal(first.a, r.a[:32])
+    monkeypatch.delenv("FG_CHUNKS_TOGETHER")
+    together = plan.solve(currents)
+    assert all(s == 0 for s in together.status)
+    for i in range(40):
+        assert together.info[i].iterations == r.info[i].iterations
+        assert rel(together.a[i], r.a[i]) <= 5e-9
 
 
 # ----------------------------------------------------------------------------- full size
@@ -287,3 +298,24 @@ def test_mixed_precision_fixtures_and_axisymmetric(gpu):
     model, currents = artifact.read_artifact(open(os.path.join(GOLDEN, "periodic_strip.gpu.json")).read())
     check_mixed(model, currents[None, :])
     check_mixed(meshes.axisymmetric_plunger(mr=12, mz=24), meshes.seeded_currents(2, 2, 30.0, 5))
+
+
+@pytest.mark.parametrize("form", [dict(precision=1),
+                                  dict(precision=1, preconditioner=1, block_size=8, from_iterate=True),
+                                  dict(preconditioner=1, block_size=8, from_iterate=True)],
+                         ids=["mixed_jacobi", "mixed_block8_from_iterate", "fp64_block8_from_iterate"])
+def test_fast_forms_on_the_saturated_sector_match_the_oracle(gpu, form):
+    """The accelerated forms on the rotor-stator sector (anti-periodic edges, iron driven to
+    2 T, about 30 relaxed Newton iterations) against the FP64 oracle of the plain method:
+    same status, Newton iterations within 2, flux linkage within 1e-8 (the bound the
+    accelerated forms are held to), A within 5e-8 (different Krylov paths to the same 1e-10
+    gate, carried through the relaxed iteration)."""
+    model = meshes.annular_sector(nr=24, nt=36)
+    currents = np.random.default_rng(41).uniform(-15.0, 15.0, size=(3, 3))
+    got = fg.Plan(model, **form).solve(currents)
+    a, b1, b2, flux, info = O.solve_batch(model, currents)
+    for k in range(3):
+        assert got.info[k].status == info[k].status == 0
+        assert abs(got.info[k].iterations - info[k].iterations) <= 2
+        assert rel(got.flux[k], flux[k]) <= 1e-8, rel(got.flux[k], flux[k])
+        assert rel(got.a[k], a[k]) <= 5e-8, rel(got.a[k], a[k])
