@@ -882,9 +882,13 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             ll = __ldg(a.row_len + rr);
             bb = static_cast<size_t>(__ldg(a.slice_off + (rr >> 5))) + (rr & 31);
           };
+          int fr = 0, flen = 0;
+          size_t fbase = 0;
           if (ws < ws1) {
             row_at(ws, r, len, base);
             issue(0, base, 0, len);
+            if (ws + kPcgWarps < ws1)
+              row_at(ws + kPcgWarps, fr, flen, fbase);
           }
           T acc[IV];
 #pragma unroll
@@ -896,8 +900,11 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             if (nw0 >= len) {
               nws = ws + kPcgWarps;
               nw0 = 0;
-              if (nws < ws1)
-                row_at(nws, nr, nlen, nbase);
+              nr = fr;
+              nlen = flen;
+              nbase = fbase;
+              if (nws + kPcgWarps < ws1)
+                row_at(nws + kPcgWarps, fr, flen, fbase);
             }
             if (nws < ws1)
               issue(stage ^ 1, nbase, nw0, nlen);

@@ -126,8 +126,9 @@ private:
   }
   // The Newton linear solve of the active items: FP64 PCG, or FP32 PCG inside FP64 defect
   // correction.  linfo[3 * item] = status, iterations, residual; solution in x_.
-  // final_tolerance: `tolerance` is the options' exact inner tolerance (the Newton steps
-  // that can converge), where the PCG from the iterate solves tighter.
+  // final_tolerance: `tolerance` is the options' exact inner tolerance in the relaxed Newton
+  // regime (steps that can converge after the first five), where the PCG from the iterate
+  // solves tighter.
   Status LinearSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
                      cudaStream_t stream, double *linfo, bool final_tolerance = true);
   Status MixedSolve(int kp, int items, uint32_t mask, double tolerance, int max_iterations,
