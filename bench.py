@@ -533,10 +533,9 @@ def sector_form(samples, check=8, fast_samples=256):
     """Shared geometry at scale: the rotor-stator sector (about 40k nodes, anti-periodic
     90-degree edges), `samples` samples with per-sample currents U[-15, 15] A and magnet
     Hc U[8.5e5, 9.5e5] A/m, solved by the plain FP64 Jacobi method through one
-    fg_solve_batch call (the library's default: here chunk after chunk, as the L2 rule
-    decides for this mesh).  On the first `fast_samples` samples: chunk after chunk, all
-    chunks forced to advance together (one multi-group PCG launch per Newton step, CUDA-graph
-    replays), and the fast forms (block-Jacobi 8 and the PCG from the Newton iterate, in
+    fg_solve_batch call (chunks of 32 one after another, the library's default).  On the
+    first `fast_samples` samples: chunk after chunk, all chunks advancing together (one
+    multi-group PCG launch per Newton step, CUDA-graph replays), and the fast forms (block-Jacobi 8 and the PCG from the Newton iterate, in
     FP64 and with the FP32 inner solve).  Host-buffer API timing.  The first `check` samples
     are compared with the FP64 oracle solving each sample's own model."""
     import femm_gpu_b200 as fg
@@ -559,11 +558,11 @@ def sector_form(samples, check=8, fast_samples=256):
     saved = os.environ.get("FG_CHUNKS_TOGETHER")
     try:
         fast = dict(preconditioner=1, block_size=8, from_iterate=True)
-        for name, kw, together, ks in (("fp64_jacobi", {}, "1", samples),
+        for name, kw, together, ks in (("fp64_jacobi", {}, "0", samples),
                                        ("fp64_jacobi_chunk_by_chunk_subset", {}, "0", fast_samples),
-                                       ("fp64_jacobi_chunks_together_forced_subset", {}, "2", fast_samples),
-                                       ("fp64_block8_from_iterate_subset", fast, "1", fast_samples),
-                                       ("mixed_block8_from_iterate_subset", dict(precision=1, **fast), "1",
+                                       ("fp64_jacobi_chunks_together_subset", {}, "2", fast_samples),
+                                       ("fp64_block8_from_iterate_subset", fast, "0", fast_samples),
+                                       ("mixed_block8_from_iterate_subset", dict(precision=1, **fast), "0",
                                         fast_samples)):
             os.environ["FG_CHUNKS_TOGETHER"] = together
             p = fg.Plan(sector, **kw)
@@ -586,7 +585,7 @@ def sector_form(samples, check=8, fast_samples=256):
         else:
             os.environ["FG_CHUNKS_TOGETHER"] = saved
     sub = out["fp64_jacobi_chunk_by_chunk_subset"]["solves_per_s_e2e"]
-    for name in ("fp64_jacobi_chunks_together_forced_subset", "fp64_block8_from_iterate_subset",
+    for name in ("fp64_jacobi_chunks_together_subset", "fp64_block8_from_iterate_subset",
                  "mixed_block8_from_iterate_subset"):
         out[name]["vs_chunk_by_chunk"] = out[name]["solves_per_s_e2e"] / sub
     return out

@@ -487,6 +487,20 @@ int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing)
   return 0;
 }
 
+int fg_plan_pcg_shapes(const fg_plan *plan, int32_t capacity, fg_pcg_shape *shapes)
+{
+  if (!plan || capacity < 0 || (capacity > 0 && !shapes))
+    return 0;
+  const auto &all = plan->plan.pcg_shapes();
+  int32_t n = 0;
+  for (const auto &entry : all) {
+    if (n < capacity)
+      shapes[n] = entry.second;
+    ++n;
+  }
+  return n;
+}
+
 int fg_bh_build(int32_t count, double *b, double *h, double *slope, double *cold_secant,
                 int32_t *smoothing_passes)
 {

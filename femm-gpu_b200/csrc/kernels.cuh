@@ -89,6 +89,10 @@ struct PcgArgs {
   // Value ring: the SpMV's operator values staged into shared memory by cp.async one chunk
   // ahead of their use (set by LaunchPcg for 16-byte item vectors).
   int32_t value_ring, value_ring_offset;
+  // Launch-shape requests of a plan's autotuner for the value ring and the column-index
+  // cache: 0 the default (environment), 1 on where the shape and shared memory allow it,
+  // 2 off.  Neither changes any arithmetic, so results do not depend on the choice.
+  int32_t ring_request, col_cache_request;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
   // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
   // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.

@@ -146,7 +146,8 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   // x 16 bytes per warp, after the block-Jacobi staging buffer.
   args.value_ring = 0;
   args.value_ring_offset = 0;
-  const bool ring_shape = (args.precision == 0 ? 8 : 4) * iv == 16 && args.value_item && ValueRingEnabled();
+  const bool want_ring = args.ring_request == 0 ? ValueRingEnabled() : args.ring_request == 1;
+  const bool ring_shape = (args.precision == 0 ? 8 : 4) * iv == 16 && args.value_item && want_ring;
   if (ring_shape) {
     const size_t offset = (smem + 15) / 16 * 16;
     const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 16;
@@ -160,7 +161,8 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   // shared memory that still leaves the grid co-resident.
   args.col_cache = 0;
   args.col_cache_offset = 0;
-  if (args.host_slice_off && ColumnCacheEnabled()) {
+  const bool want_cache = args.col_cache_request == 0 ? ColumnCacheEnabled() : args.col_cache_request == 1;
+  if (args.host_slice_off && want_cache) {
     size_t most = 0;
     for (int g = 0; g < grid; ++g) {
       const long long w0 = static_cast<long long>(warp_slices) * g / grid;

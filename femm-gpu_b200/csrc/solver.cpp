@@ -61,13 +61,14 @@ constexpr int kMaxLanes = 32;
 constexpr double kIterateFinalTightening = 0.1;
 constexpr double kIterateFinalFloor = 1e-12;
 
-// FG_CHUNKS_TOGETHER in the environment (read at every solve): 0 solves wide batches chunk
-// after chunk, 2 advances the chunks together whatever their footprint (A/B timing); unset
-// or 1 applies the L2 rule of Plan::SolveDevice.
+// FG_CHUNKS_TOGETHER in the environment (read at every solve): unset or 0 solves wide
+// batches chunk after chunk (the default: measured faster on the B200 from 1.5k to 40k
+// rows); 1 advances the chunks together where the L2 rule of Plan::SolveDevice allows, 2
+// whatever their footprint.
 int ChunksTogetherMode()
 {
   const char *v = std::getenv("FG_CHUNKS_TOGETHER");
-  return v && v[0] == '0' ? 0 : (v && v[0] == '2' ? 2 : 1);
+  return v && v[0] == '1' ? 1 : (v && v[0] == '2' ? 2 : 0);
 }
 
 // Bytes of the vectors one chunk of kMaxItems items keeps in use per CG iteration (x, r,
@@ -364,7 +365,7 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.timeout_ns = PcgWaitLimitNs();
   a.trace = trace_enabled_ ? trace_.get() : nullptr;
   int grid = 0, block = 0;
-  const cudaError_t e = LaunchPcg(a, &grid, &block, stream);
+  const cudaError_t e = LaunchShaped(a, &grid, &block, stream);
   if (e != cudaSuccess) {
     cudaGetLastError();
     return Status::kInternalError;
@@ -374,6 +375,81 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   timing_.pcg_launches += 1;
   timing_.kernel_launches += 1;
   return Status::kOk;
+}
+
+namespace
+{
+// CG iterations of each timed candidate shape (one short launch per candidate).
+constexpr int kTuneIterations = 48;
+
+bool TuningEnabled()
+{
+  const char *v = std::getenv("FG_PCG_TUNE");
+  return !(v && v[0] == '0');
+}
+} // namespace
+
+cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t stream)
+{
+  const int key = a.kp * 1000 + a.precision * 100 + (a.blocks ? a.block_size : 0);
+  auto it = shapes_.find(key);
+  if (it == shapes_.end() && TuningEnabled()) {
+    fg_pcg_shape sh{};
+    sh.items = a.kp;
+    sh.precision = a.precision;
+    sh.block_size = a.blocks ? a.block_size : 0;
+    // Candidates: ring on / off (only 16-byte item vectors of per-item operators can use
+    // it) x column cache off / on.  Each runs kTuneIterations CG iterations of this very
+    // system (tolerance 0: no item stops early); the real launch follows and overwrites
+    // every vector the timing runs wrote.
+    const int iv = a.precision == 0 ? (a.kp >= 2 ? 2 : 1) : (a.kp >= 4 ? 4 : (a.kp >= 2 ? 2 : 1));
+    const bool ring_possible = (a.precision == 0 ? 8 : 4) * iv == 16 && a.value_item;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+      cudaGetLastError();
+      if (e0)
+        cudaEventDestroy(e0);
+      return cudaErrorUnknown;
+    }
+    double best = 0.0;
+    for (int c = 0; c < 4; ++c) {
+      const int ring = c % 2 == 0 ? 1 : 2, cache = c < 2 ? 2 : 1;
+      if (ring == 1 && !ring_possible)
+        continue;
+      PcgArgs t = a;
+      t.ring_request = ring;
+      t.col_cache_request = cache;
+      t.tolerance = 0.0;
+      t.item_tolerance = nullptr;
+      t.max_iterations = kTuneIterations;
+      t.trace = nullptr;
+      float ms = 0.0f;
+      if (cudaEventRecord(e0, stream) != cudaSuccess || LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess ||
+          cudaEventRecord(e1, stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        cudaGetLastError();
+        continue;
+      }
+      timing_.kernel_launches += 1;
+      const double us = 1e3 * ms / kTuneIterations;
+      sh.us_per_iteration[c] = us;
+      ++sh.candidates;
+      if (best == 0.0 || us < best) {
+        best = us;
+        sh.value_ring = ring == 1 ? 1 : 0;
+        sh.column_cache = cache == 1 ? 1 : 0;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (sh.candidates > 0)
+      it = shapes_.emplace(key, sh).first;
+  }
+  if (it != shapes_.end()) {
+    a.ring_request = it->second.value_ring ? 1 : 2;
+    a.col_cache_request = it->second.column_cache ? 1 : 2;
+  }
+  return LaunchPcg(a, grid, block, stream);
 }
 
 Status Plan::BuildBlocks(int kp, int items, bool per_item, bool single, cudaStream_t stream)
@@ -540,7 +616,7 @@ Status Plan::MixedSolve(int kp, int items, uint32_t mask, double tolerance, int 
   a.timeout_ns = PcgWaitLimitNs();
   a.trace = trace_enabled_ ? trace_.get() : nullptr;
   int grid = 0, block = 0;
-  if (LaunchPcg(a, &grid, &block, st) != cudaSuccess) {
+  if (LaunchShaped(a, &grid, &block, st) != cudaSuccess) {
     cudaGetLastError();
     return Status::kInternalError;
   }

@@ -8,6 +8,7 @@
 #include "kernels.cuh"
 #include "model.h"
 
+#include <map>
 #include <memory>
 #include <vector>
 
@@ -58,6 +59,7 @@ public:
                       const fg_solve_options &options, double *da, double *db1, double *db2,
                       double *dflux, fg_linear_info *info);
 
+  const std::map<int, fg_pcg_shape> &pcg_shapes() const { return shapes_; }
   const HostPlan &host() const { return host_; }
   const HostModel &model() const { return model_; }
   const fg_timing &timing() const { return timing_; }
@@ -76,6 +78,10 @@ private:
   Status EnsureLanes(int lanes);
   Status SolveChunksTogether(const SolveRequest &request, int first, int chunks);
   std::vector<std::unique_ptr<Plan>> lanes_; // lanes 1 .. n (lane 0 is this plan)
+  // The launch-shape autotuner (fg_plan_pcg_shapes): LaunchShaped launches a, after timing
+  // the candidate shapes of a's key once (a short run of the same system) when unseen.
+  cudaError_t LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t stream);
+  std::map<int, fg_pcg_shape> shapes_;
   std::unique_ptr<MultiSolver> lane_solver_;
   int lane_solver_lanes_ = 0;
 

@@ -46,7 +46,7 @@ EXPORTED = [
     "fg_postprocess_default_options", "fg_postprocess_create", "fg_postprocess_destroy",
     "fg_postprocess_probe_count", "fg_postprocess_mask", "fg_postprocess_compute",
     "fg_postprocess_compute_device", "fg_postprocess_frozen", "fg_postprocess_tangent",
-    "fg_solve_tangent", "fg_plan_attach_device", "fg_set_wait_limit_ns",
+    "fg_solve_tangent", "fg_plan_attach_device", "fg_set_wait_limit_ns", "fg_plan_pcg_shapes",
 ]
 
 
@@ -133,6 +133,12 @@ class FgTiming(C.Structure):
                 ("pcg_launches", C.c_int64), ("pcg_grid", C.c_int32), ("pcg_block", C.c_int32),
                 ("pcg_phase_ms", C.c_double * 10), ("mixed_fallbacks", C.c_int64),
                 ("block_inverses", C.c_int64), ("block_fallbacks", C.c_int64)]
+
+
+class FgPcgShape(C.Structure):
+    _fields_ = [("items", C.c_int32), ("precision", C.c_int32), ("block_size", C.c_int32),
+                ("value_ring", C.c_int32), ("column_cache", C.c_int32), ("candidates", C.c_int32),
+                ("us_per_iteration", C.c_double * 4)]
 
 
 _LIB = None
@@ -421,6 +427,16 @@ class Plan:
         t = FgTiming()
         lib().fg_plan_last_timing(self._h, C.byref(t))
         return t
+
+    def pcg_shapes(self):
+        """fg_plan_pcg_shapes: the launch shapes the plan's autotuner chose, as dicts."""
+        n = lib().fg_plan_pcg_shapes(self._h, 0, None)
+        arr = (FgPcgShape * max(n, 1))()
+        n = lib().fg_plan_pcg_shapes(self._h, n, arr)
+        return [{"items": a.items, "precision": a.precision, "block_size": a.block_size,
+                 "value_ring": bool(a.value_ring), "column_cache": bool(a.column_cache),
+                 "candidates": a.candidates, "us_per_iteration": list(a.us_per_iteration)}
+                for a in arr[:n]]
 
 
 def csr_pcg(row_offsets, columns, values, diagonal, rhs, tol=1e-13, maxit=64, shared=False):

@@ -329,6 +329,25 @@ int fg_plan_attach_device(fg_plan *plan);
 /* Timing and launch counters of the last solve on this plan. */
 int fg_plan_last_timing(const fg_plan *plan, fg_timing *timing);
 
+/* The plan's PCG launch shapes.  At the first PCG launch of each (items per launch,
+ * precision, block size) a plan times its candidate shapes -- the operator-value ring in
+ * shared memory on / off, the per-CTA column-index cache off / on -- on the system it is
+ * about to solve (a short run of the same kernel), and keeps the fastest for every later
+ * launch of that key.  Neither knob changes any arithmetic: results are the same bits
+ * whatever the choice.  No counterpart in the reference (its kernel shape is fixed,
+ * gpu_solver/src/solvers/options.cpp:43-53).  FG_PCG_TUNE=0 in the environment keeps the
+ * defaults.  Writes at most `capacity` entries; returns the number of tuned keys. */
+typedef struct fg_pcg_shape {
+  int32_t items;        /* items per launch (the padded batch width) */
+  int32_t precision;    /* FG_PRECISION_FP64 or FG_PRECISION_MIXED (the inner FP32 launch) */
+  int32_t block_size;   /* 0 Jacobi, 8 or 32 block-Jacobi */
+  int32_t value_ring;   /* 1 chosen on, 0 off */
+  int32_t column_cache; /* 1 chosen on, 0 off */
+  int32_t candidates;   /* shapes timed (those the kernel shape admits) */
+  double us_per_iteration[4]; /* per candidate: ring on / off x cache off / on; 0 if not timed */
+} fg_pcg_shape;
+int fg_plan_pcg_shapes(const fg_plan *plan, int32_t capacity, fg_pcg_shape *shapes);
+
 /* FEMM DC B-H spline and evaluation (nonlinear_model.cpp:13-148): host functions
  * exposed for parity checks.  b/h are smoothed in place; slope [count]. */
 int fg_bh_build(int32_t count, double *b, double *h, double *slope, double *cold_secant,

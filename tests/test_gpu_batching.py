@@ -95,9 +95,10 @@ def test_recovery_of_exhausted_items_matches_oracle(gpu, max_newton):
         assert rel(got.flux[i], flux[i]) <= 1e-8
 
 
-def test_wide_batch_chunks_solved_together(gpu):
+def test_wide_batch_chunks_solved_together(gpu, monkeypatch):
     """A shared-geometry batch wider than one launch (80 samples: chunks of 32, 32 and 16)
-    advances all its chunks together, one multi-group PCG launch per Newton step.  Each item
+    asked to advance its chunks together (FG_CHUNKS_TOGETHER=2; chunk after chunk is the
+    default) runs one multi-group PCG launch per Newton step.  Each item
     equals the same sample solved in a batch of at most 32 (same status and Newton
     iterations; A within 5e-9 and flux within 1e-8: the multi-group launch gives a chunk
     fewer CTAs, so its reductions round differently) and the oracle's solve (A 5e-9)."""
@@ -105,9 +106,11 @@ def test_wide_batch_chunks_solved_together(gpu):
     currents = meshes.seeded_currents(80, 3, 20.0, seed=22)
     hc = np.random.default_rng(23).uniform(0.9, 1.1, size=80)
     plan = fg.Plan(model)
+    monkeypatch.setenv("FG_CHUNKS_TOGETHER", "2")
     wide = plan.solve(currents, hc_scale=hc)
     t = plan.last_timing()
     assert t.pcg_launches == t.newton_iterations  # one launch per lock-step Newton step
+    monkeypatch.delenv("FG_CHUNKS_TOGETHER")
     for first in (0, 32, 64):
         part = plan.solve(currents[first:first + 32], hc_scale=hc[first:first + 32])
         for i in range(len(part.info)):

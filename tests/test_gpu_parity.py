@@ -220,10 +220,10 @@ def test_batch_widths_match_oracle(gpu, k):
 
 
 def test_batches_beyond_32_are_chunked(gpu, monkeypatch):
-    """A batch of 40: chunks of 32 and 8.  Solved chunk after chunk, its first 32 items
-    equal a batch of those 32 bit for bit; with the chunks advancing together (the
-    default), within 5e-9 (a chunk then runs on fewer CTAs and its reductions round
-    differently) with the same Newton iteration counts."""
+    """A batch of 40: chunks of 32 and 8.  Solved chunk after chunk (the default), its first
+    32 items equal a batch of those 32 bit for bit; with the chunks advancing together
+    (FG_CHUNKS_TOGETHER=2), within 5e-9 (a chunk then runs on fewer CTAs and its reductions
+    round differently) with the same Newton iteration counts."""
     model = meshes.square_nonlinear(m=10, seed=6)
     currents = meshes.seeded_currents(40, 3, 20.0, seed=2)
     plan = fg.Plan(model)
@@ -232,7 +232,7 @@ def test_batches_beyond_32_are_chunked(gpu, monkeypatch):
     r = plan.solve(currents)
     assert all(s == 0 for s in r.status)
     assert np.array_equal(first.a, r.a[:32])
-    monkeypatch.delenv("FG_CHUNKS_TOGETHER")
+    monkeypatch.setenv("FG_CHUNKS_TOGETHER", "2")
     together = plan.solve(currents)
     assert all(s == 0 for s in together.status)
     for i in range(40):
@@ -319,3 +319,24 @@ def test_fast_forms_on_the_saturated_sector_match_the_oracle(gpu, form):
         assert abs(got.info[k].iterations - info[k].iterations) <= 2
         assert rel(got.flux[k], flux[k]) <= 1e-8, rel(got.flux[k], flux[k])
         assert rel(got.a[k], a[k]) <= 5e-8, rel(got.a[k], a[k])
+
+
+def test_autotuned_launch_shapes_leave_results_bitwise_unchanged(gpu, monkeypatch):
+    """The plan's launch-shape autotuner (fg_plan_pcg_shapes) times the value ring and the
+    column cache on the system it is about to solve and keeps the fastest; neither knob
+    changes any arithmetic, so a tuned plan answers bit for bit as an untuned one, and the
+    timing runs leave no trace in the solve."""
+    model = meshes.square_nonlinear(m=60, seed=3)
+    currents = meshes.seeded_currents(8, 3, 20.0, seed=13)
+    tuned = fg.Plan(model)
+    r1 = tuned.solve(currents)
+    shapes = tuned.pcg_shapes()
+    assert len(shapes) == 1 and shapes[0]["items"] == 8 and shapes[0]["candidates"] == 4
+    assert all(t > 0 for t in shapes[0]["us_per_iteration"])
+    monkeypatch.setenv("FG_PCG_TUNE", "0")
+    plain = fg.Plan(model)
+    r2 = plain.solve(currents)
+    assert plain.pcg_shapes() == []
+    for f in ("a", "b1", "b2", "flux"):
+        assert np.array_equal(getattr(r1, f), getattr(r2, f))
+    assert [i.linear_iterations for i in r1.info] == [i.linear_iterations for i in r2.info]
