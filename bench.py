@@ -368,6 +368,7 @@ def run_ours(args, world, rank, local):
                      "peak_source": peak_kind, "pcg_ms": pcg_ms, "pcg_iterations": pcg_its,
                      "item_pcg_iterations": item_its},
         "newton_iterations": newton,
+        "pcg_shapes_autotuned": plan.pcg_shapes(),
         "statuses_ok": sum(1 for s in statuses if s == 0), "statuses_total": len(statuses),
         "clocks": clocks.summary(),
     }
