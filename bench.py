@@ -65,8 +65,14 @@ def parse():
     p.add_argument("--all-forms", action="store_true",
                    help="also the postprocess / tangent, streaming-worker and sliding-band forms")
     p.add_argument("--only-form", choices=["postprocess_tangent_sector", "streaming_worker", "sliding_band",
-                                           "planar_2m", "reference_gpu", "learned", "sector", "hetero"],
+                                           "planar_2m", "reference_gpu", "learned", "sector", "hetero",
+                                           "pcg_launch"],
                    help="run one form alone and print its JSON (profiling)")
+    p.add_argument("--probe-mesh", type=int, default=MESH_M, help="pcg_launch: planar square size m")
+    p.add_argument("--probe-items", type=int, default=8, help="pcg_launch: samples per launch")
+    p.add_argument("--probe-iterations", type=int, default=300, help="pcg_launch: CG iterations per launch")
+    p.add_argument("--probe-launches", type=int, default=3, help="pcg_launch: launches timed")
+    p.add_argument("--probe-one-reduction", action="store_true", help="pcg_launch: the one-reduction form")
     return p.parse_args()
 
 
@@ -785,6 +791,46 @@ def pcg_bytes_per_item_iteration(n, nnz, precision, block):
     return w * nnz + 13 * w * n + (w * block * n if block else 0)
 
 
+def pcg_launch_form(dev, stream, m, k, iterations, launches, one_reduction):
+    """PCG launches of a fixed length, for profiling one launch: the planar square of size m,
+    k samples, one Newton iteration whose inner PCG is capped at `iterations` CG iterations
+    (tolerance 1e-30, so every launch runs exactly that many), repeated `launches` times on one
+    plan.  The launch-shape autotuner is off (FG_PCG_TUNE=0: the default value ring, no
+    column cache), so the PCG launches are exactly these.  Reports the CUDA-event time per CG
+    iteration of each launch and the algorithmic bytes per CG iteration."""
+    import torch
+
+    import femm_gpu_b200 as fg
+    from femm_gpu_b200 import meshes
+
+    os.environ["FG_PCG_TUNE"] = "0"
+    model = meshes.square_nonlinear(m=m, seed=2)
+    plan = fg.Plan(model, one_reduction=one_reduction)
+    peak, source = peaks()
+    cur = torch.tensor(meshes.seeded_currents(k, 3, 20.0, seed=4242), device=dev)
+    out_a = torch.empty((k, plan.N), dtype=torch.float64, device=dev)
+    opts = fg.production_options(max_newton_iterations=1, max_linear_iterations=iterations,
+                                 linear_relative_tolerance=1e-30, adaptive_linear_tolerance=0,
+                                 recover_nonconvergence=0)
+    per_item = pcg_bytes_per_item_iteration(plan.rows, plan.nnz, 0, 0)
+    shared = 4.0 * plan.nnz + 4.0 * (plan.rows + 1)
+    runs = []
+    for _ in range(launches):
+        torch.cuda.synchronize()
+        plan.solve_device(k, cur.data_ptr(), options=opts, a_ptr=out_a.data_ptr(), stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        t = plan.last_timing()
+        us = 1e3 * t.pcg_ms / max(1, t.pcg_iterations)
+        runs.append({"cg_iterations": int(t.pcg_iterations), "pcg_ms": t.pcg_ms, "us_per_cg_iteration": us})
+    plan.close()
+    best = min(r["us_per_cg_iteration"] for r in runs)
+    algo = k * per_item + shared
+    return {"form": "pcg_launch", "mesh": m, "nodes": model.node_count, "rows": plan.rows, "nnz": plan.nnz,
+            "items": k, "one_reduction": one_reduction, "runs": runs,
+            "algorithmic_bytes_per_cg_iteration": algo, "pcg_gbs": algo / best / 1e3,
+            "pcg_frac": algo / best / 1e3 / peak, "peak_gbs": peak, "peak_source": source}
+
+
 def planar_2m_form(dev, stream, flush, samples=4):
     """The mixed-precision-at-scale workload: the jittered planar square at m = 1414
     (2,002,225 nodes, 3,998,792 triangles, 1,996,569 rows) with the config-2 physics.
@@ -1182,6 +1228,9 @@ def only_form(args):
         out = planar_2m_form(dev, stream, flush)
     elif args.only_form == "sliding_band":
         out = sliding_band_form()
+    elif args.only_form == "pcg_launch":
+        out = pcg_launch_form(dev, stream, args.probe_mesh, args.probe_items, args.probe_iterations,
+                              args.probe_launches, args.probe_one_reduction)
     else:
         rng = np.random.default_rng(77)
         cur = rng.uniform(-15.0, 15.0, size=(args.sector_samples, 3))

@@ -93,6 +93,10 @@ struct PcgArgs {
   // cache: 0 the default (environment), 1 on where the shape and shared memory allow it,
   // 2 off.  Neither changes any arithmetic, so results do not depend on the choice.
   int32_t ring_request, col_cache_request;
+  // One-reduction form (FP64 Jacobi only; pcg1r_kernel.cuh): t0 / t1 are two more
+  // vectors of [n_pad][kp] doubles, and partials must hold 2 x 96 x grid doubles.
+  int32_t one_reduction;
+  void *t0, *t1;
   // Optional phase trace written by CTA 0 (nanoseconds, summed over the launch):
   // [2q] work before reduction q, [2q+1] wait at its grid barrier, [8] final partial
   // sums, [9] reductions.  q: 0 Phase A, 1 Phase B, 2 verification, 3 set-up.
@@ -144,6 +148,9 @@ int MultiPcgMaxGrid(int kp = 1);
 size_t MultiPcgRingBytes(int kp);
 // Whether a PCG kernel exists for this shape (block size 32 in FP64 stops at 16 items).
 bool PcgSupported(int kp, int precision, int block_size);
+// Doubles of the partials buffer a launch of up to `grid` CTAs needs (the one-reduction
+// form reduces three sums per item).
+size_t PcgPartialsDoubles(int grid, bool one_reduction);
 
 cudaError_t LaunchNewtonNorms(const DevicePlan &p, int kp, const double *x, const double *state,
                               double *partials, double *norms, cudaStream_t stream);

@@ -22,7 +22,7 @@ Status MultiSolver::Create(std::vector<Plan *> plans, int kp)
     return Status::kInvalidArgument;
   for (Plan *p : plans)
     if (!p || p->host_only_ || p->options_.precision != FG_PRECISION_FP64 || p->block_size() != 0 ||
-        p->from_iterate_)
+        p->from_iterate_ || p->one_reduction_)
       return p && p->host_only_ ? Status::kGpuUnavailable : Status::kUnsupportedFeature;
   for (size_t i = 0; i < plans.size(); ++i)
     for (size_t j = 0; j < i; ++j)

@@ -13,6 +13,7 @@ const void *PcgKernelF32(int kp);
 const void *PcgKernelF64Block(int kp, int bs);
 const void *PcgKernelF32Block(int kp, int bs);
 const void *MultiPcgKernelF64(int kp);
+const void *PcgKernelF64OneReduction(int kp);
 
 namespace
 {
@@ -20,8 +21,10 @@ namespace
 constexpr int kPcgThreads = 512;
 constexpr int kPcgWarps = kPcgThreads / 32;
 
-const void *SelectKernel(int kp, int precision, int bs)
+const void *SelectKernel(int kp, int precision, int bs, bool one_reduction = false)
 {
+  if (one_reduction)
+    return precision == 0 && bs == 0 ? PcgKernelF64OneReduction(kp) : nullptr;
   if (bs == 0)
     return precision == 0 ? PcgKernelF64(kp) : PcgKernelF32(kp);
   return precision == 0 ? PcgKernelF64Block(kp, bs) : PcgKernelF32Block(kp, bs);
@@ -120,11 +123,18 @@ int PcgMaxGrid(int kp)
   return grid;
 }
 
+size_t PcgPartialsDoubles(int grid, bool one_reduction)
+{
+  return static_cast<size_t>(2) * (one_reduction ? 96 : 64) * static_cast<size_t>(grid);
+}
+
 cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t stream)
 {
   const int bs = args.blocks ? args.block_size : 0;
   args.block_size = bs;
-  const void *kernel = SelectKernel(args.kp, args.precision, bs);
+  const void *kernel = SelectKernel(args.kp, args.precision, bs, args.one_reduction != 0);
+  if (args.one_reduction && (!args.t0 || !args.t1))
+    return cudaErrorInvalidValue;
   if (!kernel)
     return cudaErrorInvalidValue;
   size_t smem = StagingBytes(args.kp, args.precision, bs);

@@ -57,11 +57,15 @@ struct Control {
   double rmax[kMaxItems]; // reliable updates: largest residual since the last replacement
 };
 
-struct Reduce {
-  double warp[kPcgWarps][kMaxQ];
-  double result[kMaxQ];
+// Shared-memory staging of a grid reduction of up to QM quantities (quantities x items);
+// the partials buffer holds 2 x QM x grid doubles.
+template <int QM> struct ReduceQ {
+  static constexpr int kQ = QM;
+  double warp[kPcgWarps][QM];
+  double result[QM];
   int err;
 };
+using Reduce = ReduceQ<kMaxQ>;
 
 // Phase trace of CTA 0 (PcgArgs::trace): thread 0 accumulates wall-clock intervals.
 struct Trace {
@@ -241,7 +245,7 @@ __device__ __forceinline__ void TraceMark(const PcgArgs &a, const GridShape &gs,
 }
 
 // Grid-wide barrier over a monotonically increasing arrival counter, bounded in time.
-__device__ bool GridBarrier(const PcgArgs &a, const GridShape &gs, unsigned &epoch, Reduce &sm)
+template <class R> __device__ bool GridBarrier(const PcgArgs &a, const GridShape &gs, unsigned &epoch, R &sm)
 {
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -274,10 +278,11 @@ __device__ bool GridBarrier(const PcgArgs &a, const GridShape &gs, unsigned &epo
 
 // Sum (or max) of Q per-item quantities over the whole grid, deterministic for a
 // fixed launch shape.  v[q][j] is this thread's partial for its item item0 + j.
-template <int KP, int IV, int Q, bool kMax>
-__device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q][IV], Reduce &sm, unsigned &epoch,
+template <int KP, int IV, int Q, bool kMax, class R>
+__device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q][IV], R &sm, unsigned &epoch,
                            int &buf, Trace &tr, int phase)
 {
+  static_assert(Q * KP <= R::kQ, "reduction staging too small");
   constexpr int LR = KP / IV; // lanes per row
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -296,7 +301,7 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
   __syncthreads();
   constexpr int QK = Q * KP;
   const int G = gs.size;
-  double *part = a.partials + static_cast<size_t>(buf) * kMaxQ * G;
+  double *part = a.partials + static_cast<size_t>(buf) * R::kQ * G;
   if (threadIdx.x < QK) {
     double s = sm.warp[0][threadIdx.x];
     for (int w = 1; w < kPcgWarps; ++w)

@@ -98,7 +98,7 @@ size_t Plan::DeviceBytes() const
        circuit_rhs_.bytes() + elem_geo_.bytes() + boundary_.bytes();
   b += state_.bytes() + ev_.bytes() + er_.bytes() + values_.bytes() + diag_.bytes() +
        invd_.bytes() + rhs_.bytes() + x_.bytes() + r_.bytes() + z_.bytes() + p0_.bytes() +
-       p1_.bytes() + q_.bytes() + pcg_partials_.bytes() + staging_.bytes();
+       p1_.bytes() + q_.bytes() + t0_.bytes() + t1_.bytes() + pcg_partials_.bytes() + staging_.bytes();
   b += in_currents_.bytes() + in_hc_.bytes() + in_warm_.bytes() + out_a_.bytes() + out_b1_.bytes() +
        out_b2_.bytes() + out_flux_.bytes();
   return b;
@@ -123,6 +123,9 @@ Status Plan::Create(HostModel model, const fg_plan_options &options)
     return Status::kUnsupportedFeature;
   host_only_ = (options_.flags & FG_PLAN_HOST_ONLY) != 0;
   from_iterate_ = (options_.flags & FG_PLAN_PCG_FROM_ITERATE) != 0;
+  one_reduction_ = (options_.flags & FG_PLAN_PCG_ONE_REDUCTION) != 0;
+  if (one_reduction_ && (options_.precision != FG_PRECISION_FP64 || block_size() != 0))
+    return Status::kUnsupportedFeature;
   if (host_only_)
     return Status::kOk;
   return DeviceInit();
@@ -282,7 +285,11 @@ Status Plan::EnsureWorkspace(int kp)
   FG_EN(q_, vec);
   FG_EN(norm_partials_, static_cast<size_t>(2) * kp * 256);
   FG_EN(norms_, static_cast<size_t>(2) * kp);
-  FG_EN(pcg_partials_, static_cast<size_t>(2) * 64 * pcg_grid_cap_);
+  FG_EN(pcg_partials_, PcgPartialsDoubles(pcg_grid_cap_, one_reduction_));
+  if (one_reduction_) {
+    FG_EN(t0_, vec);
+    FG_EN(t1_, vec);
+  }
   FG_EN(pcg_info_, static_cast<size_t>(3) * kp);
   FG_EN(barrier_, 1);
   FG_EN(error_, 1);
@@ -355,6 +362,11 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
   a.p0 = p0_.get();
   a.p1 = p1_.get();
   a.q = q_.get();
+  if (one_reduction_ && !blocks) {
+    a.one_reduction = 1;
+    a.t0 = t0_.get();
+    a.t1 = t1_.get();
+  }
   a.partials = pcg_partials_.get();
   a.barrier = barrier_.get();
   a.error = error_.get();
@@ -379,8 +391,9 @@ Status Plan::RunPcg(int kp, int items, uint32_t mask, double tolerance, int max_
 
 namespace
 {
-// CG iterations of each timed candidate shape (one short launch per candidate).
-constexpr int kTuneIterations = 48;
+// CG iterations of each timed candidate launch, and rounds over the candidates.
+constexpr int kTuneIterations = 64;
+constexpr int kTuneRounds = 2;
 
 bool TuningEnabled()
 {
@@ -411,35 +424,47 @@ cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t st
         cudaEventDestroy(e0);
       return cudaErrorUnknown;
     }
-    double best = 0.0;
-    for (int c = 0; c < 4; ++c) {
-      const int ring = c % 2 == 0 ? 1 : 2, cache = c < 2 ? 2 : 1;
-      if (ring == 1 && !ring_possible)
-        continue;
-      PcgArgs t = a;
-      t.ring_request = ring;
-      t.col_cache_request = cache;
-      t.tolerance = 0.0;
-      t.item_tolerance = nullptr;
-      t.max_iterations = kTuneIterations;
-      t.trace = nullptr;
-      float ms = 0.0f;
-      if (cudaEventRecord(e0, stream) != cudaSuccess || LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess ||
-          cudaEventRecord(e1, stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-        cudaGetLastError();
-        continue;
-      }
+    // One untimed launch first (cold caches and clocks would favour whichever candidate
+    // runs later), then kTuneRounds interleaved rounds; each candidate keeps its fastest.
+    PcgArgs t = a;
+    t.tolerance = 0.0;
+    t.item_tolerance = nullptr;
+    t.max_iterations = kTuneIterations;
+    t.trace = nullptr;
+    if (LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess)
+      cudaGetLastError();
+    else
       timing_.kernel_launches += 1;
-      const double us = 1e3 * ms / kTuneIterations;
-      sh.us_per_iteration[c] = us;
-      ++sh.candidates;
-      if (best == 0.0 || us < best) {
-        best = us;
-        sh.value_ring = ring == 1 ? 1 : 0;
-        sh.column_cache = cache == 1 ? 1 : 0;
+    for (int round = 0; round < kTuneRounds; ++round)
+      for (int c = 0; c < 4; ++c) {
+        const int ring = c % 2 == 0 ? 1 : 2, cache = c < 2 ? 2 : 1;
+        if (ring == 1 && !ring_possible)
+          continue;
+        t.ring_request = ring;
+        t.col_cache_request = cache;
+        float ms = 0.0f;
+        if (cudaEventRecord(e0, stream) != cudaSuccess || LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess ||
+            cudaEventRecord(e1, stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+            cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+          cudaGetLastError();
+          continue;
+        }
+        timing_.kernel_launches += 1;
+        const double us = 1e3 * ms / kTuneIterations;
+        if (sh.us_per_iteration[c] == 0.0) {
+          ++sh.candidates;
+          sh.us_per_iteration[c] = us;
+        } else if (us < sh.us_per_iteration[c]) {
+          sh.us_per_iteration[c] = us;
+        }
       }
-    }
+    double best = 0.0;
+    for (int c = 0; c < 4; ++c)
+      if (sh.us_per_iteration[c] > 0.0 && (best == 0.0 || sh.us_per_iteration[c] < best)) {
+        best = sh.us_per_iteration[c];
+        sh.value_ring = c % 2 == 0 ? 1 : 0;
+        sh.column_cache = c < 2 ? 0 : 1;
+      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (sh.candidates > 0)
@@ -743,7 +768,8 @@ Status Plan::SolveDevice(const SolveRequest &req)
 bool Plan::ChunksTogether(const SolveRequest &req) const
 {
   return ChunksTogetherMode() != 0 && req.items > chunk_cap_ && chunk_cap_ == kMaxItems &&
-         options_.precision == FG_PRECISION_FP64 && block_size() == 0 && !from_iterate_ && !req.guard_warm &&
+         options_.precision == FG_PRECISION_FP64 && block_size() == 0 && !from_iterate_ && !one_reduction_ &&
+         !req.guard_warm &&
          !trace_enabled_ && MultiPcgMaxGrid(kMaxItems) > 0;
 }
 
@@ -953,7 +979,7 @@ Status Plan::ChunkAssemble(Chunk *c)
 
 bool Plan::ChunkPcgArgs(const Chunk &c, unsigned *barrier, int32_t *error, PcgArgs *out)
 {
-  if (options_.precision != FG_PRECISION_FP64 || block_size() != 0 || from_iterate_)
+  if (options_.precision != FG_PRECISION_FP64 || block_size() != 0 || from_iterate_ || one_reduction_)
     return false;
   PcgArgs a{};
   a.n = host_.n;

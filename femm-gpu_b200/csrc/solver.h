@@ -148,6 +148,7 @@ private:
   int kp_cap_ = 0;
   bool host_only_ = false;
   bool from_iterate_ = false; // FG_PLAN_PCG_FROM_ITERATE
+  bool one_reduction_ = false; // FG_PLAN_PCG_ONE_REDUCTION
   int pcg_grid_cap_ = 0;
   int chunk_cap_ = kMaxItems; // items per batched launch
 
@@ -161,6 +162,7 @@ private:
       curve_b_, curve_h_, curve_slope_, boundary_;
   // Batch workspace.
   DeviceArray<double> state_, ev_, er_, values_, diag_, invd_, rhs_, x_, r_, z_, p0_, p1_, q_;
+  DeviceArray<double> t0_, t1_; // the one-reduction form's extra vectors
   DeviceArray<double> norm_partials_, norms_, pcg_partials_, pcg_info_, staging_;
   // Mixed-precision form: FP32 operator, preconditioner and inner-solve vectors.
   DeviceArray<float> v32_, d32_, i32_, x32_, r32_, z32_, p032_, p132_, q32_;

@@ -32,6 +32,7 @@ STATUS_NAMES = [
 
 PLAN_HOST_ONLY = 1
 PLAN_PCG_FROM_ITERATE = 2
+PLAN_PCG_ONE_REDUCTION = 4
 
 EXPORTED = [
     "fg_production_options", "fg_status_name", "fg_abi_version", "fg_plan_create",
@@ -214,7 +215,8 @@ class Plan:
     """A device-resident model: fg_plan_create ... fg_plan_destroy."""
 
     def __init__(self, model: Model, preconditioner: int = 0, block_size: int = 8,
-                 precision: int = 0, host_only: bool = False, from_iterate: bool = False):
+                 precision: int = 0, host_only: bool = False, from_iterate: bool = False,
+                 one_reduction: bool = False):
         self.model = model
         L = lib()
         self._keep = []
@@ -243,7 +245,8 @@ class Plan:
         if ages is not None:
             self._keep.append(ages)
             fm.air_gap_count, fm.air_gap_elements = len(model.ages), C.cast(ages, C.c_void_p)
-        flags = (PLAN_HOST_ONLY if host_only else 0) | (PLAN_PCG_FROM_ITERATE if from_iterate else 0)
+        flags = ((PLAN_HOST_ONLY if host_only else 0) | (PLAN_PCG_FROM_ITERATE if from_iterate else 0) |
+                 (PLAN_PCG_ONE_REDUCTION if one_reduction else 0))
         opts = FgPlanOptions(preconditioner, block_size, precision, flags)
         self._h = C.c_void_p()
         status = L.fg_plan_create(C.byref(fm), C.byref(opts), C.byref(self._h))

@@ -130,7 +130,15 @@ typedef struct fg_plan_options {
  * Newton iterate, J delta = rhs - J x0, to ||rhs - J (x0 + delta)|| <= tol ||rhs|| -- the
  * same acceptance rule from a better starting point, so a good iterate or warm start
  * costs fewer PCG iterations. */
-enum { FG_PLAN_HOST_ONLY = 1, FG_PLAN_PCG_FROM_ITERATE = 2 };
+/* FG_PLAN_PCG_ONE_REDUCTION (no counterpart in the reference; FP64 Jacobi plans only):
+ * the inner PCG runs Chronopoulos and Gear's one-reduction rearrangement of CG -- one
+ * grid-wide synchronisation per iteration instead of two, at the price of three gathered
+ * vectors per SpMV entry instead of two and two more workspace vectors.  It pays where a
+ * CG iteration is short (meshes of tens of thousands of rows).  Acceptance is unchanged
+ * (the true-residual check); results agree with the default form within the solve's
+ * tolerance, not bit for bit.  With block-Jacobi or mixed precision fg_plan_create
+ * returns FG_UNSUPPORTED_FEATURE. */
+enum { FG_PLAN_HOST_ONLY = 1, FG_PLAN_PCG_FROM_ITERATE = 2, FG_PLAN_PCG_ONE_REDUCTION = 4 };
 
 /* NonlinearOptions (gpu_solver/src/physics/nonlinear_model.h:102-109). */
 typedef struct fg_solve_options {
@@ -363,7 +371,8 @@ void fg_bh_eval(int32_t count, const double *b, const double *h, const double *s
  * per-plan convergence; from the second iteration the assembly + PCG + norm sequence is a
  * replayed CUDA graph.  An online tuner divides the CTAs by predicted cost (rows x
  * iterations, from each plan's previous Newton step).  Plans must use the FP64 Jacobi
- * form; they are borrowed and must outlive the fg_multi.
+ * form without FG_PLAN_PCG_FROM_ITERATE or FG_PLAN_PCG_ONE_REDUCTION (FG_UNSUPPORTED_FEATURE
+ * otherwise); they are borrowed and must outlive the fg_multi.
  * ------------------------------------------------------------------------------------ */
 typedef struct fg_multi fg_multi;
 

@@ -202,3 +202,14 @@ def test_preconditioner_options_are_validated():
         with pytest.raises(fg.FgError) as e:
             fg.Plan(model, preconditioner=pre, block_size=bs, host_only=True)
         assert e.value.status == fg.capi.UNSUPPORTED_FEATURE
+
+
+def test_one_reduction_form_is_fp64_jacobi_only():
+    """FG_PLAN_PCG_ONE_REDUCTION exists for the FP64 Jacobi method alone."""
+    model = meshes.square_linear(m=6)
+    fg.Plan(model, one_reduction=True, host_only=True)
+    fg.Plan(model, one_reduction=True, from_iterate=True, host_only=True)
+    for form in (dict(precision=1), dict(preconditioner=1, block_size=8)):
+        with pytest.raises(fg.FgError) as e:
+            fg.Plan(model, one_reduction=True, host_only=True, **form)
+        assert e.value.status == fg.capi.UNSUPPORTED_FEATURE
