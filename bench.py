@@ -887,6 +887,12 @@ def planar_2m_form(dev, stream, flush, samples=4):
              "pcg_ms_per_cg_iteration": t.pcg_ms / max(1, t.pcg_iterations),
              "pcg_gbs": gbs, "pcg_frac": gbs / peak,
              "mixed_fallbacks": int(t.mixed_fallbacks), "all_converged": all(i.status == 0 for i in info)}
+        if name == "fp64_jacobi_k1":
+            per_it, src = traffic_per_cg_iteration("square1414_items1")
+            if per_it:
+                r["dram_traffic_per_cg_iteration"] = per_it
+                r["algorithmic_bytes_per_cg_iteration"] = per_item + shared
+                r["traffic_source"] = src
         if name == "fp64_jacobi_k4":
             ref = (a, b1, b2, f)
         elif ref is not None:

@@ -255,11 +255,14 @@ template <class R> __device__ bool GridBarrier(const PcgArgs &a, const GridShape
     AddRelease(a.barrier, 1u);
     const unsigned long long t0 = GlobalTimer();
     int err = 0;
-    for (;;) {
+    for (unsigned spin = 0;; ++spin) {
       const unsigned v = LoadAcquire(a.barrier);
       if (static_cast<int>(v - target) >= 0)
         break;
-      if (*reinterpret_cast<volatile int32_t *>(a.error) != 0) {
+      // Another CTA's failure ends the wait early.  Checked on every 16th poll only: the
+      // flag's load cannot start before the acquire load has returned, so checking it on
+      // every poll would double the time between polls.
+      if ((spin & 15u) == 15u && *reinterpret_cast<volatile int32_t *>(a.error) != 0) {
         err = 1;
         break;
       }
@@ -312,32 +315,45 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
   if (!GridBarrier(a, gs, epoch, sm))
     return false;
   TraceMark(a, gs, tr, 2 * phase + 1);
-  for (int t = warp; t < QK; t += kPcgWarps) {
-    // Lane-strided partials in CTA order; eight loads issued before their adds (the add
-    // order, and so the result, is that of the one-at-a-time loop).
-    const double *pt = part + static_cast<size_t>(t) * G;
-    double s = 0.0;
-    int g = lane;
-    for (; g + 32 * 7 < G; g += 32 * 8) {
-      double y[8];
+  // Lane-strided partials in CTA order.  All of a lane's partials (ten for grids of up to
+  // 320 CTAs) -- of two quantities at a time where a warp sums several -- are loaded before
+  // their adds, so each pass costs one L2 round trip.  The add order, and so the result, is
+  // that of the one-at-a-time loop.
+  constexpr int kPer = QK > kPcgWarps ? 2 : 1;
+  for (int t = warp; t < QK; t += kPer * kPcgWarps) {
+    double s[kPer];
+    bool has[kPer];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        y[u] = __ldcg(pt + g + 32 * u);
+    for (int j = 0; j < kPer; ++j) {
+      s[j] = 0.0;
+      has[j] = t + j * kPcgWarps < QK;
+    }
+    for (int g = lane; g < G; g += 32 * 10) {
+      double y[kPer][10];
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        s = kMax ? fmax(s, y[u]) : s + y[u];
-    }
-    for (; g < G; g += 32) {
-      const double y = __ldcg(pt + g);
-      s = kMax ? fmax(s, y) : s + y;
+      for (int j = 0; j < kPer; ++j)
+#pragma unroll
+        for (int u = 0; u < 10; ++u)
+          y[j][u] = has[j] && g + 32 * u < G
+                        ? __ldcg(part + static_cast<size_t>(t + j * kPcgWarps) * G + g + 32 * u)
+                        : 0.0;
+#pragma unroll
+      for (int j = 0; j < kPer; ++j)
+#pragma unroll
+        for (int u = 0; u < 10; ++u)
+          if (has[j] && g + 32 * u < G)
+            s[j] = kMax ? fmax(s[j], y[j][u]) : s[j] + y[j][u];
     }
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) {
-      const double y = __shfl_xor_sync(0xffffffffu, s, off);
-      s = kMax ? fmax(s, y) : s + y;
+    for (int j = 0; j < kPer; ++j) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double y = __shfl_xor_sync(0xffffffffu, s[j], off);
+        s[j] = kMax ? fmax(s[j], y) : s[j] + y;
+      }
+      if (lane == 0 && has[j])
+        sm.result[t + j * kPcgWarps] = s[j];
     }
-    if (lane == 0)
-      sm.result[t] = s;
   }
   __syncthreads();
   TraceMark(a, gs, tr, 8);
