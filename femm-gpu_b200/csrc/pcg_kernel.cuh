@@ -381,6 +381,13 @@ __device__ __forceinline__ void CpAsync16(void *smem, const void *gmem, unsigned
   asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(g), "l"(pol)
                : "memory");
 }
+// 4-byte asynchronous copy (cp.async.ca: the .cg form copies 16 bytes only).
+__device__ __forceinline__ void CpAsync4(void *smem, const void *gmem)
+{
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  const size_t g = __cvta_generic_to_global(gmem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
+}
 __device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void CpAsyncWait()
 {
@@ -886,14 +893,22 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           constexpr int U = 4;
           T *ring = reinterpret_cast<T *>(fg_dynamic_smem + a.value_ring_offset) +
                     static_cast<size_t>(warp) * 2 * U * 32 * IV;
+          // Column ring (col_ring): each chunk's column indices travel with its values, so
+          // the gathers of a chunk wait for no global load of their own.
+          int32_t *cring = a.col_ring ? reinterpret_cast<int32_t *>(fg_dynamic_smem + a.col_ring_offset) +
+                                            static_cast<size_t>(warp) * 2 * U * 32
+                                      : nullptr;
           const T *vals = static_cast<const T *>(a.values);
           const unsigned long long pol = EvictFirstPolicy();
           auto issue = [&](int stage, size_t base, int w0, int len) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
-              if (w0 + u < len)
+              if (w0 + u < len) {
                 CpAsync16(ring + ((stage * U + u) * 32 + lane) * IV,
                           vals + (base + 32 * static_cast<size_t>(w0 + u)) * a.value_stride + item0, pol);
+                if (cring)
+                  CpAsync4(cring + (stage * U + u) * 32 + lane, a.sell_col + base + 32 * static_cast<size_t>(w0 + u));
+              }
             CpAsyncCommit();
           };
           int ws = ws0 + warp, r = 0, len = 0, w0 = 0, stage = 0;
@@ -935,7 +950,9 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             int c[U];
 #pragma unroll
             for (int u = 0; u < U; ++u)
-              c[u] = w0 + u < len ? Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u)) : 0;
+              c[u] = w0 + u >= len ? 0
+                     : cring      ? cring[(stage * U + u) * 32 + lane]
+                                  : Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u));
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
