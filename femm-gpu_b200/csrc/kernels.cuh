@@ -89,9 +89,6 @@ struct PcgArgs {
   // Value ring: the SpMV's operator values staged into shared memory by cp.async one chunk
   // ahead of their use (set by LaunchPcg for 16-byte item vectors).
   int32_t value_ring, value_ring_offset;
-  // Column ring (with the value ring only): the chunk's SELL column indices copied beside its
-  // values (4 bytes per lane and entry), read from shared memory by the gathers.
-  int32_t col_ring, col_ring_offset;
   // Launch-shape requests of a plan's autotuner for the value ring and the column-index
   // cache: 0 the default (environment), 1 on where the shape and shared memory allow it,
   // 2 off.  Neither changes any arithmetic, so results do not depend on the choice.

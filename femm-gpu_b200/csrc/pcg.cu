@@ -89,16 +89,6 @@ bool ColumnCacheEnabled()
   return enabled;
 }
 
-// FG_PCG_COL_RING=1 copies each chunk's column indices into shared memory beside its values.
-bool ColumnRingEnabled()
-{
-  static const bool enabled = [] {
-    const char *v = std::getenv("FG_PCG_COL_RING");
-    return v && v[0] == '1';
-  }();
-  return enabled;
-}
-
 } // namespace
 
 namespace
@@ -177,24 +167,12 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
       smem = total;
     }
   }
-  // Column ring beside the value ring: 2 stages x 4 entries x 32 lanes x 4 bytes per warp.
-  args.col_ring = 0;
-  args.col_ring_offset = 0;
-  if (args.value_ring && ColumnRingEnabled()) {
-    const size_t offset = (smem + 15) / 16 * 16;
-    const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 4;
-    if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
-      args.col_ring = 1;
-      args.col_ring_offset = static_cast<int32_t>(offset);
-      smem = total;
-    }
-  }
   // Column-index cache: the largest slice range any CTA's rows touch, if it fits in the
   // shared memory that still leaves the grid co-resident.
   args.col_cache = 0;
   args.col_cache_offset = 0;
   const bool want_cache = args.col_cache_request == 0 ? ColumnCacheEnabled() : args.col_cache_request == 1;
-  if (args.host_slice_off && want_cache && !args.col_ring) {
+  if (args.host_slice_off && want_cache) {
     size_t most = 0;
     for (int g = 0; g < grid; ++g) {
       const long long w0 = static_cast<long long>(warp_slices) * g / grid;

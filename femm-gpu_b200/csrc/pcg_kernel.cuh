@@ -315,45 +315,30 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
   if (!GridBarrier(a, gs, epoch, sm))
     return false;
   TraceMark(a, gs, tr, 2 * phase + 1);
-  // Lane-strided partials in CTA order.  All of a lane's partials (ten for grids of up to
-  // 320 CTAs) -- of two quantities at a time where a warp sums several -- are loaded before
-  // their adds, so each pass costs one L2 round trip.  The add order, and so the result, is
-  // that of the one-at-a-time loop.
-  constexpr int kPer = QK > kPcgWarps ? 2 : 1;
-  for (int t = warp; t < QK; t += kPer * kPcgWarps) {
-    double s[kPer];
-    bool has[kPer];
-#pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-      s[j] = 0.0;
-      has[j] = t + j * kPcgWarps < QK;
-    }
+  for (int t = warp; t < QK; t += kPcgWarps) {
+    // Lane-strided partials in CTA order; all of a lane's partials (ten for grids of up to
+    // 320 CTAs) are loaded before their adds, so the sums cost one L2 round trip.  The add
+    // order, and so the result, is that of the one-at-a-time loop.  (Two quantities per
+    // pass where a warp sums several measured slower at 32 items.)
+    const double *pt = part + static_cast<size_t>(t) * G;
+    double s = 0.0;
     for (int g = lane; g < G; g += 32 * 10) {
-      double y[kPer][10];
+      double y[10];
 #pragma unroll
-      for (int j = 0; j < kPer; ++j)
+      for (int u = 0; u < 10; ++u)
+        y[u] = g + 32 * u < G ? __ldcg(pt + g + 32 * u) : 0.0;
 #pragma unroll
-        for (int u = 0; u < 10; ++u)
-          y[j][u] = has[j] && g + 32 * u < G
-                        ? __ldcg(part + static_cast<size_t>(t + j * kPcgWarps) * G + g + 32 * u)
-                        : 0.0;
-#pragma unroll
-      for (int j = 0; j < kPer; ++j)
-#pragma unroll
-        for (int u = 0; u < 10; ++u)
-          if (has[j] && g + 32 * u < G)
-            s[j] = kMax ? fmax(s[j], y[j][u]) : s[j] + y[j][u];
+      for (int u = 0; u < 10; ++u)
+        if (g + 32 * u < G)
+          s = kMax ? fmax(s, y[u]) : s + y[u];
     }
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) {
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) {
-        const double y = __shfl_xor_sync(0xffffffffu, s[j], off);
-        s[j] = kMax ? fmax(s[j], y) : s[j] + y;
-      }
-      if (lane == 0 && has[j])
-        sm.result[t + j * kPcgWarps] = s[j];
+    for (int off = 16; off > 0; off >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, s, off);
+      s = kMax ? fmax(s, y) : s + y;
     }
+    if (lane == 0)
+      sm.result[t] = s;
   }
   __syncthreads();
   TraceMark(a, gs, tr, 8);
@@ -380,13 +365,6 @@ __device__ __forceinline__ void CpAsync16(void *smem, const void *gmem, unsigned
   const size_t g = __cvta_generic_to_global(gmem);
   asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(s), "l"(g), "l"(pol)
                : "memory");
-}
-// 4-byte asynchronous copy (cp.async.ca: the .cg form copies 16 bytes only).
-__device__ __forceinline__ void CpAsync4(void *smem, const void *gmem)
-{
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  const size_t g = __cvta_generic_to_global(gmem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(g) : "memory");
 }
 __device__ __forceinline__ void CpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N> __device__ __forceinline__ void CpAsyncWait()
@@ -893,22 +871,14 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           constexpr int U = 4;
           T *ring = reinterpret_cast<T *>(fg_dynamic_smem + a.value_ring_offset) +
                     static_cast<size_t>(warp) * 2 * U * 32 * IV;
-          // Column ring (col_ring): each chunk's column indices travel with its values, so
-          // the gathers of a chunk wait for no global load of their own.
-          int32_t *cring = a.col_ring ? reinterpret_cast<int32_t *>(fg_dynamic_smem + a.col_ring_offset) +
-                                            static_cast<size_t>(warp) * 2 * U * 32
-                                      : nullptr;
           const T *vals = static_cast<const T *>(a.values);
           const unsigned long long pol = EvictFirstPolicy();
           auto issue = [&](int stage, size_t base, int w0, int len) {
 #pragma unroll
             for (int u = 0; u < U; ++u)
-              if (w0 + u < len) {
+              if (w0 + u < len)
                 CpAsync16(ring + ((stage * U + u) * 32 + lane) * IV,
                           vals + (base + 32 * static_cast<size_t>(w0 + u)) * a.value_stride + item0, pol);
-                if (cring)
-                  CpAsync4(cring + (stage * U + u) * 32 + lane, a.sell_col + base + 32 * static_cast<size_t>(w0 + u));
-              }
             CpAsyncCommit();
           };
           int ws = ws0 + warp, r = 0, len = 0, w0 = 0, stage = 0;
@@ -950,9 +920,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
             int c[U];
 #pragma unroll
             for (int u = 0; u < U; ++u)
-              c[u] = w0 + u >= len ? 0
-                     : cring      ? cring[(stage * U + u) * 32 + lane]
-                                  : Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u));
+              c[u] = w0 + u < len ? Column(a, colc, cbase, base + 32 * static_cast<size_t>(w0 + u)) : 0;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
               if (w0 + u < len) {
