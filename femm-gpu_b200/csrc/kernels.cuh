@@ -13,6 +13,9 @@ namespace fg
 {
 
 constexpr int kMaxItems = 32;
+// Entries per chunk of the PCG's value ring (per warp: 2 stages x kRingEntries entries x 32
+// lanes x 16 bytes of dynamic shared memory).
+constexpr int kRingEntries = 4;
 
 struct DevicePlan {
   int32_t N, E, n, n_pad, slices, C, problem_type;

@@ -152,15 +152,15 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
     grid = max_grid;
   if (grid < 1)
     grid = 1;
-  // Value ring (16-byte item vectors, per-item operators): 2 stages x 4 entries x 32 lanes
-  // x 16 bytes per warp, after the block-Jacobi staging buffer.
+  // Value ring (16-byte item vectors, per-item operators): 2 stages x kRingEntries entries x
+  // 32 lanes x 16 bytes per warp, after the block-Jacobi staging buffer.
   args.value_ring = 0;
   args.value_ring_offset = 0;
   const bool want_ring = args.ring_request == 0 ? ValueRingEnabled() : args.ring_request == 1;
   const bool ring_shape = (args.precision == 0 ? 8 : 4) * iv == 16 && args.value_item && want_ring;
   if (ring_shape) {
     const size_t offset = (smem + 15) / 16 * 16;
-    const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 16;
+    const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * kRingEntries * 32 * 16;
     if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
       args.value_ring = 1;
       args.value_ring_offset = static_cast<int32_t>(offset);
@@ -211,7 +211,7 @@ size_t MultiPcgRingBytes(int kp)
   const int iv = ItemsPerThread(kp, 0);
   if (8 * iv != 16 || !ValueRingEnabled())
     return 0;
-  return static_cast<size_t>(kPcgWarps) * 2 * 4 * 32 * 16;
+  return static_cast<size_t>(kPcgWarps) * 2 * kRingEntries * 32 * 16;
 }
 
 int MultiPcgMaxGrid(int kp)

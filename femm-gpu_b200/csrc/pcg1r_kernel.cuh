@@ -50,7 +50,7 @@ struct Control1r {
 // Rows of this warp (warp-steps ws0 + warp, + kPcgWarps, ... < ws1) through the SpMV:
 // `gather(ci, vv, acc)` accumulates entry (value vv, item-interleaved column offset ci) into
 // acc, `finish(r, acc)` ends row r.  With the value ring the operator values of the next
-// chunk of 4 entries are copied to shared memory (cp.async) while the current chunk's
+// chunk of kRingEntries entries are copied to shared memory (cp.async) while the current chunk's
 // gathers are in flight; otherwise they are streamed from global memory.
 template <int KP, int IV, class Gather, class Finish>
 __device__ __forceinline__ void SpmvRows(const PcgArgs &a, const int32_t *colc, size_t cbase, int ws0,
@@ -59,7 +59,7 @@ __device__ __forceinline__ void SpmvRows(const PcgArgs &a, const int32_t *colc, 
   using T = double;
   constexpr int LR = KP / IV;
   constexpr int S = 32 / LR;
-  constexpr int U = 4;
+  constexpr int U = kRingEntries; // the value ring's chunk (also the plain path's)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const T *vals = static_cast<const T *>(a.values);
   if constexpr (sizeof(T) * IV == 16) {

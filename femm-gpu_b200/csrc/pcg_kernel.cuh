@@ -868,7 +868,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         if (any_mine && a.value_ring) {
           // Software pipeline over this lane's (row, chunk) sequence: the values of the next
           // chunk are copied to shared memory while the current chunk's gathers are in flight.
-          constexpr int U = 4;
+          constexpr int U = kRingEntries;
           T *ring = reinterpret_cast<T *>(fg_dynamic_smem + a.value_ring_offset) +
                     static_cast<size_t>(warp) * 2 * U * 32 * IV;
           const T *vals = static_cast<const T *>(a.values);
