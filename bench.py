@@ -58,8 +58,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-forms", action="store_true", help="skip the mixed / block / learned forms")
     p.add_argument("--no-learned", action="store_true", help="skip the learned warm start form")
-    p.add_argument("--learned-train", type=int, default=1024, help="training solves of the learned form")
-    p.add_argument("--learned-held", type=int, default=256, help="held-out samples of the learned form")
+    p.add_argument("--learned-train", type=int, default=8192, help="training solves of the learned form")
+    p.add_argument("--learned-held", type=int, default=4096, help="held-out samples of the learned form")
     p.add_argument("--sector-samples", type=int, default=1024, help="samples of the shared-geometry sector form")
     p.add_argument("--hetero-meshes", type=int, default=256, help="meshes of the heterogeneous-batch form")
     p.add_argument("--all-forms", action="store_true",
