@@ -24,7 +24,7 @@
 // capture begins.
 //
 // Host waits: every call synchronises `stream` -- once after the set-up kernel, to read
-// its verdict on the system, and again after the solve, to read the solve's status before
+// what it found wrong with the system, and again after the solve, to read its status before
 // x is written -- so it returns only when x and info are final.
 #include "femm_gpu.h"
 #include "common.h"
