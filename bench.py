@@ -68,7 +68,8 @@ def parse():
                                            "planar_2m", "reference_gpu", "learned", "sector", "hetero",
                                            "pcg_launch"],
                    help="run one form alone and print its JSON (profiling)")
-    p.add_argument("--probe-mesh", type=int, default=MESH_M, help="pcg_launch: planar square size m")
+    p.add_argument("--probe-mesh", type=int, default=MESH_M,
+                   help="pcg_launch: planar square size m (0: the 40k-node rotor-stator sector)")
     p.add_argument("--probe-items", type=int, default=8, help="pcg_launch: samples per launch")
     p.add_argument("--probe-iterations", type=int, default=300, help="pcg_launch: CG iterations per launch")
     p.add_argument("--probe-launches", type=int, default=3, help="pcg_launch: launches timed")
@@ -792,10 +793,11 @@ def pcg_bytes_per_item_iteration(n, nnz, precision, block):
 
 
 def pcg_launch_form(dev, stream, m, k, iterations, launches, one_reduction):
-    """PCG launches of a fixed length, for profiling one launch: the planar square of size m,
-    k samples, one Newton iteration whose inner PCG is capped at `iterations` CG iterations
-    (tolerance 1e-30, so every launch runs exactly that many), repeated `launches` times on one
-    plan.  The launch-shape autotuner is off (FG_PCG_TUNE=0: the default value ring, no
+    """PCG launches of a fixed length, for profiling one launch: the planar square of size m
+    (m = 0: the rotor-stator sector of the shared-geometry batches, its 3 coil currents
+    U[-15, 15] A), k samples, one Newton iteration whose inner PCG is capped at `iterations`
+    CG iterations (tolerance 1e-30, so every launch runs exactly that many), repeated
+    `launches` times on one plan.  The launch-shape autotuner is off (FG_PCG_TUNE=0: the default value ring, no
     column cache), so the PCG launches are exactly these.  Reports the CUDA-event time per CG
     iteration of each launch and the algorithmic bytes per CG iteration."""
     import torch
@@ -804,10 +806,15 @@ def pcg_launch_form(dev, stream, m, k, iterations, launches, one_reduction):
     from femm_gpu_b200 import meshes
 
     os.environ["FG_PCG_TUNE"] = "0"
-    model = meshes.square_nonlinear(m=m, seed=2)
+    if m > 0:
+        model = meshes.square_nonlinear(m=m, seed=2)
+        currents = meshes.seeded_currents(k, 3, 20.0, seed=4242)
+    else:
+        model = meshes.annular_sector()
+        currents = np.random.default_rng(5).uniform(-15.0, 15.0, size=(k, model.circuit_count))
     plan = fg.Plan(model, one_reduction=one_reduction)
     peak, source = peaks()
-    cur = torch.tensor(meshes.seeded_currents(k, 3, 20.0, seed=4242), device=dev)
+    cur = torch.tensor(currents, device=dev)
     out_a = torch.empty((k, plan.N), dtype=torch.float64, device=dev)
     opts = fg.production_options(max_newton_iterations=1, max_linear_iterations=iterations,
                                  linear_relative_tolerance=1e-30, adaptive_linear_tolerance=0,
