@@ -96,6 +96,10 @@ struct PcgArgs {
   // cache: 0 the default (environment), 1 on where the shape and shared memory allow it,
   // 2 off.  Neither changes any arithmetic, so results do not depend on the choice.
   int32_t ring_request, col_cache_request;
+  // CTA shape request: 0 the default (FG_PCG_BLOCK=1024 in the environment: 1024 threads,
+  // else 512), 1 CTAs of 1024 threads where the launch allows them (FP64 Jacobi, an even
+  // number of row groups), 2 CTAs of 512.  Both shapes give the same bits.
+  int32_t block_request;
   // One-reduction form (FP64 Jacobi only; pcg1r_kernel.cuh): t0 / t1 are two more
   // vectors of [n_pad][kp] doubles, and partials must hold 2 x 96 x grid doubles.
   int32_t one_reduction;

@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <cstdlib>
+#include <cstring>
 
 namespace fg
 {
@@ -14,6 +15,7 @@ const void *PcgKernelF64Block(int kp, int bs);
 const void *PcgKernelF32Block(int kp, int bs);
 const void *MultiPcgKernelF64(int kp);
 const void *PcgKernelF64OneReduction(int kp);
+const void *PcgKernelF64Wide(int kp);
 
 namespace
 {
@@ -47,8 +49,8 @@ size_t StagingBytes(int kp, int precision, int bs)
   return static_cast<size_t>(kPcgWarps) * u * kp * (precision == 0 ? 8 : 4);
 }
 
-// Co-resident CTAs of one kernel shape (at most 2 per SM), 0 on failure.
-int KernelGrid(const void *kernel, size_t smem)
+// Co-resident CTAs of one kernel shape (at most `cap` per SM), 0 on failure.
+int KernelGrid(const void *kernel, size_t smem, int threads = kPcgThreads, int cap = 2)
 {
   int device = 0, sms = 0, per_sm = 0;
   if (!kernel || cudaGetDevice(&device) != cudaSuccess ||
@@ -58,9 +60,9 @@ int KernelGrid(const void *kernel, size_t smem)
       cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(smem)) != cudaSuccess)
     return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPcgThreads, smem) != cudaSuccess)
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess)
     return 0;
-  return sms * (per_sm < 2 ? per_sm : 2);
+  return sms * (per_sm < cap ? per_sm : cap);
 }
 
 // Dynamic shared memory a launch may use for staging plus the column cache: two CTAs of
@@ -87,6 +89,14 @@ bool ColumnCacheEnabled()
     return v && v[0] == '1';
   }();
   return enabled;
+}
+
+// FG_PCG_BLOCK=1024 selects the 1024-thread CTAs where a plan's autotuner has not chosen
+// (read at every launch).
+bool WideBlocksEnabled()
+{
+  const char *v = std::getenv("FG_PCG_BLOCK");
+  return v && std::strcmp(v, "1024") == 0;
 }
 
 } // namespace
@@ -147,11 +157,23 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   const int iv = ItemsPerThread(args.kp, args.precision);
   const int rows_per_warp = 32 * iv / args.kp;
   const int warp_slices = args.n_pad / rows_per_warp;
-  int grid = (warp_slices + kPcgWarps - 1) / kPcgWarps;
+  int grid = (warp_slices + kPcgWarps - 1) / kPcgWarps; // row groups of kPcgWarps warps
   if (grid > max_grid)
     grid = max_grid;
   if (grid < 1)
     grid = 1;
+  // Wide CTAs (FP64 Jacobi): the same row groups two to a CTA of 1024 threads, one CTA per
+  // SM -- the same rows, order and partial sums, so the same bits.
+  const bool want_wide = args.block_request == 0 ? WideBlocksEnabled() : args.block_request == 1;
+  const void *wide_kernel = want_wide && args.precision == 0 && bs == 0 && !args.one_reduction && grid % 2 == 0
+                                ? PcgKernelF64Wide(args.kp)
+                                : nullptr;
+  const bool wide = wide_kernel && KernelGrid(wide_kernel, 0, 2 * kPcgThreads, 1) >= grid / 2;
+  const int threads = wide ? 2 * kPcgThreads : kPcgThreads, warps = threads / 32;
+  const int ctas = wide ? grid / 2 : grid, cap = wide ? 1 : 2;
+  const size_t budget = wide ? 200 * 1024 : kColumnCacheBudget;
+  if (wide)
+    kernel = wide_kernel;
   // Value ring (16-byte item vectors, per-item operators): 2 stages x kRingEntries entries x
   // 32 lanes x 16 bytes per warp, after the block-Jacobi staging buffer.
   args.value_ring = 0;
@@ -160,8 +182,8 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   const bool ring_shape = (args.precision == 0 ? 8 : 4) * iv == 16 && args.value_item && want_ring;
   if (ring_shape) {
     const size_t offset = (smem + 15) / 16 * 16;
-    const size_t total = offset + static_cast<size_t>(kPcgWarps) * 2 * kRingEntries * 32 * 16;
-    if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
+    const size_t total = offset + static_cast<size_t>(warps) * 2 * kRingEntries * 32 * 16;
+    if (total <= budget && KernelGrid(kernel, total, threads, cap) >= ctas) {
       args.value_ring = 1;
       args.value_ring_offset = static_cast<int32_t>(offset);
       smem = total;
@@ -174,9 +196,9 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   const bool want_cache = args.col_cache_request == 0 ? ColumnCacheEnabled() : args.col_cache_request == 1;
   if (args.host_slice_off && want_cache) {
     size_t most = 0;
-    for (int g = 0; g < grid; ++g) {
-      const long long w0 = static_cast<long long>(warp_slices) * g / grid;
-      const long long w1 = static_cast<long long>(warp_slices) * (g + 1) / grid;
+    for (int g = 0; g < ctas; ++g) {
+      const long long w0 = static_cast<long long>(warp_slices) * g / ctas;
+      const long long w1 = static_cast<long long>(warp_slices) * (g + 1) / ctas;
       if (w1 <= w0)
         continue;
       const long long s0 = (w0 * rows_per_warp) >> 5, s1 = (w1 * rows_per_warp - 1) >> 5;
@@ -185,7 +207,7 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
     }
     const size_t offset = (smem + 15) / 16 * 16;
     const size_t total = offset + most * sizeof(int32_t);
-    if (total <= kColumnCacheBudget && KernelGrid(kernel, total) >= grid) {
+    if (total <= budget && KernelGrid(kernel, total, threads, cap) >= ctas) {
       args.col_cache = 1;
       args.col_cache_offset = static_cast<int32_t>(offset);
       smem = total;
@@ -197,11 +219,11 @@ cudaError_t LaunchPcg(PcgArgs args, int *grid_out, int *block_out, cudaStream_t 
   if (e != cudaSuccess)
     return e;
   void *params[] = {&args};
-  e = cudaLaunchCooperativeKernel(kernel, dim3(grid), dim3(kPcgThreads), params, smem, stream);
+  e = cudaLaunchCooperativeKernel(kernel, dim3(ctas), dim3(threads), params, smem, stream);
   if (grid_out)
-    *grid_out = grid;
+    *grid_out = ctas;
   if (block_out)
-    *block_out = kPcgThreads;
+    *block_out = threads;
   return e;
 }
 

@@ -57,11 +57,14 @@ struct Control {
   double rmax[kMaxItems]; // reliable updates: largest residual since the last replacement
 };
 
-// Shared-memory staging of a grid reduction of up to QM quantities (quantities x items);
-// the partials buffer holds 2 x QM x grid doubles.
-template <int QM> struct ReduceQ {
+// Shared-memory staging of a grid reduction of up to QM quantities (quantities x items) in
+// a CTA of NW warps; the partials buffer holds 2 x QM x (row groups) doubles.  A row group
+// is kPcgWarps warps with one contiguous range of rows: a CTA of 512 threads is one group,
+// a CTA of 1024 threads two, so both shapes partition the rows and sum the partials alike.
+template <int QM, int NW = kPcgWarps> struct ReduceQ {
   static constexpr int kQ = QM;
-  double warp[kPcgWarps][QM];
+  static constexpr int kW = NW;
+  double warp[NW][QM];
   double result[QM];
   int err;
 };
@@ -303,21 +306,23 @@ __device__ bool GridReduce(const PcgArgs &a, const GridShape &gs, double (&v)[Q]
     }
   __syncthreads();
   constexpr int QK = Q * KP;
-  const int G = gs.size;
+  constexpr int H = R::kW / kPcgWarps; // row groups per CTA
+  const int G = gs.size * H;            // partials per quantity, one per row group
   double *part = a.partials + static_cast<size_t>(buf) * R::kQ * G;
-  if (threadIdx.x < QK) {
-    double s = sm.warp[0][threadIdx.x];
+  if (threadIdx.x < QK * H) {
+    const int h = static_cast<int>(threadIdx.x) / QK, q = static_cast<int>(threadIdx.x) % QK;
+    double s = sm.warp[h * kPcgWarps][q];
     for (int w = 1; w < kPcgWarps; ++w)
-      s = kMax ? fmax(s, sm.warp[w][threadIdx.x]) : s + sm.warp[w][threadIdx.x];
-    part[static_cast<size_t>(threadIdx.x) * G + gs.rank] = s;
+      s = kMax ? fmax(s, sm.warp[h * kPcgWarps + w][q]) : s + sm.warp[h * kPcgWarps + w][q];
+    part[static_cast<size_t>(q) * G + gs.rank * H + h] = s;
   }
   TraceMark(a, gs, tr, 2 * phase);
   if (!GridBarrier(a, gs, epoch, sm))
     return false;
   TraceMark(a, gs, tr, 2 * phase + 1);
-  for (int t = warp; t < QK; t += kPcgWarps) {
-    // Lane-strided partials in CTA order; all of a lane's partials (ten for grids of up to
-    // 320 CTAs) are loaded before their adds, so the sums cost one L2 round trip.  The add
+  for (int t = warp; t < QK; t += R::kW) {
+    // Lane-strided partials in row-group order; all of a lane's partials (ten for up to 320
+    // row groups) are loaded before their adds, so the sums cost one L2 round trip.  The add
     // order, and so the result, is that of the one-at-a-time loop.  (Two quantities per
     // pass where a warp sums several measured slower at 32 items.)
     const double *pt = part + static_cast<size_t>(t) * G;
@@ -469,19 +474,26 @@ __device__ __forceinline__ void RowProductReliable(const PcgArgs &a, const int32
   }
 }
 
-template <typename T, int KP, int IV, int BS>
+// NW: warps per CTA, kPcgWarps (512 threads, one row group) or 2 kPcgWarps (1024 threads,
+// two row groups): a CTA of either shape runs the same rows in the same per-warp order and
+// stores one partial per row group, so both give bitwise-identical results.
+template <typename T, int KP, int IV, int BS, int NW = kPcgWarps>
 __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
 {
-  __shared__ Reduce sm;
+  __shared__ ReduceQ<kMaxQ, NW> sm;
   __shared__ Control ctl;
   __shared__ Trace tr;
   constexpr int LR = KP / IV;  // lanes per row
   constexpr int S = 32 / LR;   // rows per warp
+  constexpr int H = NW / kPcgWarps; // row groups per CTA
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // The warp's place in its row group, and the row group's index over the grid.
+  const int gw = H == 1 ? warp : (warp & (kPcgWarps - 1));
+  const int rg = H == 1 ? gs.rank : gs.rank * H + warp / kPcgWarps, RG = gs.size * H;
   const int item0 = (lane % LR) * IV;
   const int WS = a.n_pad / S;
-  const int ws0 = static_cast<int>(static_cast<long long>(WS) * gs.rank / gs.size);
-  const int ws1 = static_cast<int>(static_cast<long long>(WS) * (gs.rank + 1) / gs.size);
+  const int ws0 = static_cast<int>(static_cast<long long>(WS) * rg / RG);
+  const int ws1 = static_cast<int>(static_cast<long long>(WS) * (rg + 1) / RG);
   unsigned epoch = 0;
   int buf = 0;
   const T *B = static_cast<const T *>(a.b);
@@ -534,8 +546,8 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
   extern __shared__ __align__(16) unsigned char fg_dynamic_smem[];
   T *xb = reinterpret_cast<T *>(fg_dynamic_smem) + static_cast<size_t>(warp) * U * KP;
   const int WU = a.n_pad / U;
-  const int wu0 = static_cast<int>(static_cast<long long>(WU) * gs.rank / gs.size);
-  const int wu1 = static_cast<int>(static_cast<long long>(WU) * (gs.rank + 1) / gs.size);
+  const int wu0 = static_cast<int>(static_cast<long long>(WU) * rg / RG);
+  const int wu1 = static_cast<int>(static_cast<long long>(WU) * (rg + 1) / RG);
   const T *BLK = static_cast<const T *>(a.blocks);
 
   // Column indices of this CTA's rows (the Phase A partition, fixed for the launch) copied
@@ -544,14 +556,17 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
   size_t cbase = 0;
   if (a.col_cache) {
     int32_t *cs = reinterpret_cast<int32_t *>(fg_dynamic_smem + a.col_cache_offset);
-    if (ws1 > ws0) {
-      const int s0 = (ws0 * S) >> 5, s1 = (ws1 * S - 1) >> 5;
+    // The rows of all the CTA's row groups.
+    const int cws0 = static_cast<int>(static_cast<long long>(WS) * (gs.rank * H) / RG);
+    const int cws1 = static_cast<int>(static_cast<long long>(WS) * (gs.rank * H + H) / RG);
+    if (cws1 > cws0) {
+      const int s0 = (cws0 * S) >> 5, s1 = (cws1 * S - 1) >> 5;
       const size_t p0 = static_cast<size_t>(__ldg(a.slice_off + s0));
       const size_t p1 = static_cast<size_t>(__ldg(a.slice_off + s1 + 1));
       // Positions are multiples of 32 ints (whole slice columns): copy as int4.
       const int4 *src = reinterpret_cast<const int4 *>(a.sell_col + p0);
       int4 *dst = reinterpret_cast<int4 *>(cs);
-      for (size_t i = threadIdx.x; i < (p1 - p0) / 4; i += kPcgThreads)
+      for (size_t i = threadIdx.x; i < (p1 - p0) / 4; i += NW * 32)
         dst[i] = __ldg(src + i);
       cbase = p0;
     }
@@ -681,7 +696,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
 
 
 #define FG_ROWS_BEGIN                                                                              \
-  for (int ws = ws0 + warp; ws < ws1; ws += kPcgWarps) {                                           \
+  for (int ws = ws0 + gw; ws < ws1; ws += kPcgWarps) {                                             \
     const int r = ws * S + lane / LR;                                                              \
     const size_t ri = static_cast<size_t>(r) * KP + item0;
 #define FG_ROWS_END }
@@ -771,7 +786,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
         }
       FG_ROWS_END
     } else {
-      for (int wu = wu0 + warp; wu < wu1; wu += kPcgWarps) {
+      for (int wu = wu0 + gw; wu < wu1; wu += kPcgWarps) {
 #pragma unroll
         for (int u = 0; u < SUB; ++u) {
           const size_t ri = static_cast<size_t>(sub_row(wu, u)) * KP + item0;
@@ -881,7 +896,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
                           vals + (base + 32 * static_cast<size_t>(w0 + u)) * a.value_stride + item0, pol);
             CpAsyncCommit();
           };
-          int ws = ws0 + warp, r = 0, len = 0, w0 = 0, stage = 0;
+          int ws = ws0 + gw, r = 0, len = 0, w0 = 0, stage = 0;
           size_t base = 0;
           auto row_at = [&](int w, int &rr, int &ll, size_t &bb) {
             rr = w * S + lane / LR;
@@ -999,7 +1014,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
       }
       if constexpr (BS > 0) {
         if (__any_sync(0xffffffffu, mine))
-          for (int wu = wu0 + warp; wu < wu1; wu += kPcgWarps) {
+          for (int wu = wu0 + gw; wu < wu1; wu += kPcgWarps) {
             T xo[SUB][IV], po[SUB][IV], ro[SUB][IV], qo[SUB][IV];
 #pragma unroll
             for (int u = 0; u < SUB; ++u) {
@@ -1043,7 +1058,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
           }
       } else if (mine) {
         // Two row groups per pass: all loads are issued before the first store.
-        for (int ws = ws0 + warp; ws < ws1; ws += 2 * kPcgWarps) {
+        for (int ws = ws0 + gw; ws < ws1; ws += 2 * kPcgWarps) {
           const bool two = ws + kPcgWarps < ws1;
           const int r0 = ws * S + lane / LR, r1 = (ws + kPcgWarps) * S + lane / LR;
           const size_t i0 = static_cast<size_t>(r0) * KP + item0;
@@ -1205,7 +1220,7 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
       }
       if constexpr (BS > 0) {
         if (__any_sync(0xffffffffu, any_mine))
-          for (int wu = wu0 + warp; wu < wu1; wu += kPcgWarps) {
+          for (int wu = wu0 + gw; wu < wu1; wu += kPcgWarps) {
 #pragma unroll
             for (int u = 0; u < SUB; ++u) {
               T rv[IV];
@@ -1387,10 +1402,10 @@ __device__ __forceinline__ void PcgBody(const PcgArgs &a, const GridShape gs)
       a.trace[s] += tr.slot[s];
 }
 
-template <typename T, int KP, int IV, int BS>
-__global__ void __launch_bounds__(kPcgThreads, 2) PcgKernel(PcgArgs a)
+template <typename T, int KP, int IV, int BS, int NW = kPcgWarps>
+__global__ void __launch_bounds__(NW * 32, 2 * kPcgWarps / NW) PcgKernel(PcgArgs a)
 {
-  PcgBody<T, KP, IV, BS>(a, GridShape{static_cast<int>(gridDim.x), static_cast<int>(blockIdx.x)});
+  PcgBody<T, KP, IV, BS, NW>(a, GridShape{static_cast<int>(gridDim.x), static_cast<int>(blockIdx.x)});
 }
 
 // Several independent PCG solves (one per plan: its own operator, vectors, barrier and

@@ -411,10 +411,11 @@ cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t st
     sh.items = a.kp;
     sh.precision = a.precision;
     sh.block_size = a.blocks ? a.block_size : 0;
-    // Candidates: ring on / off (only 16-byte item vectors of per-item operators can use
-    // it) x column cache off / on.  Each runs kTuneIterations CG iterations of this very
-    // system (tolerance 0: no item stops early); the real launch follows and overwrites
-    // every vector the timing runs wrote.
+    // Candidates: 512-thread CTAs with the ring on / off (only 16-byte item vectors of
+    // per-item operators can use it) x column cache off / on, and 1024-thread CTAs with the
+    // ring (FP64 Jacobi, where the launch admits them).  Each runs kTuneIterations CG
+    // iterations of this very system (tolerance 0: no item stops early); the real launch
+    // follows and overwrites every vector the timing runs wrote.
     const int iv = a.precision == 0 ? (a.kp >= 2 ? 2 : 1) : (a.kp >= 4 ? 4 : (a.kp >= 2 ? 2 : 1));
     const bool ring_possible = (a.precision == 0 ? 8 : 4) * iv == 16 && a.value_item;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -431,25 +432,30 @@ cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t st
     t.item_tolerance = nullptr;
     t.max_iterations = kTuneIterations;
     t.trace = nullptr;
+    t.block_request = 2;
     if (LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess)
       cudaGetLastError();
     else
       timing_.kernel_launches += 1;
     for (int round = 0; round < kTuneRounds; ++round)
-      for (int c = 0; c < 4; ++c) {
-        const int ring = c % 2 == 0 ? 1 : 2, cache = c < 2 ? 2 : 1;
+      for (int c = 0; c < 5; ++c) {
+        const int ring = c % 2 == 0 ? 1 : 2, cache = c == 2 || c == 3 ? 1 : 2;
         if (ring == 1 && !ring_possible)
           continue;
         t.ring_request = ring;
         t.col_cache_request = cache;
+        t.block_request = c == 4 ? 1 : 2;
         float ms = 0.0f;
-        if (cudaEventRecord(e0, stream) != cudaSuccess || LaunchPcg(t, nullptr, nullptr, stream) != cudaSuccess ||
+        int threads = 0;
+        if (cudaEventRecord(e0, stream) != cudaSuccess || LaunchPcg(t, nullptr, &threads, stream) != cudaSuccess ||
             cudaEventRecord(e1, stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
             cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
           cudaGetLastError();
           continue;
         }
         timing_.kernel_launches += 1;
+        if (c == 4 && threads != 1024)
+          continue; // the launch fell back to 512 threads: not a candidate of its own
         const double us = 1e3 * ms / kTuneIterations;
         if (sh.us_per_iteration[c] == 0.0) {
           ++sh.candidates;
@@ -459,11 +465,12 @@ cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t st
         }
       }
     double best = 0.0;
-    for (int c = 0; c < 4; ++c)
+    for (int c = 0; c < 5; ++c)
       if (sh.us_per_iteration[c] > 0.0 && (best == 0.0 || sh.us_per_iteration[c] < best)) {
         best = sh.us_per_iteration[c];
         sh.value_ring = c % 2 == 0 ? 1 : 0;
-        sh.column_cache = c < 2 ? 0 : 1;
+        sh.column_cache = c == 2 || c == 3 ? 1 : 0;
+        sh.threads_per_block = c == 4 ? 1024 : 512;
       }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -473,6 +480,7 @@ cudaError_t Plan::LaunchShaped(PcgArgs a, int *grid, int *block, cudaStream_t st
   if (it != shapes_.end()) {
     a.ring_request = it->second.value_ring ? 1 : 2;
     a.col_cache_request = it->second.column_cache ? 1 : 2;
+    a.block_request = it->second.threads_per_block == 1024 ? 1 : 2;
   }
   return LaunchPcg(a, grid, block, stream);
 }

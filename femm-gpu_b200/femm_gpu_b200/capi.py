@@ -139,7 +139,8 @@ class FgTiming(C.Structure):
 class FgPcgShape(C.Structure):
     _fields_ = [("items", C.c_int32), ("precision", C.c_int32), ("block_size", C.c_int32),
                 ("value_ring", C.c_int32), ("column_cache", C.c_int32), ("candidates", C.c_int32),
-                ("us_per_iteration", C.c_double * 4)]
+                ("us_per_iteration", C.c_double * 5), ("threads_per_block", C.c_int32),
+                ("reserved", C.c_int32)]
 
 
 _LIB = None
@@ -438,7 +439,8 @@ class Plan:
         n = lib().fg_plan_pcg_shapes(self._h, n, arr)
         return [{"items": a.items, "precision": a.precision, "block_size": a.block_size,
                  "value_ring": bool(a.value_ring), "column_cache": bool(a.column_cache),
-                 "candidates": a.candidates, "us_per_iteration": list(a.us_per_iteration)}
+                 "candidates": a.candidates, "us_per_iteration": list(a.us_per_iteration),
+                 "threads_per_block": a.threads_per_block}
                 for a in arr[:n]]
 
 

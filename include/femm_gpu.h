@@ -352,7 +352,12 @@ typedef struct fg_pcg_shape {
   int32_t value_ring;   /* 1 chosen on, 0 off */
   int32_t column_cache; /* 1 chosen on, 0 off */
   int32_t candidates;   /* shapes timed (those the kernel shape admits) */
-  double us_per_iteration[4]; /* per candidate: ring on / off x cache off / on; 0 if not timed */
+  /* per candidate: [0..3] 512-thread CTAs, ring on / off x cache off / on; [4] 1024-thread
+   * CTAs (two row groups each, FP64 Jacobi with an even number of row groups), ring on,
+   * cache off; 0 if not timed */
+  double us_per_iteration[5];
+  int32_t threads_per_block; /* the chosen CTA shape: 512 or 1024 (the same bits either way) */
+  int32_t reserved;
 } fg_pcg_shape;
 int fg_plan_pcg_shapes(const fg_plan *plan, int32_t capacity, fg_pcg_shape *shapes);
 

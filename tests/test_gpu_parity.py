@@ -331,8 +331,11 @@ def test_autotuned_launch_shapes_leave_results_bitwise_unchanged(gpu, monkeypatc
     tuned = fg.Plan(model)
     r1 = tuned.solve(currents)
     shapes = tuned.pcg_shapes()
-    assert len(shapes) == 1 and shapes[0]["items"] == 8 and shapes[0]["candidates"] == 4
+    # 3,481 rows in 28 row groups of 16 warp-steps: an even count, so the 1024-thread CTAs
+    # are the fifth candidate
+    assert len(shapes) == 1 and shapes[0]["items"] == 8 and shapes[0]["candidates"] == 5
     assert all(t > 0 for t in shapes[0]["us_per_iteration"])
+    assert shapes[0]["threads_per_block"] in (512, 1024)
     monkeypatch.setenv("FG_PCG_TUNE", "0")
     plain = fg.Plan(model)
     r2 = plain.solve(currents)
@@ -340,3 +343,34 @@ def test_autotuned_launch_shapes_leave_results_bitwise_unchanged(gpu, monkeypatc
     for f in ("a", "b1", "b2", "flux"):
         assert np.array_equal(getattr(r1, f), getattr(r2, f))
     assert [i.linear_iterations for i in r1.info] == [i.linear_iterations for i in r2.info]
+
+
+@pytest.mark.parametrize("workload", ["square250_k8", "sector_k32"])
+def test_wide_ctas_give_the_same_bits(gpu, monkeypatch, workload):
+    """CTAs of 1024 threads (two row groups each, one CTA per SM) run the same rows in the
+    same per-warp order and store one partial sum per row group, so they answer bit for bit
+    as the 512-thread CTAs; the autotuner may therefore pick either shape."""
+    if workload == "square250_k8":
+        model, currents = meshes.square_nonlinear(m=250, seed=2), meshes.seeded_currents(8, 3, 20.0, seed=7)
+    else:
+        model = meshes.annular_sector()
+        currents = np.random.default_rng(5).uniform(-15.0, 15.0, size=(32, 3))
+    monkeypatch.setenv("FG_PCG_TUNE", "0")
+    narrow = fg.Plan(model)
+    r1 = narrow.solve(currents)
+    assert narrow.last_timing().pcg_block == 512
+    monkeypatch.setenv("FG_PCG_BLOCK", "1024")
+    wide = fg.Plan(model)
+    r2 = wide.solve(currents)
+    t = wide.last_timing()
+    assert t.pcg_block == 1024 and 2 * t.pcg_grid == narrow.last_timing().pcg_grid
+    for f in ("a", "b1", "b2", "flux"):
+        assert np.array_equal(getattr(r1, f), getattr(r2, f)), f
+    assert [i.linear_iterations for i in r1.info] == [i.linear_iterations for i in r2.info]
+    monkeypatch.delenv("FG_PCG_BLOCK")
+    tuned = fg.Plan(model)
+    monkeypatch.delenv("FG_PCG_TUNE")
+    r3 = tuned.solve(currents)
+    shape = tuned.pcg_shapes()[0]
+    assert shape["candidates"] == 5 and shape["us_per_iteration"][4] > 0
+    assert np.array_equal(r3.a, r1.a) and np.array_equal(r3.flux, r1.flux)
